@@ -1,0 +1,388 @@
+"""Benchmark of the GPU alignment path on the 2 x 100 Mbp chromosome-set workload.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
+
+One step = one pass of the GPU path over the whole contig set, inputs resident
+in HBM: closed-syncmer extraction -> 24-bit-prefix bucket sort -> semantic
+LCPs -> k-mer table entries + prefix table -> adaptamer merge -> seed
+reimport + diagonal sort of the N and C units.  Local_Alignment / .1aln are
+not yet on the GPU, so the metric is input Mbp/s through those stages.
+
+value  = input bases (both genomes, Mbp) per second, max device time over ranks
+e2e    = the same through the C ABI with host buffers: every step uploads the
+         .bps image and contig table and reads back both units' sorted seed
+         panels (reference byte format)
+roofline = the index build (extract + sort + LCP + entries), whose algorithmic
+         bytes are ceil(G/4) + 5*N*R + N*E + 2^27
+cpu_baseline = the reference pipeline compiled from source (oracle/_ref), or
+         the oracle's C restatement when that is absent, on a bounded sample.
+
+With N > 1 every rank runs an independent replica (the path has no exchange
+step on one node's workload): weak scaling, no collective in the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "input Mbp/s per B200 through extract->sort->merge->diagonal sort (Local_Alignment not yet on GPU)"
+UNIT = "Mbp/s"
+WORKLOAD = "chromset: 2 x 100 Mbp, 40% GC, log-normal contigs (median 2 Mbp, sigma 1), 10% repeats; k=40, FREQ=10"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+        self.out = ""
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.out += line
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().split("\n"):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def make_contigs(scale: float):
+    from distributedpanga_b200 import gdb, synth
+    cache = os.path.join(tempfile.gettempdir(), "pga_chromset_%g.npz" % scale)
+    if os.path.exists(cache):
+        z = np.load(cache)
+        return gdb.ContigSet(bps=z["bps"], clen=z["clen"], boff=z["boff"], freq=z["freq"]), None
+    contigs = synth.make("chromset", scale=scale)
+    cs = gdb.from_contigs(contigs)
+    try:
+        np.savez(cache, bps=cs.bps, clen=cs.clen, boff=cs.boff, freq=cs.freq)
+    except OSError:
+        pass
+    return cs, contigs
+
+
+def index_bytes(cs, nrec: int) -> float:
+    from distributedpanga_b200 import gdb
+    posb, ctgb, rsize = gdb.record_sizing(cs)
+    ebytes = rsize - 3
+    return (cs.seqtot + 3) // 4 + 5.0 * nrec * rsize + nrec * ebytes + (1 << 27)
+
+
+# ---- reference / oracle CPU timing -------------------------------------------
+
+class ReferenceSample:
+    """The reference pipeline (oracle/_ref) on a sample of the workload: the
+    GDB and its .gix are built once; each run() times one pga-mpi-merge and
+    returns the seconds of the stages the GPU path covers (from its own
+    [o1-0] / [pr1] stage timers)."""
+
+    def __init__(self, scale: float):
+        from distributedpanga_b200 import gdb, synth
+        from oracle import binding as orc
+        self.tmp = tempfile.TemporaryDirectory()
+        contigs = synth.make("chromset", scale=scale)
+        self.mbp = gdb.from_contigs(contigs).seqtot / 1e6
+        fa = os.path.join(self.tmp.name, "s.fa")
+        self.stem = os.path.join(self.tmp.name, "s")
+        synth.write_fasta(fa, contigs)
+        orc.ref_make_gdb(fa, self.stem)
+        env = dict(os.environ)
+        with open(os.path.join(self.tmp.name, "gix.log"), "w") as log:
+            subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T8", self.stem + ".1gdb"], check=True,
+                           stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
+
+    def run(self) -> float:
+        from oracle import binding as orc
+        env = dict(os.environ)
+        env["PATH"] = orc.REF_DIR + os.pathsep + env.get("PATH", "")
+        env.setdefault("PGA_SCRATCH_DIR", tempfile.gettempdir())
+        logp = os.path.join(self.tmp.name, "merge.log")
+        with open(logp, "w") as log:
+            subprocess.run([os.path.join(orc.REF_DIR, "pga-mpi-merge"), self.stem], check=True, stdout=log,
+                           stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
+        text = open(logp).read()
+        o1 = dict(re.findall(r"(\w+)=([0-9.]+)", text.split("[o1-0]")[1].split("\n")[0]))
+        pr = dict(re.findall(r"(\w+)=([0-9.]+)", text.split("[pr1]")[1].split("\n")[0]))
+        return (float(o1["extract_s"]) + float(o1["sort_stage_s"]) + float(pr["adapter_s"]) +
+                float(pr["merge_core_s"]) + float(pr["reimport_n_s"]) + float(pr["reimport_c_s"]) +
+                float(pr["sort_n_s"]) + float(pr["sort_c_s"]))
+
+
+def port_sample(scale: float):
+    """The oracle's C restatement on a sample; returns (Mbp, seconds)."""
+    from distributedpanga_b200 import gdb, synth
+    from oracle import binding as orc
+    cs = gdb.from_contigs(synth.make("chromset", scale=scale))
+    posb, ctgb, _ = gdb.record_sizing(cs)
+    dbyte, _ = gdb.diag_sizing(cs, ctgb)
+    t0 = time.time()
+    srt = orc.sort_records(orc.extract(cs, posb, ctgb))
+    ent, cum, _ = orc.build_adapter(srt, posb, ctgb)
+    ns, css, _, _ = orc.merge(ent, cum, posb, ctgb, 10, cs.ncontig)
+    orc.reimport_sort(ns, posb, ctgb, 0, cs.ncontig, cs.maxctg, dbyte)
+    orc.reimport_sort(css, posb, ctgb, 1, cs.ncontig, cs.maxctg, dbyte)
+    return cs.seqtot / 1e6, time.time() - t0
+
+
+def cpu_baseline(sample_scale: float) -> dict:
+    from oracle import binding as orc
+    cores_total = os.cpu_count()
+    if orc.ref_available():
+        r = ReferenceSample(sample_scale)
+        sec = min(r.run() for _ in range(2))
+        mbp = r.mbp
+        return {"value": mbp / sec, "unit": UNIT, "cores": 4, "kind": "reference",
+                "sample": "chromset generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
+                          "(oracle/_ref), stages extract+sort+adapter+merge+reimport+seed sort; msd_sort uses "
+                          "4 threads, the rest 1; host has %d cores" % (sample_scale, mbp, cores_total),
+                "seconds": sec}
+    orc.build()
+    mbp, sec = port_sample(sample_scale)
+    return {"value": mbp / sec, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "chromset generator at scale %g (%.1f Mbp), oracle C restatement, 1 thread; host has %d cores"
+                      % (sample_scale, mbp, cores_total), "seconds": sec}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from oracle import binding as orc
+    vals = []
+    detail = None
+    ref = ReferenceSample(args.ref_scale) if orc.ref_available() else None
+    for it in range(args.warmup + args.steps):
+        if ref is not None:
+            mbp, sec = ref.mbp, ref.run()
+            kind, cores = "reference", 4
+        else:
+            orc.build()
+            mbp, sec = port_sample(args.ref_scale)
+            kind, cores = "port", 1
+        if it >= args.warmup:
+            vals.append(mbp / sec)
+        detail = (mbp, kind, cores)
+    v = statistics.median(vals)
+    mbp, kind, cores = detail
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mbp / v * 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "sample_scale": args.ref_scale},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": "chromset generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---- GPU arm ---------------------------------------------------------------------
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    from distributedpanga_b200 import gdb, pipeline
+    torch.cuda.set_device(local_rank)
+    cs, _ = make_contigs(args.scale)
+    posb, ctgb, rsize = gdb.record_sizing(cs)
+    dev = pipeline.Device(local_rank)
+    stream = torch.cuda.current_stream()
+    dev.set_stream(stream.cuda_stream)
+    dev.gdb_load(cs)
+
+    def step():
+        dev.index_build(want_entries=True)
+        dev.merge(10)
+        dev.diag_sort(0)
+        dev.diag_sort(1)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    l0 = dev.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = (dev.launches() - l0) // args.steps
+    clk = clocks.stop()
+    nrec = dev.nrec
+    nseeds = dev.nseeds
+
+    # stage times of one more step
+    dev.enable_timing(True)
+    step()
+    st = dev.stage_times()
+    dev.enable_timing(False)
+
+    # end to end through the C ABI with host buffers
+    swide = None
+    h2d = int(cs.bps.size + 16 * cs.ncontig)
+    d2h = 0
+    e2e_ms = []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        dev.gdb_load(cs)
+        dev.index_build(want_entries=True)
+        dev.merge(10)
+        d2h = 0
+        for comp in (0, 1):
+            sw, cnt = dev.diag_sort(comp)
+            arr, off = dev.diag_records(comp, sw, cnt)
+            d2h += arr.nbytes + off.nbytes
+            swide = sw
+        t1.record(stream)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            e2e_ms.append(t0.elapsed_time(t1))
+    e2e_ms_step = statistics.median(e2e_ms)
+
+    t = torch.tensor([ms, e2e_ms_step], device="cuda", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms_step = float(t[0]), float(t[1])
+    mbp = cs.seqtot / 1e6
+    value = world * mbp / (ms / 1000.0)
+    e2e = world * mbp / (e2e_ms_step / 1000.0)
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    idx_ms = sum(st[k] for k in ("extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
+                                 "entries_prefix_table"))
+    ab = index_bytes(cs, nrec)
+    achieved = ab / (idx_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tr = json.load(f)
+        traffic = tr.get("index_build_bytes_per_launch_at_scale", {}).get(str(args.scale))
+    except Exception:
+        pass
+    base = None
+    if not args.no_cpu_baseline:
+        try:
+            base = cpu_baseline(args.ref_scale)
+        except Exception as e:  # a missing toolchain must not hide the GPU number
+            base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": "failed: %s" % e}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, chromset workload)",
+        "config": {"workload": WORKLOAD, "scale": args.scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
+                   "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
+                   "record_bytes": rsize, "swide": swide,
+                   "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "stage_ms": st,
+        "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
+                                               "k_lcp, k_entries, k_prefix_table)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": ab,
+                     "ms": idx_ms},
+        "cpu_baseline": base,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = 2 x 100 Mbp)")
+    ap.add_argument("--ref-scale", type=float, default=0.02, help="CPU sample scale")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

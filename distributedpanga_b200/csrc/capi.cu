@@ -1,0 +1,981 @@
+// C-ABI layer: context, device buffers, stage drivers and the drop-in entry
+// points declared in include/pga_b200.h.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "index.cuh"
+#include "merge.cuh"
+#include "radix.cuh"
+#include "scan.cuh"
+#include "seeds.cuh"
+#include "../../include/pga_b200.h"
+
+using namespace pga;
+
+namespace {
+
+struct DBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+enum StageId { ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_N };
+
+}  // namespace
+
+struct pga_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t st = nullptr;
+  char err[512] = {0};
+  int64_t launches = 0;
+  bool timing = false;
+  cudaEvent_t ev[ST_N][2] = {};
+  float stage_ms[ST_N] = {0};
+  bool stage_used[ST_N] = {false};
+
+  // GDB
+  bool have_gdb = false;
+  int ncontig = 0;
+  int64_t maxctg = 0;
+  std::vector<int64_t> clen, boff;
+  int posb = 0, ctgb = 0, rsize = 0;
+  DBuf bps, dclen, dboff, tile_ctg, tile_j0;
+  int ntiles = 0;
+  std::vector<int32_t> h_tile_ctg;
+
+  // index
+  DBuf hist, start, scan_tmp, rec, rec2, lcp, ent, cum, qmed, qbig, qcount, maxrun, u64tmp;
+  int64_t nrec = 0;
+  bool have_index = false, have_entries = false;
+  int64_t largest = 0;
+
+  // merge
+  DBuf blk_n, blk_c, blk_tmp, seed[2];
+  int64_t nseed[2] = {0, 0};
+  bool have_seeds = false;
+  int freq = 0;
+
+  // diagonal sort
+  DBuf keys[2], keys_alt, rhist, rscan, panel[2];
+  U128 *sorted[2] = {nullptr, nullptr};
+  SeedKeyLayout lay[2];
+  bool have_diag[2] = {false, false};
+
+  // generic byte staging
+  DBuf io, io2;
+};
+
+namespace {
+
+int fail(pga_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(c->err, sizeof(c->err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                            \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return fail(ctx, PGA_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
+                  __LINE__);                                                                \
+  } while (0)
+
+#define LAUNCHED(k) (ctx->launches += (k))
+
+int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.cap >= bytes) return PGA_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  b.cap = bytes;
+  return PGA_OK;
+}
+
+#define ENSURE(b, bytes)                      \
+  do {                                        \
+    int _r = ensure(ctx, (b), (bytes));       \
+    if (_r != PGA_OK) return _r;              \
+  } while (0)
+
+template <typename T>
+T *P(DBuf &b) { return (T *)b.p; }
+
+int grid_for(int64_t n, int threads, int cap = 148 * 32) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+void stage_begin(pga_ctx *ctx, int s) {
+  if (ctx->timing) cudaEventRecord(ctx->ev[s][0], ctx->st);
+}
+void stage_end(pga_ctx *ctx, int s) {
+  if (ctx->timing) {
+    cudaEventRecord(ctx->ev[s][1], ctx->st);
+    ctx->stage_used[s] = true;
+  }
+}
+
+int bytes_inclusive(int64_t maxv) {
+  int b = 0;
+  int64_t cum = 1;
+  while (cum < maxv + 1) {
+    cum *= 256;
+    b += 1;
+  }
+  return b;
+}
+
+int bitlen(uint64_t v) {
+  int b = 0;
+  while (v) {
+    b++;
+    v >>= 1;
+  }
+  return b;
+}
+
+// ---- index stages ---------------------------------------------------------
+
+// Buckets are already scattered by prefix into ctx->rec; `start` holds the
+// exclusive scan (NPREFIX+1 entries).  Sort each bucket.
+int sort_buckets(pga_ctx *ctx) {
+  ENSURE(ctx->qmed, sizeof(uint32_t) * NPREFIX);
+  ENSURE(ctx->qbig, sizeof(uint32_t) * NPREFIX);
+  ENSURE(ctx->qcount, sizeof(uint32_t) * 4);
+  CK(cudaMemsetAsync(ctx->qcount.p, 0, sizeof(uint32_t) * 4, ctx->st));
+  k_bucket_small<<<NPREFIX / 256, 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint32_t>(ctx->start),
+                                                      P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
+                                                      P<uint32_t>(ctx->qcount));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  uint32_t q[4];
+  CK(cudaMemcpyAsync(q, ctx->qcount.p, sizeof(q), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (q[0] > 0) {
+    k_bucket_medium<<<q[0], BK_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint32_t>(ctx->start),
+                                                      P<uint32_t>(ctx->qmed));
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+  }
+  if (q[1] > 0) {
+    uint32_t np2 = 1;
+    while (np2 < q[2]) np2 <<= 1;
+    for (uint32_t k = 2; k <= np2; k <<= 1)
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        dim3 g((np2 / 2 + 255) / 256, q[1]);
+        k_bucket_big_step<<<g, 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint32_t>(ctx->start),
+                                                  P<uint32_t>(ctx->qbig), k, j);
+        LAUNCHED(1);
+      }
+    CK(cudaGetLastError());
+  }
+  return PGA_OK;
+}
+
+// LCP bytes, optional entries, prefix table and the largest prefix group.
+int finish_index(pga_ctx *ctx, bool want_entries) {
+  int64_t n = ctx->nrec;
+  ENSURE(ctx->lcp, (size_t)n + 16);
+  stage_begin(ctx, ST_LCP);
+  if (n > 0) {
+    k_lcp<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), n, P<uint8_t>(ctx->lcp));
+    LAUNCHED(1);
+  }
+  stage_end(ctx, ST_LCP);
+  stage_begin(ctx, ST_ENTRIES);
+  ENSURE(ctx->maxrun, 16);
+  CK(cudaMemsetAsync(ctx->maxrun.p, 0, 4, ctx->st));
+  int64_t *cum = nullptr;
+  if (want_entries) {
+    int eb = 9 + ctx->posb + ctx->ctgb;
+    ENSURE(ctx->ent, (size_t)n * eb + 16);
+    ENSURE(ctx->cum, sizeof(int64_t) * NPREFIX);
+    if (n > 0) {
+      k_entries<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n,
+                                                       ctx->posb, ctx->ctgb, P<uint8_t>(ctx->ent));
+      LAUNCHED(1);
+    }
+    cum = P<int64_t>(ctx->cum);
+  }
+  k_prefix_table<<<NPREFIX / 256, 256, 0, ctx->st>>>(P<uint32_t>(ctx->start), cum, P<uint32_t>(ctx->maxrun));
+  LAUNCHED(1);
+  stage_end(ctx, ST_ENTRIES);
+  CK(cudaGetLastError());
+  uint32_t mr = 0;
+  CK(cudaMemcpyAsync(&mr, ctx->maxrun.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->largest = mr;
+  ctx->have_index = true;
+  ctx->have_entries = want_entries;
+  ctx->have_seeds = false;
+  ctx->have_diag[0] = ctx->have_diag[1] = false;
+  return PGA_OK;
+}
+
+// hist (NPREFIX) -> start (NPREFIX+1, exclusive scan) and cursor = start.
+int scan_hist(pga_ctx *ctx, int64_t *total) {
+  ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(NPREFIX + 1));
+  uint32_t *h = P<uint32_t>(ctx->hist), *s = P<uint32_t>(ctx->start);
+  CK(cudaMemsetAsync(h + NPREFIX, 0, sizeof(uint32_t), ctx->st));
+  CK(exclusive_scan<uint32_t>(h, s, NPREFIX + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr, ctx->st));
+  LAUNCHED(3);
+  CK(cudaMemcpyAsync(h, s, sizeof(uint32_t) * NPREFIX, cudaMemcpyDeviceToDevice, ctx->st));  // cursor
+  uint32_t t = 0;
+  CK(cudaMemcpyAsync(&t, s + NPREFIX, 4, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  *total = t;
+  return PGA_OK;
+}
+
+int check_records_fit(pga_ctx *ctx, int64_t n) {
+  if (n >= (int64_t)0xffffffffLL)
+    return fail(ctx, PGA_ERR_LIMIT, "%lld records: at most 2^32-2 supported", (long long)n);
+  return PGA_OK;
+}
+
+// Host records (reference format) -> sorted device index (drop-in path).
+int index_from_host(pga_ctx *ctx, const uint8_t *records, int64_t count, int posb, int ctgb) {
+  int r = check_records_fit(ctx, count);
+  if (r) return r;
+  int rs = 12 + posb + ctgb;
+  ctx->posb = posb;
+  ctx->ctgb = ctgb;
+  ctx->rsize = rs;
+  ctx->nrec = count;
+  ENSURE(ctx->io, (size_t)count * rs + 16);
+  ENSURE(ctx->rec, sizeof(Rec) * (size_t)count + 16);
+  ENSURE(ctx->rec2, sizeof(Rec) * (size_t)count + 16);
+  ENSURE(ctx->hist, sizeof(uint32_t) * (NPREFIX + 1));
+  ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
+  if (count > 0) {
+    CK(cudaMemcpyAsync(ctx->io.p, records, (size_t)count * rs, cudaMemcpyHostToDevice, ctx->st));
+    k_records_in<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), count, posb, ctgb, P<Rec>(ctx->rec2), nullptr);
+    LAUNCHED(1);
+  }
+  CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(uint32_t) * NPREFIX, ctx->st));
+  if (count > 0) {
+    k_prefix_hist<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec2), count, P<uint32_t>(ctx->hist));
+    LAUNCHED(1);
+  }
+  int64_t tot = 0;
+  r = scan_hist(ctx, &tot);
+  if (r) return r;
+  if (count > 0) {
+    k_prefix_scatter<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec2), count, P<uint32_t>(ctx->hist),
+                                                                P<Rec>(ctx->rec));
+    LAUNCHED(1);
+  }
+  CK(cudaGetLastError());
+  return sort_buckets(ctx);
+}
+
+// Entries + prefix table (reference format, host) -> device records + LCPs.
+__global__ void k_entries_in(const uint8_t *__restrict__ ent, const int64_t *__restrict__ cum, int64_t n,
+                             int posb, int ctgb, Rec *__restrict__ rec, uint8_t *__restrict__ lcp) {
+  const int eb = 9 + posb + ctgb;
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= NPREFIX) return;
+  int64_t a = p ? cum[p - 1] : 0, b = cum[p];
+  if (b > n) b = n;
+  for (int64_t i = a; i < b; i++) {
+    const uint8_t *d = ent + i * eb;
+    uint64_t hi = (uint64_t)p << 40;
+    for (int k = 0; k < 5; k++) hi |= (uint64_t)d[k] << (32 - 8 * k);
+    uint64_t lo16 = ((uint64_t)d[5] << 8) | d[6];
+    uint64_t pos = 0, cs = 0;
+    for (int k = 0; k < posb; k++) pos |= (uint64_t)d[9 + k] << (8 * k);
+    for (int k = 0; k < ctgb; k++) cs |= (uint64_t)d[9 + posb + k] << (8 * k);
+    Rec r;
+    r.hi = hi;
+    r.lo = (lo16 << 48) | (cs << 32) | pos;
+    rec[i] = r;
+    lcp[i] = d[8];
+  }
+}
+
+// ---- merge ------------------------------------------------------------------
+
+int run_merge(pga_ctx *ctx, int freq) {
+  int64_t n = ctx->nrec;
+  int nb = (int)((n + MERGE_THREADS - 1) / MERGE_THREADS);
+  if (nb < 1) nb = 1;
+  ENSURE(ctx->blk_n, sizeof(uint32_t) * (nb + 1));
+  ENSURE(ctx->blk_c, sizeof(uint32_t) * (nb + 1));
+  ENSURE(ctx->blk_tmp, sizeof(uint32_t) * scan_tmp_elems(nb + 1) + 64);
+  ENSURE(ctx->u64tmp, 64);
+  stage_begin(ctx, ST_MERGE);
+  uint32_t *bn = P<uint32_t>(ctx->blk_n), *bc = P<uint32_t>(ctx->blk_c);
+  CK(cudaMemsetAsync(bn, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
+  CK(cudaMemsetAsync(bc, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
+  if (n > 0) {
+    k_merge<false><<<nb, MERGE_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
+                                                      nullptr, nullptr, ctx->ctgb);
+    LAUNCHED(1);
+  }
+  uint32_t *tot = P<uint32_t>(ctx->u64tmp);
+  CK(exclusive_scan<uint32_t>(bn, bn, nb + 1, P<uint32_t>(ctx->blk_tmp), tot, ctx->st));
+  CK(exclusive_scan<uint32_t>(bc, bc, nb + 1, P<uint32_t>(ctx->blk_tmp), tot + 1, ctx->st));
+  LAUNCHED(6);
+  uint32_t t[2];
+  CK(cudaMemcpyAsync(t, tot, 8, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->nseed[0] = t[0];
+  ctx->nseed[1] = t[1];
+  ENSURE(ctx->seed[0], sizeof(Seed) * (size_t)t[0] + 16);
+  ENSURE(ctx->seed[1], sizeof(Seed) * (size_t)t[1] + 16);
+  if (n > 0) {
+    k_merge<true><<<nb, MERGE_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
+                                                     P<Seed>(ctx->seed[0]), P<Seed>(ctx->seed[1]), ctx->ctgb);
+    LAUNCHED(1);
+  }
+  stage_end(ctx, ST_MERGE);
+  CK(cudaGetLastError());
+  ctx->have_seeds = true;
+  ctx->freq = freq;
+  ctx->have_diag[0] = ctx->have_diag[1] = false;
+  return PGA_OK;
+}
+
+// Per-A-contig seed counts of a device seed array (host result).
+__global__ void k_seed_buck(const Seed *__restrict__ sd, int64_t n, unsigned long long *__restrict__ buck) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&buck[sd[i].b & 0xffffu], 1ull);
+}
+
+// ---- diagonal sort ------------------------------------------------------------
+
+SeedKeyLayout make_layout(int comp, int ncontig, int64_t amxpos, int dbyte, int ctgb) {
+  SeedKeyLayout L;
+  L.comp = comp;
+  L.amxpos = amxpos;
+  L.bmxpos = amxpos;
+  L.maxdag = 2 * amxpos;
+  L.dbyte = dbyte;
+  L.ctgb = ctgb;
+  L.dmask = dbyte >= 8 ? ~0ull : ((1ull << (8 * dbyte)) - 1);
+  L.jmask = (1ull << (8 * ctgb - 1)) - 1;
+  uint64_t amax = std::min<uint64_t>((uint64_t)L.maxdag, L.dmask);
+  uint64_t bmax = std::min<uint64_t>((uint64_t)(L.maxdag >> 6), L.dmask);
+  int wc = bitlen((uint64_t)(ncontig > 1 ? ncontig - 1 : 1));
+  L.off_dlow = 6;
+  L.off_anti = 12;
+  L.off_band = L.off_anti + bitlen(amax);
+  L.off_j = L.off_band + bitlen(bmax);
+  L.off_i = L.off_j + wc;
+  L.w_i = wc;
+  L.total_bits = L.off_i + wc;
+  return L;
+}
+
+// Seeds of unit comp in ctx->seed[comp] -> sorted keys.
+int run_diag(pga_ctx *ctx, int comp, int ncontig, int64_t amxpos, int dbyte, int ctgb) {
+  int64_t n = ctx->nseed[comp];
+  SeedKeyLayout L = make_layout(comp, ncontig, amxpos, dbyte, ctgb);
+  if (L.total_bits > 128) return fail(ctx, PGA_ERR_LIMIT, "diagonal sort key needs %d bits", L.total_bits);
+  ctx->lay[comp] = L;
+  ENSURE(ctx->keys[comp], sizeof(U128) * (size_t)n + 16);
+  ENSURE(ctx->keys_alt, sizeof(U128) * (size_t)n + 16);
+  ENSURE(ctx->rhist, sizeof(uint32_t) * radix_hist_elems(n) + 64);
+  ENSURE(ctx->rscan, sizeof(uint32_t) * scan_tmp_elems(radix_hist_elems(n)) + 64);
+  ENSURE(ctx->u64tmp, 64);
+  stage_begin(ctx, ST_DIAG);
+  U128 *keys = P<U128>(ctx->keys[comp]);
+  int passes[16], np = 0;
+  if (n > 0) {
+    k_seed_keys<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Seed>(ctx->seed[comp]), n, L, keys);
+    LAUNCHED(1);
+    unsigned long long *acc = P<unsigned long long>(ctx->u64tmp);
+    CK(cudaMemsetAsync(acc, 0, 16, ctx->st));
+    k_u128_diffbits<<<grid_for(n, 256, 148 * 4), 256, 0, ctx->st>>>(keys, n, acc);
+    LAUNCHED(1);
+    unsigned long long diff[2];
+    CK(cudaMemcpyAsync(diff, acc, 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int s = 0; s < 128; s += 8) {
+      uint64_t w = s < 64 ? diff[0] : diff[1];
+      if ((w >> (s & 63)) & 0xffull) passes[np++] = s;
+    }
+  }
+  U128 *res = keys;
+  CK(radix_sort_u128(keys, P<U128>(ctx->keys_alt), n, passes, np, P<uint32_t>(ctx->rhist),
+                     P<uint32_t>(ctx->rscan), &res, ctx->st));
+  LAUNCHED(5 * np);
+  if (res != keys)  // keep the sorted keys in this unit's own buffer
+    CK(cudaMemcpyAsync(keys, res, sizeof(U128) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
+  stage_end(ctx, ST_DIAG);
+  ctx->sorted[comp] = keys;
+  ctx->have_diag[comp] = true;
+  return PGA_OK;
+}
+
+int copy_diag(pga_ctx *ctx, int comp, int ncontig, uint8_t *out, int64_t *panel_off) {
+  int64_t n = ctx->nseed[comp];
+  const SeedKeyLayout &L = ctx->lay[comp];
+  int sw = 2 * L.dbyte + L.ctgb + 2;
+  ENSURE(ctx->io, (size_t)n * sw + 16);
+  ENSURE(ctx->panel[comp], sizeof(int64_t) * (ncontig + 1));
+  if (n > 0) {
+    k_seed_records<<<grid_for(n, 256), 256, 0, ctx->st>>>(ctx->sorted[comp], n, L, P<uint8_t>(ctx->io));
+    LAUNCHED(1);
+  }
+  k_panel_bounds<<<(ncontig + 1 + 255) / 256, 256, 0, ctx->st>>>(ctx->sorted[comp], n, L, ncontig,
+                                                                 P<int64_t>(ctx->panel[comp]));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  if (out && n > 0) CK(cudaMemcpyAsync(out, ctx->io.p, (size_t)n * sw, cudaMemcpyDeviceToHost, ctx->st));
+  if (panel_off)
+    CK(cudaMemcpyAsync(panel_off, ctx->panel[comp].p, sizeof(int64_t) * (ncontig + 1), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+int copy_seeds(pga_ctx *ctx, int comp, uint8_t *out, int64_t *buck) {
+  int64_t n = ctx->nseed[comp];
+  int sb = 1 + 2 * (ctx->posb + ctx->ctgb);
+  if (out) {
+    ENSURE(ctx->io, (size_t)n * sb + 16);
+    if (n > 0) {
+      k_seeds_out<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Seed>(ctx->seed[comp]), n, ctx->posb, ctx->ctgb,
+                                                         P<uint8_t>(ctx->io));
+      LAUNCHED(1);
+      CK(cudaMemcpyAsync(out, ctx->io.p, (size_t)n * sb, cudaMemcpyDeviceToHost, ctx->st));
+    }
+  }
+  if (buck) {
+    ENSURE(ctx->io2, sizeof(uint64_t) * (ctx->ncontig + 1));
+    CK(cudaMemsetAsync(ctx->io2.p, 0, sizeof(uint64_t) * ctx->ncontig, ctx->st));
+    if (n > 0) {
+      k_seed_buck<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Seed>(ctx->seed[comp]), n,
+                                                         P<unsigned long long>(ctx->io2));
+      LAUNCHED(1);
+    }
+    CK(cudaMemcpyAsync(buck, ctx->io2.p, sizeof(int64_t) * ctx->ncontig, cudaMemcpyDeviceToHost, ctx->st));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+
+extern "C" {
+
+int pga_ctx_create(int device, pga_ctx **out) {
+  if (!out) return PGA_ERR_ARG;
+  *out = nullptr;
+  pga_ctx *ctx = new (std::nothrow) pga_ctx();
+  if (!ctx) return PGA_ERR_NOMEM;
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return PGA_ERR_CUDA;
+  }
+  ctx->st = ctx->own;
+  for (int s = 0; s < ST_N; s++) {
+    cudaEventCreate(&ctx->ev[s][0]);
+    cudaEventCreate(&ctx->ev[s][1]);
+  }
+  *out = ctx;
+  return PGA_OK;
+}
+
+void pga_ctx_destroy(pga_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->st);
+  DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
+                  &ctx->scan_tmp, &ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->cum, &ctx->qmed,
+                  &ctx->qbig, &ctx->qcount, &ctx->maxrun, &ctx->u64tmp, &ctx->blk_n, &ctx->blk_c,
+                  &ctx->blk_tmp, &ctx->seed[0], &ctx->seed[1], &ctx->keys[0], &ctx->keys[1],
+                  &ctx->keys_alt, &ctx->rhist, &ctx->rscan, &ctx->panel[0], &ctx->panel[1], &ctx->io,
+                  &ctx->io2};
+  for (DBuf *b : bufs)
+    if (b->p) cudaFree(b->p);
+  for (int s = 0; s < ST_N; s++) {
+    cudaEventDestroy(ctx->ev[s][0]);
+    cudaEventDestroy(ctx->ev[s][1]);
+  }
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+
+const char *pga_last_error(const pga_ctx *ctx) { return ctx ? ctx->err : "null context"; }
+
+int pga_ctx_set_stream(pga_ctx *ctx, void *stream) {
+  if (!ctx) return PGA_ERR_ARG;
+  ctx->st = stream ? (cudaStream_t)stream : ctx->own;
+  return PGA_OK;
+}
+
+int pga_ctx_synchronize(pga_ctx *ctx) {
+  if (!ctx) return PGA_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+int64_t pga_kernel_launches(const pga_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int pga_ctx_enable_timing(pga_ctx *ctx, int on) {
+  if (!ctx) return PGA_ERR_ARG;
+  ctx->timing = on != 0;
+  for (int s = 0; s < ST_N; s++) ctx->stage_used[s] = false;
+  return PGA_OK;
+}
+
+int pga_stage_times(const pga_ctx *cctx, float *ms8) {
+  pga_ctx *ctx = const_cast<pga_ctx *>(cctx);
+  if (!ctx || !ms8) return PGA_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int s = 0; s < ST_N; s++) {
+    ms8[s] = 0.f;
+    if (ctx->stage_used[s]) cudaEventElapsedTime(&ms8[s], ctx->ev[s][0], ctx->ev[s][1]);
+  }
+  return PGA_OK;
+}
+
+int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int ncontig, const int64_t *clen,
+                 const int64_t *boff) {
+  if (!ctx || ncontig < 0 || (ncontig > 0 && (!clen || !boff)) || bps_bytes < 0) return PGA_ERR_ARG;
+  if (ncontig >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%d contigs: at most 32767 supported", ncontig);
+  CK(cudaSetDevice(ctx->device));
+  ctx->ncontig = ncontig;
+  ctx->clen.assign(clen, clen + ncontig);
+  ctx->boff.assign(boff, boff + ncontig);
+  ctx->maxctg = 0;
+  for (int i = 0; i < ncontig; i++) {
+    if (clen[i] < 0) return fail(ctx, PGA_ERR_ARG, "contig %d has negative length", i);
+    if (clen[i] >= ((int64_t)1 << 31)) return fail(ctx, PGA_ERR_LIMIT, "contig %d longer than 2^31-1", i);
+    if (boff[i] >= 0 && boff[i] + (clen[i] + 3) / 4 > bps_bytes)
+      return fail(ctx, PGA_ERR_ARG, "contig %d extends past the sequence image", i);
+    ctx->maxctg = std::max(ctx->maxctg, clen[i]);
+  }
+  ctx->posb = bytes_inclusive(ctx->maxctg);
+  ctx->ctgb = bytes_inclusive(2 * (int64_t)ncontig - 1);
+  if (ctx->ctgb < 1) ctx->ctgb = 1;
+  ctx->rsize = 12 + ctx->posb + ctx->ctgb;
+  ENSURE(ctx->bps, (size_t)bps_bytes + 16);
+  ENSURE(ctx->dclen, sizeof(int64_t) * (ncontig + 1));
+  ENSURE(ctx->dboff, sizeof(int64_t) * (ncontig + 1));
+  if (bps_bytes > 0) CK(cudaMemcpyAsync(ctx->bps.p, bps, bps_bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (ncontig > 0) {
+    CK(cudaMemcpyAsync(ctx->dclen.p, clen, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->dboff.p, boff, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
+  }
+  std::vector<int64_t> tj;
+  ctx->h_tile_ctg.clear();
+  for (int r = 0; r < ncontig; r++) {
+    if (boff[r] < 0 || clen[r] < TMER) continue;
+    int64_t npos = clen[r] - TMER + 1;
+    for (int64_t j0 = 0; j0 < npos; j0 += EXT_TILE) {
+      ctx->h_tile_ctg.push_back(r);
+      tj.push_back(j0);
+    }
+  }
+  ctx->ntiles = (int)tj.size();
+  ENSURE(ctx->tile_ctg, sizeof(int32_t) * (ctx->ntiles + 1));
+  ENSURE(ctx->tile_j0, sizeof(int64_t) * (ctx->ntiles + 1));
+  if (ctx->ntiles > 0) {
+    CK(cudaMemcpyAsync(ctx->tile_ctg.p, ctx->h_tile_ctg.data(), sizeof(int32_t) * ctx->ntiles,
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->tile_j0.p, tj.data(), sizeof(int64_t) * ctx->ntiles, cudaMemcpyHostToDevice, ctx->st));
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->have_gdb = true;
+  ctx->have_index = false;
+  ctx->have_seeds = false;
+  ctx->have_diag[0] = ctx->have_diag[1] = false;
+  return PGA_OK;
+}
+
+int pga_record_sizing(const pga_ctx *ctx, int *posb, int *ctgb, int *rsize) {
+  if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
+  if (posb) *posb = ctx->posb;
+  if (ctgb) *ctgb = ctx->ctgb;
+  if (rsize) *rsize = ctx->rsize;
+  return PGA_OK;
+}
+
+int pga_extract_to_records(pga_ctx *ctx, int num_workers, int worker_id, uint8_t **records, int64_t *count) {
+  if (!ctx || !ctx->have_gdb || !records || !count || num_workers < 1 || worker_id < 0 ||
+      worker_id >= num_workers)
+    return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  *records = nullptr;
+  *count = 0;
+  // Contig split by cumulative bases (compute_work_split, src/work_split.c:3-26).
+  int64_t total = 0;
+  for (int r = 0; r < ctx->ncontig; r++) total += ctx->clen[r];
+  std::vector<int> split(num_workers + 1, 0);
+  {
+    int64_t so_far = 0, next = total / num_workers;
+    int nw = 1;
+    for (int r = 0; r < ctx->ncontig; r++) {
+      so_far += ctx->clen[r];
+      while (so_far >= next && nw < num_workers) {
+        split[nw] = r + 1;
+        nw += 1;
+        next = (total * nw) / num_workers;
+      }
+    }
+    split[num_workers] = ctx->ncontig;
+  }
+  int rbeg = split[worker_id], rend = split[worker_id + 1];
+  int tbeg = 0, tend = 0;
+  while (tbeg < ctx->ntiles && ctx->h_tile_ctg[tbeg] < rbeg) tbeg++;
+  tend = tbeg;
+  while (tend < ctx->ntiles && ctx->h_tile_ctg[tend] < rend) tend++;
+  int nt = tend - tbeg;
+  int64_t nthr = (int64_t)nt * EXT_THREADS;
+  ENSURE(ctx->u64tmp, 64);
+  ENSURE(ctx->io2, sizeof(uint64_t) * (nthr + 1) + 64);
+  ENSURE(ctx->scan_tmp, sizeof(uint64_t) * scan_tmp_elems(nthr + 1) + 64);
+  uint32_t *cnt32 = P<uint32_t>(ctx->hist);
+  ENSURE(ctx->hist, sizeof(uint32_t) * std::max<int64_t>(NPREFIX + 1, nthr + 1));
+  cnt32 = P<uint32_t>(ctx->hist);
+  uint64_t *off = P<uint64_t>(ctx->io2);
+  uint64_t total_rec = 0;
+  if (nt > 0) {
+    const int32_t *tc = P<int32_t>(ctx->tile_ctg) + tbeg;
+    const int64_t *tj = P<int64_t>(ctx->tile_j0) + tbeg;
+    k_extract<EXT_COUNT><<<nt, EXT_THREADS, 0, ctx->st>>>(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen),
+                                                           P<int64_t>(ctx->dboff), tc, tj, ctx->ctgb, cnt32,
+                                                           nullptr, nullptr, nullptr, nullptr);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    // widen the counts to 64 bits for the offsets scan
+    std::vector<uint32_t> hc(nthr);
+    CK(cudaMemcpyAsync(hc.data(), cnt32, sizeof(uint32_t) * nthr, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::vector<uint64_t> ho(nthr);
+    for (int64_t i = 0; i < nthr; i++) {
+      ho[i] = total_rec;
+      total_rec += hc[i];
+    }
+    int r = check_records_fit(ctx, (int64_t)total_rec);
+    if (r) return r;
+    CK(cudaMemcpyAsync(off, ho.data(), sizeof(uint64_t) * nthr, cudaMemcpyHostToDevice, ctx->st));
+    ENSURE(ctx->rec2, sizeof(Rec) * total_rec + 16);
+    k_extract<EXT_WRITE><<<nt, EXT_THREADS, 0, ctx->st>>>(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen),
+                                                           P<int64_t>(ctx->dboff), tc, tj, ctx->ctgb, nullptr,
+                                                           off, P<Rec>(ctx->rec2), nullptr, nullptr);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+  }
+  size_t bytes = (size_t)total_rec * ctx->rsize;
+  uint8_t *h = (uint8_t *)malloc(bytes + 1);
+  if (!h) return fail(ctx, PGA_ERR_NOMEM, "malloc(%zu)", bytes + 1);
+  if (total_rec > 0) {
+    int r = ensure(ctx, ctx->io, bytes + 16);
+    if (r) {
+      free(h);
+      return r;
+    }
+    k_records_out<<<grid_for(total_rec, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec2), nullptr, total_rec, ctx->posb,
+                                                                  ctx->ctgb, P<uint8_t>(ctx->io));
+    LAUNCHED(1);
+    cudaError_t e = cudaMemcpyAsync(h, ctx->io.p, bytes, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) {
+      free(h);
+      return fail(ctx, PGA_ERR_CUDA, "extract copy: %s", cudaGetErrorString(e));
+    }
+  }
+  *records = h;
+  *count = (int64_t)total_rec;
+  ctx->have_index = false;
+  return PGA_OK;
+}
+
+int pga_sort_records(pga_ctx *ctx, uint8_t *records, int64_t count, int posb, int ctgb) {
+  if (!ctx || count < 0 || (count > 0 && !records) || posb < 1 || posb > 4 || ctgb < 1 || ctgb > 2)
+    return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = index_from_host(ctx, records, count, posb, ctgb);
+  if (r) return r;
+  int rs = 12 + posb + ctgb;
+  ENSURE(ctx->lcp, (size_t)count + 16);
+  if (count > 0) {
+    k_lcp<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), count, P<uint8_t>(ctx->lcp));
+    k_records_out<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), count, posb,
+                                                              ctgb, P<uint8_t>(ctx->io));
+    LAUNCHED(2);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(records, ctx->io.p, (size_t)count * rs, cudaMemcpyDeviceToHost, ctx->st));
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->have_index = false;
+  return PGA_OK;
+}
+
+int pga_build_kmer_adapter(pga_ctx *ctx, const uint8_t *records, int64_t count, int posb, int ctgb,
+                           uint8_t *entries, int64_t *cum, int64_t *largest) {
+  if (!ctx || count < 0 || (count > 0 && (!records || !entries)) || !cum || posb < 1 || posb > 4 || ctgb < 1 ||
+      ctgb > 2)
+    return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = check_records_fit(ctx, count);
+  if (r) return r;
+  int rs = 12 + posb + ctgb, eb = 9 + posb + ctgb;
+  ENSURE(ctx->io, (size_t)count * rs + 16);
+  ENSURE(ctx->rec, sizeof(Rec) * (size_t)count + 16);
+  ENSURE(ctx->lcp, (size_t)count + 16);
+  ENSURE(ctx->ent, (size_t)count * eb + 16);
+  ENSURE(ctx->cum, sizeof(int64_t) * NPREFIX);
+  ENSURE(ctx->hist, sizeof(uint32_t) * (NPREFIX + 1));
+  ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
+  ENSURE(ctx->maxrun, 16);
+  // The records are already sorted: their prefixes' histogram scan gives the table.
+  CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(uint32_t) * NPREFIX, ctx->st));
+  if (count > 0) {
+    CK(cudaMemcpyAsync(ctx->io.p, records, (size_t)count * rs, cudaMemcpyHostToDevice, ctx->st));
+    k_records_in<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), count, posb, ctgb, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp));
+    k_prefix_hist<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), count, P<uint32_t>(ctx->hist));
+    LAUNCHED(2);
+  }
+  ctx->posb = posb;
+  ctx->ctgb = ctgb;
+  ctx->rsize = rs;
+  ctx->nrec = count;
+  int64_t tot = 0;
+  r = scan_hist(ctx, &tot);
+  if (r) return r;
+  // LCP bytes are the records' own (byte 0), not recomputed.
+  if (count > 0) {
+    k_entries<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), count, posb, ctgb,
+                                                         P<uint8_t>(ctx->ent));
+    LAUNCHED(1);
+  }
+  CK(cudaMemsetAsync(ctx->maxrun.p, 0, 4, ctx->st));
+  k_prefix_table<<<NPREFIX / 256, 256, 0, ctx->st>>>(P<uint32_t>(ctx->start), P<int64_t>(ctx->cum),
+                                                     P<uint32_t>(ctx->maxrun));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  if (count > 0) CK(cudaMemcpyAsync(entries, ctx->ent.p, (size_t)count * eb, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(cum, ctx->cum.p, sizeof(int64_t) * NPREFIX, cudaMemcpyDeviceToHost, ctx->st));
+  uint32_t mr = 0;
+  CK(cudaMemcpyAsync(&mr, ctx->maxrun.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (largest) *largest = mr;
+  ctx->have_index = true;
+  ctx->have_entries = true;
+  ctx->largest = mr;
+  return PGA_OK;
+}
+
+int pga_self_adaptamer_merge(pga_ctx *ctx, const uint8_t *entries, const int64_t *cum, int64_t count, int posb,
+                             int ctgb, int freq, int ncontig, uint8_t **nseeds, int64_t *nlen, uint8_t **cseeds,
+                             int64_t *clen_out, int64_t *nbuck, int64_t *cbuck) {
+  if (!ctx || count < 0 || (count > 0 && !entries) || !cum || !nseeds || !nlen || !cseeds || !clen_out ||
+      posb < 1 || posb > 4 || ctgb < 1 || ctgb > 2 || freq < 1 || ncontig < 1)
+    return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = check_records_fit(ctx, count);
+  if (r) return r;
+  *nseeds = *cseeds = nullptr;
+  *nlen = *clen_out = 0;
+  int eb = 9 + posb + ctgb;
+  ENSURE(ctx->io, (size_t)count * eb + 16);
+  ENSURE(ctx->cum, sizeof(int64_t) * NPREFIX);
+  ENSURE(ctx->rec, sizeof(Rec) * (size_t)count + 16);
+  ENSURE(ctx->lcp, (size_t)count + 16);
+  if (count > 0) CK(cudaMemcpyAsync(ctx->io.p, entries, (size_t)count * eb, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->cum.p, cum, sizeof(int64_t) * NPREFIX, cudaMemcpyHostToDevice, ctx->st));
+  k_entries_in<<<NPREFIX / 256, 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), P<int64_t>(ctx->cum), count, posb, ctgb,
+                                                   P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  ctx->posb = posb;
+  ctx->ctgb = ctgb;
+  ctx->nrec = count;
+  int saved_nc = ctx->ncontig;
+  ctx->ncontig = ncontig;
+  r = run_merge(ctx, freq);
+  if (r) {
+    ctx->ncontig = saved_nc;
+    return r;
+  }
+  int sb = 1 + 2 * (posb + ctgb);
+  uint8_t *hs[2] = {nullptr, nullptr};
+  int64_t *bk[2] = {nbuck, cbuck};
+  for (int u = 0; u < 2; u++) {
+    hs[u] = (uint8_t *)malloc((size_t)ctx->nseed[u] * sb + 1);
+    if (!hs[u]) {
+      free(hs[0]);
+      ctx->ncontig = saved_nc;
+      return fail(ctx, PGA_ERR_NOMEM, "malloc seeds");
+    }
+    r = copy_seeds(ctx, u, hs[u], bk[u]);
+    if (r) {
+      free(hs[0]);
+      free(hs[1]);
+      ctx->ncontig = saved_nc;
+      return r;
+    }
+  }
+  ctx->ncontig = saved_nc;
+  *nseeds = hs[0];
+  *cseeds = hs[1];
+  *nlen = ctx->nseed[0] * sb;
+  *clen_out = ctx->nseed[1] * sb;
+  return PGA_OK;
+}
+
+int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb, int ctgb, int comp, int ncontig,
+                      int64_t amxpos, int dbyte, uint8_t *out, int64_t *panel_off) {
+  if (!ctx || len < 0 || (len > 0 && (!seeds || !out)) || !panel_off || posb < 1 || posb > 4 || ctgb < 1 ||
+      ctgb > 2 || (comp != 0 && comp != 1) || ncontig < 1 || dbyte < 1 || dbyte > 4 || amxpos < 0)
+    return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int sb = 1 + 2 * (posb + ctgb);
+  int64_t n = len / sb;
+  if (n >= (int64_t)0xffffffffLL) return fail(ctx, PGA_ERR_LIMIT, "too many seeds");
+  ENSURE(ctx->io, (size_t)len + 16);
+  ENSURE(ctx->seed[comp], sizeof(Seed) * (size_t)n + 16);
+  if (n > 0) {
+    CK(cudaMemcpyAsync(ctx->io.p, seeds, (size_t)n * sb, cudaMemcpyHostToDevice, ctx->st));
+    k_seeds_in<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), n, posb, ctgb, P<Seed>(ctx->seed[comp]));
+    LAUNCHED(1);
+  }
+  ctx->nseed[comp] = n;
+  int r = run_diag(ctx, comp, ncontig, amxpos, dbyte, ctgb);
+  if (r) return r;
+  return copy_diag(ctx, comp, ncontig, out, panel_off);
+}
+
+int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
+  if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  ENSURE(ctx->hist, sizeof(uint32_t) * (NPREFIX + 1));
+  ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
+  const uint8_t *bps = P<uint8_t>(ctx->bps);
+  const int64_t *cl = P<int64_t>(ctx->dclen), *bo = P<int64_t>(ctx->dboff);
+  const int32_t *tc = P<int32_t>(ctx->tile_ctg);
+  const int64_t *tj = P<int64_t>(ctx->tile_j0);
+  stage_begin(ctx, ST_EXTRACT_HIST);
+  CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(uint32_t) * NPREFIX, ctx->st));
+  if (ctx->ntiles > 0) {
+    k_extract<EXT_HIST><<<ctx->ntiles, EXT_THREADS, 0, ctx->st>>>(bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
+                                                                   nullptr, P<uint32_t>(ctx->hist), nullptr);
+    LAUNCHED(1);
+  }
+  stage_end(ctx, ST_EXTRACT_HIST);
+  CK(cudaGetLastError());
+  stage_begin(ctx, ST_SCAN);
+  int64_t n = 0;
+  int r = scan_hist(ctx, &n);
+  if (r) return r;
+  stage_end(ctx, ST_SCAN);
+  r = check_records_fit(ctx, n);
+  if (r) return r;
+  ctx->nrec = n;
+  ENSURE(ctx->rec, sizeof(Rec) * (size_t)n + 16);
+  stage_begin(ctx, ST_EXTRACT_SCATTER);
+  if (ctx->ntiles > 0) {
+    k_extract<EXT_SCATTER><<<ctx->ntiles, EXT_THREADS, 0, ctx->st>>>(bps, cl, bo, tc, tj, ctx->ctgb, nullptr,
+                                                                      nullptr, P<Rec>(ctx->rec), nullptr,
+                                                                      P<uint32_t>(ctx->hist));
+    LAUNCHED(1);
+  }
+  stage_end(ctx, ST_EXTRACT_SCATTER);
+  CK(cudaGetLastError());
+  stage_begin(ctx, ST_BUCKET);
+  r = sort_buckets(ctx);
+  if (r) return r;
+  stage_end(ctx, ST_BUCKET);
+  r = finish_index(ctx, want_entries != 0);
+  if (r) return r;
+  if (count) *count = n;
+  return PGA_OK;
+}
+
+int pga_index_copy_records(pga_ctx *ctx, uint8_t *records) {
+  if (!ctx || !ctx->have_index || (!records && ctx->nrec > 0)) return PGA_ERR_ARG;
+  int64_t n = ctx->nrec;
+  ENSURE(ctx->io, (size_t)n * ctx->rsize + 16);
+  if (n > 0) {
+    k_records_out<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, ctx->posb,
+                                                         ctx->ctgb, P<uint8_t>(ctx->io));
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(records, ctx->io.p, (size_t)n * ctx->rsize, cudaMemcpyDeviceToHost, ctx->st));
+  }
+  CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t *largest) {
+  if (!ctx || !ctx->have_index || !ctx->have_entries) return PGA_ERR_ARG;
+  int eb = 9 + ctx->posb + ctx->ctgb;
+  if (entries && ctx->nrec > 0)
+    CK(cudaMemcpyAsync(entries, ctx->ent.p, (size_t)ctx->nrec * eb, cudaMemcpyDeviceToHost, ctx->st));
+  if (cum) CK(cudaMemcpyAsync(cum, ctx->cum.p, sizeof(int64_t) * NPREFIX, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (largest) *largest = ctx->largest;
+  return PGA_OK;
+}
+
+int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds) {
+  if (!ctx || !ctx->have_index || freq < 1) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = run_merge(ctx, freq);
+  if (r) return r;
+  if (nseeds) *nseeds = ctx->nseed[0];
+  if (cseeds) *cseeds = ctx->nseed[1];
+  return PGA_OK;
+}
+
+int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck) {
+  if (!ctx || !ctx->have_seeds || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
+  return copy_seeds(ctx, comp, seeds, buck);
+}
+
+int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count) {
+  if (!ctx || !ctx->have_seeds || !ctx->have_gdb || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int64_t maxdag = 2 * ctx->maxctg, cum = 1;
+  int dbyte = 0;
+  while (cum < maxdag) {
+    cum *= 256;
+    dbyte++;
+  }
+  if (dbyte > 4) return fail(ctx, PGA_ERR_LIMIT, "DBYTE %d > 4", dbyte);
+  if (dbyte < 1) dbyte = 1;
+  int r = run_diag(ctx, comp, ctx->ncontig, ctx->maxctg, dbyte, ctx->ctgb);
+  if (r) return r;
+  if (swide) *swide = 2 * dbyte + ctx->ctgb + 2;
+  if (count) *count = ctx->nseed[comp];
+  return PGA_OK;
+}
+
+int pga_diag_copy(pga_ctx *ctx, int comp, uint8_t *records, int64_t *panel_off) {
+  if (!ctx || (comp != 0 && comp != 1) || !ctx->have_diag[comp]) return PGA_ERR_ARG;
+  return copy_diag(ctx, comp, ctx->ncontig, records, panel_off);
+}
+
+}  // extern "C"

@@ -1,0 +1,395 @@
+// Index build on the GPU: closed-syncmer extraction from the 2-bit GDB,
+// bucketing by the 24-bit k-mer prefix, in-bucket sort, semantic LCPs, the
+// k-mer table entries and the 2^24 cumulative prefix table.
+//
+// Reference path replaced (one process, world size 1):
+//   extract_to_records     src/extract.c:85-358, src/pack.c:29-78
+//   run_stage2 sort + LCP  src/dsort.c:369-518, src/sort.c:38-115, lib/MSDsort.c:404-507
+//   build_kmer_adapter     src/kmer_adapter.c:6-96
+//
+// The MPI bucket exchange of run_stage2 becomes the first (24-bit prefix)
+// pass of an in-HBM MSD sort: a histogram of the prefixes, its exclusive
+// scan (which is also the k-mer table's cumulative prefix index), a scatter
+// of the records into their prefix buckets, and a per-bucket finishing sort.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "index.cuh"
+
+namespace pga {
+
+// The syncmer hash's 4-mer scramble table (src/tables.c:5-22); part of the
+// selection rule's definition, so the values are the reference's.
+__constant__ uint8_t c_tmap[256] = {
+  0xff,0xd4,0xf5,0xfd,0xe4,0xad,0x21,0xa5,0xed,0x64,0xbf,0xa9,0xf3,0x70,0xd6,0xf0,
+  0xca,0x89,0xcb,0xc9,0x82,0x9d,0x13,0x79,0x0a,0x0f,0x25,0x19,0x3e,0x47,0xa3,0xa8,
+  0xf9,0x5e,0xe8,0xa1,0xb0,0x71,0x1d,0x8c,0xde,0x69,0xe7,0x7c,0x56,0x3f,0x90,0xa4,
+  0xeb,0x45,0x59,0xf1,0x97,0x4c,0x08,0xa0,0xb8,0x4a,0x86,0xc8,0xcd,0x98,0x7d,0xfc,
+  0xef,0x4d,0x83,0x7e,0xdc,0x66,0x2b,0x8e,0xe0,0xa7,0xd0,0xa2,0x88,0x5f,0x7f,0xd9,
+  0x9b,0x78,0xd1,0x8b,0xc3,0x8f,0x2d,0xe6,0x18,0x27,0x2c,0x24,0x94,0xb7,0xce,0xbd,
+  0x0d,0x04,0x1c,0x09,0x16,0x23,0x00,0x1e,0x1a,0x29,0x2e,0x15,0x01,0x10,0x2a,0x20,
+  0xbe,0x31,0x43,0x58,0xc2,0xaa,0x1f,0xe5,0xc5,0x9e,0xcf,0xc6,0x68,0xb2,0x80,0xf4,
+  0xf8,0x53,0xb6,0x93,0x76,0x37,0x11,0x40,0xda,0x51,0xba,0x46,0x42,0x30,0x60,0x6d,
+  0x5c,0x39,0x9f,0x48,0x6c,0x62,0x28,0x67,0x06,0x12,0x26,0x0e,0x33,0x50,0xa6,0x63,
+  0xdd,0x3b,0xab,0x4b,0x72,0x5b,0x22,0x6f,0xb4,0x61,0x92,0x99,0x36,0x38,0x65,0xac,
+  0x4f,0x2f,0x32,0x44,0x54,0x3c,0x03,0x5d,0x73,0x3a,0x77,0x84,0x8d,0x4e,0x49,0xd2,
+  0xfb,0x91,0x6a,0xcc,0x8a,0x35,0x02,0x55,0x7a,0x34,0x96,0x3d,0xd3,0x41,0x85,0xf2,
+  0xb1,0x75,0xc4,0xb5,0xbb,0xb3,0x1b,0xd5,0x07,0x05,0x17,0x0b,0x7b,0xd7,0xdf,0xea,
+  0xe3,0x57,0xc0,0x95,0x9c,0x6e,0x14,0xae,0xb9,0x6b,0xc1,0x81,0x87,0x74,0xd8,0xe2,
+  0xec,0x52,0xbc,0xe9,0xe1,0xdb,0x0c,0xf7,0xaf,0x5a,0x9a,0xc7,0xfa,0xf6,0xee,0xfe };
+
+__host__ __device__ __forceinline__ uint32_t rc4(uint32_t x) {
+  uint32_t y = 0;
+  for (int i = 0; i < 4; i++) {
+    y = (y << 2) | (3u - (x & 3u));
+    x >>= 2;
+  }
+  return y;
+}
+
+// ---------------------------------------------------------------------------
+// Extraction.  One CTA = EXT_TILE consecutive syncmer offsets j of one contig;
+// each thread owns EXT_PER consecutive offsets and walks them with rolling
+// 80-bit forward and reverse-complement k-mer registers and a five-wide
+// window of canonical 8-mer hashes.  The selection is the closed (12,8)
+// syncmer rule: j is kept iff the first of the five 8-mer hashes of the
+// 12-mer at j is a minimum or the last one is (src/extract.c:168-196).
+// ---------------------------------------------------------------------------
+
+struct K80 {
+  uint64_t hi;  // bases 0..31, base 0 in bits 63..62
+  uint32_t lo;  // bases 32..39 in bits 15..0
+};
+
+__device__ __forceinline__ void k80_push_back(K80 &k, uint32_t b) {  // forward: shift left
+  k.hi = (k.hi << 2) | (k.lo >> 14);
+  k.lo = ((k.lo << 2) | b) & 0xffffu;
+}
+__device__ __forceinline__ void k80_push_front(K80 &k, uint32_t b) {  // reverse complement
+  k.lo = (k.lo >> 2) | ((uint32_t)(k.hi & 3u) << 14);
+  k.hi = (k.hi >> 2) | ((uint64_t)b << 62);
+}
+
+__device__ __forceinline__ uint32_t hash8(uint32_t qa, uint32_t qb, const uint8_t *tm,
+                                          const uint8_t *tmrc) {
+  uint32_t f = ((uint32_t)tm[qa] << 8) | tm[qb];
+  uint32_t r = ((uint32_t)tmrc[qb] << 8) | tmrc[qa];
+  return f < r ? f : r;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(EXT_THREADS)
+k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
+          const int64_t *__restrict__ boff, const int32_t *__restrict__ tile_ctg,
+          const int64_t *__restrict__ tile_j0, int ctgb, uint32_t *__restrict__ counts,
+          const uint64_t *__restrict__ offsets, Rec *__restrict__ out,
+          uint32_t *__restrict__ hist, uint32_t *__restrict__ cursor) {
+  __shared__ uint8_t s[EXT_SPAN];
+  __shared__ uint8_t tm[256], tmrc[256];
+  const int tid = threadIdx.x;
+  const int ctg = tile_ctg[blockIdx.x];
+  const int64_t j0 = tile_j0[blockIdx.x];
+  const int64_t len = clen[ctg];
+  const uint8_t *cb = bps + boff[ctg];
+  const int64_t xs = j0 - EXT_LEFT;  // contig position of s[0]; a multiple of 4
+
+  tm[tid] = c_tmap[tid];
+  tmrc[tid] = c_tmap[rc4(tid)];
+  for (int k = tid; k < EXT_SPAN / 4; k += EXT_THREADS) {
+    int64_t x = xs + 4 * (int64_t)k;
+    uint32_t b = (x >= 0 && x < len) ? cb[x >> 2] : 0u;
+#pragma unroll
+    for (int q = 0; q < 4; q++) s[4 * k + q] = (x + q >= 0 && x + q < len) ? ((b >> (2 * q)) & 3u) : 0;
+  }
+  __syncthreads();
+
+  const int64_t jlast = len - TMER;  // last 12-mer offset
+  const int64_t ja = j0 + (int64_t)tid * EXT_PER;
+  const int64_t jb = min(ja + EXT_PER, jlast + 1);
+  uint32_t nrec = 0;
+  uint64_t woff = 0;
+  if (MODE == EXT_WRITE) woff = offsets[(int64_t)blockIdx.x * EXT_THREADS + tid];
+  const uint64_t strand_bit = (uint64_t)1 << (8 * ctgb - 1);
+
+  if (ja < jb) {
+    const uint8_t *p = s + (ja - xs);  // p[i] = base ja + i
+    K80 fw = {0, 0}, rc = {0, 0};
+    for (int i = 0; i < 40; i++) k80_push_back(fw, p[i]);
+    for (int i = -28; i < 12; i++) k80_push_front(rc, 3u - p[i]);
+    uint32_t h0, h1, h2, h3;
+    {
+      uint32_t q[12];
+      for (int i = 0; i < 11; i++) q[i] = (p[i] << 6) | (p[i + 1] << 4) | (p[i + 2] << 2) | p[i + 3];
+      h0 = hash8(q[0], q[4], tm, tmrc);
+      h1 = hash8(q[1], q[5], tm, tmrc);
+      h2 = hash8(q[2], q[6], tm, tmrc);
+      h3 = hash8(q[3], q[7], tm, tmrc);
+    }
+    for (int64_t j = ja; j < jb; j++) {
+      uint32_t h4 = hash8((uint32_t)(fw.hi >> 48) & 0xffu, (uint32_t)(fw.hi >> 40) & 0xffu, tm, tmrc);
+      uint32_t m03 = min(min(h0, h1), min(h2, h3));
+      uint32_t m14 = min(min(h1, h2), min(h3, h4));
+      if (h0 <= m14 || h4 <= m03) {
+#pragma unroll
+        for (int strand = 0; strand < 2; strand++) {
+          bool ok = strand == 0 ? (j <= len - KMER) : (j >= KMER - TMER);
+          if (!ok) continue;
+          const K80 &k = strand == 0 ? fw : rc;
+          uint64_t pos = strand == 0 ? (uint64_t)j : (uint64_t)(j + TMER);
+          uint64_t cs = (uint64_t)ctg | (strand ? strand_bit : 0);
+          if (MODE == EXT_COUNT) {
+            nrec++;
+          } else {
+            Rec r;
+            r.hi = k.hi;
+            r.lo = ((uint64_t)k.lo << 48) | (cs << 32) | pos;
+            if (MODE == EXT_WRITE) {
+              out[woff++] = r;
+            } else if (MODE == EXT_HIST) {
+              atomicAdd(&hist[rec_prefix(r)], 1u);
+            } else {  // EXT_SCATTER
+              uint32_t slot = atomicAdd(&cursor[rec_prefix(r)], 1u);
+              out[slot] = r;
+            }
+          }
+        }
+      }
+      h0 = h1; h1 = h2; h2 = h3; h3 = h4;
+      k80_push_back(fw, p[j - ja + 40]);
+      k80_push_front(rc, 3u - p[j - ja + 12]);
+    }
+  }
+  if (MODE == EXT_COUNT) counts[(int64_t)blockIdx.x * EXT_THREADS + tid] = nrec;
+}
+
+template __global__ void k_extract<EXT_COUNT>(const uint8_t *, const int64_t *, const int64_t *,
+                                              const int32_t *, const int64_t *, int, uint32_t *,
+                                              const uint64_t *, Rec *, uint32_t *, uint32_t *);
+template __global__ void k_extract<EXT_WRITE>(const uint8_t *, const int64_t *, const int64_t *,
+                                              const int32_t *, const int64_t *, int, uint32_t *,
+                                              const uint64_t *, Rec *, uint32_t *, uint32_t *);
+template __global__ void k_extract<EXT_HIST>(const uint8_t *, const int64_t *, const int64_t *,
+                                             const int32_t *, const int64_t *, int, uint32_t *,
+                                             const uint64_t *, Rec *, uint32_t *, uint32_t *);
+template __global__ void k_extract<EXT_SCATTER>(const uint8_t *, const int64_t *, const int64_t *,
+                                                const int32_t *, const int64_t *, int, uint32_t *,
+                                                const uint64_t *, Rec *, uint32_t *, uint32_t *);
+
+// ---------------------------------------------------------------------------
+// Prefix histogram of records already in HBM (used when records come from
+// the host instead of from extraction), and the scatter into buckets.
+// ---------------------------------------------------------------------------
+
+__global__ void k_prefix_hist(const Rec *__restrict__ rec, int64_t n, uint32_t *__restrict__ hist) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&hist[rec_prefix(rec[i])], 1u);
+}
+
+__global__ void k_prefix_scatter(const Rec *__restrict__ in, int64_t n, uint32_t *__restrict__ cursor,
+                                 Rec *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Rec r = in[i];
+    uint32_t slot = atomicAdd(&cursor[rec_prefix(r)], 1u);
+    out[slot] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Finishing sort of each prefix bucket, by (k-mer, contig|strand, position).
+// Buckets of up to BK_SMALL records are sorted by one thread each; larger
+// ones are queued and sorted by one CTA in shared memory (up to BK_MEDIUM)
+// or by a batched global-memory bitonic network.
+// ---------------------------------------------------------------------------
+
+__global__ void k_bucket_small(Rec *__restrict__ rec, const uint32_t *__restrict__ start,
+                               uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig,
+                               uint32_t *__restrict__ qcount) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= NPREFIX) return;
+  uint32_t a = start[p], b = start[p + 1];
+  uint32_t n = b - a;
+  if (n <= 1) return;
+  if (n > BK_SMALL) {
+    if (n <= BK_MEDIUM) qmed[atomicAdd(&qcount[0], 1u)] = p;
+    else {
+      uint32_t q = atomicAdd(&qcount[1], 1u);
+      qbig[q] = p;
+      atomicMax(&qcount[2], n);
+    }
+    return;
+  }
+  Rec v[BK_SMALL];
+  for (uint32_t i = 0; i < n; i++) v[i] = rec[a + i];
+  for (uint32_t i = 1; i < n; i++) {
+    Rec x = v[i];
+    int k = (int)i - 1;
+    while (k >= 0 && rec_less(x, v[k])) {
+      v[k + 1] = v[k];
+      k--;
+    }
+    v[k + 1] = x;
+  }
+  for (uint32_t i = 0; i < n; i++) rec[a + i] = v[i];
+}
+
+__device__ __forceinline__ void cswap(Rec &x, Rec &y) {
+  if (rec_less(y, x)) {
+    Rec t = x;
+    x = y;
+    y = t;
+  }
+}
+
+// Bitonic sort variant whose every compare is ascending (the first step of
+// each merge mirrors within the block), so a length that is not a power of
+// two behaves as if padded with +infinity.
+__global__ void __launch_bounds__(BK_THREADS)
+k_bucket_medium(Rec *__restrict__ rec, const uint32_t *__restrict__ start,
+                const uint32_t *__restrict__ qmed) {
+  __shared__ Rec v[BK_MEDIUM];
+  uint32_t p = qmed[blockIdx.x];
+  uint32_t a = start[p];
+  uint32_t n = start[p + 1] - a;
+  for (uint32_t i = threadIdx.x; i < n; i += BK_THREADS) v[i] = rec[a + i];
+  uint32_t np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  __syncthreads();
+  for (uint32_t k = 2; k <= np2; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t t = threadIdx.x; t < np2 / 2; t += BK_THREADS) {
+        uint32_t i, q;
+        if (j == (k >> 1)) {  // mirrored compare inside the k-block
+          uint32_t blk = (t / j) * k, off = t % j;
+          i = blk + off;
+          q = blk + k - 1 - off;
+        } else {
+          i = (t / j) * 2 * j + (t % j);
+          q = i + j;
+        }
+        if (q < n) cswap(v[i], v[q]);
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < n; i += BK_THREADS) rec[a + i] = v[i];
+}
+
+// One compare step of the same network over every queued big bucket
+// (grid.y = queue slot).
+__global__ void k_bucket_big_step(Rec *__restrict__ rec, const uint32_t *__restrict__ start,
+                                  const uint32_t *__restrict__ qbig, uint32_t k, uint32_t j) {
+  uint32_t p = qbig[blockIdx.y];
+  uint32_t a = start[p];
+  uint32_t n = start[p + 1] - a;
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i, q;
+  if (j == (k >> 1)) {
+    uint64_t blk = (t / (k >> 1)) * k;
+    uint32_t off = (uint32_t)(t % (k >> 1));
+    i = (uint32_t)(blk + off);
+    q = (uint32_t)(blk + (k - 1 - off));
+  } else {
+    i = (uint32_t)((t / j) * 2 * j + (t % j));
+    q = i + j;
+  }
+  if (q < n) {
+    Rec x = rec[a + i], y = rec[a + q];
+    if (rec_less(y, x)) {
+      rec[a + i] = y;
+      rec[a + q] = x;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// LCPs, k-mer table entries, reference-format sorted records, prefix table.
+// ---------------------------------------------------------------------------
+
+__global__ void k_lcp(const Rec *__restrict__ rec, int64_t n, uint8_t *__restrict__ lcp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    lcp[i] = (uint8_t)(i == 0 ? 0 : kmer_lcp(rec[i - 1], rec[i]));
+}
+
+// Entry layout (src/kmer_adapter.c:60-65): k-mer bytes 3..9, mask 0, LCP,
+// position (posb bytes LE), contig|strand (ctgb bytes LE).
+__global__ void k_entries(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
+                          int posb, int ctgb, uint8_t *__restrict__ ent) {
+  const int eb = 9 + posb + ctgb;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Rec r = rec[i];
+    uint8_t *d = ent + i * eb;
+    // k-mer byte b (0..9): b < 8 from hi, else from the top of lo
+#pragma unroll
+    for (int b = 3; b < 8; b++) d[b - 3] = (uint8_t)(r.hi >> (56 - 8 * b));
+    d[5] = (uint8_t)(r.lo >> 56);
+    d[6] = (uint8_t)(r.lo >> 48);
+    d[7] = 0;
+    d[8] = lcp[i];
+    uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
+    for (int b = 0; b < posb; b++) d[9 + b] = (uint8_t)(pos >> (8 * b));
+    for (int b = 0; b < ctgb; b++) d[9 + posb + b] = (uint8_t)(cs >> (8 * b));
+  }
+}
+
+// Record layout (src/record.h:8-26): LCP, k-mer 10 bytes, mask 0, position,
+// contig|strand.  lcp may be null (extraction order: LCP byte 0).
+__global__ void k_records_out(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
+                              int posb, int ctgb, uint8_t *__restrict__ out) {
+  const int rs = 12 + posb + ctgb;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Rec r = rec[i];
+    uint8_t *d = out + i * rs;
+    d[0] = lcp ? lcp[i] : 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) d[1 + b] = (uint8_t)(r.hi >> (56 - 8 * b));
+    d[9] = (uint8_t)(r.lo >> 56);
+    d[10] = (uint8_t)(r.lo >> 48);
+    d[11] = 0;
+    uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
+    for (int b = 0; b < posb; b++) d[12 + b] = (uint8_t)(pos >> (8 * b));
+    for (int b = 0; b < ctgb; b++) d[12 + posb + b] = (uint8_t)(cs >> (8 * b));
+  }
+}
+
+// Host-format records (rs bytes) -> Rec (and their LCP bytes when lcp != null).
+__global__ void k_records_in(const uint8_t *__restrict__ in, int64_t n, int posb, int ctgb,
+                             Rec *__restrict__ rec, uint8_t *__restrict__ lcp) {
+  const int rs = 12 + posb + ctgb;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t *s = in + i * rs;
+    uint64_t hi = 0, pos = 0, cs = 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) hi = (hi << 8) | s[1 + b];
+    uint64_t lo16 = ((uint64_t)s[9] << 8) | s[10];
+    for (int b = 0; b < posb; b++) pos |= (uint64_t)s[12 + b] << (8 * b);
+    for (int b = 0; b < ctgb; b++) cs |= (uint64_t)s[12 + posb + b] << (8 * b);
+    Rec r;
+    r.hi = hi;
+    r.lo = (lo16 << 48) | (cs << 32) | pos;
+    rec[i] = r;
+    if (lcp) lcp[i] = s[0];
+  }
+}
+
+// cum[p] = number of records with prefix <= p = start[p+1]; also the largest
+// bucket (the longest prefix group, which sizes FastGA's merge cache).
+__global__ void k_prefix_table(const uint32_t *__restrict__ start, int64_t *__restrict__ cum,
+                               uint32_t *__restrict__ maxrun) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t best = 0;
+  if (p < NPREFIX) {
+    uint32_t e = start[p + 1];
+    if (cum) cum[p] = (int64_t)e;
+    best = e - start[p];
+  }
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0 && best) atomicMax(maxrun, best);
+}
+
+}  // namespace pga

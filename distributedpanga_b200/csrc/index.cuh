@@ -1,0 +1,38 @@
+// Index-build kernels (index.cu) and their launch constants.
+#pragma once
+#include <cstdint>
+#include "common.cuh"
+
+namespace pga {
+
+enum { EXT_COUNT = 0, EXT_WRITE = 1, EXT_HIST = 2, EXT_SCATTER = 3 };
+
+constexpr int EXT_THREADS = 256;                   // threads per extraction CTA
+constexpr int EXT_PER = 32;                        // syncmer offsets per thread
+constexpr int EXT_TILE = EXT_THREADS * EXT_PER;    // offsets per CTA (multiple of 4)
+constexpr int EXT_LEFT = 32;                       // bases staged before the tile (>= 28, multiple of 4)
+constexpr int EXT_SPAN = EXT_TILE + 80;            // staged bases (>= EXT_LEFT + EXT_TILE + 40 + 4)
+
+constexpr int BK_SMALL = 32;      // bucket sizes sorted by one thread
+constexpr int BK_MEDIUM = 2048;   // bucket sizes sorted by one CTA in shared memory
+constexpr int BK_THREADS = 256;
+
+template <int MODE>
+__global__ void k_extract(const uint8_t *bps, const int64_t *clen, const int64_t *boff,
+                          const int32_t *tile_ctg, const int64_t *tile_j0, int ctgb, uint32_t *counts,
+                          const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor);
+__global__ void k_prefix_hist(const Rec *rec, int64_t n, uint32_t *hist);
+__global__ void k_prefix_scatter(const Rec *in, int64_t n, uint32_t *cursor, Rec *out);
+__global__ void k_bucket_small(Rec *rec, const uint32_t *start, uint32_t *qmed, uint32_t *qbig,
+                               uint32_t *qcount);
+__global__ void k_bucket_medium(Rec *rec, const uint32_t *start, const uint32_t *qmed);
+__global__ void k_bucket_big_step(Rec *rec, const uint32_t *start, const uint32_t *qbig, uint32_t k,
+                                  uint32_t j);
+__global__ void k_lcp(const Rec *rec, int64_t n, uint8_t *lcp);
+__global__ void k_entries(const Rec *rec, const uint8_t *lcp, int64_t n, int posb, int ctgb, uint8_t *ent);
+__global__ void k_records_out(const Rec *rec, const uint8_t *lcp, int64_t n, int posb, int ctgb,
+                              uint8_t *out);
+__global__ void k_records_in(const uint8_t *in, int64_t n, int posb, int ctgb, Rec *rec, uint8_t *lcp);
+__global__ void k_prefix_table(const uint32_t *start, int64_t *cum, uint32_t *maxrun);
+
+}  // namespace pga

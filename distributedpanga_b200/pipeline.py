@@ -1,0 +1,267 @@
+"""Host-side mirror of the reference's stage interfaces over the C ABI.
+
+Function names follow the reference's entry points for this path and take
+and return its byte formats, as numpy arrays:
+
+  extract_to_records     src/extract.h:40
+  sort_records           src/sort.h:10  (with recalc_all_lcps: run_stage2 at world size 1)
+  build_kmer_adapter     src/kmer_adapter.h:46
+  self_adaptamer_merge   src/fastga_pipeline.h:18
+  reimport_sort          reimport_thread + rmsd_sort, src/fastga_pipeline.c:1391, lib/RSDsort.c:292
+
+``Device`` additionally keeps a GDB resident in HBM and runs the stages
+without host round trips (``index_build`` -> ``merge`` -> ``diag_sort``).
+
+There is no CPU fallback: every call goes to libpga_b200.so on a CUDA device,
+and loading fails loudly when the library or the GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import gdb as _gdb
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpga_b200.so")
+
+PGA_OK = 0
+_ERRNAMES = {1: "CUDA error", 2: "bad argument", 3: "out of memory", 4: "beyond limits"}
+
+i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+vp = C.c_void_p
+
+_SIGS = {
+    "pga_ctx_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+    "pga_ctx_destroy": (None, [vp]),
+    "pga_last_error": (C.c_char_p, [vp]),
+    "pga_ctx_set_stream": (C.c_int, [vp, vp]),
+    "pga_ctx_synchronize": (C.c_int, [vp]),
+    "pga_kernel_launches": (C.c_int64, [vp]),
+    "pga_ctx_enable_timing": (C.c_int, [vp, C.c_int]),
+    "pga_stage_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "pga_gdb_load": (C.c_int, [vp, u8p, C.c_int64, C.c_int, i64p, i64p]),
+    "pga_record_sizing": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pga_extract_to_records": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_uint8)),
+                                         C.POINTER(C.c_int64)]),
+    "pga_sort_records": (C.c_int, [vp, vp, C.c_int64, C.c_int, C.c_int]),
+    "pga_build_kmer_adapter": (C.c_int, [vp, vp, C.c_int64, C.c_int, C.c_int, vp, i64p,
+                                         C.POINTER(C.c_int64)]),
+    "pga_self_adaptamer_merge": (C.c_int, [vp, vp, i64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_int64),
+                                           C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_int64),
+                                           i64p, i64p]),
+    "pga_reimport_sort": (C.c_int, [vp, vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
+                                    C.c_int, vp, i64p]),
+    "pga_index_build": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int64)]),
+    "pga_index_copy_records": (C.c_int, [vp, vp]),
+    "pga_index_copy_entries": (C.c_int, [vp, vp, vp, C.POINTER(C.c_int64)]),
+    "pga_merge": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "pga_seeds_copy": (C.c_int, [vp, C.c_int, vp, vp]),
+    "pga_diag_sort": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+    "pga_diag_copy": (C.c_int, [vp, C.c_int, vp, vp]),
+}
+
+_LIB = None
+
+
+def load_library():
+    """The C-ABI library; raises if it is not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libpga_b200.so is not built (run distributedpanga_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        L.free_ptr = C.CDLL(None).free
+        L.free_ptr.argtypes = [vp]
+        L.free_ptr.restype = None
+        _LIB = L
+    return _LIB
+
+
+class PgaError(RuntimeError):
+    pass
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(vp) if a.size else None
+
+
+def _take(L, p, nbytes: int) -> np.ndarray:
+    """Copy a malloc'd C buffer into numpy and free it."""
+    out = np.empty(nbytes, dtype=np.uint8)
+    if nbytes:
+        C.memmove(out.ctypes.data, p, nbytes)
+    if p:
+        L.free_ptr(C.cast(p, vp))
+    return out
+
+
+class Device:
+    """One pga_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        h = vp()
+        rc = self.L.pga_ctx_create(device, C.byref(h))
+        if rc != PGA_OK:
+            raise PgaError("pga_ctx_create(%d) failed: %s" % (device, _ERRNAMES.get(rc, rc)))
+        self.h = h
+        self.cs = None
+
+    def close(self):
+        if self.h:
+            self.L.pga_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int, what: str):
+        if rc != PGA_OK:
+            msg = self.L.pga_last_error(self.h)
+            raise PgaError("%s: %s: %s" % (what, _ERRNAMES.get(rc, rc), msg.decode() if msg else ""))
+
+    # ---- plumbing --------------------------------------------------------
+    def set_stream(self, stream_handle: int | None):
+        self._ck(self.L.pga_ctx_set_stream(self.h, stream_handle or None), "set_stream")
+
+    def synchronize(self):
+        self._ck(self.L.pga_ctx_synchronize(self.h), "synchronize")
+
+    def launches(self) -> int:
+        return int(self.L.pga_kernel_launches(self.h))
+
+    def enable_timing(self, on: bool = True):
+        self._ck(self.L.pga_ctx_enable_timing(self.h, 1 if on else 0), "enable_timing")
+
+    def stage_times(self) -> dict:
+        a = (C.c_float * 8)()
+        self._ck(self.L.pga_stage_times(self.h, a), "stage_times")
+        names = ["extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
+                 "entries_prefix_table", "merge", "diag_sort"]
+        return dict(zip(names, [float(x) for x in a]))
+
+    # ---- GDB -------------------------------------------------------------
+    def gdb_load(self, cs: _gdb.ContigSet):
+        bps = np.ascontiguousarray(cs.bps, dtype=np.uint8)
+        if bps.size == 0:
+            bps = np.zeros(1, dtype=np.uint8)
+        self._ck(self.L.pga_gdb_load(self.h, bps, int(cs.bps.size), cs.ncontig,
+                                     np.ascontiguousarray(cs.clen, dtype=np.int64),
+                                     np.ascontiguousarray(cs.boff, dtype=np.int64)), "gdb_load")
+        self.cs = cs
+
+    def record_sizing(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._ck(self.L.pga_record_sizing(self.h, C.byref(a), C.byref(b), C.byref(c)), "record_sizing")
+        return a.value, b.value, c.value
+
+    # ---- drop-in stages ----------------------------------------------------
+    def extract_to_records(self, num_workers: int = 1, worker_id: int = 0) -> np.ndarray:
+        p = C.POINTER(C.c_uint8)()
+        n = C.c_int64()
+        self._ck(self.L.pga_extract_to_records(self.h, num_workers, worker_id, C.byref(p), C.byref(n)),
+                 "extract_to_records")
+        rs = self.record_sizing()[2]
+        return _take(self.L, p, n.value * rs).reshape(n.value, rs)
+
+    def sort_records(self, rec: np.ndarray, posb: int, ctgb: int) -> np.ndarray:
+        out = np.ascontiguousarray(rec, dtype=np.uint8).copy()
+        self._ck(self.L.pga_sort_records(self.h, _ptr(out), out.shape[0], posb, ctgb), "sort_records")
+        return out
+
+    def build_kmer_adapter(self, rec: np.ndarray, posb: int, ctgb: int):
+        rec = np.ascontiguousarray(rec, dtype=np.uint8)
+        n = rec.shape[0]
+        eb = 9 + posb + ctgb
+        ent = np.zeros((n, eb), dtype=np.uint8)
+        cum = np.zeros(1 << 24, dtype=np.int64)
+        big = C.c_int64()
+        self._ck(self.L.pga_build_kmer_adapter(self.h, _ptr(rec), n, posb, ctgb, _ptr(ent), cum,
+                                               C.byref(big)), "build_kmer_adapter")
+        return ent, cum, big.value
+
+    def self_adaptamer_merge(self, ent: np.ndarray, cum: np.ndarray, posb: int, ctgb: int,
+                             freq: int, ncontig: int):
+        ent = np.ascontiguousarray(ent, dtype=np.uint8)
+        pn, pc = C.POINTER(C.c_uint8)(), C.POINTER(C.c_uint8)()
+        nl, cl = C.c_int64(), C.c_int64()
+        nb = np.zeros(ncontig, dtype=np.int64)
+        cb = np.zeros(ncontig, dtype=np.int64)
+        self._ck(self.L.pga_self_adaptamer_merge(self.h, _ptr(ent), np.ascontiguousarray(cum, dtype=np.int64),
+                                                 ent.shape[0], posb, ctgb, freq, ncontig, C.byref(pn),
+                                                 C.byref(nl), C.byref(pc), C.byref(cl), nb, cb),
+                 "self_adaptamer_merge")
+        sb = 1 + 2 * (posb + ctgb)
+        ns = _take(self.L, pn, nl.value).reshape(-1, sb)
+        css = _take(self.L, pc, cl.value).reshape(-1, sb)
+        return ns, css, nb, cb
+
+    def reimport_sort(self, seeds: np.ndarray, posb: int, ctgb: int, comp: int, ncontig: int,
+                      amxpos: int, dbyte: int):
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint8)
+        swide = 2 * dbyte + ctgb + 2
+        ns = seeds.shape[0]
+        out = np.zeros((ns, swide), dtype=np.uint8)
+        off = np.zeros(ncontig + 1, dtype=np.int64)
+        self._ck(self.L.pga_reimport_sort(self.h, _ptr(seeds), seeds.size, posb, ctgb, comp, ncontig, amxpos,
+                                          dbyte, _ptr(out), off), "reimport_sort")
+        return out, off
+
+    # ---- resident pipeline ---------------------------------------------------
+    def index_build(self, want_entries: bool = True) -> int:
+        n = C.c_int64()
+        self._ck(self.L.pga_index_build(self.h, 1 if want_entries else 0, C.byref(n)), "index_build")
+        self.nrec = n.value
+        return n.value
+
+    def index_records(self) -> np.ndarray:
+        rs = self.record_sizing()[2]
+        out = np.zeros((self.nrec, rs), dtype=np.uint8)
+        self._ck(self.L.pga_index_copy_records(self.h, _ptr(out)), "index_copy_records")
+        return out
+
+    def index_entries(self):
+        posb, ctgb, _ = self.record_sizing()
+        ent = np.zeros((self.nrec, 9 + posb + ctgb), dtype=np.uint8)
+        cum = np.zeros(1 << 24, dtype=np.int64)
+        big = C.c_int64()
+        self._ck(self.L.pga_index_copy_entries(self.h, _ptr(ent), cum.ctypes.data_as(vp), C.byref(big)),
+                 "index_copy_entries")
+        return ent, cum, big.value
+
+    def merge(self, freq: int = 10):
+        a, b = C.c_int64(), C.c_int64()
+        self._ck(self.L.pga_merge(self.h, freq, C.byref(a), C.byref(b)), "merge")
+        self.nseeds = (a.value, b.value)
+        return a.value, b.value
+
+    def seeds(self, comp: int):
+        posb, ctgb, _ = self.record_sizing()
+        sb = 1 + 2 * (posb + ctgb)
+        out = np.zeros((self.nseeds[comp], sb), dtype=np.uint8)
+        buck = np.zeros(self.cs.ncontig, dtype=np.int64)
+        self._ck(self.L.pga_seeds_copy(self.h, comp, _ptr(out), buck.ctypes.data_as(vp)), "seeds_copy")
+        return out, buck
+
+    def diag_sort(self, comp: int):
+        sw, n = C.c_int(), C.c_int64()
+        self._ck(self.L.pga_diag_sort(self.h, comp, C.byref(sw), C.byref(n)), "diag_sort")
+        return sw.value, n.value
+
+    def diag_records(self, comp: int, swide: int, count: int):
+        out = np.zeros((count, swide), dtype=np.uint8)
+        off = np.zeros(self.cs.ncontig + 1, dtype=np.int64)
+        self._ck(self.L.pga_diag_copy(self.h, comp, _ptr(out), off.ctypes.data_as(vp)), "diag_copy")
+        return out, off

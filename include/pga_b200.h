@@ -1,0 +1,132 @@
+/* pga_b200 -- B200 (sm_100a) implementation of DistributedPanGA's FastGA
+ * alignment path, behind a plain C ABI.
+ *
+ * Two kinds of entry points:
+ *
+ *  1. Drop-in stages.  Each takes and returns host buffers in the reference's
+ *     own byte formats and replaces one reference function at world size 1
+ *     (the function is named beside it).  Buffers the reference allocates
+ *     with malloc are allocated here with malloc too; free them with free().
+ *
+ *  2. The resident pipeline.  pga_gdb_load puts a GDB's 2-bit sequence and
+ *     contig table in HBM; pga_index_build, pga_merge and pga_diag_sort then
+ *     run extraction -> index sort -> LCPs -> k-mer table -> adaptamer merge ->
+ *     seed reimport -> diagonal sort without leaving the device; the
+ *     pga_*_copy functions read any stage's result back in the reference's
+ *     format.
+ *
+ * Every function returns PGA_OK or an error code; pga_last_error() gives
+ * the message.  A context is not thread-safe; use one per host thread.
+ * Limits: contigs < 32768 (contig|strand fits 2 bytes), contig length
+ * < 2^31, fewer than 2^32 - 1 k-mer records and seeds per unit.
+ */
+#ifndef PGA_B200_H
+#define PGA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGA_OK            0
+#define PGA_ERR_CUDA      1   /* a CUDA call failed (message has the CUDA error) */
+#define PGA_ERR_ARG       2   /* bad argument or call order */
+#define PGA_ERR_NOMEM     3   /* device or host allocation failed */
+#define PGA_ERR_LIMIT     4   /* input beyond the limits above */
+
+typedef struct pga_ctx pga_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+
+int         pga_ctx_create(int device, pga_ctx **out);
+void        pga_ctx_destroy(pga_ctx *ctx);
+const char *pga_last_error(const pga_ctx *ctx);
+/* Run the context's work on an existing cudaStream_t (NULL: the context's
+ * own stream).  Lets a caller bracket the kernels with its own events. */
+int         pga_ctx_set_stream(pga_ctx *ctx, void *stream);
+int         pga_ctx_synchronize(pga_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+int64_t     pga_kernel_launches(const pga_ctx *ctx);
+/* Per-stage device times (ms) of the last pipeline calls when timing is on:
+ * [0] extract+histogram [1] prefix scan [2] extract+scatter [3] bucket sort
+ * [4] LCP [5] k-mer entries+prefix table [6] merge [7] diagonal sort. */
+int         pga_ctx_enable_timing(pga_ctx *ctx, int on);
+int         pga_stage_times(const pga_ctx *ctx, float *ms8);
+
+/* ---- GDB ------------------------------------------------------------------ */
+
+/* Replaces reading the GDB's sequence for extraction (Read_GDB
+ * lib/GDB.c:1171 + Get_Contig_Piece lib/GDB.c:1831): `bps` is the .bps image
+ * (2-bit, base i of contig r at byte boff[r] + i/4, bits 2*(i%4)), clen/boff
+ * the contig table (GDB_CONTIG, lib/GDB.h:29-35).  boff < 0 marks a contig
+ * without sequence (skipped, as src/extract.c:101). */
+int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int ncontig,
+                 const int64_t *clen, const int64_t *boff);
+
+/* Record sizing of the loaded GDB (compute_record_sizing, src/record.c:18). */
+int pga_record_sizing(const pga_ctx *ctx, int *position_bytes, int *contig_strand_bytes,
+                      int *record_size);
+
+/* ---- drop-in stages ------------------------------------------------------- */
+
+/* extract_to_records (src/extract.h:40, src/extract.c:358): the records of
+ * worker `worker_id` of `num_workers` (contig split of src/work_split.c:3),
+ * in the reference's emission order, LCP byte 0.  *records is malloc'd with
+ * one spare byte (msd_sort's sentinel, src/extract.c:268). */
+int pga_extract_to_records(pga_ctx *ctx, int num_workers, int worker_id, uint8_t **records,
+                           int64_t *count);
+
+/* sort_records + recalc_all_lcps (src/sort.h:10-13), i.e. run_stage2 at world
+ * size 1 (src/dsort.h:82): sorts `count` records of `record_size` bytes in
+ * place by k-mer -- equal k-mers by payload -- and sets byte 0 to the bases
+ * in common with the predecessor. */
+int pga_sort_records(pga_ctx *ctx, uint8_t *records, int64_t count, int position_bytes,
+                     int contig_strand_bytes);
+
+/* build_kmer_adapter (src/kmer_adapter.h:46): entries (count x
+ * (9 + position_bytes + contig_strand_bytes) bytes), the 2^24 cumulative
+ * prefix counts and the largest prefix group, from sorted records. */
+int pga_build_kmer_adapter(pga_ctx *ctx, const uint8_t *records, int64_t count, int position_bytes,
+                           int contig_strand_bytes, uint8_t *entries, int64_t *cum,
+                           int64_t *largest_group);
+
+/* self_adaptamer_merge (src/fastga_pipeline.h:18) with one routing unit:
+ * the N (same strand) and C seed byte streams (1 + 2*(posb+ctgb) bytes per
+ * seed, malloc'd) and seeds per A contig (nbuck, cbuck: ncontig each). */
+int pga_self_adaptamer_merge(pga_ctx *ctx, const uint8_t *entries, const int64_t *cum, int64_t count,
+                             int position_bytes, int contig_strand_bytes, int freq, int ncontig,
+                             uint8_t **nseeds, int64_t *nlen, uint8_t **cseeds, int64_t *clen,
+                             int64_t *nbuck, int64_t *cbuck);
+
+/* reimport_thread + rmsd_sort (src/fastga_pipeline.c:1391-1450,
+ * lib/RSDsort.c:292): `len` bytes of seeds -> swide-byte records, panel by A
+ * contig, each panel sorted; panel_off (ncontig+1) gets record offsets.
+ * comp = 0 for N seeds, 1 for C.  out needs (len/seed_bytes) * swide bytes,
+ * swide = 2*dbyte + contig_strand_bytes + 2. */
+int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int position_bytes,
+                      int contig_strand_bytes, int comp, int ncontig, int64_t amxpos, int dbyte,
+                      uint8_t *out, int64_t *panel_off);
+
+/* ---- resident pipeline ---------------------------------------------------- */
+
+/* Extract + sort + LCP + k-mer table of the loaded GDB; want_entries = 0
+ * skips writing the reference-format entries (the merge reads the device
+ * records directly).  *count receives the record count. */
+int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count);
+int pga_index_copy_records(pga_ctx *ctx, uint8_t *records);           /* count x record_size */
+int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t *largest_group);
+
+/* Adaptamer merge of the built index: seeds stay in HBM. */
+int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds);
+int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck);
+
+/* Reimport + diagonal sort of unit comp (0 = N, 1 = C) in HBM. */
+int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count);
+int pga_diag_copy(pga_ctx *ctx, int comp, uint8_t *records, int64_t *panel_off);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,45 @@
+"""Shared fixtures.  Tests marked ``gpu`` need a CUDA device and call the
+product through its C ABI; everything else runs on the CPU."""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, ROOT)
+
+GOLDEN_CASES = ["small_s002", "chromset_s0005", "edge_mix", "many_contigs"]
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU; calls the product through its C ABI")
+
+
+def load_case(name: str):
+    from distributedpanga_b200 import gdb
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    cs = gdb.ContigSet(bps=z["bps"], clen=z["clen"], boff=z["boff"], freq=z["freq"])
+    with open(os.path.join(GOLDEN, name + ".json")) as f:
+        dig = json.load(f)
+    return cs, dig
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import binding
+    binding.build()
+    return binding
+
+
+@pytest.fixture(scope="session")
+def dev():
+    from distributedpanga_b200 import build, pipeline
+    build.build()
+    d = pipeline.Device(0)
+    yield d
+    d.close()

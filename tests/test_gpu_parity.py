@@ -1,0 +1,133 @@
+"""GPU parity: every stage of the CUDA path through the C ABI, against the
+oracle (bit-exact, same order) and the golden digests of the reference."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_case
+from helpers import check_diag, check_index, check_seeds
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_dropin_stages(dev, oracle, case):
+    cs, dig = load_case(case)
+    posb, ctgb = dig["posb"], dig["ctgb"]
+    dev.gdb_load(cs)
+    assert dev.record_sizing() == (posb, ctgb, dig["rsize"])
+
+    ext = dev.extract_to_records()                      # extract_to_records
+    want = oracle.extract(cs, posb, ctgb)
+    assert np.array_equal(ext, want)                    # same records, same emission order
+
+    srt = dev.sort_records(ext, posb, ctgb)            # run_stage2: sort + LCP
+    check_index(srt, dig)
+    assert np.array_equal(srt, oracle.sort_records(want))
+
+    ent, cum, big = dev.build_kmer_adapter(srt, posb, ctgb)
+    oent, ocum, obig = oracle.build_adapter(srt, posb, ctgb)
+    assert np.array_equal(ent, oent) and np.array_equal(cum, ocum) and big == obig
+
+    ns, css, nb, cb = dev.self_adaptamer_merge(ent, cum, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+    ons, ocs, onb, ocb = oracle.merge(oent, ocum, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+    assert np.array_equal(ns, ons) and np.array_equal(css, ocs)
+    assert np.array_equal(nb, onb) and np.array_equal(cb, ocb)
+    check_seeds(ns, css, nb, cb, dig)
+
+    for u, seeds in (("N", ns), ("C", css)):
+        arr, off = dev.reimport_sort(seeds, posb, ctgb, 1 if u == "C" else 0, cs.ncontig, cs.maxctg,
+                                     dig["dbyte"])
+        check_diag(arr, off, u, dig)
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_resident_pipeline(dev, oracle, case):
+    cs, dig = load_case(case)
+    posb, ctgb = dig["posb"], dig["ctgb"]
+    dev.gdb_load(cs)
+    n = dev.index_build(want_entries=True)
+    assert n == dig["index"]["count"]
+    srt = dev.index_records()
+    check_index(srt, dig)
+    osrt = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    assert np.array_equal(srt, osrt)
+    ent, cum, big = dev.index_entries()
+    oent, ocum, obig = oracle.build_adapter(osrt, posb, ctgb)
+    assert np.array_equal(ent, oent) and np.array_equal(cum, ocum) and big == obig
+    dev.merge(dig["freq_cutoff"])
+    ns, nb = dev.seeds(0)
+    css, cb = dev.seeds(1)
+    check_seeds(ns, css, nb, cb, dig)
+    ons, ocs, _, _ = oracle.merge(oent, ocum, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+    assert np.array_equal(ns, ons) and np.array_equal(css, ocs)
+    for comp, u in ((0, "N"), (1, "C")):
+        sw, cnt = dev.diag_sort(comp)
+        assert sw == dig["swide"]
+        arr, off = dev.diag_records(comp, sw, cnt)
+        check_diag(arr, off, u, dig)
+
+
+def test_small_workload_full_size(dev, oracle):
+    """The 2 + 2 Mbp workload at full size: every stage bit-exact vs the oracle."""
+    from distributedpanga_b200 import gdb, synth
+    cs = gdb.from_contigs(synth.make("small"))
+    posb, ctgb, rsize = gdb.record_sizing(cs)
+    dbyte, swide = gdb.diag_sizing(cs, ctgb)
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=True)
+    srt = dev.index_records()
+    osrt = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    assert np.array_equal(srt, osrt)
+    dev.merge(10)
+    ns, nb = dev.seeds(0)
+    css, cb = dev.seeds(1)
+    oent, ocum, _ = oracle.build_adapter(osrt, posb, ctgb)
+    ons, ocs, onb, ocb = oracle.merge(oent, ocum, posb, ctgb, 10, cs.ncontig)
+    assert np.array_equal(ns, ons) and np.array_equal(css, ocs)
+    assert np.array_equal(nb, onb) and np.array_equal(cb, ocb)
+    for comp, seeds in ((0, ons), (1, ocs)):
+        sw, cnt = dev.diag_sort(comp)
+        arr, off = dev.diag_records(comp, sw, cnt)
+        oarr, ooff = oracle.reimport_sort(seeds, posb, ctgb, comp, cs.ncontig, cs.maxctg, dbyte)
+        assert np.array_equal(arr, oarr) and np.array_equal(off, ooff)
+
+
+def test_degenerate_inputs(dev, oracle):
+    from distributedpanga_b200 import gdb
+    rng = np.random.default_rng(3)
+    # only contigs too short for a 12-mer: no records at all
+    cs = gdb.from_contigs([rng.integers(0, 4, n).astype(np.uint8) for n in (1, 5, 11)])
+    dev.gdb_load(cs)
+    assert dev.index_build() == 0
+    assert dev.extract_to_records().shape[0] == 0
+    assert dev.merge(10) == (0, 0)
+    # a single 12-mer
+    cs = gdb.from_contigs([rng.integers(0, 4, 12).astype(np.uint8)])
+    posb, ctgb, _ = gdb.record_sizing(cs)
+    dev.gdb_load(cs)
+    assert np.array_equal(dev.extract_to_records(), oracle.extract(cs, posb, ctgb))
+
+
+def test_sort_matches_property_at_scale(dev):
+    """Size-independent properties of the index at 2 x 20 Mbp: sorted order,
+    LCPs equal to the recomputed bases-in-common, prefix table consistent."""
+    from distributedpanga_b200 import gdb, synth
+    cs = gdb.from_contigs(synth.make("chromset", scale=0.2))
+    dev.gdb_load(cs)
+    n = dev.index_build(want_entries=True)
+    rec = dev.index_records()
+    assert rec.shape[0] == n
+    k = rec[:, 1:11]
+    # lexicographic non-decreasing k-mers
+    v = np.ascontiguousarray(k).view(np.dtype((np.void, 10))).reshape(-1)
+    assert np.all(v[1:] >= v[:-1])
+    # LCP = leading equal bases of neighbours
+    x = np.bitwise_xor(k[1:], k[:-1])
+    first = np.argmax(x != 0, axis=1)
+    allsame = ~np.any(x != 0, axis=1)
+    byte = x[np.arange(len(x)), first]
+    lead = np.where(byte >= 64, 0, np.where(byte >= 16, 1, np.where(byte >= 4, 2, 3)))
+    want = np.where(allsame, 40, 4 * first + lead)
+    assert rec[0, 0] == 0 and np.array_equal(rec[1:, 0], want)
+    ent, cum, big = dev.index_entries()
+    assert cum[-1] == n and big == int(np.max(np.diff(np.concatenate([[0], cum]))))

@@ -1,0 +1,171 @@
+"""The oracle against the reference's own known answers for this path.
+
+Cases restate the fixtures of the reference's unit tests (test IDs from its
+tests/CATALOG.md): E-01/E-02 packing, E-06 the syncmer contract against an
+independent pure-Python extractor, E-08/E-09 emission ranges, S-01/S-02 LCP
+values, R-03 the position-256 sizing, K-03 the k-mer table entry layout."""
+import numpy as np
+import pytest
+
+from distributedpanga_b200 import gdb
+
+def cs_of(seqs):
+    return gdb.from_contigs([np.asarray(s, dtype=np.uint8) for s in seqs])
+
+
+def records(oracle, seqs):
+    cs = cs_of(seqs)
+    posb, ctgb, _ = gdb.record_sizing(cs)
+    return oracle.extract(cs, posb, ctgb), posb, ctgb
+
+
+def test_e01_forward_packing(oracle):
+    # ACGT x 13: a forward 40-mer is 2 bits per base, first base most significant;
+    # at phase r of the period every byte is the packed rotation (0x1B at r = 0)
+    seq = np.tile(np.array([0, 1, 2, 3], np.uint8), 13)
+    rec, posb, ctgb = records(oracle, [seq])
+    pos = rec[:, 12].astype(int)
+    strand = rec[:, 12 + posb + ctgb - 1] >> 7
+    fwd = rec[strand == 0]
+    assert len(fwd) > 0
+    want = {0: 0x1B, 1: 0x6C, 2: 0xB1, 3: 0xC6}
+    for r, p in zip(fwd, pos[strand == 0]):
+        assert np.all(r[1:11] == want[p % 4])
+
+
+def test_e02_rc_packing(oracle):
+    # 40 x A: the reverse complement is 40 x T -> 0xFF bytes
+    rec, posb, ctgb = records(oracle, [np.zeros(60, np.uint8)])
+    strand = rec[:, 12 + posb + ctgb - 1] >> 7
+    assert np.any(strand == 1)
+    assert np.all(rec[strand == 1][:, 1:11] == 0xFF)
+    assert np.all(rec[strand == 0][:, 1:11] == 0x00)
+
+
+def _lcp(oracle, a, b):
+    return oracle.lib().orc_lcp_bases(np.asarray(a, np.uint8), np.asarray(b, np.uint8))
+
+
+@pytest.mark.parametrize("byte,aval,bval,want", [
+    (-1, 0, 0, 40), (0, 0x00, 0x40, 0), (0, 0x00, 0x01, 3), (1, 0x00, 0x40, 4),
+    (1, 0x00, 0x01, 7), (2, 0x00, 0x80, 8), (9, 0x00, 0x01, 39)])
+def test_s01_lcp_table(oracle, byte, aval, bval, want):
+    a = np.zeros(10, np.uint8)
+    b = np.zeros(10, np.uint8)
+    if byte >= 0:
+        a[byte], b[byte] = aval, bval
+    assert _lcp(oracle, a, b) == want
+
+
+def test_s02_recalc(oracle):
+    # k-mers [k1, k1, k2], k2 first differs at base 17 -> LCPs 0, 40, 17
+    k1 = np.zeros(10, np.uint8)
+    k2 = k1.copy()
+    k2[4] = 0x10
+    rec = np.zeros((3, 16), np.uint8)
+    rec[:, 0] = 99
+    rec[0, 1:11] = k1
+    rec[1, 1:11] = k1
+    rec[2, 1:11] = k2
+    rec[0, 12], rec[1, 12], rec[2, 12] = 100, 200, 44
+    out = oracle.sort_records(rec)
+    assert out[:, 0].tolist() == [0, 40, 17]
+
+
+def _rc4(x):
+    y = 0
+    for _ in range(4):
+        y = (y << 2) | (3 - (x & 3))
+        x >>= 2
+    return y
+
+
+def _independent_extract(tm, seq, contig=0):
+    """The E-06 contract written out naively: for every 12-mer offset j take
+    the canonical hashes h[0..4] of its five 8-mers; keep j iff the earliest
+    minimum is h[0] or h[4] ties the minimum.  Returns (records, branch counts)."""
+    n = len(seq)
+    s = [int(x) for x in seq]
+    q = lambda i: (s[i] << 6) | (s[i + 1] << 4) | (s[i + 2] << 2) | s[i + 3]
+
+    def h8(i):
+        a, b = q(i), q(i + 4)
+        f = (int(tm[a]) << 8) | int(tm[b])
+        r = (int(tm[_rc4(b)]) << 8) | int(tm[_rc4(a)])
+        return min(f, r)
+    out, right, left, tie = [], 0, 0, 0
+    for j in range(0, n - 11):
+        h = [h8(j + t) for t in range(5)]
+        m = min(h)
+        a = h.index(m)
+        if not (a == 0 or h[4] == m):
+            continue
+        if a == 0:
+            left += 1
+        elif a == 4:
+            right += 1
+        else:
+            tie += 1
+        if j <= n - 40:
+            km = bytes(q(j + 4 * t) for t in range(10))
+            out.append((contig, j, 0, km))
+        if j >= 28:
+            km = bytes(_rc4(q(j - 28 + 36 - 4 * t)) for t in range(10))
+            out.append((contig, j + 12, 1, km))
+    return out, (right, left, tie)
+
+
+def test_e06_oracle_matches_independent_extractor(oracle):
+    tm = oracle.tmap()
+    rng = np.random.default_rng(20260912)
+    seq = rng.integers(0, 4, 20000).astype(np.uint8)
+    want, (right, left, tie) = _independent_extract(tm, seq)
+    assert right > 0 and left > 0 and tie > 0          # every selection branch is exercised
+    rec, posb, ctgb = records(oracle, [seq])
+    got = []
+    for r in rec:
+        pos = int.from_bytes(bytes(r[12:12 + posb]), "little")
+        cs = int.from_bytes(bytes(r[12 + posb:12 + posb + ctgb]), "little")
+        strand = cs >> (8 * ctgb - 1)
+        got.append((cs & ((1 << (8 * ctgb - 1)) - 1), pos, strand, bytes(r[1:11])))
+    assert got == want                                    # same records, same emission order
+
+
+def test_e08_e09_ranges(oracle):
+    rng = np.random.default_rng(5)
+    for n in (41, 67, 68):
+        seq = rng.integers(0, 4, n).astype(np.uint8)
+        rec, posb, ctgb = records(oracle, [seq])
+        pos = rec[:, 12].astype(int)
+        strand = rec[:, 12 + posb + ctgb - 1] >> 7
+        assert np.all(pos[strand == 0] <= n - 40)
+        assert np.all(pos[strand == 1] - 12 >= 28)
+        assert np.all(pos[strand == 1] - 12 <= n - 12)
+
+
+def test_r03_position_256_sizing():
+    # maxctg = 256: an RC record stores j + 12 = 256, so positions need 2 bytes
+    cs = cs_of([np.zeros(256, np.uint8)])
+    posb, ctgb, rsize = gdb.record_sizing(cs)
+    assert (posb, ctgb, rsize) == (2, 1, 15)
+    cs = cs_of([np.zeros(255, np.uint8)] * 128)
+    assert gdb.record_sizing(cs) == (1, 1, 14)        # E-10: 128 contigs fit 1 byte with the strand bit
+    cs = cs_of([np.zeros(255, np.uint8)] * 129)
+    assert gdb.record_sizing(cs)[1] == 2
+
+
+def test_k03_entry_layout(oracle):
+    rng = np.random.default_rng(9)
+    seq = rng.integers(0, 4, 3000).astype(np.uint8)
+    rec, posb, ctgb = records(oracle, [seq])
+    srt = oracle.sort_records(rec)
+    ent, cum, big = oracle.build_adapter(srt, posb, ctgb)
+    assert ent.shape == (len(srt), 9 + posb + ctgb)
+    assert np.array_equal(ent[:, 0:7], srt[:, 4:11])      # k-mer bytes 3..9
+    assert np.all(ent[:, 7] == 0)                         # mask
+    assert np.array_equal(ent[:, 8], srt[:, 0])           # LCP
+    assert np.array_equal(ent[:, 9:], srt[:, 12:])        # payload
+    pre = (srt[:, 1].astype(np.int64) << 16) | (srt[:, 2].astype(np.int64) << 8) | srt[:, 3]
+    assert cum[-1] == len(srt)
+    assert np.array_equal(np.cumsum(np.bincount(pre, minlength=1 << 24)), cum)
+    assert big == np.bincount(pre).max()
