@@ -327,8 +327,8 @@ int run_merge(pga_ctx *ctx, int freq) {
   CK(cudaMemsetAsync(bn, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
   CK(cudaMemsetAsync(bc, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
   if (n > 0) {
-    k_merge<false><<<nb, MERGE_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
-                                                      nullptr, nullptr, ctx->ctgb);
+    launch_merge(false, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc, nullptr, nullptr,
+                 ctx->ctgb);
     LAUNCHED(1);
   }
   uint32_t *tot = P<uint32_t>(ctx->u64tmp);
@@ -343,8 +343,8 @@ int run_merge(pga_ctx *ctx, int freq) {
   ENSURE(ctx->seed[0], sizeof(Seed) * (size_t)t[0] + 16);
   ENSURE(ctx->seed[1], sizeof(Seed) * (size_t)t[1] + 16);
   if (n > 0) {
-    k_merge<true><<<nb, MERGE_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
-                                                     P<Seed>(ctx->seed[0]), P<Seed>(ctx->seed[1]), ctx->ctgb);
+    launch_merge(true, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
+                 P<Seed>(ctx->seed[0]), P<Seed>(ctx->seed[1]), ctx->ctgb);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_MERGE);
@@ -663,9 +663,8 @@ int pga_extract_to_records(pga_ctx *ctx, int num_workers, int worker_id, uint8_t
   if (nt > 0) {
     const int32_t *tc = P<int32_t>(ctx->tile_ctg) + tbeg;
     const int64_t *tj = P<int64_t>(ctx->tile_j0) + tbeg;
-    k_extract<EXT_COUNT><<<nt, EXT_THREADS, 0, ctx->st>>>(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen),
-                                                           P<int64_t>(ctx->dboff), tc, tj, ctx->ctgb, cnt32,
-                                                           nullptr, nullptr, nullptr, nullptr);
+    launch_extract(EXT_COUNT, nt, ctx->st, P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen), P<int64_t>(ctx->dboff),
+                   tc, tj, ctx->ctgb, cnt32, nullptr, nullptr, nullptr, nullptr);
     LAUNCHED(1);
     CK(cudaGetLastError());
     // widen the counts to 64 bits for the offsets scan
@@ -681,9 +680,8 @@ int pga_extract_to_records(pga_ctx *ctx, int num_workers, int worker_id, uint8_t
     if (r) return r;
     CK(cudaMemcpyAsync(off, ho.data(), sizeof(uint64_t) * nthr, cudaMemcpyHostToDevice, ctx->st));
     ENSURE(ctx->rec2, sizeof(Rec) * total_rec + 16);
-    k_extract<EXT_WRITE><<<nt, EXT_THREADS, 0, ctx->st>>>(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen),
-                                                           P<int64_t>(ctx->dboff), tc, tj, ctx->ctgb, nullptr,
-                                                           off, P<Rec>(ctx->rec2), nullptr, nullptr);
+    launch_extract(EXT_WRITE, nt, ctx->st, P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen), P<int64_t>(ctx->dboff),
+                   tc, tj, ctx->ctgb, nullptr, off, P<Rec>(ctx->rec2), nullptr, nullptr);
     LAUNCHED(1);
     CK(cudaGetLastError());
   }
@@ -708,7 +706,6 @@ int pga_extract_to_records(pga_ctx *ctx, int num_workers, int worker_id, uint8_t
   }
   *records = h;
   *count = (int64_t)total_rec;
-  ctx->have_index = false;
   return PGA_OK;
 }
 
@@ -880,8 +877,8 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   stage_begin(ctx, ST_EXTRACT_HIST);
   CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(uint32_t) * NPREFIX, ctx->st));
   if (ctx->ntiles > 0) {
-    k_extract<EXT_HIST><<<ctx->ntiles, EXT_THREADS, 0, ctx->st>>>(bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
-                                                                   nullptr, P<uint32_t>(ctx->hist), nullptr);
+    launch_extract(EXT_HIST, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr,
+                   P<uint32_t>(ctx->hist), nullptr);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_HIST);
@@ -897,9 +894,8 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   ENSURE(ctx->rec, sizeof(Rec) * (size_t)n + 16);
   stage_begin(ctx, ST_EXTRACT_SCATTER);
   if (ctx->ntiles > 0) {
-    k_extract<EXT_SCATTER><<<ctx->ntiles, EXT_THREADS, 0, ctx->st>>>(bps, cl, bo, tc, tj, ctx->ctgb, nullptr,
-                                                                      nullptr, P<Rec>(ctx->rec), nullptr,
-                                                                      P<uint32_t>(ctx->hist));
+    launch_extract(EXT_SCATTER, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
+                   P<Rec>(ctx->rec), nullptr, P<uint32_t>(ctx->hist));
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_SCATTER);

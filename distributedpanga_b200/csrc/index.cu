@@ -162,18 +162,28 @@ k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
   if (MODE == EXT_COUNT) counts[(int64_t)blockIdx.x * EXT_THREADS + tid] = nrec;
 }
 
-template __global__ void k_extract<EXT_COUNT>(const uint8_t *, const int64_t *, const int64_t *,
-                                              const int32_t *, const int64_t *, int, uint32_t *,
-                                              const uint64_t *, Rec *, uint32_t *, uint32_t *);
-template __global__ void k_extract<EXT_WRITE>(const uint8_t *, const int64_t *, const int64_t *,
-                                              const int32_t *, const int64_t *, int, uint32_t *,
-                                              const uint64_t *, Rec *, uint32_t *, uint32_t *);
-template __global__ void k_extract<EXT_HIST>(const uint8_t *, const int64_t *, const int64_t *,
-                                             const int32_t *, const int64_t *, int, uint32_t *,
-                                             const uint64_t *, Rec *, uint32_t *, uint32_t *);
-template __global__ void k_extract<EXT_SCATTER>(const uint8_t *, const int64_t *, const int64_t *,
-                                                const int32_t *, const int64_t *, int, uint32_t *,
-                                                const uint64_t *, Rec *, uint32_t *, uint32_t *);
+void launch_extract(int mode, int ntiles, cudaStream_t st, const uint8_t *bps, const int64_t *clen,
+                    const int64_t *boff, const int32_t *tile_ctg, const int64_t *tile_j0, int ctgb,
+                    uint32_t *counts, const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor) {
+  if (ntiles <= 0) return;
+  switch (mode) {
+    case EXT_COUNT:
+      k_extract<EXT_COUNT><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
+                                                           offsets, out, hist, cursor);
+      break;
+    case EXT_WRITE:
+      k_extract<EXT_WRITE><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
+                                                           offsets, out, hist, cursor);
+      break;
+    case EXT_HIST:
+      k_extract<EXT_HIST><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
+                                                          offsets, out, hist, cursor);
+      break;
+    default:
+      k_extract<EXT_SCATTER><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
+                                                             offsets, out, hist, cursor);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Prefix histogram of records already in HBM (used when records come from

@@ -1,6 +1,7 @@
 // Index-build kernels (index.cu) and their launch constants.
 #pragma once
 #include <cstdint>
+#include <cuda_runtime.h>
 #include "common.cuh"
 
 namespace pga {
@@ -17,10 +18,10 @@ constexpr int BK_SMALL = 32;      // bucket sizes sorted by one thread
 constexpr int BK_MEDIUM = 2048;   // bucket sizes sorted by one CTA in shared memory
 constexpr int BK_THREADS = 256;
 
-template <int MODE>
-__global__ void k_extract(const uint8_t *bps, const int64_t *clen, const int64_t *boff,
-                          const int32_t *tile_ctg, const int64_t *tile_j0, int ctgb, uint32_t *counts,
-                          const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor);
+// Launches the extraction kernel in one of the EXT_* modes (one CTA per tile).
+void launch_extract(int mode, int ntiles, cudaStream_t st, const uint8_t *bps, const int64_t *clen,
+                    const int64_t *boff, const int32_t *tile_ctg, const int64_t *tile_j0, int ctgb,
+                    uint32_t *counts, const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor);
 __global__ void k_prefix_hist(const Rec *rec, int64_t n, uint32_t *hist);
 __global__ void k_prefix_scatter(const Rec *in, int64_t n, uint32_t *cursor, Rec *out);
 __global__ void k_bucket_small(Rec *rec, const uint32_t *start, uint32_t *qmed, uint32_t *qbig,

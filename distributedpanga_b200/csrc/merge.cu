@@ -39,9 +39,9 @@ __device__ __forceinline__ Run adaptamer_run(const uint8_t *__restrict__ lcp, in
   r.emit = false;
   r.s = r.t = i;
   if (r.plen < 12) return r;
-  // run start: the last r <= i with lcp[r] < plen (lcp[0] == 0 stops the walk)
+  // run start: the last r <= i with lcp[r] < plen, or the table's first entry
   int64_t s = i;
-  while (lcp[s] >= r.plen) {
+  while (s > 0 && lcp[s] >= r.plen) {
     s--;
     if (i + 1 - s >= freq) return r;
   }
@@ -109,10 +109,14 @@ k_merge(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
   }
 }
 
-template __global__ void k_merge<false>(const Rec *, const uint8_t *, int64_t, int, uint32_t *,
-                                        uint32_t *, Seed *, Seed *, int);
-template __global__ void k_merge<true>(const Rec *, const uint8_t *, int64_t, int, uint32_t *,
-                                       uint32_t *, Seed *, Seed *, int);
+void launch_merge(bool write, int nb, cudaStream_t st, const Rec *rec, const uint8_t *lcp, int64_t n, int freq,
+                  uint32_t *blk_n, uint32_t *blk_c, Seed *nseed, Seed *cseed, int ctgb) {
+  if (nb <= 0) return;
+  if (write)
+    k_merge<true><<<nb, MERGE_THREADS, 0, st>>>(rec, lcp, n, freq, blk_n, blk_c, nseed, cseed, ctgb);
+  else
+    k_merge<false><<<nb, MERGE_THREADS, 0, st>>>(rec, lcp, n, freq, blk_n, blk_c, nseed, cseed, ctgb);
+}
 
 // Seeds in the reference's byte format (src/fastga_pipeline.c:391-397):
 // [plen][A position, A contig (strand cleared)][B position, B contig|strand].

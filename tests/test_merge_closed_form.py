@@ -24,7 +24,7 @@ def closed_form_merge(srt, posb, ctgb, freq):
         if plen < 12:
             continue
         s = i
-        while lcp[s] >= plen:
+        while s > 0 and lcp[s] >= plen:
             s -= 1
         t = i + 1
         while t < n and lcp[t] >= plen:
