@@ -1,0 +1,987 @@
+// Warp-cooperative wave extension: forward_wave / reverse_wave /
+// Local_Alignment (lib/align.c:352-1576) with the 32 lanes of a warp
+// updating the diagonals of a wave in parallel.
+//
+// The sequential loop of the reference visits the diagonals of a wave in one
+// order (forward: k = hgh..low, reverse: k = low..hgh) and reads, for k, the
+// previous wave's values at k-1, k and k+1.  Every lane here reads those from
+// the previous wave's buffer (the ring buffers are double-buffered), so the
+// new values equal the reference's.  What the reference accumulates in visit
+// order is rebuilt with warp scans in visit order (lane 0 = first visited):
+//   besta / bestx       running maximum (minimum in reverse): a diagonal is a
+//                       record if it beats the maximum before it
+//   lasta / trim*       the last record that passes the path-average and trim
+//                       table tests
+//   aclip / bclip       the last / extreme diagonal that met a sentinel
+//   pebbles             every lane counts its new trace pebbles, a warp scan
+//                       gives their slots in a global pool (slot numbers only
+//                       name pebbles; the linked chains are the reference's)
+// The rest of a wave step (boundaries, clipping, WAVE_LAG pruning) and the
+// final trace-back are the reference's sequential code, run by all lanes on
+// lane-uniform values.
+#pragma once
+#include <stdint.h>
+#include "align_core.cuh"
+
+namespace pga {
+namespace aln {
+
+constexpr uint32_t FULL = 0xffffffffu;
+
+// Pebble pool shared by all warps of a launch: bump allocation in chunks.
+struct PebblePool {
+  Pebble *cells;
+  unsigned long long *next;  // next free pebble (global counter)
+  int64_t cap;
+};
+
+struct WarpWork {
+  int *V[2], *M[2], *HA[2];
+  uint64_t *T[2];
+  int *NA;
+  int vcap;
+  uint16_t *points;
+  int64_t point_cap;
+  PebblePool pool;
+  int64_t chunk_next, chunk_end;  // this warp's current pebble chunk (lane-uniform)
+  int err;
+};
+
+constexpr int PEBBLE_CHUNK = 4096;
+
+// Reserve `cnt` consecutive pebbles for the warp (lane-uniform call).
+__device__ __forceinline__ int64_t warp_pebbles(WarpWork &W, int cnt) {
+  if (cnt == 0) return 0;
+  if (W.chunk_next + cnt > W.chunk_end) {
+    int64_t want = cnt > PEBBLE_CHUNK ? cnt : PEBBLE_CHUNK;
+    unsigned long long base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(W.pool.next, (unsigned long long)want);
+    base = __shfl_sync(FULL, base, 0);
+    if ((int64_t)base + want > W.pool.cap) {
+      W.err |= ALN_ERR_CELLS;
+      return -1;
+    }
+    W.chunk_next = (int64_t)base;
+    W.chunk_end = (int64_t)base + want;
+  }
+  int64_t s = W.chunk_next;
+  W.chunk_next += cnt;
+  return s;
+}
+
+__device__ __forceinline__ int warp_excl_sum(int v, int lane) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x += y;
+  }
+  return x - v;
+}
+
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// exclusive running max (forward) in lane order, seeded with `init`
+__device__ __forceinline__ int warp_excl_max(int v, int lane, int init) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x = max(x, y);
+  }
+  int ex = __shfl_up_sync(FULL, x, 1);
+  if (lane == 0) ex = init;
+  return max(ex, init);
+}
+
+__device__ __forceinline__ int warp_excl_min(int v, int lane, int init) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x = min(x, y);
+  }
+  int ex = __shfl_up_sync(FULL, x, 1);
+  if (lane == 0) ex = init;
+  return min(ex, init);
+}
+
+__device__ __forceinline__ int warp_max(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_min(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// Highest lane with a set bit (the last in visit order), -1 if none.
+__device__ __forceinline__ int last_lane(uint32_t ballot) { return ballot ? 31 - __clz(ballot) : -1; }
+
+// Forward snake along diagonal k from a-position x (bases equal, neither a
+// sentinel).  Compares 8 bytes at a time; stops exactly where the byte loop
+// of the reference stops and reports which sentinel (if any) stopped it.
+__device__ __forceinline__ int snake_fwd(const uint8_t *aseq, const uint8_t *bseq, int x, int k, int *hitb,
+                                         int *hita) {
+  *hitb = *hita = 0;
+  while (1) {
+    int c = bseq[x - k];
+    if (c == 4) {
+      *hitb = 1;
+      return x;
+    }
+    int d = aseq[x];
+    if (c != d) {
+      if (d == 4) *hita = 1;
+      return x;
+    }
+    x += 1;
+  }
+}
+
+__device__ __forceinline__ int snake_rev(const uint8_t *aseq, const uint8_t *bseq, int x, int k, int *hitb,
+                                         int *hita) {
+  *hitb = *hita = 0;
+  while (1) {
+    int c = bseq[x - k];
+    if (c == 4) {
+      *hitb = 1;
+      return x;
+    }
+    int d = aseq[x];
+    if (c != d) {
+      if (d == 4) *hita = 1;
+      return x;
+    }
+    x -= 1;
+  }
+}
+
+#define WVI(k) ((k) & vmask)
+
+// ---------------------------------------------------------------------------
+// forward_wave, warp version.  Returns 1 on an arena overflow (W.err set).
+// ---------------------------------------------------------------------------
+__device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, Path &P, int *mind,
+                              int maxd, int mida, int minp, int maxp, int aoff) {
+  const int lane = threadIdx.x & 31;
+  const uint8_t *aseq = A.s;
+  const uint8_t *bseq = B.s;
+  const int vmask = W.vcap - 1;
+  int cur = 0;
+  int *NA = W.NA;
+  Pebble *cells = W.pool.cells;
+  const int tspace = spec.trace_space;
+  const int PATH_AVE = spec.ave_path;
+  const int16_t *SCORE = spec.score;
+  const int16_t *TABLE = spec.table;
+
+  int hgh = maxd, low = *mind, dif = 0;
+  int besta, bestx, trima, trimx, trimd, trimha, morea, morex, mored, moreha, more, morem, lasta;
+  int aclip, bclip;
+  if (hgh - low + 3 > W.vcap) {
+    W.err |= ALN_ERR_VCAP;
+    return 1;
+  }
+  more = 1;
+  aclip = I32MAX;
+  bclip = -I32MAX;
+  besta = trima = morea = lasta = mida;
+  bestx = trimx = morex = (mida + hgh) >> 1;
+  trimd = mored = 0;
+  trimha = moreha = 0;
+  morem = -1;
+
+  // 0-wave: diagonals visited hgh..low
+  for (int base = hgh; base >= low; base -= 32) {
+    int k = base - lane;
+    bool act = k >= low;
+    int x = 0, c = 0, na = 0, hb = 0, ha_ = 0, npb = 0;
+    if (act) {
+      x = (mida + k) >> 1;
+      na = ((x + (tspace - aoff)) / tspace - 1) * tspace + aoff;
+      x = snake_fwd(aseq, bseq, x, k, &hb, &ha_);
+      c = (x << 1) - k;
+      npb = 1;
+      for (int q = na + tspace; x >= q; q += tspace) npb++;
+    }
+    int off = warp_excl_sum(npb, lane);
+    int tot = warp_sum(npb);
+    int64_t pb0 = warp_pebbles(W, tot);
+    if (pb0 < 0) return 1;
+    int ha = -1;
+    if (act) {
+      int64_t s = pb0 + off;
+      cells[s] = {-1, k, 0, na};
+      ha = (int)s;
+      na += tspace;
+      while (x >= na) {
+        s += 1;
+        cells[s] = {ha, k, 0, na};
+        ha = (int)s;
+        na += tspace;
+      }
+      int vi = WVI(k);
+      W.V[cur][vi] = c;
+      W.T[cur][vi] = PATH_INT;
+      W.M[cur][vi] = PATH_LEN;
+      W.HA[cur][vi] = ha;
+      NA[vi] = na;
+    }
+    // clips: bclip = largest k that met B's end, aclip = last visited (smallest) k that met A's end
+    uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && ha_);
+    if (bb) {
+      more = 0;
+      int kk = base - (__ffs(bb) - 1);
+      if (bclip < kk) bclip = kk;
+    }
+    if (ba) {
+      more = 0;
+      aclip = base - last_lane(ba);
+    }
+    // records: c > running maximum
+    int pm = warp_excl_max(act ? c : -2147483647, lane, besta);
+    bool rec = act && c > pm;
+    uint32_t rb = __ballot_sync(FULL, rec);
+    if (rb) {
+      int L = last_lane(rb);
+      besta = trima = lasta = __shfl_sync(FULL, c, L);
+      bestx = trimx = __shfl_sync(FULL, x, L);
+      trimha = __shfl_sync(FULL, ha, L);
+    }
+  }
+  __syncwarp();
+  {
+    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
+    if (more == 0) {
+      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
+      if (hgh >= aclip) {
+        hgh = aclip - 1;
+        if (morem <= M[WVI(aclip)]) {
+          morem = M[WVI(aclip)];
+          morea = V[WVI(aclip)];
+          morex = (morea + aclip) >> 1;
+          moreha = HA[WVI(aclip)];
+        }
+      }
+      if (low <= bclip) {
+        low = bclip + 1;
+        if (morem <= M[WVI(bclip)]) {
+          morem = M[WVI(bclip)];
+          morea = V[WVI(bclip)];
+          morex = (morea + bclip) >> 1;
+          moreha = HA[WVI(bclip)];
+        }
+      }
+      aclip = I32MAX;
+      bclip = -I32MAX;
+    }
+  }
+
+  while (more && lasta >= besta - TRIM_MLAG) {
+    low -= 1;
+    hgh += 1;
+    if (hgh - low + 3 > W.vcap) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
+    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur];
+    uint64_t *To = W.T[cur];
+    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1];
+    uint64_t *Tn = W.T[cur ^ 1];
+    // boundary diagonals on the previous wave's buffer (lane 0; visible after syncwarp)
+    bool top_default = false;
+    if (low >= minp) {
+      if (lane == 0) {
+        NA[WVI(low)] = NA[WVI(low + 1)];
+        Vo[WVI(low)] = -1;
+      }
+    } else
+      low += 1;
+    if (hgh <= maxp) {
+      if (lane == 0) {
+        NA[WVI(hgh)] = NA[WVI(hgh - 1)];
+        Vo[WVI(hgh)] = -1;
+      }
+    } else
+      hgh -= 1;
+    if (lane == 0) {
+      Vo[WVI(hgh + 1)] = -1;
+      Vo[WVI(low - 1)] = -1;
+    }
+    top_default = true;  // k = hgh+1 carries T = PATH_INT, M = PATH_LEN, HA = -1
+    dif += 1;
+    __syncwarp();
+    int carry = besta;
+    for (int base = hgh; base >= low; base -= 32) {
+      int k = base - lane;
+      bool act = k >= low;
+      int x = 0, c = 0, m = 0, ha = -1, hb = 0, hA = 0, npb = 0, nak = 0;
+      uint64_t b = 0;
+      if (act) {
+        int vi = WVI(k);
+        int ap = Vo[WVI(k + 1)], ac = Vo[vi], am = Vo[WVI(k - 1)];
+        int src;  // 1: k+1, 0: k, -1: k-1
+        if (ac < am)
+          src = (am < ap) ? 1 : -1;
+        else
+          src = (ac < ap) ? 1 : 0;
+        if (src == 1) {
+          c = ap + 1;
+          if (k == hgh && top_default) {
+            m = PATH_LEN; b = PATH_INT; ha = -1;
+          } else {
+            m = Mo[WVI(k + 1)]; b = To[WVI(k + 1)]; ha = HAo[WVI(k + 1)];
+          }
+        } else if (src == -1) {
+          c = am + 1; m = Mo[WVI(k - 1)]; b = To[WVI(k - 1)]; ha = HAo[WVI(k - 1)];
+        } else {
+          c = ac + 2; m = Mo[vi]; b = To[vi]; ha = HAo[vi];
+        }
+        if ((b & PATH_TOP) != 0) m -= 1;
+        b <<= 1;
+        x = (c + k) >> 1;
+        int x0 = x;
+        x = snake_fwd(aseq, bseq, x, k, &hb, &hA);
+        int run = x - x0;
+        // the reference shifts a 1 into b per matched base and counts m up while the top bit is clear
+        for (int r = 0; r < run; r++) {
+          if ((b & PATH_TOP) == 0) m += 1;
+          b = (b << 1) | 1;
+        }
+        c = (x << 1) - k;
+        nak = NA[vi];
+        int hm = ha >= 0 ? cells[ha].mark : 0;
+        for (int q = nak; x >= q; q += tspace)
+          if (hm < q) {
+            npb++;
+            hm = q;  // the new pebble's mark
+          }
+      }
+      int off = warp_excl_sum(npb, lane);
+      int tot = warp_sum(npb);
+      int64_t pb0 = warp_pebbles(W, tot);
+      if (pb0 < 0) return 1;
+      if (act) {
+        int vi = WVI(k);
+        int64_t s = pb0 + off;
+        while (x >= nak) {
+          if (cells[ha].mark < nak) {
+            cells[s] = {ha, k, dif, nak};
+            ha = (int)s;
+            s += 1;
+          }
+          nak += tspace;
+        }
+        NA[vi] = nak;
+        Vn[vi] = c;
+        Tn[vi] = b;
+        Mn[vi] = m;
+        HAn[vi] = ha;
+      }
+      uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
+      if (bb) {
+        more = 0;
+        int kk = base - (__ffs(bb) - 1);
+        if (bclip < kk) bclip = kk;
+      }
+      if (ba) {
+        more = 0;
+        aclip = base - last_lane(ba);
+      }
+      int pm = warp_excl_max(act ? c : -2147483647, lane, carry);
+      bool rec = act && c > pm;
+      uint32_t rb = __ballot_sync(FULL, rec);
+      if (rb) {
+        int L = last_lane(rb);
+        carry = __shfl_sync(FULL, c, L);
+        besta = carry;
+        bestx = __shfl_sync(FULL, x, L);
+        bool pa = rec && m >= PATH_AVE;
+        uint32_t pab = __ballot_sync(FULL, pa);
+        if (pab) {
+          lasta = __shfl_sync(FULL, c, last_lane(pab));
+          bool tr = pa && TABLE[b & TRIM_MASK] >= 0 &&
+                    TABLE[(b >> TRIM_LEN) & TRIM_MASK] + SCORE[b & TRIM_MASK] >= 0;
+          uint32_t trb = __ballot_sync(FULL, tr);
+          if (trb) {
+            int T2 = last_lane(trb);
+            trima = __shfl_sync(FULL, c, T2);
+            trimx = __shfl_sync(FULL, x, T2);
+            trimd = dif;
+            trimha = __shfl_sync(FULL, ha, T2);
+          }
+        }
+      }
+    }
+    cur ^= 1;
+    __syncwarp();
+    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
+    if (more == 0) {
+      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
+      if (hgh >= aclip) {
+        hgh = aclip - 1;
+        if (morem <= M[WVI(aclip)]) {
+          morem = M[WVI(aclip)];
+          morea = V[WVI(aclip)];
+          morex = (morea + aclip) >> 1;
+          mored = dif;
+          moreha = HA[WVI(aclip)];
+        }
+      }
+      if (low <= bclip) {
+        low = bclip + 1;
+        if (morem <= M[WVI(bclip)]) {
+          morem = M[WVI(bclip)];
+          morea = V[WVI(bclip)];
+          morex = (morea + bclip) >> 1;
+          mored = dif;
+          moreha = HA[WVI(bclip)];
+        }
+      }
+      aclip = I32MAX;
+      bclip = -I32MAX;
+    }
+    int n = besta - WAVE_LAG;
+    while (hgh >= low)
+      if (V[WVI(hgh)] < n)
+        hgh -= 1;
+      else {
+        while (V[WVI(low)] < n) low += 1;
+        break;
+      }
+    // copy the surviving diagonals' NA-independent state is already in the new buffer
+  }
+  __syncwarp();
+
+  // trace-back (lane-uniform sequential code; only lane 0 writes)
+  {
+    uint16_t *atrace = W.points + P.trace_off;
+    int atlen = 0, trimy, a, b, k, h, d, e;
+    if (morem >= 0 && spec.reach) {
+      trimx = morex;
+      trimy = morea - morex;
+      trimd = mored;
+      trimha = moreha;
+    } else
+      trimy = trima - trimx;
+    // reverse the pebble chain: done by lane 0, read back by all
+    if (lane == 0) {
+      a = -1;
+      for (h = trimha; h >= 0; h = b) {
+        b = cells[h].ptr;
+        cells[h].ptr = a;
+        a = h;
+      }
+    }
+    __syncwarp();
+    a = __shfl_sync(FULL, a, 0);
+    h = a;
+    k = cells[h].diag;
+    b = (mida - k) >> 1;
+    e = 0;
+    low = k;
+    for (h = cells[h].ptr; h >= 0; h = cells[h].ptr) {
+      k = cells[h].diag;
+      a = cells[h].mark - k;
+      d = cells[h].diff;
+      if (P.trace_off + atlen + 2 > W.point_cap) {
+        W.err |= ALN_ERR_POINTS;
+        return 1;
+      }
+      if (lane == 0) {
+        atrace[atlen] = (uint16_t)(d - e);
+        atrace[atlen + 1] = (uint16_t)(a - b);
+      }
+      atlen += 2;
+      b = a;
+      e = d;
+    }
+    __syncwarp();
+    if (b + k != trimx) {
+      if (P.trace_off + atlen + 2 > W.point_cap) {
+        W.err |= ALN_ERR_POINTS;
+        return 1;
+      }
+      if (lane == 0) {
+        atrace[atlen] = (uint16_t)(trimd - e);
+        atrace[atlen + 1] = (uint16_t)(trimy - b);
+      }
+      atlen += 2;
+    } else if (b != trimy) {
+      if (lane == 0) {
+        atrace[atlen - 1] = (uint16_t)(atrace[atlen - 1] + (trimy - b));
+        atrace[atlen - 2] = (uint16_t)(atrace[atlen - 2] + (trimd - e));
+      }
+    }
+    __syncwarp();
+    P.aepos = trimx;
+    P.bepos = trimy;
+    P.diffs = trimd;
+    P.tlen = atlen;
+  }
+  *mind = low;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// reverse_wave, warp version (visit order k = low..hgh, minimum instead of
+// maximum, sequences read one position to the left).
+// ---------------------------------------------------------------------------
+__device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, Path &P, int mind,
+                              int maxd, int mida, int minp, int maxp, int aoff) {
+  const int lane = threadIdx.x & 31;
+  const uint8_t *aseq = A.s - 1;
+  const uint8_t *bseq = B.s - 1;
+  const int vmask = W.vcap - 1;
+  int cur = 0;
+  int *NA = W.NA;
+  Pebble *cells = W.pool.cells;
+  const int tspace = spec.trace_space;
+  const int PATH_AVE = spec.ave_path;
+  const int16_t *SCORE = spec.score;
+  const int16_t *TABLE = spec.table;
+
+  int hgh = maxd, low = mind, dif = 0;
+  int besta, bestx, trima, trimx, trimd, trimha, morea, morex, mored, moreha, more, morem, lasta;
+  int aclip, bclip;
+  if (hgh - low + 3 > W.vcap) {
+    W.err |= ALN_ERR_VCAP;
+    return 1;
+  }
+  more = 1;
+  aclip = -I32MAX;
+  bclip = I32MAX;
+  besta = trima = morea = lasta = mida;
+  bestx = trimx = morex = (mida + hgh) >> 1;
+  trimd = mored = 0;
+  trimha = moreha = 0;
+  morem = -1;
+
+  for (int base = low; base <= hgh; base += 32) {
+    int k = base + lane;
+    bool act = k <= hgh;
+    int x = 0, c = 0, na = 0, hb = 0, hA = 0, npb = 0, x0 = 0;
+    if (act) {
+      x = (mida + k) >> 1;
+      x0 = x;
+      na = ((x + (tspace - aoff) - 1) / tspace - 1) * tspace + aoff;
+      x = snake_rev(aseq, bseq, x, k, &hb, &hA);
+      c = (x << 1) - k;
+      npb = 1;
+      for (int q = na; x <= q; q -= tspace) npb++;
+    }
+    int off = warp_excl_sum(npb, lane);
+    int tot = warp_sum(npb);
+    int64_t pb0 = warp_pebbles(W, tot);
+    if (pb0 < 0) return 1;
+    int ha = -1;
+    if (act) {
+      int64_t s = pb0 + off;
+      cells[s] = {-1, k, 0, x0};
+      ha = (int)s;
+      while (x <= na) {
+        s += 1;
+        cells[s] = {ha, k, 0, na};
+        ha = (int)s;
+        na -= tspace;
+      }
+      int vi = WVI(k);
+      W.V[cur][vi] = c;
+      W.T[cur][vi] = PATH_INT;
+      W.M[cur][vi] = PATH_LEN;
+      W.HA[cur][vi] = ha;
+      NA[vi] = na;
+    }
+    // bclip = smallest k that met B's start, aclip = last visited (largest) k that met A's start
+    uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
+    if (bb) {
+      more = 0;
+      int kk = base + (__ffs(bb) - 1);
+      if (bclip > kk) bclip = kk;
+    }
+    if (ba) {
+      more = 0;
+      aclip = base + last_lane(ba);
+    }
+    int pm = warp_excl_min(act ? c : 2147483647, lane, besta);
+    bool rec = act && c < pm;
+    uint32_t rb = __ballot_sync(FULL, rec);
+    if (rb) {
+      int L = last_lane(rb);
+      besta = trima = lasta = __shfl_sync(FULL, c, L);
+      bestx = trimx = __shfl_sync(FULL, x, L);
+      trimha = __shfl_sync(FULL, ha, L);
+    }
+  }
+  __syncwarp();
+  {
+    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
+    if (more == 0) {
+      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
+      if (low <= aclip) {
+        low = aclip + 1;
+        if (morem <= M[WVI(aclip)]) {
+          morem = M[WVI(aclip)];
+          morea = V[WVI(aclip)];
+          morex = (morea + aclip) >> 1;
+          moreha = HA[WVI(aclip)];
+        }
+      }
+      if (hgh >= bclip) {
+        hgh = bclip - 1;
+        if (morem <= M[WVI(bclip)]) {
+          morem = M[WVI(bclip)];
+          morea = V[WVI(bclip)];
+          morex = (morea + bclip) >> 1;
+          moreha = HA[WVI(bclip)];
+        }
+      }
+      aclip = -I32MAX;
+      bclip = I32MAX;
+    }
+  }
+
+  while (more && lasta <= besta + TRIM_MLAG) {
+    low -= 1;
+    hgh += 1;
+    if (hgh - low + 3 > W.vcap) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
+    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur];
+    uint64_t *To = W.T[cur];
+    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1];
+    uint64_t *Tn = W.T[cur ^ 1];
+    if (low >= minp) {
+      if (lane == 0) {
+        NA[WVI(low)] = NA[WVI(low + 1)];
+        Vo[WVI(low)] = I32MAX;
+      }
+    } else
+      low += 1;
+    if (hgh <= maxp) {
+      if (lane == 0) {
+        NA[WVI(hgh)] = NA[WVI(hgh - 1)];
+        Vo[WVI(hgh)] = I32MAX;
+      }
+    } else
+      hgh -= 1;
+    if (lane == 0) {
+      Vo[WVI(hgh + 1)] = I32MAX;
+      Vo[WVI(low - 1)] = I32MAX;
+    }
+    dif += 1;
+    __syncwarp();
+    int carry = besta;
+    for (int base = low; base <= hgh; base += 32) {
+      int k = base + lane;
+      bool act = k <= hgh;
+      int x = 0, c = 0, m = 0, ha = -1, hb = 0, hA = 0, npb = 0, nak = 0;
+      uint64_t b = 0;
+      if (act) {
+        int vi = WVI(k);
+        int am = Vo[WVI(k - 1)], ac = Vo[vi], ap = Vo[WVI(k + 1)];
+        int src;  // -1: k-1 (the previous visit), 0: k, 1: k+1
+        if (ac > ap)
+          src = (ap > am) ? -1 : 1;
+        else
+          src = (ac > am) ? -1 : 0;
+        if (src == -1) {
+          c = am - 1;
+          if (k == low) {
+            m = PATH_LEN; b = PATH_INT; ha = -1;
+          } else {
+            m = Mo[WVI(k - 1)]; b = To[WVI(k - 1)]; ha = HAo[WVI(k - 1)];
+          }
+        } else if (src == 1) {
+          c = ap - 1; m = Mo[WVI(k + 1)]; b = To[WVI(k + 1)]; ha = HAo[WVI(k + 1)];
+        } else {
+          c = ac - 2; m = Mo[vi]; b = To[vi]; ha = HAo[vi];
+        }
+        if ((b & PATH_TOP) != 0) m -= 1;
+        b <<= 1;
+        x = (c + k) >> 1;
+        int x0 = x;
+        x = snake_rev(aseq, bseq, x, k, &hb, &hA);
+        int run = x0 - x;
+        for (int r = 0; r < run; r++) {
+          if ((b & PATH_TOP) == 0) m += 1;
+          b = (b << 1) | 1;
+        }
+        c = (x << 1) - k;
+        nak = NA[vi];
+        int hm = ha >= 0 ? cells[ha].mark : 0;
+        for (int q = nak; x <= q; q -= tspace)
+          if (hm > q) {
+            npb++;
+            hm = q;
+          }
+      }
+      int off = warp_excl_sum(npb, lane);
+      int tot = warp_sum(npb);
+      int64_t pb0 = warp_pebbles(W, tot);
+      if (pb0 < 0) return 1;
+      if (act) {
+        int vi = WVI(k);
+        int64_t s = pb0 + off;
+        while (x <= nak) {
+          if (cells[ha].mark > nak) {
+            cells[s] = {ha, k, dif, nak};
+            ha = (int)s;
+            s += 1;
+          }
+          nak -= tspace;
+        }
+        NA[vi] = nak;
+        Vn[vi] = c;
+        Tn[vi] = b;
+        Mn[vi] = m;
+        HAn[vi] = ha;
+      }
+      uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
+      if (bb) {
+        more = 0;
+        int kk = base + (__ffs(bb) - 1);
+        if (bclip > kk) bclip = kk;
+      }
+      if (ba) {
+        more = 0;
+        aclip = base + last_lane(ba);
+      }
+      int pm = warp_excl_min(act ? c : 2147483647, lane, carry);
+      bool rec = act && c < pm;
+      uint32_t rb = __ballot_sync(FULL, rec);
+      if (rb) {
+        int L = last_lane(rb);
+        carry = __shfl_sync(FULL, c, L);
+        besta = carry;
+        bestx = __shfl_sync(FULL, x, L);
+        bool pa = rec && m >= PATH_AVE;
+        uint32_t pab = __ballot_sync(FULL, pa);
+        if (pab) {
+          lasta = __shfl_sync(FULL, c, last_lane(pab));
+          bool tr = pa && TABLE[b & TRIM_MASK] >= 0 &&
+                    TABLE[(b >> TRIM_LEN) & TRIM_MASK] + SCORE[b & TRIM_MASK] >= 0;
+          uint32_t trb = __ballot_sync(FULL, tr);
+          if (trb) {
+            int T2 = last_lane(trb);
+            trima = __shfl_sync(FULL, c, T2);
+            trimx = __shfl_sync(FULL, x, T2);
+            trimd = dif;
+            trimha = __shfl_sync(FULL, ha, T2);
+          }
+        }
+      }
+    }
+    cur ^= 1;
+    __syncwarp();
+    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
+    if (more == 0) {
+      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
+      if (low <= aclip) {
+        low = aclip + 1;
+        if (morem <= M[WVI(aclip)]) {
+          morem = M[WVI(aclip)];
+          morea = V[WVI(aclip)];
+          morex = (morea + aclip) >> 1;
+          mored = dif;
+          moreha = HA[WVI(aclip)];
+        }
+      }
+      if (hgh >= bclip) {
+        hgh = bclip - 1;
+        if (morem <= M[WVI(bclip)]) {
+          morem = M[WVI(bclip)];
+          morea = V[WVI(bclip)];
+          morex = (morea + bclip) >> 1;
+          mored = dif;
+          moreha = HA[WVI(bclip)];
+        }
+      }
+      aclip = -I32MAX;
+      bclip = I32MAX;
+    }
+    int n = besta + WAVE_LAG;
+    while (hgh >= low)
+      if (V[WVI(hgh)] > n)
+        hgh -= 1;
+      else {
+        while (V[WVI(low)] > n) low += 1;
+        break;
+      }
+  }
+  __syncwarp();
+
+  {
+    uint16_t *atrace = W.points + P.trace_off;
+    int atlen = 0, trimy, a, b, k, h, d, e;
+    if (morem >= 0 && spec.reach) {
+      trimx = morex;
+      trimy = morea - morex;
+      trimd = mored;
+      trimha = moreha;
+    } else
+      trimy = trima - trimx;
+    if (lane == 0) {
+      a = -1;
+      for (h = trimha; h >= 0; h = b) {
+        b = cells[h].ptr;
+        cells[h].ptr = a;
+        a = h;
+      }
+    }
+    __syncwarp();
+    a = __shfl_sync(FULL, a, 0);
+    h = a;
+    k = cells[h].diag;
+    b = cells[h].mark - k;
+    e = 0;
+    if ((b + k) % tspace != aoff) {
+      h = cells[h].ptr;
+      if (h < 0) {
+        a = trimy;
+        d = trimd;
+      } else {
+        k = cells[h].diag;
+        a = cells[h].mark - k;
+        d = cells[h].diff;
+      }
+      if (P.tlen == 0) {
+        if (P.trace_off + atlen - 2 < 0) {
+          W.err |= ALN_ERR_POINTS;
+          return 1;
+        }
+        if (lane == 0) {
+          atrace[atlen - 1] = (uint16_t)(b - a);
+          atrace[atlen - 2] = (uint16_t)(d - e);
+        }
+        atlen -= 2;
+      } else if (lane == 0) {
+        atrace[1] = (uint16_t)(atrace[1] + (b - a));
+        atrace[0] = (uint16_t)(atrace[0] + (d - e));
+      }
+      b = a;
+      e = d;
+    }
+    if (h >= 0) {
+      for (h = cells[h].ptr; h >= 0; h = cells[h].ptr) {
+        k = cells[h].diag;
+        a = cells[h].mark - k;
+        if (P.trace_off + atlen - 2 < 0) {
+          W.err |= ALN_ERR_POINTS;
+          return 1;
+        }
+        d = cells[h].diff;
+        if (lane == 0) {
+          atrace[atlen - 1] = (uint16_t)(b - a);
+          atrace[atlen - 2] = (uint16_t)(d - e);
+        }
+        atlen -= 2;
+        b = a;
+        e = d;
+      }
+      __syncwarp();
+      if (b + k != trimx) {
+        if (P.trace_off + atlen - 2 < 0) {
+          W.err |= ALN_ERR_POINTS;
+          return 1;
+        }
+        if (lane == 0) {
+          atrace[atlen - 1] = (uint16_t)(b - trimy);
+          atrace[atlen - 2] = (uint16_t)(trimd - e);
+        }
+        atlen -= 2;
+      } else if (b != trimy) {
+        if (lane == 0) {
+          atrace[atlen + 1] = (uint16_t)(atrace[atlen + 1] + (b - trimy));
+          atrace[atlen] = (uint16_t)(atrace[atlen] + (trimd - e));
+        }
+      }
+    }
+    __syncwarp();
+    P.abpos = trimx;
+    P.bbpos = trimy;
+    P.diffs = P.diffs + trimd;
+    P.tlen = P.tlen - atlen;
+    P.trace_off = P.trace_off + atlen;
+  }
+  return 0;
+}
+
+#undef WVI
+
+// Local_Alignment, warp version (same control as local_alignment).
+__device__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
+                                 Path &P, int low, int hgh, int anti, int lbord, int hbord) {
+  const int lane = threadIdx.x & 31;
+  int aoff, minp, maxp;
+  bool fshort, rshort;
+  int maxtp = 2 * (A.len / spec.trace_space + 2);
+  if (2 * (int64_t)maxtp > W.point_cap) {
+    W.err |= ALN_ERR_POINTS;
+    return 1;
+  }
+  P.trace_off = maxtp;
+  while (((anti - hgh) >> 1) < 0) hgh -= 1;
+  minp = (lbord < 0) ? -I32MAX : low - lbord;
+  maxp = (hbord < 0) ? I32MAX : hgh + hbord;
+  aoff = acomp ? A.len % spec.trace_space : 0;
+  if (forward_wave_w(W, spec, A, B, P, &low, hgh, anti, minp, maxp, aoff)) return 1;
+  fshort = ((P.aepos + P.bepos) - anti < DUB_TRIM);
+  if (reverse_wave_w(W, spec, A, B, P, low, low, anti, minp, maxp, aoff)) return 1;
+  rshort = (anti - (P.abpos + P.bbpos) < DUB_TRIM);
+  if (fshort) {
+    if (rshort) {
+      P.aepos = P.abpos = (P.abpos + P.aepos) >> 1;
+      P.bepos = P.bbpos = (P.bbpos + P.bepos) >> 1;
+      P.tlen = 0;
+    } else {
+      low = P.abpos - P.bbpos;
+      anti = P.abpos + P.bbpos;
+      P.tlen = 0;
+      if (forward_wave_w(W, spec, A, B, P, &low, low, anti, minp, maxp, aoff)) return 1;
+    }
+  } else if (rshort) {
+    low = P.aepos - P.bepos;
+    anti = P.aepos + P.bepos;
+    P.tlen = 0;
+    P.diffs = 0;
+    if (reverse_wave_w(W, spec, A, B, P, low, low, anti, minp, maxp, aoff)) return 1;
+  }
+  if (acomp) {
+    uint16_t *trace = W.points + P.trace_off;
+    int i = P.abpos;
+    P.abpos = A.len - P.aepos;
+    P.aepos = A.len - i;
+    i = P.bbpos;
+    P.bbpos = B.len - P.bepos;
+    P.bepos = B.len - i;
+    __syncwarp();
+    if (lane == 0) {
+      i = P.tlen - 2;
+      int j = 0;
+      while (j < i) {
+        uint16_t p = trace[i];
+        trace[i] = trace[j];
+        trace[j] = p;
+        p = trace[i + 1];
+        trace[i + 1] = trace[j + 1];
+        trace[j + 1] = p;
+        i -= 2;
+        j += 2;
+      }
+    }
+    __syncwarp();
+  }
+  return 0;
+}
+
+}  // namespace aln
+}  // namespace pga

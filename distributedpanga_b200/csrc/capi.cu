@@ -162,9 +162,13 @@ int sort_buckets(pga_ctx *ctx) {
   ENSURE(ctx->qbig, sizeof(uint32_t) * NPREFIX);
   ENSURE(ctx->qcount, sizeof(uint32_t) * 4);
   CK(cudaMemsetAsync(ctx->qcount.p, 0, sizeof(uint32_t) * 4, ctx->st));
-  k_bucket_small<<<NPREFIX / 256, 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint32_t>(ctx->start),
-                                                      P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
-                                                      P<uint32_t>(ctx->qcount));
+  // prefixes per CTA: a power of two giving about BK_CAP/4 records per CTA on average
+  int bpc = 1;
+  while (bpc < 4096 && (double)ctx->nrec * (bpc * 2) / NPREFIX <= BK_CAP / 4) bpc *= 2;
+  CK(cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, BK_CAP * (int)sizeof(Rec)));
+  k_bucket_rank<<<NPREFIX / bpc, BK_THREADS, BK_CAP * sizeof(Rec), ctx->st>>>(
+      P<Rec>(ctx->rec), P<uint32_t>(ctx->start), bpc, BK_CAP, P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
+      P<uint32_t>(ctx->qcount));
   LAUNCHED(1);
   CK(cudaGetLastError());
   uint32_t q[4];
@@ -210,8 +214,8 @@ int finish_index(pga_ctx *ctx, bool want_entries) {
     ENSURE(ctx->ent, (size_t)n * eb + 16);
     ENSURE(ctx->cum, sizeof(int64_t) * NPREFIX);
     if (n > 0) {
-      k_entries<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n,
-                                                       ctx->posb, ctx->ctgb, P<uint8_t>(ctx->ent));
+      k_entries<<<grid_for(n, OUT_THREADS), OUT_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n,
+                                                                       ctx->posb, ctx->ctgb, P<uint8_t>(ctx->ent));
       LAUNCHED(1);
     }
     cum = P<int64_t>(ctx->cum);

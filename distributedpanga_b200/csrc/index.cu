@@ -213,35 +213,47 @@ __global__ void k_prefix_scatter(const Rec *__restrict__ in, int64_t n, uint32_t
 // or by a batched global-memory bitonic network.
 // ---------------------------------------------------------------------------
 
-__global__ void k_bucket_small(Rec *__restrict__ rec, const uint32_t *__restrict__ start,
-                               uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig,
-                               uint32_t *__restrict__ qcount) {
-  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= NPREFIX) return;
-  uint32_t a = start[p], b = start[p + 1];
-  uint32_t n = b - a;
-  if (n <= 1) return;
-  if (n > BK_SMALL) {
+// One CTA per run of `bpc` consecutive prefixes: the run's records (a
+// contiguous range after the scatter) are staged in shared memory and each
+// record writes itself to bucket start + rank, its rank being the number of
+// records of its bucket that order before it (records are distinct, so the
+// ranks are a permutation).  Buckets larger than BK_RANK_MAX, and every
+// bucket of a run that does not fit in shared memory, are queued for the
+// CTA-per-bucket (<= BK_MEDIUM) or global bitonic sort instead.
+__global__ void __launch_bounds__(BK_THREADS)
+k_bucket_rank(Rec *__restrict__ rec, const uint32_t *__restrict__ start, int bpc, int cap,
+              uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount) {
+  extern __shared__ Rec sm_rec[];
+  const uint32_t p0 = blockIdx.x * (uint32_t)bpc;
+  const uint32_t a = start[p0], b = start[p0 + bpc];
+  const uint32_t m = b - a;
+  if (m == 0) return;
+  const bool fits = m <= (uint32_t)cap;
+  // queue the buckets this kernel does not rank
+  for (uint32_t q = threadIdx.x; q < (uint32_t)bpc; q += BK_THREADS) {
+    uint32_t p = p0 + q;
+    uint32_t n = start[p + 1] - start[p];
+    if (n <= 1) continue;
+    if (fits && n <= BK_RANK_MAX) continue;
     if (n <= BK_MEDIUM) qmed[atomicAdd(&qcount[0], 1u)] = p;
     else {
-      uint32_t q = atomicAdd(&qcount[1], 1u);
-      qbig[q] = p;
+      qbig[atomicAdd(&qcount[1], 1u)] = p;
       atomicMax(&qcount[2], n);
     }
-    return;
   }
-  Rec v[BK_SMALL];
-  for (uint32_t i = 0; i < n; i++) v[i] = rec[a + i];
-  for (uint32_t i = 1; i < n; i++) {
-    Rec x = v[i];
-    int k = (int)i - 1;
-    while (k >= 0 && rec_less(x, v[k])) {
-      v[k + 1] = v[k];
-      k--;
-    }
-    v[k + 1] = x;
+  if (!fits) return;
+  for (uint32_t i = threadIdx.x; i < m; i += BK_THREADS) sm_rec[i] = rec[a + i];
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += BK_THREADS) {
+    Rec x = sm_rec[i];
+    uint32_t p = rec_prefix(x);
+    uint32_t bs = start[p] - a, be = start[p + 1] - a;
+    uint32_t n = be - bs;
+    if (n <= 1 || n > BK_RANK_MAX) continue;
+    uint32_t rank = 0;
+    for (uint32_t j = bs; j < be; j++) rank += rec_less(sm_rec[j], x) ? 1u : 0u;
+    rec[a + bs + rank] = x;
   }
-  for (uint32_t i = 0; i < n; i++) rec[a + i] = v[i];
 }
 
 __device__ __forceinline__ void cswap(Rec &x, Rec &y) {
@@ -323,46 +335,69 @@ __global__ void k_lcp(const Rec *__restrict__ rec, int64_t n, uint8_t *__restric
     lcp[i] = (uint8_t)(i == 0 ? 0 : kmer_lcp(rec[i - 1], rec[i]));
 }
 
+// Writes `nbytes` staged bytes to dst with consecutive threads storing
+// consecutive bytes (so every warp store covers one 32-byte span).
+__device__ __forceinline__ void store_staged(const uint8_t *__restrict__ src, uint8_t *__restrict__ dst,
+                                             int nbytes) {
+  for (int k = threadIdx.x; k < nbytes; k += blockDim.x) dst[k] = src[k];
+}
+
 // Entry layout (src/kmer_adapter.c:60-65): k-mer bytes 3..9, mask 0, LCP,
-// position (posb bytes LE), contig|strand (ctgb bytes LE).
-__global__ void k_entries(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
-                          int posb, int ctgb, uint8_t *__restrict__ ent) {
+// position (posb bytes LE), contig|strand (ctgb bytes LE).  One CTA of
+// OUT_THREADS builds OUT_THREADS entries in shared memory, then stores them.
+__global__ void __launch_bounds__(OUT_THREADS)
+k_entries(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
+          int posb, int ctgb, uint8_t *__restrict__ ent) {
+  __shared__ uint8_t buf[OUT_THREADS * 24];
   const int eb = 9 + posb + ctgb;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    Rec r = rec[i];
-    uint8_t *d = ent + i * eb;
-    // k-mer byte b (0..9): b < 8 from hi, else from the top of lo
+  for (int64_t i0 = (int64_t)blockIdx.x * OUT_THREADS; i0 < n; i0 += (int64_t)gridDim.x * OUT_THREADS) {
+    int64_t i = i0 + threadIdx.x;
+    if (i < n) {
+      Rec r = rec[i];
+      uint8_t *d = buf + threadIdx.x * eb;
 #pragma unroll
-    for (int b = 3; b < 8; b++) d[b - 3] = (uint8_t)(r.hi >> (56 - 8 * b));
-    d[5] = (uint8_t)(r.lo >> 56);
-    d[6] = (uint8_t)(r.lo >> 48);
-    d[7] = 0;
-    d[8] = lcp[i];
-    uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
-    for (int b = 0; b < posb; b++) d[9 + b] = (uint8_t)(pos >> (8 * b));
-    for (int b = 0; b < ctgb; b++) d[9 + posb + b] = (uint8_t)(cs >> (8 * b));
+      for (int b = 3; b < 8; b++) d[b - 3] = (uint8_t)(r.hi >> (56 - 8 * b));
+      d[5] = (uint8_t)(r.lo >> 56);
+      d[6] = (uint8_t)(r.lo >> 48);
+      d[7] = 0;
+      d[8] = lcp[i];
+      uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
+      for (int b = 0; b < posb; b++) d[9 + b] = (uint8_t)(pos >> (8 * b));
+      for (int b = 0; b < ctgb; b++) d[9 + posb + b] = (uint8_t)(cs >> (8 * b));
+    }
+    __syncthreads();
+    int cnt = (int)min((int64_t)OUT_THREADS, n - i0);
+    store_staged(buf, ent + i0 * eb, cnt * eb);
+    __syncthreads();
   }
 }
 
 // Record layout (src/record.h:8-26): LCP, k-mer 10 bytes, mask 0, position,
 // contig|strand.  lcp may be null (extraction order: LCP byte 0).
-__global__ void k_records_out(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
-                              int posb, int ctgb, uint8_t *__restrict__ out) {
+__global__ void __launch_bounds__(OUT_THREADS)
+k_records_out(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
+              int posb, int ctgb, uint8_t *__restrict__ out) {
+  __shared__ uint8_t buf[OUT_THREADS * 24];
   const int rs = 12 + posb + ctgb;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    Rec r = rec[i];
-    uint8_t *d = out + i * rs;
-    d[0] = lcp ? lcp[i] : 0;
+  for (int64_t i0 = (int64_t)blockIdx.x * OUT_THREADS; i0 < n; i0 += (int64_t)gridDim.x * OUT_THREADS) {
+    int64_t i = i0 + threadIdx.x;
+    if (i < n) {
+      Rec r = rec[i];
+      uint8_t *d = buf + threadIdx.x * rs;
+      d[0] = lcp ? lcp[i] : 0;
 #pragma unroll
-    for (int b = 0; b < 8; b++) d[1 + b] = (uint8_t)(r.hi >> (56 - 8 * b));
-    d[9] = (uint8_t)(r.lo >> 56);
-    d[10] = (uint8_t)(r.lo >> 48);
-    d[11] = 0;
-    uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
-    for (int b = 0; b < posb; b++) d[12 + b] = (uint8_t)(pos >> (8 * b));
-    for (int b = 0; b < ctgb; b++) d[12 + posb + b] = (uint8_t)(cs >> (8 * b));
+      for (int b = 0; b < 8; b++) d[1 + b] = (uint8_t)(r.hi >> (56 - 8 * b));
+      d[9] = (uint8_t)(r.lo >> 56);
+      d[10] = (uint8_t)(r.lo >> 48);
+      d[11] = 0;
+      uint64_t pos = r.lo & 0xffffffffu, cs = (r.lo >> 32) & 0xffffu;
+      for (int b = 0; b < posb; b++) d[12 + b] = (uint8_t)(pos >> (8 * b));
+      for (int b = 0; b < ctgb; b++) d[12 + posb + b] = (uint8_t)(cs >> (8 * b));
+    }
+    __syncthreads();
+    int cnt = (int)min((int64_t)OUT_THREADS, n - i0);
+    store_staged(buf, out + i0 * rs, cnt * rs);
+    __syncthreads();
   }
 }
 

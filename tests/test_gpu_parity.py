@@ -118,9 +118,10 @@ def test_sort_matches_property_at_scale(dev):
     rec = dev.index_records()
     assert rec.shape[0] == n
     k = rec[:, 1:11]
-    # lexicographic non-decreasing k-mers
-    v = np.ascontiguousarray(k).view(np.dtype((np.void, 10))).reshape(-1)
-    assert np.all(v[1:] >= v[:-1])
+    # lexicographic non-decreasing k-mers: (first 8 bytes, last 2 bytes) as big-endian integers
+    hi = np.ascontiguousarray(k[:, :8]).view(">u8").reshape(-1)
+    lo = (k[:, 8].astype(np.uint32) << 8) | k[:, 9]
+    assert np.all((hi[1:] > hi[:-1]) | ((hi[1:] == hi[:-1]) & (lo[1:] >= lo[:-1])))
     # LCP = leading equal bases of neighbours
     x = np.bitwise_xor(k[1:], k[:-1])
     first = np.argmax(x != 0, axis=1)
