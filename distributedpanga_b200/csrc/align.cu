@@ -1,0 +1,274 @@
+// Alignment stage on the GPU: every (anchor, partner) contig pair of a unit
+// is one task; a persistent kernel gives each warp the next task (tasks come
+// largest first), and the warp runs FastGA's chain driver and Local_Alignment
+// for it (align_core.cuh, align_warp.cuh), then the pair's sort / elimination
+// / entwine step on lane 0, and appends the surviving alignments.
+//
+// Reference: search_seeds / align_contigs / Local_Alignment
+// (src/fastga_pipeline.c:576-1138, lib/align.c:1423-1576).
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "align.cuh"
+#include "align_warp.cuh"
+#include "seeds.cuh"
+
+namespace pga {
+
+using namespace aln;
+
+struct KeySeeds {
+  const U128 *k;
+  int64_t n;
+  SeedKeyLayout L;
+  __device__ int64_t anti(int64_t i) const { return (int64_t)key_bits(k[i], L.off_anti, L.off_band - L.off_anti); }
+  __device__ int64_t band(int64_t i) const { return (int64_t)key_bits(k[i], L.off_band, L.off_j - L.off_band); }
+  __device__ int lcp(int64_t i) const { return (int)key_bits(k[i], 0, 6); }
+  __device__ int dlow(int64_t i) const { return (int)key_bits(k[i], L.off_dlow, 6); }
+};
+
+struct WarpAligner {
+  WarpWork &W;
+  const AlignSpec &spec;
+  __device__ int call(const Seq &A, const Seq &B, bool acomp, Path &P, int low, int hgh, int anti, int lbord,
+                      int hbord) {
+    return local_alignment_w(W, spec, A, B, acomp, P, low, hgh, anti, lbord, hbord);
+  }
+  __device__ const uint16_t *points() const { return W.points; }
+  __device__ int err() const { return W.err; }
+};
+
+__global__ void __launch_bounds__(ALIGN_THREADS)
+k_align_pairs(AlignLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
+  if (wid >= P.nwarps) return;
+  AlignSpec spec;
+  spec.trace_space = TSPACE;
+  spec.ave_path = P.ave_path;
+  spec.reach = 0;
+  spec.score = P.score;
+  spec.table = P.table;
+
+  WarpWork W;
+  int *wb = P.wave + wid * (int64_t)P.vcap * WAVE_INTS;
+  W.V[0] = wb;
+  W.V[1] = wb + P.vcap;
+  W.M[0] = wb + 2 * P.vcap;
+  W.M[1] = wb + 3 * P.vcap;
+  W.HA[0] = wb + 4 * P.vcap;
+  W.HA[1] = wb + 5 * P.vcap;
+  W.NA = wb + 6 * P.vcap;
+  W.T[0] = (uint64_t *)(wb + 7 * P.vcap);
+  W.T[1] = (uint64_t *)(wb + 9 * P.vcap);
+  W.vcap = P.vcap;
+  W.points = P.points + wid * P.point_cap;
+  W.point_cap = P.point_cap;
+  W.pool.cells = P.cells;
+  W.pool.next = P.cell_next;
+  W.pool.cap = P.cell_cap;
+  W.chunk_next = W.chunk_end = 0;
+
+  OvlArena O;
+  O.ovl = P.ovl + wid * P.ovl_cap;
+  O.perm = P.perm + wid * P.ovl_cap;
+  O.ovl_cap = P.ovl_cap;
+  O.bytes = P.cand_bytes;
+  O.pool_next = P.cand_next;
+  O.pool_cap = P.cand_cap;
+  O.nbyte = O.byte_cap = 0;
+
+  while (true) {
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(P.next_task, 1u);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= (unsigned)P.ntasks) break;
+    const PairTask tk = P.tasks[t];
+    W.err = 0;
+    O.err = 0;
+    const SeedKeyLayout &L = tk.comp ? P.layC : P.layN;
+    KeySeeds S{(tk.comp ? P.keysC : P.keysN) + tk.lo, tk.hi - tk.lo, L};
+    const uint8_t *abuf = tk.comp ? P.rc : P.fwd;
+    Seq A{abuf + P.soff[tk.a], (int)P.clen[tk.a]};
+    Seq B{P.fwd + P.soff[tk.b], (int)P.clen[tk.b]};
+    Path path;
+    path.tlen = path.diffs = path.abpos = path.bbpos = path.aepos = 0;
+    path.bepos = tk.entry_bepos;
+    path.trace_off = 0;
+    PairResult R;
+    WarpAligner AL{W, spec};
+    int rc = align_pair(S, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane, 32);
+    __syncwarp();
+    PairOut po;
+    po.calls = R.calls;
+    po.exit_bepos = R.exit_bepos;
+    po.nsurv = 0;
+    po.rec_off = 0;
+    po.err = rc ? (W.err | O.err | 0x100) : 0;
+    if (rc == 0) {
+      if (lane == 0) finish_pair(O);
+      __syncwarp();
+      int ferr = __shfl_sync(FULL, O.err, 0);
+      if (ferr) po.err = ferr | 0x200;
+    }
+    if (po.err == 0) {
+      // survivors in the pair's output order (perm order)
+      int ns = 0;
+      int64_t tb = 0;
+      if (lane == 0)
+        for (int64_t q = 0; q < O.nov; q++) {
+          const Ovl &o = O.ovl[O.perm[q]];
+          if (o.flags & ELIMINATED) continue;
+          ns++;
+          tb += o.tlen;
+        }
+      ns = __shfl_sync(FULL, ns, 0);
+      tb = __shfl_sync(FULL, tb, 0);
+      unsigned long long r0 = 0, b0 = 0;
+      if (lane == 0 && ns > 0) {
+        r0 = atomicAdd(P.rec_next, (unsigned long long)ns);
+        b0 = atomicAdd(P.out_next, (unsigned long long)tb);
+      }
+      r0 = __shfl_sync(FULL, r0, 0);
+      b0 = __shfl_sync(FULL, b0, 0);
+      if (ns > 0 && ((int64_t)(r0 + ns) > P.rec_cap || (int64_t)(b0 + tb) > P.out_cap)) {
+        po.err = ALN_ERR_OVLS | 0x400;
+      } else if (ns > 0) {
+        int64_t rr = (int64_t)r0, bb = (int64_t)b0;
+        int rank = 0;
+        for (int64_t q = 0; q < O.nov; q++) {
+          const Ovl o = O.ovl[O.perm[q]];
+          if (o.flags & ELIMINATED) continue;
+          if (lane == 0) {
+            AlnRec &a = P.recs[rr];
+            a.aread = tk.a;
+            a.bread = tk.b;
+            a.comp = tk.comp;
+            a.abpos = o.abpos;
+            a.aepos = o.aepos;
+            a.bbpos = o.bbpos;
+            a.bepos = o.bepos;
+            a.diffs = o.diffs;
+            a.tlen = o.tlen;
+            a.rank = rank;
+            a.toff = bb;
+          }
+          for (int q2 = lane; q2 < o.tlen; q2 += 32) P.out_bytes[bb + q2] = P.cand_bytes[o.toff + q2];
+          rr++;
+          bb += o.tlen;
+          rank++;
+        }
+        po.nsurv = ns;
+        po.rec_off = (int64_t)r0;
+      }
+    }
+    if (lane == 0) P.pout[t] = po;
+    __syncwarp();
+  }
+}
+
+// NUMERIC copies of every contig, each between sentinel bytes (value 4):
+// fwd holds the contig, rc its reverse complement (Complement_Seq,
+// lib/align.c:4082), both starting at soff[c].
+__global__ void k_numeric(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
+                          const int64_t *__restrict__ boff, const int64_t *__restrict__ soff, int ncontig,
+                          uint8_t *__restrict__ fwd, uint8_t *__restrict__ rc) {
+  int c = blockIdx.y;
+  if (c >= ncontig) return;
+  int64_t n = clen[c], o = soff[c];
+  const uint8_t *cb = bps + boff[c];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint8_t b = (cb[i >> 2] >> (2 * (i & 3))) & 3;
+    fwd[o + i] = b;
+    rc[o + (n - 1 - i)] = 3 - b;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    fwd[o - 1] = fwd[o + n] = 4;
+    rc[o - 1] = rc[o + n] = 4;
+  }
+}
+
+// Pair boundaries of a sorted key array: flag[i] = 1 where (icont, jcont)
+// differs from key i-1.
+__global__ void k_pair_flags(const U128 *__restrict__ keys, int64_t n, SeedKeyLayout L, uint32_t *__restrict__ flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t f = 1;
+    if (i > 0) {
+      uint64_t a = key_bits(keys[i], L.off_j, L.w_i + (L.off_i - L.off_j));
+      uint64_t b = key_bits(keys[i - 1], L.off_j, L.w_i + (L.off_i - L.off_j));
+      f = a != b;
+    }
+    flag[i] = f;
+  }
+}
+
+// Compact the pair starts: pos[idx[i]] = i where flag[i]; also the pair's
+// anchor and partner.
+__global__ void k_pair_starts(const U128 *__restrict__ keys, int64_t n, SeedKeyLayout L,
+                              const uint32_t *__restrict__ flag, const uint32_t *__restrict__ idx,
+                              int64_t *__restrict__ start, int32_t *__restrict__ ab) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    uint32_t p = idx[i];
+    start[p] = i;
+    ab[2 * p] = (int32_t)key_bits(keys[i], L.off_i, L.w_i);
+    ab[2 * p + 1] = (int32_t)key_bits(keys[i], L.off_j, L.off_i - L.off_j);
+  }
+}
+
+// Base counts (A, C, G, T) over all contigs with sequence.
+__global__ void k_base_counts(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
+                              const int64_t *__restrict__ boff, int ncontig, unsigned long long *__restrict__ cnt) {
+  __shared__ unsigned long long sc[4];
+  if (threadIdx.x < 4) sc[threadIdx.x] = 0;
+  __syncthreads();
+  int c = blockIdx.y;
+  unsigned long long l[4] = {0, 0, 0, 0};
+  if (c < ncontig && boff[c] >= 0) {
+    int64_t n = clen[c];
+    const uint8_t *cb = bps + boff[c];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      l[(cb[i >> 2] >> (2 * (i & 3))) & 3]++;
+  }
+  for (int q = 0; q < 4; q++) {
+    unsigned long long v = l[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sc[q], v);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) atomicAdd(&cnt[threadIdx.x], sc[threadIdx.x]);
+}
+
+void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *boff, int ncontig,
+                        unsigned long long *cnt, cudaStream_t st) {
+  if (ncontig <= 0) return;
+  dim3 g(16, ncontig);
+  k_base_counts<<<g, 256, 0, st>>>(bps, clen, boff, ncontig, cnt);
+}
+
+void launch_align(const AlignLaunch &P, int grid, cudaStream_t st) {
+  k_align_pairs<<<grid, ALIGN_THREADS, 0, st>>>(P);
+}
+
+void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,
+                    uint8_t *fwd, uint8_t *rc, cudaStream_t st) {
+  if (ncontig <= 0) return;
+  dim3 g(64, ncontig);
+  k_numeric<<<g, 256, 0, st>>>(bps, clen, boff, soff, ncontig, fwd, rc);
+}
+
+void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st) {
+  if (n <= 0) return;
+  int g = (int)((n + 255) / 256);
+  if (g > 148 * 32) g = 148 * 32;
+  k_pair_flags<<<g, 256, 0, st>>>(keys, n, L, flag);
+}
+
+void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint32_t *flag, const uint32_t *idx,
+                        int64_t *start, int32_t *ab, cudaStream_t st) {
+  if (n <= 0) return;
+  int g = (int)((n + 255) / 256);
+  if (g > 148 * 32) g = 148 * 32;
+  k_pair_starts<<<g, 256, 0, st>>>(keys, n, L, flag, idx, start, ab);
+}
+
+}  // namespace pga

@@ -1,0 +1,75 @@
+// Alignment-stage launch description and records (align.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "align_core.cuh"
+#include "common.cuh"
+#include "seeds.cuh"
+
+namespace pga {
+
+constexpr int ALIGN_THREADS = 128;  // 4 warps per CTA, one pair per warp at a time
+constexpr int WAVE_INTS = 11;       // per diagonal slot: V,M,HA x2, NA, T x2 (uint64)
+
+// One (anchor, partner) pair of a unit: seeds [lo, hi) of the unit's sorted keys.
+struct PairTask {
+  int comp, a, b, self, entry_bepos, pad;
+  int64_t lo, hi;
+};
+
+struct PairOut {
+  int calls, exit_bepos, nsurv, err;
+  int64_t rec_off;
+};
+
+// One surviving alignment; trace bytes (uint8 pairs: diffs, b-delta per
+// trace interval) at toff in the output byte array.
+struct AlnRec {
+  int aread, bread, comp, abpos, aepos, bbpos, bepos, diffs, tlen, rank;
+  int64_t toff;
+};
+
+struct AlignLaunch {
+  const PairTask *tasks;
+  int ntasks;
+  unsigned *next_task;
+  const U128 *keysN, *keysC;
+  SeedKeyLayout layN, layC;
+  const uint8_t *fwd, *rc;
+  const int64_t *soff, *clen;
+  const int16_t *score, *table;
+  int ave_path;
+  int64_t amxpos, maxdag;
+  int64_t nwarps;
+  int *wave;
+  int vcap;
+  uint16_t *points;
+  int64_t point_cap;
+  aln::Pebble *cells;
+  unsigned long long *cell_next;
+  int64_t cell_cap;
+  aln::Ovl *ovl;
+  int *perm;
+  int64_t ovl_cap;
+  uint8_t *cand_bytes;
+  unsigned long long *cand_next;
+  int64_t cand_cap;
+  PairOut *pout;
+  AlnRec *recs;
+  unsigned long long *rec_next;
+  int64_t rec_cap;
+  uint8_t *out_bytes;
+  unsigned long long *out_next;
+  int64_t out_cap;
+};
+
+void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
+void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *boff, int ncontig,
+                        unsigned long long *cnt, cudaStream_t st);
+void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,
+                    uint8_t *fwd, uint8_t *rc, cudaStream_t st);
+void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st);
+void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint32_t *flag, const uint32_t *idx,
+                        int64_t *start, int32_t *ab, cudaStream_t st);
+
+}  // namespace pga

@@ -796,6 +796,30 @@ struct OvlArena {
   int64_t nov;    // candidates so far
   int64_t nbyte;  // trace bytes used
   int err;
+  // Device pool mode: bytes is a pool shared by all warps and [nbyte,
+  // byte_cap) this warp's current chunk, refilled from *pool_next.
+  unsigned long long *pool_next;
+  int64_t pool_cap;
+
+  // Room for `need` more bytes.  In pool mode `warp` says whether all 32
+  // lanes call this together (else one thread does).
+  PGA_HD bool reserve(int64_t need, bool warp) {
+    if (nbyte + need <= byte_cap) return true;
+    if (pool_next == nullptr) return false;
+#if defined(__CUDA_ARCH__)
+    int64_t want = need > (1 << 16) ? need : (1 << 16);
+    unsigned long long b0 = 0;
+    if (!warp || (threadIdx.x & 31) == 0) b0 = atomicAdd(pool_next, (unsigned long long)want);
+    if (warp) b0 = __shfl_sync(0xffffffffu, b0, 0);
+    if ((int64_t)b0 + want > pool_cap) return false;
+    nbyte = (int64_t)b0;
+    byte_cap = (int64_t)b0 + want;
+    return true;
+#else
+    (void)warp;
+    return false;
+#endif
+  }
 };
 
 constexpr int ELIMINATED = 0x4;
@@ -927,7 +951,7 @@ PGA_HD void finish_pair(OvlArena &O) {
         int ocut = 2 * (((where - o.abpos) - 1) / TSPACE + 1);
         int wcut = 2 * (((where - w.abpos) - 1) / TSPACE + 1);
         int ntlen = ocut + (w.tlen - wcut);
-        if (O.nbyte + ntlen > O.byte_cap) {
+        if (!O.reserve(ntlen, false)) {
           O.err |= ALN_ERR_TRACE;
           return;
         }
@@ -1024,7 +1048,7 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
   R.nlas = 0;
   R.exit_bepos = path.bepos;
   O.nov = 0;
-  O.nbyte = 0;
+  if (O.pool_next == nullptr) O.nbyte = 0;
   if (n == 0) return 0;
 
   int64_t b = 0, e = 0, m;
@@ -1125,7 +1149,7 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
                     O.err |= ALN_ERR_OVLS;
                     return 1;
                   }
-                  if (O.nbyte + path.tlen > O.byte_cap) {
+                  if (!O.reserve(path.tlen, nl > 1)) {
                     O.err |= ALN_ERR_TRACE;
                     return 1;
                   }

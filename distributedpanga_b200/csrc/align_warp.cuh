@@ -127,16 +127,19 @@ __device__ __forceinline__ int last_lane(uint32_t ballot) { return ballot ? 31 -
 // Forward snake along diagonal k from a-position x (bases equal, neither a
 // sentinel).  Compares 8 bytes at a time; stops exactly where the byte loop
 // of the reference stops and reports which sentinel (if any) stopped it.
-__device__ __forceinline__ int snake_fwd(const uint8_t *aseq, const uint8_t *bseq, int x, int k, int *hitb,
-                                         int *hita) {
+// Reads outside [-1, len] of either sequence count as its sentinel: legal
+// inputs never get there, and a wrong start can then not run off the buffers.
+__device__ __forceinline__ int snake_fwd(const uint8_t *aseq, const uint8_t *bseq, int alen, int blen, int x, int k,
+                                         int *hitb, int *hita) {
   *hitb = *hita = 0;
   while (1) {
-    int c = bseq[x - k];
+    int y = x - k;
+    int c = (y < -1 || y > blen) ? 4 : bseq[y];
     if (c == 4) {
       *hitb = 1;
       return x;
     }
-    int d = aseq[x];
+    int d = (x < -1 || x > alen) ? 4 : aseq[x];
     if (c != d) {
       if (d == 4) *hita = 1;
       return x;
@@ -145,16 +148,18 @@ __device__ __forceinline__ int snake_fwd(const uint8_t *aseq, const uint8_t *bse
   }
 }
 
-__device__ __forceinline__ int snake_rev(const uint8_t *aseq, const uint8_t *bseq, int x, int k, int *hitb,
-                                         int *hita) {
+// (aseq, bseq here start one position left: valid indices 0..len+1)
+__device__ __forceinline__ int snake_rev(const uint8_t *aseq, const uint8_t *bseq, int alen, int blen, int x, int k,
+                                         int *hitb, int *hita) {
   *hitb = *hita = 0;
   while (1) {
-    int c = bseq[x - k];
+    int y = x - k;
+    int c = (y < 0 || y > blen + 1) ? 4 : bseq[y];
     if (c == 4) {
       *hitb = 1;
       return x;
     }
-    int d = aseq[x];
+    int d = (x < 0 || x > alen + 1) ? 4 : aseq[x];
     if (c != d) {
       if (d == 4) *hita = 1;
       return x;
@@ -197,6 +202,8 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   trimd = mored = 0;
   trimha = moreha = 0;
   morem = -1;
+  int64_t call_base = -1;  // this call's first pebble: the reference's cells[0]
+  const int max_waves = A.len + B.len + 1024;
 
   // 0-wave: diagonals visited hgh..low
   for (int base = hgh; base >= low; base -= 32) {
@@ -206,7 +213,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     if (act) {
       x = (mida + k) >> 1;
       na = ((x + (tspace - aoff)) / tspace - 1) * tspace + aoff;
-      x = snake_fwd(aseq, bseq, x, k, &hb, &ha_);
+      x = snake_fwd(aseq, bseq, A.len, B.len, x, k, &hb, &ha_);
       c = (x << 1) - k;
       npb = 1;
       for (int q = na + tspace; x >= q; q += tspace) npb++;
@@ -215,6 +222,10 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     int tot = warp_sum(npb);
     int64_t pb0 = warp_pebbles(W, tot);
     if (pb0 < 0) return 1;
+    if (call_base < 0) {
+      call_base = pb0;
+      trimha = moreha = (int)pb0;
+    }
     int ha = -1;
     if (act) {
       int64_t s = pb0 + off;
@@ -285,6 +296,10 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   }
 
   while (more && lasta >= besta - TRIM_MLAG) {
+    if (dif > max_waves) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
     low -= 1;
     hgh += 1;
     if (hgh - low + 3 > W.vcap) {
@@ -348,7 +363,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         b <<= 1;
         x = (c + k) >> 1;
         int x0 = x;
-        x = snake_fwd(aseq, bseq, x, k, &hb, &hA);
+        x = snake_fwd(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
         int run = x - x0;
         // the reference shifts a 1 into b per matched base and counts m up while the top bit is clear
         for (int r = 0; r < run; r++) {
@@ -472,13 +487,23 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     } else
       trimy = trima - trimx;
     // reverse the pebble chain: done by lane 0, read back by all
+    int bad = 0;
     if (lane == 0) {
+      int64_t steps = 0, lim = W.chunk_next - call_base + 1;
       a = -1;
       for (h = trimha; h >= 0; h = b) {
+        if (h < call_base || ++steps > lim) {
+          bad = 1;
+          break;
+        }
         b = cells[h].ptr;
         cells[h].ptr = a;
         a = h;
       }
+    }
+    if (__shfl_sync(FULL, bad, 0)) {
+      W.err |= ALN_ERR_CELLS;
+      return 1;
     }
     __syncwarp();
     a = __shfl_sync(FULL, a, 0);
@@ -563,6 +588,8 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   trimd = mored = 0;
   trimha = moreha = 0;
   morem = -1;
+  int64_t call_base = -1;  // this call's first pebble: the reference's cells[0]
+  const int max_waves = A.len + B.len + 1024;
 
   for (int base = low; base <= hgh; base += 32) {
     int k = base + lane;
@@ -572,7 +599,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       x = (mida + k) >> 1;
       x0 = x;
       na = ((x + (tspace - aoff) - 1) / tspace - 1) * tspace + aoff;
-      x = snake_rev(aseq, bseq, x, k, &hb, &hA);
+      x = snake_rev(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
       c = (x << 1) - k;
       npb = 1;
       for (int q = na; x <= q; q -= tspace) npb++;
@@ -581,6 +608,10 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     int tot = warp_sum(npb);
     int64_t pb0 = warp_pebbles(W, tot);
     if (pb0 < 0) return 1;
+    if (call_base < 0) {
+      call_base = pb0;
+      trimha = moreha = (int)pb0;
+    }
     int ha = -1;
     if (act) {
       int64_t s = pb0 + off;
@@ -649,6 +680,10 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   }
 
   while (more && lasta <= besta + TRIM_MLAG) {
+    if (dif > max_waves) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
     low -= 1;
     hgh += 1;
     if (hgh - low + 3 > W.vcap) {
@@ -709,7 +744,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         b <<= 1;
         x = (c + k) >> 1;
         int x0 = x;
-        x = snake_rev(aseq, bseq, x, k, &hb, &hA);
+        x = snake_rev(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
         int run = x0 - x;
         for (int r = 0; r < run; r++) {
           if ((b & PATH_TOP) == 0) m += 1;
@@ -829,13 +864,23 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       trimha = moreha;
     } else
       trimy = trima - trimx;
+    int bad = 0;
     if (lane == 0) {
+      int64_t steps = 0, lim = W.chunk_next - call_base + 1;
       a = -1;
       for (h = trimha; h >= 0; h = b) {
+        if (h < call_base || ++steps > lim) {
+          bad = 1;
+          break;
+        }
         b = cells[h].ptr;
         cells[h].ptr = a;
         a = h;
       }
+    }
+    if (__shfl_sync(FULL, bad, 0)) {
+      W.err |= ALN_ERR_CELLS;
+      return 1;
     }
     __syncwarp();
     a = __shfl_sync(FULL, a, 0);

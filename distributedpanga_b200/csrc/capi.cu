@@ -15,6 +15,8 @@
 #include "radix.cuh"
 #include "scan.cuh"
 #include "seeds.cuh"
+#include "align.cuh"
+#include "align_spec.h"
 #include "../../include/pga_b200.h"
 
 using namespace pga;
@@ -68,6 +70,18 @@ struct pga_ctx {
   U128 *sorted[2] = {nullptr, nullptr};
   SeedKeyLayout lay[2];
   bool have_diag[2] = {false, false};
+
+  // alignment
+  float base_freq[4] = {.25f, .25f, .25f, .25f};
+  bool freq_set = false;
+  bool have_numeric = false;
+  DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
+      cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab;
+  std::vector<AlnRec> h_recs;      // survivors in la_sort order
+  std::vector<uint8_t> h_trace;    // their trace bytes
+  std::vector<int64_t> h_toff;     // offsets into h_trace
+  int64_t align_stats[8] = {0};    // pairs, self pairs, calls, candidates, survivors, rounds, reruns, 0
+  bool have_align = false;
 
   // generic byte staging
   DBuf io, io2;
@@ -480,6 +494,397 @@ int copy_seeds(pga_ctx *ctx, int comp, uint8_t *out, int64_t *buck) {
   return PGA_OK;
 }
 
+
+// ---- alignment ------------------------------------------------------------------
+
+// FastGA's order of contigs (the .gix permutation: longest first, equal
+// lengths in contig order -- GIXmake's qsort on length, which glibc runs as a
+// stable merge sort) and the self-pair entry rules of src/fastga_order_core.c.
+struct FastgaOrder {
+  int n = 0;
+  std::vector<int> at, pos, range_start;
+};
+
+int64_t fo_key(int pos_b, int bepos) { return (((int64_t)(pos_b + 1)) << 32) | (uint32_t)bepos; }
+
+// fo_compute_ranges (src/fastga_order_core.c:50-140) restated.
+void fo_ranges(int n, const std::vector<int64_t> &clen_pos, int64_t npost, const std::vector<int64_t> &seeds,
+               int64_t swide, int T, std::vector<int> &range_start) {
+  std::vector<int> split(T + 1, 0);
+  int p = 0, r = T;
+  int64_t t = npost / T, cum = n > 0 ? clen_pos[0] : 0;
+  for (int x = 1; x < n; x++) {
+    if (cum >= t && x >= r) {
+      p += 1;
+      split[p] = x;
+      t = (npost * (p + 1)) / T;
+      r += T;
+    }
+    cum += clen_pos[x];
+  }
+  int nparts = p + 1;
+  split[nparts] = n;
+  range_start.resize(n);
+  for (int x = 0; x < n; x++) range_start[x] = x;
+  for (int i = 0; i < nparts; i++) {
+    int64_t asize = 0;
+    for (int x = split[i]; x < split[i + 1]; x++) asize += seeds[x] * swide;
+    if (asize == 0) continue;
+    int k = 0, beg, x;
+    int64_t thr = asize / T, sum = 0;
+    for (x = split[i]; x < split[i + 1]; x++)
+      if (seeds[x] > 0) break;
+    beg = x;
+    for (; x < split[i + 1]; x++)
+      if (seeds[x] > 0) {
+        sum += seeds[x] * swide;
+        if (sum >= thr) {
+          for (int y = beg; y <= x; y++) range_start[y] = beg;
+          k += 1;
+          thr = (asize * (k + 1)) / T;
+          beg = x + 1;
+        }
+      }
+  }
+}
+
+int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &tasks, std::vector<PairOut> &outs) {
+  outs.assign(tasks.size(), PairOut{});
+  if (tasks.empty()) return PGA_OK;
+  ENSURE(ctx->tasks, sizeof(PairTask) * tasks.size());
+  ENSURE(ctx->pout, sizeof(PairOut) * tasks.size());
+  CK(cudaMemcpyAsync(ctx->tasks.p, tasks.data(), sizeof(PairTask) * tasks.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
+  L.tasks = P<PairTask>(ctx->tasks);
+  L.ntasks = (int)tasks.size();
+  L.pout = P<PairOut>(ctx->pout);
+  int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
+  launch_align(L, grid, ctx->st);
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(outs.data(), ctx->pout.p, sizeof(PairOut) * tasks.size(), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (size_t i = 0; i < outs.size(); i++)
+    if (outs[i].err)
+      return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
+                  tasks[i].a, tasks[i].b, tasks[i].comp ? "C" : "N", outs[i].err);
+  return PGA_OK;
+}
+
+int run_align(pga_ctx *ctx) {
+  const int nc = ctx->ncontig;
+  int64_t maxctg = ctx->maxctg;
+  // 1. the two units must be diagonal-sorted
+  for (int comp = 0; comp < 2; comp++)
+    if (!ctx->have_diag[comp]) {
+      int64_t cnt;
+      int sw;
+      int r = pga_diag_sort(ctx, comp, &sw, &cnt);
+      if (r) return r;
+    }
+  // 2. NUMERIC sequences and base frequencies
+  if (!ctx->have_numeric) {
+    std::vector<int64_t> so(nc + 1);
+    int64_t o = 1;
+    for (int c = 0; c < nc; c++) {
+      so[c] = o;
+      o += ctx->clen[c] + 1;
+    }
+    so[nc] = o;
+    ENSURE(ctx->numf, o + 16);
+    ENSURE(ctx->numr, o + 16);
+    ENSURE(ctx->soff, sizeof(int64_t) * (nc + 1));
+    CK(cudaMemcpyAsync(ctx->soff.p, so.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, ctx->st));
+    launch_numeric(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen), P<int64_t>(ctx->dboff), P<int64_t>(ctx->soff), nc,
+                   P<uint8_t>(ctx->numf), P<uint8_t>(ctx->numr), ctx->st);
+    LAUNCHED(1);
+    if (!ctx->freq_set) {
+      ENSURE(ctx->u64tmp, 64);
+      CK(cudaMemsetAsync(ctx->u64tmp.p, 0, 32, ctx->st));
+      launch_base_counts(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen), P<int64_t>(ctx->dboff), nc,
+                         P<unsigned long long>(ctx->u64tmp), ctx->st);
+      LAUNCHED(1);
+      unsigned long long cnt[4];
+      CK(cudaMemcpyAsync(cnt, ctx->u64tmp.p, 32, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+      unsigned long long tot = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+      for (int q = 0; q < 4; q++) ctx->base_freq[q] = tot ? (float)((1. * cnt[q]) / tot) : .25f;
+    }
+    ctx->have_numeric = true;
+  }
+  std::vector<int16_t> tab(2 * 32768);
+  int ave_path = aln::build_align_spec(ctx->base_freq, tab.data(), tab.data() + 32768);
+  ENSURE(ctx->spec_tab, sizeof(int16_t) * tab.size());
+  CK(cudaMemcpyAsync(ctx->spec_tab.p, tab.data(), sizeof(int16_t) * tab.size(), cudaMemcpyHostToDevice, ctx->st));
+
+  // 3. pair lists of both units
+  std::vector<PairTask> pairs[2];
+  for (int comp = 0; comp < 2; comp++) {
+    int64_t n = ctx->nseed[comp];
+    if (n == 0) continue;
+    ENSURE(ctx->pflag, sizeof(uint32_t) * (n + 1));
+    ENSURE(ctx->pidx, sizeof(uint32_t) * (n + 1));
+    ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(n + 1) + 64);
+    ENSURE(ctx->u64tmp, 64);
+    launch_pair_flags(ctx->sorted[comp], n, ctx->lay[comp], P<uint32_t>(ctx->pflag), ctx->st);
+    uint32_t *tot = P<uint32_t>(ctx->u64tmp);
+    CK(exclusive_scan<uint32_t>(P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), n, P<uint32_t>(ctx->scan_tmp), tot,
+                                ctx->st));
+    LAUNCHED(4);
+    uint32_t np = 0;
+    CK(cudaMemcpyAsync(&np, tot, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ENSURE(ctx->pstart, sizeof(int64_t) * (np + 1));
+    ENSURE(ctx->pab, sizeof(int32_t) * 2 * (np + 1));
+    launch_pair_starts(ctx->sorted[comp], n, ctx->lay[comp], P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
+                       P<int64_t>(ctx->pstart), P<int32_t>(ctx->pab), ctx->st);
+    LAUNCHED(1);
+    std::vector<int64_t> st(np);
+    std::vector<int32_t> ab(2 * np);
+    CK(cudaMemcpyAsync(st.data(), ctx->pstart.p, sizeof(int64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ab.data(), ctx->pab.p, sizeof(int32_t) * 2 * np, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (uint32_t p = 0; p < np; p++) {
+      PairTask t;
+      t.comp = comp;
+      t.a = ab[2 * p];
+      t.b = ab[2 * p + 1];
+      t.self = (comp == 0 && t.a == t.b);
+      t.entry_bepos = 0;
+      t.pad = 0;
+      t.lo = st[p];
+      t.hi = (p + 1 < np) ? st[p + 1] : n;
+      pairs[comp].push_back(t);
+    }
+  }
+
+  // 4. work spaces
+  AlignLaunch L;
+  memset(&L, 0, sizeof(L));
+  L.keysN = ctx->sorted[0];
+  L.keysC = ctx->sorted[1];
+  L.layN = ctx->lay[0];
+  L.layC = ctx->lay[1];
+  L.fwd = P<uint8_t>(ctx->numf);
+  L.rc = P<uint8_t>(ctx->numr);
+  L.soff = P<int64_t>(ctx->soff);
+  L.clen = P<int64_t>(ctx->dclen);
+  L.score = P<int16_t>(ctx->spec_tab);
+  L.table = P<int16_t>(ctx->spec_tab) + 32768;
+  L.ave_path = ave_path;
+  L.amxpos = maxctg;
+  L.maxdag = 2 * maxctg;
+  L.nwarps = 148 * 16;
+  L.vcap = 8192;
+  L.point_cap = 4 * (maxctg / 100 + 4) + 64;
+  L.ovl_cap = 16384;
+  L.cell_cap = (int64_t)1 << 30;   // 16 GB of pebbles
+  L.cand_cap = (int64_t)4 << 30;   // 4 GB of candidate traces
+  L.rec_cap = (int64_t)1 << 24;    // 16M surviving alignments
+  L.out_cap = (int64_t)2 << 30;    // 2 GB of surviving traces
+  ENSURE(ctx->task_next, 64);
+  ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
+  ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
+  ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * L.ovl_cap);
+  ENSURE(ctx->perm, sizeof(int) * (size_t)L.nwarps * L.ovl_cap);
+  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)L.cell_cap);
+  ENSURE(ctx->cand, (size_t)L.cand_cap);
+  ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)L.rec_cap);
+  ENSURE(ctx->outb, (size_t)L.out_cap);
+  ENSURE(ctx->cell_next, 64);
+  ENSURE(ctx->cand_next, 64);
+  ENSURE(ctx->rec_next, 64);
+  ENSURE(ctx->out_next, 64);
+  CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
+  CK(cudaMemsetAsync(ctx->cand_next.p, 0, 8, ctx->st));
+  CK(cudaMemsetAsync(ctx->rec_next.p, 0, 8, ctx->st));
+  CK(cudaMemsetAsync(ctx->out_next.p, 0, 8, ctx->st));
+  L.next_task = P<unsigned>(ctx->task_next);
+  L.wave = P<int>(ctx->wave);
+  L.points = P<uint16_t>(ctx->points);
+  L.ovl = P<aln::Ovl>(ctx->ovl);
+  L.perm = P<int>(ctx->perm);
+  L.cells = P<aln::Pebble>(ctx->cells);
+  L.cell_next = P<unsigned long long>(ctx->cell_next);
+  L.cand_bytes = P<uint8_t>(ctx->cand);
+  L.cand_next = P<unsigned long long>(ctx->cand_next);
+  L.recs = P<AlnRec>(ctx->recs);
+  L.rec_next = P<unsigned long long>(ctx->rec_next);
+  L.out_bytes = P<uint8_t>(ctx->outb);
+  L.out_next = P<unsigned long long>(ctx->out_next);
+
+  // 5. launch 1: every pair that does not read a leftover value (all C pairs,
+  // every N pair of two different contigs), largest first
+  std::vector<PairTask> first;
+  std::vector<int> self_idx;
+  for (int comp = 0; comp < 2; comp++)
+    for (size_t i = 0; i < pairs[comp].size(); i++) {
+      if (pairs[comp][i].self) self_idx.push_back((int)i);
+      else first.push_back(pairs[comp][i]);
+    }
+  std::stable_sort(first.begin(), first.end(),
+                   [](const PairTask &x, const PairTask &y) { return (x.hi - x.lo) > (y.hi - y.lo); });
+  std::vector<PairOut> out1;
+  int r = align_run_tasks(ctx, L, first, out1);
+  if (r) return r;
+  int64_t calls = 0;
+  for (auto &o : out1) calls += o.calls;
+
+  // 6. self pairs: entry values by FastGA's order (src/fastga_order.c)
+  int64_t nrounds = 0;
+  if (!self_idx.empty()) {
+    FastgaOrder F;
+    F.n = nc;
+    F.at.resize(nc);
+    for (int i = 0; i < nc; i++) F.at[i] = i;
+    std::stable_sort(F.at.begin(), F.at.end(), [&](int x, int y) { return ctx->clen[x] > ctx->clen[y]; });
+    F.pos.resize(nc);
+    for (int i = 0; i < nc; i++) F.pos[F.at[i]] = i;
+    std::vector<int64_t> nseeds(nc, 0);
+    for (auto &t : pairs[0]) nseeds[t.a] += t.hi - t.lo;
+    std::vector<int64_t> clen_pos(nc), seeds_pos(nc);
+    int64_t seqtot = 0;
+    for (int i = 0; i < nc; i++) {
+      clen_pos[i] = ctx->clen[F.at[i]];
+      seeds_pos[i] = nseeds[F.at[i]];
+      seqtot += ctx->clen[i];
+    }
+    int swide = 2 * ctx->lay[0].dbyte + ctx->ctgb + 2;
+    fo_ranges(nc, clen_pos, seqtot, seeds_pos, swide, 32, F.range_start);
+    // results of the N pairs of two contigs, by anchor position
+    std::vector<std::vector<std::pair<int, int>>> earlier(nc);  // per xa: (xb, answer)
+    std::vector<int64_t> Lk(nc, 0);
+    for (size_t i = 0; i < first.size(); i++) {
+      const PairTask &t = first[i];
+      if (t.comp) continue;
+      int xa = F.pos[t.a], xb = F.pos[t.b];
+      if (out1[i].calls > 0) {
+        int64_t key = fo_key(xb, out1[i].exit_bepos);
+        if (key > Lk[xa]) Lk[xa] = key;
+      }
+      if (xb < xa) earlier[xa].push_back({xb, out1[i].calls > 0 ? out1[i].exit_bepos : -2});
+    }
+    const int UNSET_MAIN = 32767;
+    auto unset = [&](int rs) { return rs == 0 ? UNSET_MAIN : 0; };
+    std::vector<int64_t> S(nc, 0);  // 0 none, 1 pending, 2 no call, 3+bepos called
+    std::vector<int> val(self_idx.size(), 0), state(self_idx.size(), 0);  // 0 undetermined, 1 known
+    for (size_t q = 0; q < self_idx.size(); q++) {
+      const PairTask &t = pairs[0][self_idx[q]];
+      int x = F.pos[t.a];
+      S[x] = 1;
+      auto &e = earlier[x];
+      std::sort(e.begin(), e.end(), [](const std::pair<int, int> &u, const std::pair<int, int> &v) {
+        return u.first > v.first;  // nearest (latest) earlier partner first
+      });
+      bool found = false;
+      for (auto &pr : e)
+        if (pr.second >= 0) {
+          val[q] = pr.second;
+          found = true;
+          break;
+        }
+      if (found) state[q] = 1;
+      else if (F.range_start[x] == x) {
+        val[q] = unset(F.range_start[x]);
+        state[q] = 1;
+      }
+    }
+    std::vector<char> done(self_idx.size(), 0);
+    while (true) {
+      std::vector<PairTask> batch;
+      std::vector<size_t> bq;
+      for (size_t q = 0; q < self_idx.size(); q++) {
+        if (done[q]) continue;
+        if (!state[q]) {
+          // fo_from_rows (src/fastga_order_core.c:167-192)
+          const PairTask &t = pairs[0][self_idx[q]];
+          int x = F.pos[t.a], rs = F.range_start[x];
+          bool known = false, wait = false;
+          int bep = 0;
+          for (int y = x - 1; y >= rs; y--) {
+            int64_t k = Lk[y], sv = S[y];
+            if (k != 0 && (int)(k >> 32) - 1 > y) {
+              bep = (int)(k & 0xffffffffll);
+              known = true;
+            } else if (sv == 1) {
+              wait = true;
+            } else if (sv >= 3) {
+              bep = (int)(sv - 3);
+              known = true;
+            } else if (k != 0) {
+              bep = (int)(k & 0xffffffffll);
+              known = true;
+            } else
+              continue;
+            break;
+          }
+          if (wait) continue;
+          val[q] = known ? bep : unset(rs);
+          state[q] = 1;
+        }
+        PairTask t = pairs[0][self_idx[q]];
+        t.entry_bepos = val[q];
+        batch.push_back(t);
+        bq.push_back(q);
+      }
+      if (batch.empty()) break;
+      nrounds++;
+      std::vector<PairOut> ob;
+      r = align_run_tasks(ctx, L, batch, ob);
+      if (r) return r;
+      for (size_t i = 0; i < batch.size(); i++) {
+        size_t q = bq[i];
+        done[q] = 1;
+        int x = F.pos[batch[i].a];
+        S[x] = ob[i].calls > 0 ? 3 + (int64_t)ob[i].exit_bepos : 2;
+        calls += ob[i].calls;
+      }
+    }
+    for (size_t q = 0; q < self_idx.size(); q++)
+      if (!done[q]) return fail(ctx, PGA_ERR_ARG, "self pairs that cannot be resolved");
+  }
+
+  // 7. survivors in la_sort order: (aread, abpos, bread, comp), ties in the
+  // pair's own output order (src/fastga_pipeline.c:1500-1515)
+  unsigned long long nrec = 0, nbytes = 0;
+  CK(cudaMemcpyAsync(&nrec, ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(&nbytes, ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  std::vector<AlnRec> recs(nrec);
+  std::vector<uint8_t> bytes(nbytes);
+  if (nrec) CK(cudaMemcpyAsync(recs.data(), ctx->recs.p, sizeof(AlnRec) * nrec, cudaMemcpyDeviceToHost, ctx->st));
+  if (nbytes) CK(cudaMemcpyAsync(bytes.data(), ctx->outb.p, nbytes, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  std::vector<int64_t> order(nrec);
+  for (int64_t i = 0; i < (int64_t)nrec; i++) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+    const AlnRec &a = recs[x], &b = recs[y];
+    if (a.aread != b.aread) return a.aread < b.aread;
+    if (a.abpos != b.abpos) return a.abpos < b.abpos;
+    if (a.bread != b.bread) return a.bread < b.bread;
+    if (a.comp != b.comp) return a.comp < b.comp;
+    return a.rank < b.rank;
+  });
+  ctx->h_recs.resize(nrec);
+  ctx->h_toff.assign(nrec + 1, 0);
+  ctx->h_trace.resize(nbytes);
+  int64_t o = 0;
+  for (int64_t i = 0; i < (int64_t)nrec; i++) {
+    const AlnRec &a = recs[order[i]];
+    ctx->h_recs[i] = a;
+    ctx->h_toff[i] = o;
+    memcpy(ctx->h_trace.data() + o, bytes.data() + a.toff, a.tlen);
+    o += a.tlen;
+  }
+  ctx->h_toff[nrec] = o;
+  ctx->align_stats[0] = (int64_t)(pairs[0].size() + pairs[1].size());
+  ctx->align_stats[1] = (int64_t)self_idx.size();
+  ctx->align_stats[2] = calls;
+  ctx->align_stats[4] = (int64_t)nrec;
+  ctx->align_stats[5] = nrounds;
+  ctx->have_align = true;
+  return PGA_OK;
+}
 }  // namespace
 
 // =============================================================================
@@ -513,6 +918,12 @@ void pga_ctx_destroy(pga_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->st);
+  DBuf *abufs[] = {&ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout,
+                   &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
+                   &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
+                   &ctx->pidx, &ctx->pstart, &ctx->pab};
+  for (DBuf *b : abufs)
+    if (b->p) cudaFree(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
                   &ctx->scan_tmp, &ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->cum, &ctx->qmed,
                   &ctx->qbig, &ctx->qcount, &ctx->maxrun, &ctx->u64tmp, &ctx->blk_n, &ctx->blk_c,
@@ -610,10 +1021,13 @@ int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int nconti
     CK(cudaMemcpyAsync(ctx->tile_j0.p, tj.data(), sizeof(int64_t) * ctx->ntiles, cudaMemcpyHostToDevice, ctx->st));
   }
   CK(cudaStreamSynchronize(ctx->st));
+  ctx->freq_set = false;
   ctx->have_gdb = true;
   ctx->have_index = false;
   ctx->have_seeds = false;
+  ctx->have_numeric = false;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
+  ctx->have_align = false;
   return PGA_OK;
 }
 
@@ -976,6 +1390,44 @@ int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count) {
 int pga_diag_copy(pga_ctx *ctx, int comp, uint8_t *records, int64_t *panel_off) {
   if (!ctx || (comp != 0 && comp != 1) || !ctx->have_diag[comp]) return PGA_ERR_ARG;
   return copy_diag(ctx, comp, ctx->ncontig, records, panel_off);
+}
+
+int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4) {
+  if (!ctx || !freq4) return PGA_ERR_ARG;
+  for (int q = 0; q < 4; q++) ctx->base_freq[q] = freq4[q];
+  ctx->freq_set = true;
+  return PGA_OK;
+}
+
+int pga_align(pga_ctx *ctx, int64_t *nalign) {
+  if (!ctx || !ctx->have_seeds || !ctx->have_gdb) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = run_align(ctx);
+  if (r) return r;
+  if (nalign) *nalign = (int64_t)ctx->h_recs.size();
+  return PGA_OK;
+}
+
+int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *trace) {
+  if (!ctx || !ctx->have_align) return PGA_ERR_ARG;
+  int64_t n = (int64_t)ctx->h_recs.size();
+  for (int64_t i = 0; i < n; i++) {
+    const AlnRec &a = ctx->h_recs[i];
+    if (recs9) {
+      int32_t *d = recs9 + 9 * i;
+      d[0] = a.aread; d[1] = a.abpos; d[2] = a.aepos; d[3] = a.bread; d[4] = a.bbpos; d[5] = a.bepos;
+      d[6] = a.comp; d[7] = a.diffs; d[8] = a.tlen;
+    }
+  }
+  if (trace_off) memcpy(trace_off, ctx->h_toff.data(), sizeof(int64_t) * (n + 1));
+  if (trace && !ctx->h_trace.empty()) memcpy(trace, ctx->h_trace.data(), ctx->h_trace.size());
+  return PGA_OK;
+}
+
+int pga_align_stats(const pga_ctx *ctx, int64_t *stats8) {
+  if (!ctx || !stats8) return PGA_ERR_ARG;
+  for (int i = 0; i < 8; i++) stats8[i] = ctx->align_stats[i];
+  return PGA_OK;
 }
 
 }  // extern "C"

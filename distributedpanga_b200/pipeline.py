@@ -63,6 +63,10 @@ _SIGS = {
     "pga_seeds_copy": (C.c_int, [vp, C.c_int, vp, vp]),
     "pga_diag_sort": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
     "pga_diag_copy": (C.c_int, [vp, C.c_int, vp, vp]),
+    "pga_gdb_set_freq": (C.c_int, [vp, vp]),
+    "pga_align": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+    "pga_align_copy": (C.c_int, [vp, vp, vp, vp]),
+    "pga_align_stats": (C.c_int, [vp, vp]),
 }
 
 _LIB = None
@@ -265,3 +269,44 @@ class Device:
         off = np.zeros(self.cs.ncontig + 1, dtype=np.int64)
         self._ck(self.L.pga_diag_copy(self.h, comp, _ptr(out), off.ctypes.data_as(vp)), "diag_copy")
         return out, off
+
+    # ---- alignment -------------------------------------------------------------
+    def set_freq(self, freq):
+        f = np.ascontiguousarray(freq, dtype=np.float32)
+        self._ck(self.L.pga_gdb_set_freq(self.h, f.ctypes.data_as(vp)), "gdb_set_freq")
+
+    def align(self) -> int:
+        n = C.c_int64()
+        self._ck(self.L.pga_align(self.h, C.byref(n)), "align")
+        self.nalign = n.value
+        return n.value
+
+    def alignments(self):
+        """(records (n, 9) int32: aread abpos aepos bread bbpos bepos comp diffs tlen,
+        trace offsets (n+1), trace bytes) in la_sort order."""
+        n = self.nalign
+        recs = np.zeros((n, 9), dtype=np.int32)
+        toff = np.zeros(n + 1, dtype=np.int64)
+        self._ck(self.L.pga_align_copy(self.h, recs.ctypes.data_as(vp), toff.ctypes.data_as(vp), None),
+                 "align_copy")
+        tr = np.zeros(max(1, int(toff[-1])), dtype=np.uint8)
+        self._ck(self.L.pga_align_copy(self.h, None, None, tr.ctypes.data_as(vp)), "align_copy")
+        return recs, toff, tr[: int(toff[-1])]
+
+    def align_stats(self) -> dict:
+        a = np.zeros(8, dtype=np.int64)
+        self._ck(self.L.pga_align_stats(self.h, a.ctypes.data_as(vp)), "align_stats")
+        return {"pairs": int(a[0]), "self_pairs": int(a[1]), "calls": int(a[2]), "alignments": int(a[4]),
+                "self_rounds": int(a[5])}
+
+
+def alignment_lines(recs, toff, tr):
+    """The .1aln record stream as text, one alignment per line:
+    aread abpos aepos bread bbpos bepos comp diffs ; T b-deltas ; X diffs."""
+    out = []
+    for i, r in enumerate(recs):
+        t = tr[toff[i]:toff[i + 1]]
+        out.append("%d %d %d %d %d %d %d %d ; %s ; %s" % (r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7],
+                                                          " ".join(map(str, t[1::2].tolist())),
+                                                          " ".join(map(str, t[0::2].tolist()))))
+    return out

@@ -125,6 +125,31 @@ int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck);
 int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count);
 int pga_diag_copy(pga_ctx *ctx, int comp, uint8_t *records, int64_t *panel_off);
 
+/* ---- alignment ------------------------------------------------------------ */
+
+/* Base frequencies of the GDB (GDB.freq, lib/GDB.h:67); they set the
+ * aligner's scoring tables (New_Align_Spec, lib/align.c:222).  Without this
+ * call they are computed from the loaded sequence as the GDB stores them. */
+int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4);
+
+/* pair_sort_search's alignment half (src/fastga_pipeline.c:1686-1892 with
+ * fastga_order's self-pair entry values, src/fastga_order.c:276): chains and
+ * Local_Alignment (lib/align.c:1423) over every (anchor, partner) pair of the
+ * N and C units, the per-pair elimination / entwine step, and la_sort's
+ * order (aread, abpos, bread, comp).  Runs pga_diag_sort on both units if
+ * needed.  *nalign = surviving alignments. */
+int pga_align(pga_ctx *ctx, int64_t *nalign);
+
+/* The alignments in la_sort order: per alignment 9 ints (aread abpos aepos
+ * bread bbpos bepos comp diffs tlen), trace_off (nalign+1) and the trace
+ * bytes (uint8 pairs: differences, b-delta per 100-base A interval, as
+ * Compress_TraceTo8 leaves them, lib/align.c:3892). */
+int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *trace);
+
+/* [0] pairs [1] self pairs [2] Local_Alignment calls [3] 0 [4] alignments
+ * [5] self-pair rounds [6..7] 0 */
+int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,11 +73,17 @@ def case_many_contigs():
 
 
 CASES = {
+    "small_full": lambda: synth.make("small"),
     "small_s002": lambda: synth.make("small", scale=0.02),
     "chromset_s0005": lambda: synth.make("chromset", scale=0.0005),
     "edge_mix": case_edge_mix,
     "many_contigs": case_many_contigs,
 }
+
+
+# Cases whose inputs are regenerated from the seeded generator by the tests
+# (input_sha pins them) instead of being stored.
+REGENERATED = {"small_full"}
 
 
 def sha(a) -> str:
@@ -118,6 +124,9 @@ def run_case(name: str) -> None:
                            "panel": [0] * cs.ncontig}
         aln = subprocess.run([os.path.join(B.REF_DIR, "alndump"), out["aln"]], check=True,
                              capture_output=True, text=True).stdout
+        with open(stem + ".gix", "rb") as f:
+            f.seek(4 * 4 + 8 * (1 << 24) + 4 * 3 + 8 + 4 * 2)
+            gix_perm = np.frombuffer(f.read(4 * cs.ncontig), np.int32).tolist()
     lines = [l for l in aln.split("\n") if l and not l.startswith("#")]
     pre = (rec[:, 1].astype(np.int64) << 16) | (rec[:, 2].astype(np.int64) << 8) | rec[:, 3]
     cum = np.cumsum(np.bincount(pre, minlength=1 << 24)).astype(np.int64) if len(rec) else np.zeros(1 << 24, np.int64)
@@ -135,9 +144,11 @@ def run_case(name: str) -> None:
                   "nbuck": nb.tolist(), "cbuck": cb.tolist()},
         "diag": diag,
         "aln": {"count": len(lines), "sha": hashlib.sha256("\n".join(lines).encode()).hexdigest()},
+        "gix_perm": gix_perm,
     }
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), bps=cs.bps, clen=cs.clen, boff=cs.boff,
-                        freq=cs.freq)
+    if name not in REGENERATED:
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), bps=cs.bps, clen=cs.clen, boff=cs.boff,
+                            freq=cs.freq)
     with open(os.path.join(HERE, name + ".json"), "w") as f:
         json.dump(dig, f, indent=1)
     with gzip.open(os.path.join(HERE, name + ".aln.txt.gz"), "wt") as f:

@@ -59,6 +59,8 @@ int aht_align_unit(const uint8_t *bps, int ncontig, const int64_t *clen, const i
   std::vector<uint8_t> bytes(bcap);
   O.ovl = ovl.data(); O.perm = perm.data(); O.ovl_cap = ovl_cap; O.bytes = bytes.data(); O.byte_cap = bcap;
   O.err = 0;
+  O.pool_next = nullptr;
+  O.pool_cap = 0;
   Path path;
   memset(&path, 0, sizeof(path));
   *nrows = 0; *ntr = 0; *npairs = 0;

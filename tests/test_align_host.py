@@ -1,0 +1,183 @@
+"""The restated aligner (align_core.cuh, the code the GPU kernel's chain
+driver shares) run on the host from the oracle's diagonal-sorted seeds: its
+alignments must be the reference's .1aln record stream, record for record.
+Self pairs start from the entry values of FastGA's order rules
+(src/fastga_order_core.c), computed here in Python from the host results."""
+import ctypes as C
+import gzip
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, GOLDEN_CASES, ROOT, load_case
+
+NATIVE = os.path.join(ROOT, "tests", "native")
+ALL_CASES = GOLDEN_CASES + ["small_full"]
+
+
+@pytest.fixture(scope="module")
+def aht():
+    so = os.path.join(NATIVE, "libalign_host.so")
+    src = os.path.join(NATIVE, "align_host.cu")
+    deps = [src] + [os.path.join(ROOT, "distributedpanga_b200", "csrc", f)
+                    for f in ("align_core.cuh", "align_spec.h")]
+    if not os.path.exists(so) or any(os.path.getmtime(d) > os.path.getmtime(so) for d in deps):
+        subprocess.run(["/usr/local/cuda/bin/nvcc", "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                        "-Wno-deprecated-gpu-targets", "-o", so, src], check=True)
+    L = C.CDLL(so)
+    vp, i64, ci = C.c_void_p, C.c_int64, C.c_int
+    L.aht_align_unit.argtypes = [vp, ci, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp, ci, i64, i64, vp, i64, vp, vp,
+                                 i64, vp, vp, i64, vp]
+    L.aht_align_unit.restype = ci
+    return L
+
+
+def run_unit(L, cs, arr, off, dig, comp, self_entry=None):
+    rows = np.zeros((400000, 9), np.int32)
+    tr = np.zeros(64_000_000, np.uint8)
+    pairs = np.zeros((200000, 4), np.int32)
+    nr, nt, npair = C.c_int64(), C.c_int64(), C.c_int64()
+    se = None if self_entry is None else np.ascontiguousarray(self_entry, np.int32)
+    rc = L.aht_align_unit(cs.bps.ctypes.data, cs.ncontig, cs.clen.ctypes.data, cs.boff.ctypes.data,
+                          cs.freq.ctypes.data, np.ascontiguousarray(arr).ctypes.data, off.ctypes.data,
+                          dig["swide"], dig["dbyte"], dig["ctgb"], comp,
+                          se.ctypes.data if se is not None else None, 8192, 50_000_000, 1_000_000,
+                          rows.ctypes.data, len(rows), C.byref(nr), tr.ctypes.data, len(tr), C.byref(nt),
+                          pairs.ctypes.data, len(pairs), C.byref(npair))
+    assert rc == 0, rc
+    out, o = [], 0
+    for r in rows[: nr.value]:
+        t = tr[o:o + r[8]]
+        o += r[8]
+        out.append((int(r[0]), int(r[3]), int(r[1]), int(r[2]), int(r[4]), int(r[5]), int(r[6]), int(r[7]),
+                    t[1::2].tolist(), t[0::2].tolist()))
+    return out, pairs[: npair.value].copy()
+
+
+def fastga_self_entries(cs, pairs_n, nseeds_by_contig, swide, perm):
+    """Entry bepos of every self pair (src/fastga_order_core.c:147-192)."""
+    n = cs.ncontig
+    pos = np.empty(n, int)
+    pos[perm] = np.arange(n)
+    clen_pos = cs.clen[perm]
+    seeds_pos = nseeds_by_contig[perm]
+    T, npost = 32, int(cs.clen.sum())
+    split, p, r, t, cum = [0] * (T + 1), 0, T, npost // T, int(clen_pos[0]) if n else 0
+    for x in range(1, n):
+        if cum >= t and x >= r:
+            p += 1
+            split[p] = x
+            t = (npost * (p + 1)) // T
+            r += T
+        cum += int(clen_pos[x])
+    nparts = p + 1
+    split[nparts] = n
+    rs = list(range(n))
+    for i in range(nparts):
+        asize = sum(int(seeds_pos[x]) * swide for x in range(split[i], split[i + 1]))
+        if asize == 0:
+            continue
+        k, thr, s = 0, asize // T, 0
+        x = split[i]
+        while x < split[i + 1] and seeds_pos[x] == 0:
+            x += 1
+        beg = x
+        while x < split[i + 1]:
+            if seeds_pos[x] > 0:
+                s += int(seeds_pos[x]) * swide
+                if s >= thr:
+                    for y in range(beg, x + 1):
+                        rs[y] = beg
+                    k += 1
+                    thr = (asize * (k + 1)) // T
+                    beg = x + 1
+            x += 1
+    res = {(int(a), int(b)): (int(c), int(e)) for a, b, c, e in pairs_n}
+    Lk = [0] * n
+    for (a, b), (calls, bep) in res.items():
+        if a != b and calls > 0:
+            key = ((int(pos[b]) + 1) << 32) | (bep & 0xffffffff)
+            Lk[pos[a]] = max(Lk[pos[a]], key)
+    return pos, rs, res, Lk
+
+
+def aln_lines(out):
+    out = sorted(out, key=lambda x: (x[0], x[1], x[2], x[3]))
+    return ["%d %d %d %d %d %d %d %d ; %s ; %s" % (a, ab, ae, b, bb, be, c, d, " ".join(map(str, T)),
+                                                   " ".join(map(str, X)))
+            for (a, ab, b, c, ae, bb, be, d, T, X) in out]
+
+
+@pytest.mark.parametrize("case", ALL_CASES)
+def test_host_aligner_matches_reference(oracle, aht, case):
+    cs, dig = load_case(case)
+    posb, ctgb = dig["posb"], dig["ctgb"]
+    srt = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    ent, cum, _ = oracle.build_adapter(srt, posb, ctgb)
+    ns, css, nb, _ = oracle.merge(ent, cum, posb, ctgb, 10, cs.ncontig)
+    arrN, offN = oracle.reimport_sort(ns, posb, ctgb, 0, cs.ncontig, cs.maxctg, dig["dbyte"])
+    arrC, offC = oracle.reimport_sort(css, posb, ctgb, 1, cs.ncontig, cs.maxctg, dig["dbyte"])
+    # pass 1: every pair; the results of pairs of two contigs fix the self pairs' entry values
+    perm = np.argsort(-cs.clen, kind="stable")
+    assert perm.tolist() == dig["gix_perm"]           # FastGA's contig order = the .gix permutation
+    _, pairsN = run_unit(aht, cs, arrN, offN, dig, 0)
+    pos, rs, res, Lk = fastga_self_entries(cs, pairsN, nb, dig["swide"], perm)
+    entry = np.zeros(cs.ncontig, np.int32)
+    S = [0] * cs.ncontig
+    selfs = sorted([a for (a, b) in res if a == b], key=lambda c: pos[c])
+    known = {}
+    for c in selfs:
+        x = pos[c]
+        S[x] = 1
+        earlier = sorted([(pos[b], res[(c, b)]) for (a, b) in res if a == c and pos[b] < x], reverse=True)
+        v = next((bep for _, (calls, bep) in earlier if calls > 0), None)
+        if v is not None:
+            known[c] = v
+        elif rs[x] == x:
+            known[c] = 32767 if rs[x] == 0 else 0
+    # self pairs whose value comes from earlier rows: resolve in rounds
+    for c in selfs:
+        if c in known:
+            entry[c] = known[c]
+    for _ in range(len(selfs) + 1):
+        _, pairsN = run_unit(aht, cs, arrN, offN, dig, 0, entry)
+        res = {(int(a), int(b)): (int(cc), int(e)) for a, b, cc, e in pairsN}
+        for c in selfs:
+            if c in known:
+                calls, bep = res[(c, c)]
+                S[pos[c]] = 3 + bep if calls > 0 else 2
+        progress = False
+        for c in selfs:
+            if c in known:
+                continue
+            x = pos[c]
+            val, wait = None, False
+            for y in range(x - 1, rs[x] - 1, -1):
+                k, s = Lk[y], S[y]
+                if k and (k >> 32) - 1 > y:
+                    val = k & 0xffffffff
+                elif s == 1:
+                    wait = True
+                elif s >= 3:
+                    val = s - 3
+                elif k:
+                    val = k & 0xffffffff
+                else:
+                    continue
+                break
+            if wait:
+                continue
+            known[c] = val if val is not None else (32767 if rs[x] == 0 else 0)
+            entry[c] = known[c]
+            progress = True
+        if not progress:
+            break
+    outN, _ = run_unit(aht, cs, arrN, offN, dig, 0, entry)
+    outC, _ = run_unit(aht, cs, arrC, offC, dig, 1)
+    mine = [" ".join(l.split()) for l in aln_lines(outN + outC)]
+    ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n")
+           if l.strip()]
+    assert len(mine) == dig["aln"]["count"]
+    assert mine == ref

@@ -132,3 +132,26 @@ def test_sort_matches_property_at_scale(dev):
     assert rec[0, 0] == 0 and np.array_equal(rec[1:, 0], want)
     ent, cum, big = dev.index_entries()
     assert cum[-1] == n and big == int(np.max(np.diff(np.concatenate([[0], cum]))))
+
+
+def _aln_norm(lines):
+    return [" ".join(l.split()) for l in lines if l.strip()]
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES + ["small_full"])
+def test_alignments_match_reference(dev, case):
+    """The whole path on the GPU; the .1aln record stream equals the reference's."""
+    import gzip
+    import os
+    from conftest import GOLDEN
+    from distributedpanga_b200.pipeline import alignment_lines
+    cs, dig = load_case(case)
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=False)
+    dev.merge(dig["freq_cutoff"])
+    n = dev.align()
+    recs, toff, tr = dev.alignments()
+    mine = _aln_norm(alignment_lines(recs, toff, tr))
+    ref = _aln_norm(gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n"))
+    assert n == dig["aln"]["count"]
+    assert mine == ref
