@@ -2,16 +2,16 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
 
-One step = one pass of the GPU path over the whole contig set, inputs resident
-in HBM: closed-syncmer extraction -> 24-bit-prefix bucket sort -> semantic
-LCPs -> k-mer table entries + prefix table -> adaptamer merge -> seed
-reimport + diagonal sort of the N and C units.  Local_Alignment / .1aln are
-not yet on the GPU, so the metric is input Mbp/s through those stages.
+One step = one pass of the whole alignment path over the contig set, inputs
+resident in HBM: closed-syncmer extraction -> 24-bit-prefix bucket sort ->
+semantic LCPs -> k-mer table entries + prefix table -> adaptamer merge ->
+seed reimport + diagonal sort of the N and C units -> chaining and
+Local_Alignment of every contig pair (FastGA-order self pairs) -> the
+alignment records in la_sort order, read back to the host.
 
 value  = input bases (both genomes, Mbp) per second, max device time over ranks
-e2e    = the same through the C ABI with host buffers: every step uploads the
-         .bps image and contig table and reads back both units' sorted seed
-         panels (reference byte format)
+e2e    = the same through the C ABI with host buffers: every step also uploads
+         the .bps image and contig table
 roofline = the index build (extract + sort + LCP + entries), whose algorithmic
          bytes are ceil(G/4) + 5*N*R + N*E + 2^27
 cpu_baseline = the reference pipeline compiled from source (oracle/_ref), or
@@ -38,7 +38,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "input Mbp/s per B200 through extract->sort->merge->diagonal sort (Local_Alignment not yet on GPU)"
+METRIC = "aligned Mbp/s per B200 (input bases of both genomes / end-to-end seconds, plain method)"
 UNIT = "Mbp/s"
 WORKLOAD = "chromset: 2 x 100 Mbp, 40% GC, log-normal contigs (median 2 Mbp, sigma 1), 10% repeats; k=40, FREQ=10"
 
@@ -150,7 +150,7 @@ class ReferenceSample:
             subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T8", self.stem + ".1gdb"], check=True,
                            stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
 
-    def run(self) -> float:
+    def run(self, whole: bool = True) -> float:
         from oracle import binding as orc
         env = dict(os.environ)
         env["PATH"] = orc.REF_DIR + os.pathsep + env.get("PATH", "")
@@ -160,6 +160,11 @@ class ReferenceSample:
             subprocess.run([os.path.join(orc.REF_DIR, "pga-mpi-merge"), self.stem], check=True, stdout=log,
                            stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
         text = open(logp).read()
+        if whole:
+            # the driver's own stage timers: extract, sort, merge, alignments
+            # (src/pga-mpi-merge.c:669-688); alignments includes ALNtoPAF, here a copy
+            tot = re.search(r"TOTAL\s+([0-9.]+)s", text)
+            return float(tot.group(1))
         o1 = dict(re.findall(r"(\w+)=([0-9.]+)", text.split("[o1-0]")[1].split("\n")[0]))
         pr = dict(re.findall(r"(\w+)=([0-9.]+)", text.split("[pr1]")[1].split("\n")[0]))
         return (float(o1["extract_s"]) + float(o1["sort_stage_s"]) + float(pr["adapter_s"]) +
@@ -192,8 +197,8 @@ def cpu_baseline(sample_scale: float) -> dict:
         mbp = r.mbp
         return {"value": mbp / sec, "unit": UNIT, "cores": 4, "kind": "reference",
                 "sample": "chromset generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
-                          "(oracle/_ref), stages extract+sort+adapter+merge+reimport+seed sort; msd_sort uses "
-                          "4 threads, the rest 1; host has %d cores" % (sample_scale, mbp, cores_total),
+                          "(oracle/_ref), whole path (its TOTAL stage time: extract, sort, merge, alignments); "
+                          "msd_sort uses 4 threads, the rest 1; host has %d cores" % (sample_scale, mbp, cores_total),
                 "seconds": sec}
     orc.build()
     mbp, sec = port_sample(sample_scale)
@@ -251,6 +256,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dev.merge(10)
         dev.diag_sort(0)
         dev.diag_sort(1)
+        dev.align()
 
     for _ in range(args.warmup):
         step()
@@ -279,7 +285,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     st = dev.stage_times()
     dev.enable_timing(False)
 
-    # end to end through the C ABI with host buffers
+    astats = dev.align_stats()
+    recs, toff, tr = dev.alignments()
+    aligned_bases = int((recs[:, 2] - recs[:, 1]).sum()) if len(recs) else 0
+
+    # end to end through the C ABI with host buffers: upload the GDB, run the
+    # path, read the alignments back
     swide = None
     h2d = int(cs.bps.size + 16 * cs.ncontig)
     d2h = 0
@@ -292,12 +303,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dev.gdb_load(cs)
         dev.index_build(want_entries=True)
         dev.merge(10)
-        d2h = 0
-        for comp in (0, 1):
-            sw, cnt = dev.diag_sort(comp)
-            arr, off = dev.diag_records(comp, sw, cnt)
-            d2h += arr.nbytes + off.nbytes
-            swide = sw
+        swide, _ = dev.diag_sort(0)
+        dev.diag_sort(1)
+        dev.align()
+        r2, o2, t2 = dev.alignments()
+        d2h = r2.nbytes + o2.nbytes + t2.nbytes
         t1.record(stream)
         torch.cuda.synchronize()
         if it >= args.warmup:
@@ -338,6 +348,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, chromset workload)",
         "config": {"workload": WORKLOAD, "scale": args.scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
                    "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
+                   "pairs": astats["pairs"], "self_pairs": astats["self_pairs"],
+                   "local_alignment_calls": astats["calls"], "alignments": astats["alignments"],
+                   "aligned_bases": aligned_bases,
                    "record_bytes": rsize, "swide": swide,
                    "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},

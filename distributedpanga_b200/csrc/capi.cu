@@ -28,7 +28,7 @@ struct DBuf {
   size_t cap = 0;
 };
 
-enum StageId { ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_N };
+enum StageId { ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_ALIGN, ST_N };
 
 }  // namespace
 
@@ -963,13 +963,13 @@ int pga_ctx_enable_timing(pga_ctx *ctx, int on) {
   return PGA_OK;
 }
 
-int pga_stage_times(const pga_ctx *cctx, float *ms8) {
+int pga_stage_times(const pga_ctx *cctx, float *ms9) {
   pga_ctx *ctx = const_cast<pga_ctx *>(cctx);
-  if (!ctx || !ms8) return PGA_ERR_ARG;
+  if (!ctx || !ms9) return PGA_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->st));
   for (int s = 0; s < ST_N; s++) {
-    ms8[s] = 0.f;
-    if (ctx->stage_used[s]) cudaEventElapsedTime(&ms8[s], ctx->ev[s][0], ctx->ev[s][1]);
+    ms9[s] = 0.f;
+    if (ctx->stage_used[s]) cudaEventElapsedTime(&ms9[s], ctx->ev[s][0], ctx->ev[s][1]);
   }
   return PGA_OK;
 }
@@ -1402,8 +1402,10 @@ int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4) {
 int pga_align(pga_ctx *ctx, int64_t *nalign) {
   if (!ctx || !ctx->have_seeds || !ctx->have_gdb) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
+  stage_begin(ctx, ST_ALIGN);
   int r = run_align(ctx);
   if (r) return r;
+  stage_end(ctx, ST_ALIGN);
   if (nalign) *nalign = (int64_t)ctx->h_recs.size();
   return PGA_OK;
 }

@@ -150,10 +150,10 @@ class Device:
         self._ck(self.L.pga_ctx_enable_timing(self.h, 1 if on else 0), "enable_timing")
 
     def stage_times(self) -> dict:
-        a = (C.c_float * 8)()
+        a = (C.c_float * 9)()
         self._ck(self.L.pga_stage_times(self.h, a), "stage_times")
         names = ["extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
-                 "entries_prefix_table", "merge", "diag_sort"]
+                 "entries_prefix_table", "merge", "diag_sort", "align"]
         return dict(zip(names, [float(x) for x in a]))
 
     # ---- GDB -------------------------------------------------------------
