@@ -58,8 +58,10 @@ k_align_pairs(AlignLaunch P) {
   W.HA[0] = wb + 4 * P.vcap;
   W.HA[1] = wb + 5 * P.vcap;
   W.NA = wb + 6 * P.vcap;
-  W.T[0] = (uint64_t *)(wb + 7 * P.vcap);
-  W.T[1] = (uint64_t *)(wb + 9 * P.vcap);
+  W.HM[0] = wb + 7 * P.vcap;
+  W.HM[1] = wb + 8 * P.vcap;
+  W.T[0] = (uint64_t *)(wb + 9 * P.vcap);
+  W.T[1] = (uint64_t *)(wb + 11 * P.vcap);
   W.vcap = P.vcap;
   W.points = P.points + wid * P.point_cap;
   W.point_cap = P.point_cap;
@@ -90,6 +92,11 @@ k_align_pairs(AlignLaunch P) {
     const uint8_t *abuf = tk.comp ? P.rc : P.fwd;
     Seq A{abuf + P.soff[tk.a], (int)P.clen[tk.a]};
     Seq B{P.fwd + P.soff[tk.b], (int)P.clen[tk.b]};
+    A.pf = P.pk + P.poff[tk.a] * 4 + (tk.comp ? 2 : 0) * P.pwords[tk.a];
+    A.pr = P.pk + P.poff[tk.a] * 4 + (tk.comp ? 3 : 1) * P.pwords[tk.a];
+    B.pf = P.pk + P.poff[tk.b] * 4;
+    B.pr = P.pk + P.poff[tk.b] * 4 + P.pwords[tk.b];
+    long long t0 = clock64();
     Path path;
     path.tlen = path.diffs = path.abpos = path.bbpos = path.aepos = 0;
     path.bepos = tk.entry_bepos;
@@ -161,6 +168,7 @@ k_align_pairs(AlignLaunch P) {
         po.rec_off = (int64_t)r0;
       }
     }
+    po.cycles = clock64() - t0;
     if (lane == 0) P.pout[t] = po;
     __syncwarp();
   }
@@ -185,6 +193,46 @@ __global__ void k_numeric(const uint8_t *__restrict__ bps, const int64_t *__rest
     fwd[o - 1] = fwd[o + n] = 4;
     rc[o - 1] = rc[o + n] = 4;
   }
+}
+
+// 2-bit packed copies of every contig, 32 bases per word, first base in the
+// top bits, one zero pad word after each: forward, reversed, reverse
+// complement and complement-only (the reverse of the reverse complement) --
+// the packed forms of the sequences the forward and reverse snakes read.
+__global__ void k_pack(const uint8_t *__restrict__ fwd, const int64_t *__restrict__ soff,
+                       const int64_t *__restrict__ clen, const int64_t *__restrict__ poff,
+                       const int64_t *__restrict__ pwords, int ncontig, uint64_t *__restrict__ pk) {
+  int c = blockIdx.y;
+  if (c >= ncontig) return;
+  int64_t n = clen[c], nw = pwords[c];
+  const uint8_t *s = fwd + soff[c];
+  uint64_t *F = pk + poff[c] * 4, *R = F + nw, *RC = F + 2 * nw, *CO = F + 3 * nw;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t f = 0, r = 0, rc = 0, co = 0;
+    for (int q = 0; q < 32; q++) {
+      int64_t i = 32 * w + q;
+      uint64_t bf = 0, br = 0;
+      if (i < n) {
+        bf = s[i];
+        br = s[n - 1 - i];
+      }
+      f |= bf << (62 - 2 * q);
+      r |= br << (62 - 2 * q);
+      rc |= (i < n ? (3 - br) : 0) << (62 - 2 * q);
+      co |= (i < n ? (3 - bf) : 0) << (62 - 2 * q);
+    }
+    F[w] = f;
+    R[w] = r;
+    RC[w] = rc;
+    CO[w] = co;
+  }
+}
+
+void launch_pack(const uint8_t *fwd, const int64_t *soff, const int64_t *clen, const int64_t *poff,
+                 const int64_t *pwords, int ncontig, uint64_t *pk, cudaStream_t st) {
+  if (ncontig <= 0) return;
+  dim3 g(64, ncontig);
+  k_pack<<<g, 256, 0, st>>>(fwd, soff, clen, poff, pwords, ncontig, pk);
 }
 
 // Pair boundaries of a sorted key array: flag[i] = 1 where (icont, jcont)

@@ -9,7 +9,7 @@
 namespace pga {
 
 constexpr int ALIGN_THREADS = 128;  // 4 warps per CTA, one pair per warp at a time
-constexpr int WAVE_INTS = 11;       // per diagonal slot: V,M,HA x2, NA, T x2 (uint64)
+constexpr int WAVE_INTS = 13;       // per diagonal slot: V,M,HA,HM x2, NA, T x2 (uint64)
 
 // One (anchor, partner) pair of a unit: seeds [lo, hi) of the unit's sorted keys.
 struct PairTask {
@@ -20,6 +20,7 @@ struct PairTask {
 struct PairOut {
   int calls, exit_bepos, nsurv, err;
   int64_t rec_off;
+  long long cycles;  // SM clock cycles the warp spent on the pair
 };
 
 // One surviving alignment; trace bytes (uint8 pairs: diffs, b-delta per
@@ -37,6 +38,8 @@ struct AlignLaunch {
   SeedKeyLayout layN, layC;
   const uint8_t *fwd, *rc;
   const int64_t *soff, *clen;
+  const uint64_t *pk;            // packed sequences: contig c at word 4*poff[c]: F, R, RC, CO (pwords[c] each)
+  const int64_t *poff, *pwords;
   const int16_t *score, *table;
   int ave_path;
   int64_t amxpos, maxdag;
@@ -68,6 +71,8 @@ void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *
                         unsigned long long *cnt, cudaStream_t st);
 void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,
                     uint8_t *fwd, uint8_t *rc, cudaStream_t st);
+void launch_pack(const uint8_t *fwd, const int64_t *soff, const int64_t *clen, const int64_t *poff,
+                 const int64_t *pwords, int ncontig, uint64_t *pk, cudaStream_t st);
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st);
 void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint32_t *flag, const uint32_t *idx,
                         int64_t *start, int32_t *ab, cudaStream_t st);

@@ -82,9 +82,14 @@ struct WaveWork {
 };
 
 // A sequence with sentinel value 4 at [-1] and [len], NUMERIC bases 0..3.
+// The device aligner also reads it 2-bit packed, 32 bases per word with the
+// first base in the top bits: pf forwards, pr reversed (pr's base i is
+// s[len-1-i]); both end with a zero pad word.  The host code leaves them null.
 struct Seq {
   const uint8_t *s;
   int len;
+  const uint64_t *pf = nullptr;
+  const uint64_t *pr = nullptr;
 };
 
 #define PGA_VI(k) ((k) & vmask)

@@ -36,7 +36,7 @@ struct PebblePool {
 };
 
 struct WarpWork {
-  int *V[2], *M[2], *HA[2];
+  int *V[2], *M[2], *HA[2], *HM[2];  // HM: mark of pebble HA (marks never change once written)
   uint64_t *T[2];
   int *NA;
   int vcap;
@@ -124,48 +124,85 @@ __device__ __forceinline__ int warp_min(int v) {
 // Highest lane with a set bit (the last in visit order), -1 if none.
 __device__ __forceinline__ int last_lane(uint32_t ballot) { return ballot ? 31 - __clz(ballot) : -1; }
 
-// Forward snake along diagonal k from a-position x (bases equal, neither a
-// sentinel).  Compares 8 bytes at a time; stops exactly where the byte loop
-// of the reference stops and reports which sentinel (if any) stopped it.
-// Reads outside [-1, len] of either sequence count as its sentinel: legal
-// inputs never get there, and a wrong start can then not run off the buffers.
-__device__ __forceinline__ int snake_fwd(const uint8_t *aseq, const uint8_t *bseq, int alen, int blen, int x, int k,
-                                         int *hitb, int *hita) {
-  *hitb = *hita = 0;
-  while (1) {
-    int y = x - k;
-    int c = (y < -1 || y > blen) ? 4 : bseq[y];
-    if (c == 4) {
-      *hitb = 1;
-      return x;
-    }
-    int d = (x < -1 || x > alen) ? 4 : aseq[x];
-    if (c != d) {
-      if (d == 4) *hita = 1;
-      return x;
-    }
-    x += 1;
-  }
+// 32 bases of a packed sequence starting at base o.
+__device__ __forceinline__ uint64_t bases32(const uint64_t *p, int o) {
+  int w = o >> 5, sh = (o & 31) << 1;
+  uint64_t v = p[w];
+  return sh ? (v << sh) | (p[w + 1] >> (64 - sh)) : v;
 }
 
-// (aseq, bseq here start one position left: valid indices 0..len+1)
-__device__ __forceinline__ int snake_rev(const uint8_t *aseq, const uint8_t *bseq, int alen, int blen, int x, int k,
-                                         int *hitb, int *hita) {
-  *hitb = *hita = 0;
-  while (1) {
-    int y = x - k;
-    int c = (y < 0 || y > blen + 1) ? 4 : bseq[y];
-    if (c == 4) {
-      *hitb = 1;
-      return x;
+// Matching run of two packed sequences from offsets oa, ob, at most mx bases.
+__device__ __forceinline__ int match_run(const uint64_t *pa, int oa, const uint64_t *pb, int ob, int mx) {
+  int t = 0;
+  while (t < mx) {
+    uint64_t d = bases32(pa, oa + t) ^ bases32(pb, ob + t);
+    int chunk = mx - t < 32 ? mx - t : 32;
+    if (d) {
+      int lead = __clzll(d) >> 1;
+      if (lead < chunk) return t + lead;
     }
-    int d = (x < 0 || x > alen + 1) ? 4 : aseq[x];
-    if (c != d) {
-      if (d == 4) *hita = 1;
-      return x;
-    }
-    x -= 1;
+    t += chunk;
   }
+  return mx;
+}
+
+// Forward snake along diagonal k from a-position x (A[x..], B[x-k..]): the
+// reference's byte loop stops at the first mismatch, or at B's sentinel
+// (B[blen], checked first) or A's (A[alen]).  Starts outside the sequences
+// count as meeting that sequence's sentinel, so no read leaves the buffers.
+__device__ __forceinline__ int snake_fwd(const Seq &A, const Seq &B, int x, int k, int *hitb, int *hita) {
+  int y = x - k;
+  *hitb = *hita = 0;
+  if (y < 0 || y > B.len) {
+    *hitb = 1;
+    return x;
+  }
+  if (x < 0 || x > A.len) {
+    *hita = 1;
+    return x;
+  }
+  int ra = A.len - x, rb = B.len - y;
+  int mx = ra < rb ? ra : rb;
+  int t = match_run(A.pf, x, B.pf, y, mx);
+  if (t == mx) {
+    if (rb <= ra) *hitb = 1;
+    else *hita = 1;
+  }
+  return x + t;
+}
+
+// Reverse snake along diagonal k from x: compares A[x-1], A[x-2], .. with
+// B[x-k-1], ..; sentinels A[-1] and B[-1] (read through the reversed copies).
+__device__ __forceinline__ int snake_rev(const Seq &A, const Seq &B, int x, int k, int *hitb, int *hita) {
+  int y = x - k;
+  *hitb = *hita = 0;
+  if (y <= 0 || y >= B.len + 1) {  // B[-1], B[blen] or outside
+    *hitb = 1;
+    return x;
+  }
+  if (x <= 0 || x > A.len) {
+    *hita = 1;
+    return x;
+  }
+  int ra = x, rb = y;
+  int mx = ra < rb ? ra : rb;
+  int t = match_run(A.pr, A.len - x, B.pr, B.len - y, mx);
+  if (t == mx) {
+    if (rb <= ra) *hitb = 1;
+    else *hita = 1;
+  }
+  return x - t;
+}
+
+// The reference shifts one 1 into the match history b per matched base and
+// counts m up while b's PATH_TOP bit is clear (lib/align.c:663-668): the
+// closed form for a run of r bases.
+__device__ __forceinline__ void history_run(uint64_t &b, int &m, int r) {
+  if (r <= 0) return;
+  int L = r < 61 ? r : 61;
+  uint64_t mask = ((1ull << L) - 1) << (61 - L);
+  m += L - __popcll(b & mask);
+  b = r >= 64 ? ~0ull : ((b << r) | ((1ull << r) - 1));
 }
 
 #define WVI(k) ((k) & vmask)
@@ -213,7 +250,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     if (act) {
       x = (mida + k) >> 1;
       na = ((x + (tspace - aoff)) / tspace - 1) * tspace + aoff;
-      x = snake_fwd(aseq, bseq, A.len, B.len, x, k, &hb, &ha_);
+      x = snake_fwd(A, B, x, k, &hb, &ha_);
       c = (x << 1) - k;
       npb = 1;
       for (int q = na + tspace; x >= q; q += tspace) npb++;
@@ -231,11 +268,13 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       int64_t s = pb0 + off;
       cells[s] = {-1, k, 0, na};
       ha = (int)s;
+      int hm = na;
       na += tspace;
       while (x >= na) {
         s += 1;
         cells[s] = {ha, k, 0, na};
         ha = (int)s;
+        hm = na;
         na += tspace;
       }
       int vi = WVI(k);
@@ -243,6 +282,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.T[cur][vi] = PATH_INT;
       W.M[cur][vi] = PATH_LEN;
       W.HA[cur][vi] = ha;
+      W.HM[cur][vi] = hm;
       NA[vi] = na;
     }
     // clips: bclip = largest k that met B's end, aclip = last visited (smallest) k that met A's end
@@ -306,9 +346,9 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.err |= ALN_ERR_VCAP;
       return 1;
     }
-    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur];
+    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur], *HMo = W.HM[cur];
     uint64_t *To = W.T[cur];
-    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1];
+    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1], *HMn = W.HM[cur ^ 1];
     uint64_t *Tn = W.T[cur ^ 1];
     // boundary diagonals on the previous wave's buffer (lane 0; visible after syncwarp)
     bool top_default = false;
@@ -337,7 +377,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     for (int base = hgh; base >= low; base -= 32) {
       int k = base - lane;
       bool act = k >= low;
-      int x = 0, c = 0, m = 0, ha = -1, hb = 0, hA = 0, npb = 0, nak = 0;
+      int x = 0, c = 0, m = 0, ha = -1, hm = 0, hb = 0, hA = 0, npb = 0, nak = 0;
       uint64_t b = 0;
       if (act) {
         int vi = WVI(k);
@@ -347,36 +387,27 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
           src = (am < ap) ? 1 : -1;
         else
           src = (ac < ap) ? 1 : 0;
-        if (src == 1) {
-          c = ap + 1;
-          if (k == hgh && top_default) {
-            m = PATH_LEN; b = PATH_INT; ha = -1;
-          } else {
-            m = Mo[WVI(k + 1)]; b = To[WVI(k + 1)]; ha = HAo[WVI(k + 1)];
-          }
-        } else if (src == -1) {
-          c = am + 1; m = Mo[WVI(k - 1)]; b = To[WVI(k - 1)]; ha = HAo[WVI(k - 1)];
+        int sk = k + src;
+        c = src == 1 ? ap + 1 : (src == -1 ? am + 1 : ac + 2);
+        if (src == 1 && k == hgh && top_default) {
+          m = PATH_LEN; b = PATH_INT; ha = -1;
         } else {
-          c = ac + 2; m = Mo[vi]; b = To[vi]; ha = HAo[vi];
+          int si = WVI(sk);
+          m = Mo[si]; b = To[si]; ha = HAo[si]; hm = HMo[si];
         }
         if ((b & PATH_TOP) != 0) m -= 1;
         b <<= 1;
         x = (c + k) >> 1;
         int x0 = x;
-        x = snake_fwd(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
-        int run = x - x0;
-        // the reference shifts a 1 into b per matched base and counts m up while the top bit is clear
-        for (int r = 0; r < run; r++) {
-          if ((b & PATH_TOP) == 0) m += 1;
-          b = (b << 1) | 1;
-        }
+        x = snake_fwd(A, B, x, k, &hb, &hA);
+        history_run(b, m, x - x0);
         c = (x << 1) - k;
         nak = NA[vi];
-        int hm = ha >= 0 ? cells[ha].mark : 0;
+        int hq = hm;
         for (int q = nak; x >= q; q += tspace)
-          if (hm < q) {
+          if (hq < q) {
             npb++;
-            hm = q;  // the new pebble's mark
+            hq = q;  // the new pebble's mark
           }
       }
       int off = warp_excl_sum(npb, lane);
@@ -387,9 +418,10 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         int vi = WVI(k);
         int64_t s = pb0 + off;
         while (x >= nak) {
-          if (cells[ha].mark < nak) {
+          if (hm < nak) {
             cells[s] = {ha, k, dif, nak};
             ha = (int)s;
+            hm = nak;
             s += 1;
           }
           nak += tspace;
@@ -399,6 +431,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         Tn[vi] = b;
         Mn[vi] = m;
         HAn[vi] = ha;
+        HMn[vi] = hm;
       }
       uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
       if (bb) {
@@ -599,7 +632,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       x = (mida + k) >> 1;
       x0 = x;
       na = ((x + (tspace - aoff) - 1) / tspace - 1) * tspace + aoff;
-      x = snake_rev(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
+      x = snake_rev(A, B, x, k, &hb, &hA);
       c = (x << 1) - k;
       npb = 1;
       for (int q = na; x <= q; q -= tspace) npb++;
@@ -617,10 +650,12 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       int64_t s = pb0 + off;
       cells[s] = {-1, k, 0, x0};
       ha = (int)s;
+      int hm = x0;
       while (x <= na) {
         s += 1;
         cells[s] = {ha, k, 0, na};
         ha = (int)s;
+        hm = na;
         na -= tspace;
       }
       int vi = WVI(k);
@@ -628,6 +663,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.T[cur][vi] = PATH_INT;
       W.M[cur][vi] = PATH_LEN;
       W.HA[cur][vi] = ha;
+      W.HM[cur][vi] = hm;
       NA[vi] = na;
     }
     // bclip = smallest k that met B's start, aclip = last visited (largest) k that met A's start
@@ -690,9 +726,9 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.err |= ALN_ERR_VCAP;
       return 1;
     }
-    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur];
+    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur], *HMo = W.HM[cur];
     uint64_t *To = W.T[cur];
-    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1];
+    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1], *HMn = W.HM[cur ^ 1];
     uint64_t *Tn = W.T[cur ^ 1];
     if (low >= minp) {
       if (lane == 0) {
@@ -718,7 +754,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     for (int base = low; base <= hgh; base += 32) {
       int k = base + lane;
       bool act = k <= hgh;
-      int x = 0, c = 0, m = 0, ha = -1, hb = 0, hA = 0, npb = 0, nak = 0;
+      int x = 0, c = 0, m = 0, ha = -1, hm = 0, hb = 0, hA = 0, npb = 0, nak = 0;
       uint64_t b = 0;
       if (act) {
         int vi = WVI(k);
@@ -728,35 +764,27 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
           src = (ap > am) ? -1 : 1;
         else
           src = (ac > am) ? -1 : 0;
-        if (src == -1) {
-          c = am - 1;
-          if (k == low) {
-            m = PATH_LEN; b = PATH_INT; ha = -1;
-          } else {
-            m = Mo[WVI(k - 1)]; b = To[WVI(k - 1)]; ha = HAo[WVI(k - 1)];
-          }
-        } else if (src == 1) {
-          c = ap - 1; m = Mo[WVI(k + 1)]; b = To[WVI(k + 1)]; ha = HAo[WVI(k + 1)];
+        int sk = k + src;
+        c = src == -1 ? am - 1 : (src == 1 ? ap - 1 : ac - 2);
+        if (src == -1 && k == low) {
+          m = PATH_LEN; b = PATH_INT; ha = -1;
         } else {
-          c = ac - 2; m = Mo[vi]; b = To[vi]; ha = HAo[vi];
+          int si = WVI(sk);
+          m = Mo[si]; b = To[si]; ha = HAo[si]; hm = HMo[si];
         }
         if ((b & PATH_TOP) != 0) m -= 1;
         b <<= 1;
         x = (c + k) >> 1;
         int x0 = x;
-        x = snake_rev(aseq, bseq, A.len, B.len, x, k, &hb, &hA);
-        int run = x0 - x;
-        for (int r = 0; r < run; r++) {
-          if ((b & PATH_TOP) == 0) m += 1;
-          b = (b << 1) | 1;
-        }
+        x = snake_rev(A, B, x, k, &hb, &hA);
+        history_run(b, m, x0 - x);
         c = (x << 1) - k;
         nak = NA[vi];
-        int hm = ha >= 0 ? cells[ha].mark : 0;
+        int hq = hm;
         for (int q = nak; x <= q; q -= tspace)
-          if (hm > q) {
+          if (hq > q) {
             npb++;
-            hm = q;
+            hq = q;
           }
       }
       int off = warp_excl_sum(npb, lane);
@@ -767,9 +795,10 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         int vi = WVI(k);
         int64_t s = pb0 + off;
         while (x <= nak) {
-          if (cells[ha].mark > nak) {
+          if (hm > nak) {
             cells[s] = {ha, k, dif, nak};
             ha = (int)s;
+            hm = nak;
             s += 1;
           }
           nak -= tspace;
@@ -779,6 +808,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
         Tn[vi] = b;
         Mn[vi] = m;
         HAn[vi] = ha;
+        HMn[vi] = hm;
       }
       uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
       if (bb) {

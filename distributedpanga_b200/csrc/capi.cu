@@ -75,6 +75,7 @@ struct pga_ctx {
   float base_freq[4] = {.25f, .25f, .25f, .25f};
   bool freq_set = false;
   bool have_numeric = false;
+  DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab;
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
@@ -598,6 +599,21 @@ int run_align(pga_ctx *ctx) {
     launch_numeric(P<uint8_t>(ctx->bps), P<int64_t>(ctx->dclen), P<int64_t>(ctx->dboff), P<int64_t>(ctx->soff), nc,
                    P<uint8_t>(ctx->numf), P<uint8_t>(ctx->numr), ctx->st);
     LAUNCHED(1);
+    std::vector<int64_t> po(nc + 1), pw(nc + 1);
+    int64_t wsum = 0;
+    for (int c = 0; c < nc; c++) {
+      pw[c] = ctx->clen[c] / 32 + 2;
+      po[c] = wsum;
+      wsum += pw[c];
+    }
+    ENSURE(ctx->pk, sizeof(uint64_t) * 4 * (size_t)(wsum + 1));
+    ENSURE(ctx->poff, sizeof(int64_t) * (nc + 1));
+    ENSURE(ctx->pwords, sizeof(int64_t) * (nc + 1));
+    CK(cudaMemcpyAsync(ctx->poff.p, po.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->pwords.p, pw.data(), sizeof(int64_t) * (nc + 1), cudaMemcpyHostToDevice, ctx->st));
+    launch_pack(P<uint8_t>(ctx->numf), P<int64_t>(ctx->soff), P<int64_t>(ctx->dclen), P<int64_t>(ctx->poff),
+                P<int64_t>(ctx->pwords), nc, P<uint64_t>(ctx->pk), ctx->st);
+    LAUNCHED(1);
     if (!ctx->freq_set) {
       ENSURE(ctx->u64tmp, 64);
       CK(cudaMemsetAsync(ctx->u64tmp.p, 0, 32, ctx->st));
@@ -669,6 +685,9 @@ int run_align(pga_ctx *ctx) {
   L.rc = P<uint8_t>(ctx->numr);
   L.soff = P<int64_t>(ctx->soff);
   L.clen = P<int64_t>(ctx->dclen);
+  L.pk = P<uint64_t>(ctx->pk);
+  L.poff = P<int64_t>(ctx->poff);
+  L.pwords = P<int64_t>(ctx->pwords);
   L.score = P<int16_t>(ctx->spec_tab);
   L.table = P<int16_t>(ctx->spec_tab) + 32768;
   L.ave_path = ave_path;
@@ -728,7 +747,12 @@ int run_align(pga_ctx *ctx) {
   int r = align_run_tasks(ctx, L, first, out1);
   if (r) return r;
   int64_t calls = 0;
-  for (auto &o : out1) calls += o.calls;
+  long long maxcyc = 0, sumcyc = 0;
+  for (auto &o : out1) {
+    calls += o.calls;
+    maxcyc = std::max(maxcyc, o.cycles);
+    sumcyc += o.cycles;
+  }
 
   // 6. self pairs: entry values by FastGA's order (src/fastga_order.c)
   int64_t nrounds = 0;
@@ -838,6 +862,8 @@ int run_align(pga_ctx *ctx) {
         int x = F.pos[batch[i].a];
         S[x] = ob[i].calls > 0 ? 3 + (int64_t)ob[i].exit_bepos : 2;
         calls += ob[i].calls;
+        maxcyc = std::max(maxcyc, ob[i].cycles);
+        sumcyc += ob[i].cycles;
       }
     }
     for (size_t q = 0; q < self_idx.size(); q++)
@@ -880,8 +906,10 @@ int run_align(pga_ctx *ctx) {
   ctx->align_stats[0] = (int64_t)(pairs[0].size() + pairs[1].size());
   ctx->align_stats[1] = (int64_t)self_idx.size();
   ctx->align_stats[2] = calls;
+  ctx->align_stats[3] = maxcyc;
   ctx->align_stats[4] = (int64_t)nrec;
   ctx->align_stats[5] = nrounds;
+  ctx->align_stats[6] = sumcyc;
   ctx->have_align = true;
   return PGA_OK;
 }
@@ -918,7 +946,7 @@ void pga_ctx_destroy(pga_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->st);
-  DBuf *abufs[] = {&ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout,
+  DBuf *abufs[] = {&ctx->pk, &ctx->poff, &ctx->pwords, &ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout,
                    &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab};

@@ -147,8 +147,9 @@ int pga_align(pga_ctx *ctx, int64_t *nalign);
  * Compress_TraceTo8 leaves them, lib/align.c:3892). */
 int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *trace);
 
-/* [0] pairs [1] self pairs [2] Local_Alignment calls [3] 0 [4] alignments
- * [5] self-pair rounds [6..7] 0 */
+/* [0] pairs [1] self pairs [2] Local_Alignment calls [3] SM cycles of the
+ * longest pair [4] alignments [5] self-pair rounds [6] SM cycles of all pairs
+ * [7] 0 */
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
 
 #ifdef __cplusplus
