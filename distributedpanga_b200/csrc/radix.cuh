@@ -22,7 +22,7 @@ __device__ __forceinline__ uint32_t u128_digit(const U128 &k, int shift) {
   return (uint32_t)(((shift < 64) ? (k.lo >> shift) : (k.hi >> (shift - 64))) & 0xff);
 }
 
-__global__ void k_radix_hist(const U128 *__restrict__ keys, int64_t n, int shift,
+static __global__ void k_radix_hist(const U128 *__restrict__ keys, int64_t n, int shift,
                              uint32_t *__restrict__ hist, int nb) {
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
@@ -36,7 +36,7 @@ __global__ void k_radix_hist(const U128 *__restrict__ keys, int64_t n, int shift
   hist[(int64_t)threadIdx.x * nb + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void k_radix_scatter(const U128 *__restrict__ in, U128 *__restrict__ out, int64_t n,
+static __global__ void k_radix_scatter(const U128 *__restrict__ in, U128 *__restrict__ out, int64_t n,
                                 int shift, const uint32_t *__restrict__ offs, int nb) {
   __shared__ uint32_t run[256];
   __shared__ uint32_t wc[RADIX_THREADS / 32][256];
@@ -77,7 +77,7 @@ __global__ void k_radix_scatter(const U128 *__restrict__ in, U128 *__restrict__ 
 }
 
 // Bits in which any key differs from key 0: OR of (key ^ key0).
-__global__ void k_u128_diffbits(const U128 *__restrict__ keys, int64_t n, unsigned long long *acc) {
+static __global__ void k_u128_diffbits(const U128 *__restrict__ keys, int64_t n, unsigned long long *acc) {
   __shared__ unsigned long long slo, shi;
   if (threadIdx.x == 0) { slo = 0; shi = 0; }
   __syncthreads();

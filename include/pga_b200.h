@@ -152,6 +152,29 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
  * [7] 0 */
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
 
+/* ---- seed diagonal sort without device allocation ---------------------------- */
+
+/* No counterpart in the reference: the reference runs on the host and never
+ * meets this constraint.  The same result as pga_reimport_sort, for callers
+ * that may not call cudaMalloc -- for instance a program living inside
+ * another framework's device memory pool (PyTorch's caching allocator, a
+ * serving runtime's arena) that owns the GPU memory it may use.  The caller
+ * passes device buffers it already owns: `seeds_dev` (len bytes of seeds),
+ * `out_dev` ((len/seed_bytes) * swide bytes) and `panel_off_dev`
+ * (ncontig+1 int64); no context is needed.  All other work space is one
+ * fixed array compiled into the library (about 12 MB, held on every GPU that
+ * loads it until the process exits).  At most 262,144 seeds per call
+ * (PGA_ERR_LIMIT beyond).  The first call on a device looks the array's
+ * address up once for that device; make that first call before any stream
+ * capture.  The call synchronizes `stream` (a cudaStream_t, NULL for the
+ * default stream) once, midway; the last kernels are left queued on it.
+ * Calls share the array: calls that overlap on the GPU (several host
+ * threads or streams) race.  Returns PGA_OK, PGA_ERR_ARG, PGA_ERR_LIMIT or
+ * PGA_ERR_CUDA. */
+int pga_reimport_sort_noalloc(const uint8_t *seeds_dev, int64_t len, int position_bytes,
+                              int contig_strand_bytes, int comp, int ncontig, int64_t amxpos, int dbyte,
+                              uint8_t *out_dev, int64_t *panel_off_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
