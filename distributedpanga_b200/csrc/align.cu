@@ -37,6 +37,100 @@ struct WarpAligner {
   __device__ int err() const { return W.err; }
 };
 
+__device__ OvlArena warp_arena(const AlignLaunch &P, int64_t wid) {
+  OvlArena O;
+  O.ovl = P.ovl + wid * P.ovl_cap;
+  O.perm = P.perm + wid * 2 * P.ovl_cap;
+  O.tmp = O.perm + P.ovl_cap;
+  O.ovl_cap = P.ovl_cap;
+  O.bytes = P.cand_bytes;
+  O.pool_next = P.cand_next;
+  O.pool_cap = P.cand_cap;
+  O.nbyte = O.byte_cap = 0;
+  O.nov = 0;
+  O.err = 0;
+  return O;
+}
+
+// First index >= x in [x, hi) whose band differs from its predecessor's
+// (x itself when x == 0), else hi; warp-wide.
+__device__ int64_t next_band_start(const KeySeeds &S, int64_t x, int64_t hi, int lane) {
+  if (x <= 0) return 0;
+  for (int64_t base = x; base < hi; base += 32) {
+    int64_t i = base + lane;
+    bool f = i < hi && S.band(i) != S.band(i - 1);
+    unsigned m = __ballot_sync(FULL, f);
+    if (m) return base + __ffs(m) - 1;
+  }
+  return hi;
+}
+
+// The sort / elimination step of a pair whose candidates are in O, then its
+// survivors appended to the output in the pair's order (lane 0 ranks them).
+__device__ void finish_and_emit(const AlignLaunch &P, OvlArena &O, int a, int b, int comp, PairOut &po,
+                                int lane) {
+  if (lane == 0) finish_pair(O);
+  __syncwarp();
+  // lane 0 may have taken trace bytes from the pool (entwine merges): every
+  // lane continues from its chunk
+  O.nbyte = __shfl_sync(FULL, O.nbyte, 0);
+  O.byte_cap = __shfl_sync(FULL, O.byte_cap, 0);
+  int ferr = __shfl_sync(FULL, O.err, 0);
+  if (ferr) {
+    po.err = ferr | 0x200;
+    return;
+  }
+  int ns = 0;
+  int64_t tb = 0;
+  if (lane == 0)
+    for (int64_t q = 0; q < O.nov; q++) {
+      const Ovl &o = O.ovl[O.perm[q]];
+      if (o.flags & ELIMINATED) continue;
+      ns++;
+      tb += o.tlen;
+    }
+  ns = __shfl_sync(FULL, ns, 0);
+  tb = __shfl_sync(FULL, tb, 0);
+  unsigned long long r0 = 0, b0 = 0;
+  if (lane == 0 && ns > 0) {
+    r0 = atomicAdd(P.rec_next, (unsigned long long)ns);
+    b0 = atomicAdd(P.out_next, (unsigned long long)tb);
+  }
+  r0 = __shfl_sync(FULL, r0, 0);
+  b0 = __shfl_sync(FULL, b0, 0);
+  if (ns > 0 && ((int64_t)(r0 + ns) > P.rec_cap || (int64_t)(b0 + tb) > P.out_cap)) {
+    po.err = ALN_ERR_OVLS | 0x400;
+    return;
+  }
+  if (ns == 0) return;
+  int64_t rr = (int64_t)r0, bb = (int64_t)b0;
+  int rank = 0;
+  for (int64_t q = 0; q < O.nov; q++) {
+    const Ovl o = O.ovl[O.perm[q]];
+    if (o.flags & ELIMINATED) continue;
+    if (lane == 0) {
+      AlnRec &r = P.recs[rr];
+      r.aread = a;
+      r.bread = b;
+      r.comp = comp;
+      r.abpos = o.abpos;
+      r.aepos = o.aepos;
+      r.bbpos = o.bbpos;
+      r.bepos = o.bepos;
+      r.diffs = o.diffs;
+      r.tlen = o.tlen;
+      r.rank = rank;
+      r.toff = bb;
+    }
+    for (int q2 = lane; q2 < o.tlen; q2 += 32) P.out_bytes[bb + q2] = P.cand_bytes[o.toff + q2];
+    rr++;
+    bb += o.tlen;
+    rank++;
+  }
+  po.nsurv = ns;
+  po.rec_off = (int64_t)r0;
+}
+
 __global__ void __launch_bounds__(ALIGN_THREADS)
 k_align_pairs(AlignLaunch P) {
   const int lane = threadIdx.x & 31;
@@ -70,14 +164,7 @@ k_align_pairs(AlignLaunch P) {
   W.pool.cap = P.cell_cap;
   W.chunk_next = W.chunk_end = 0;
 
-  OvlArena O;
-  O.ovl = P.ovl + wid * P.ovl_cap;
-  O.perm = P.perm + wid * P.ovl_cap;
-  O.ovl_cap = P.ovl_cap;
-  O.bytes = P.cand_bytes;
-  O.pool_next = P.cand_next;
-  O.pool_cap = P.cand_cap;
-  O.nbyte = O.byte_cap = 0;
+  OvlArena O = warp_arena(P, wid);
 
   while (true) {
     unsigned t = 0;
@@ -101,9 +188,14 @@ k_align_pairs(AlignLaunch P) {
     path.tlen = path.diffs = path.abpos = path.bbpos = path.aepos = 0;
     path.bepos = tk.entry_bepos;
     path.trace_off = 0;
+    int64_t blo = 0, bhi = S.n;
+    if (tk.seg >= 0) {
+      blo = next_band_start(S, tk.slo - tk.lo, S.n, lane);
+      bhi = next_band_start(S, tk.shi - tk.lo, S.n, lane);
+    }
     PairResult R;
     WarpAligner AL{W, spec};
-    int rc = align_pair(S, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane, 32);
+    int rc = align_pair(S, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane, 32, blo, bhi);
     __syncwarp();
     PairOut po;
     po.calls = R.calls;
@@ -111,63 +203,62 @@ k_align_pairs(AlignLaunch P) {
     po.nsurv = 0;
     po.rec_off = 0;
     po.err = rc ? (W.err | O.err | 0x100) : 0;
-    if (rc == 0) {
-      if (lane == 0) finish_pair(O);
-      __syncwarp();
-      int ferr = __shfl_sync(FULL, O.err, 0);
-      if (ferr) po.err = ferr | 0x200;
-    }
-    if (po.err == 0) {
-      // survivors in the pair's output order (perm order)
-      int ns = 0;
-      int64_t tb = 0;
-      if (lane == 0)
-        for (int64_t q = 0; q < O.nov; q++) {
-          const Ovl &o = O.ovl[O.perm[q]];
-          if (o.flags & ELIMINATED) continue;
-          ns++;
-          tb += o.tlen;
-        }
-      ns = __shfl_sync(FULL, ns, 0);
-      tb = __shfl_sync(FULL, tb, 0);
-      unsigned long long r0 = 0, b0 = 0;
-      if (lane == 0 && ns > 0) {
-        r0 = atomicAdd(P.rec_next, (unsigned long long)ns);
-        b0 = atomicAdd(P.out_next, (unsigned long long)tb);
+    if (rc == 0 && tk.seg >= 0) {
+      // a band range: its candidates to the range store, in order
+      unsigned long long g0 = 0;
+      if (lane == 0 && O.nov > 0) g0 = atomicAdd(P.rng_next, (unsigned long long)O.nov);
+      g0 = __shfl_sync(FULL, g0, 0);
+      if ((int64_t)g0 + O.nov > P.rng_cap) {
+        po.err = ALN_ERR_OVLS | 0x800;
+      } else {
+        for (int64_t q = lane; q < O.nov; q += 32) P.rng_ovl[g0 + q] = O.ovl[q];
+        po.nsurv = (int)O.nov;
+        po.rec_off = (int64_t)g0;
       }
-      r0 = __shfl_sync(FULL, r0, 0);
-      b0 = __shfl_sync(FULL, b0, 0);
-      if (ns > 0 && ((int64_t)(r0 + ns) > P.rec_cap || (int64_t)(b0 + tb) > P.out_cap)) {
-        po.err = ALN_ERR_OVLS | 0x400;
-      } else if (ns > 0) {
-        int64_t rr = (int64_t)r0, bb = (int64_t)b0;
-        int rank = 0;
-        for (int64_t q = 0; q < O.nov; q++) {
-          const Ovl o = O.ovl[O.perm[q]];
-          if (o.flags & ELIMINATED) continue;
-          if (lane == 0) {
-            AlnRec &a = P.recs[rr];
-            a.aread = tk.a;
-            a.bread = tk.b;
-            a.comp = tk.comp;
-            a.abpos = o.abpos;
-            a.aepos = o.aepos;
-            a.bbpos = o.bbpos;
-            a.bepos = o.bepos;
-            a.diffs = o.diffs;
-            a.tlen = o.tlen;
-            a.rank = rank;
-            a.toff = bb;
-          }
-          for (int q2 = lane; q2 < o.tlen; q2 += 32) P.out_bytes[bb + q2] = P.cand_bytes[o.toff + q2];
-          rr++;
-          bb += o.tlen;
-          rank++;
-        }
-        po.nsurv = ns;
-        po.rec_off = (int64_t)r0;
-      }
+    } else if (rc == 0) {
+      finish_and_emit(P, O, tk.a, tk.b, tk.comp, po, lane);
     }
+    po.cycles = clock64() - t0;
+    if (lane == 0) P.pout[t] = po;
+    __syncwarp();
+  }
+}
+
+// Finishes the pairs that ran as band ranges: gathers each pair's candidates
+// from its ranges in range order (the order one warp running the whole pair
+// would have made them in), then the pair's sort / elimination step and
+// output.  The pair's calls are the ranges' sum and its exit bepos the last
+// range's with a call (the entry value when none called).
+__global__ void __launch_bounds__(ALIGN_THREADS)
+k_finish_pairs(AlignLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
+  if (wid >= P.nwarps) return;
+  OvlArena O = warp_arena(P, wid);
+  for (int64_t t = wid; t < P.nftasks; t += P.nwarps) {
+    const FinishTask ft = P.ftasks[t];
+    long long t0 = clock64();
+    PairOut po;
+    po.calls = 0;
+    po.exit_bepos = ft.entry_bepos;
+    po.nsurv = 0;
+    po.rec_off = 0;
+    po.err = 0;
+    O.nov = 0;
+    O.err = 0;
+    for (int k = 0; k < ft.nseg; k++) {
+      const PairOut ro = P.range_out[P.range_idx[ft.first + k]];
+      po.calls += ro.calls;
+      if (ro.calls > 0) po.exit_bepos = ro.exit_bepos;
+      if (O.nov + ro.nsurv > O.ovl_cap) {
+        po.err = ALN_ERR_OVLS | 0x1000;
+        break;
+      }
+      for (int q = lane; q < ro.nsurv; q += 32) O.ovl[O.nov + q] = P.rng_ovl[ro.rec_off + q];
+      O.nov += ro.nsurv;
+    }
+    __syncwarp();
+    if (po.err == 0) finish_and_emit(P, O, ft.a, ft.b, ft.comp, po, lane);
     po.cycles = clock64() - t0;
     if (lane == 0) P.pout[t] = po;
     __syncwarp();
@@ -295,6 +386,10 @@ void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st) {
   k_align_pairs<<<grid, ALIGN_THREADS, 0, st>>>(P);
+}
+
+void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st) {
+  k_finish_pairs<<<grid, ALIGN_THREADS, 0, st>>>(P);
 }
 
 void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,

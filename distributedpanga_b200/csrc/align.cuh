@@ -11,16 +11,29 @@ namespace pga {
 constexpr int ALIGN_THREADS = 128;  // 4 warps per CTA, one pair per warp at a time
 constexpr int WAVE_INTS = 13;       // per diagonal slot: V,M,HA,HM x2, NA, T x2 (uint64)
 
-// One (anchor, partner) pair of a unit: seeds [lo, hi) of the unit's sorted keys.
+// One (anchor, partner) pair of a unit: seeds [lo, hi) of the unit's sorted
+// keys.  seg < 0: the whole pair, finished by the same warp.  seg >= 0: one
+// band range of a large pair of two different contigs: the band blocks
+// whose first stream starts in [slo, shi), both moved forward to the next
+// band start; its candidates go to the range store and k_finish_pairs
+// finishes the pair.
 struct PairTask {
-  int comp, a, b, self, entry_bepos, pad;
-  int64_t lo, hi;
+  int comp, a, b, self, entry_bepos, seg;
+  int64_t lo, hi, slo, shi;
 };
 
+// Per task.  For a range task nsurv is its candidate count and rec_off the
+// offset of its candidates in the range store.
 struct PairOut {
   int calls, exit_bepos, nsurv, err;
   int64_t rec_off;
-  long long cycles;  // SM clock cycles the warp spent on the pair
+  long long cycles;  // SM clock cycles the warp spent on the task
+};
+
+// A pair split into ranges: its ranges' PairOut indices are
+// range_idx[first .. first + nseg).
+struct FinishTask {
+  int comp, a, b, entry_bepos, first, nseg;
 };
 
 // One surviving alignment; trace bytes (uint8 pairs: diffs, b-delta per
@@ -52,8 +65,15 @@ struct AlignLaunch {
   unsigned long long *cell_next;
   int64_t cell_cap;
   aln::Ovl *ovl;
-  int *perm;
+  int *perm;  // 2 * ovl_cap ints per warp: the order and the merge sort's buffer
   int64_t ovl_cap;
+  aln::Ovl *rng_ovl;                 // range store: candidates of range tasks
+  unsigned long long *rng_next;
+  int64_t rng_cap;
+  const FinishTask *ftasks;          // k_finish_pairs
+  int nftasks;
+  const int *range_idx;
+  const PairOut *range_out;
   uint8_t *cand_bytes;
   unsigned long long *cand_next;
   int64_t cand_cap;
@@ -67,6 +87,7 @@ struct AlignLaunch {
 };
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
+void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *boff, int ncontig,
                         unsigned long long *cnt, cudaStream_t st);
 void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,

@@ -795,6 +795,7 @@ struct Ovl {
 struct OvlArena {
   Ovl *ovl;
   int *perm;
+  int *tmp;  // ovl_cap ints for the merge sort in finish_pair (nullptr: insertion sort)
   int64_t ovl_cap;
   uint8_t *bytes;
   int64_t byte_cap;
@@ -895,15 +896,35 @@ PGA_HD void finish_pair(OvlArena &O) {
   Ovl *ov = O.ovl;
   int *perm = O.perm;
   for (int64_t j = 0; j < nlas; j++) perm[j] = (int)j;
-  // stable insertion sort by abpos (ALIGN_SORT under glibc's stable qsort)
-  for (int64_t j = 1; j < nlas; j++) {
-    int x = perm[j];
-    int64_t k = j - 1;
-    while (k >= 0 && ov[perm[k]].abpos > ov[x].abpos) {
-      perm[k + 1] = perm[k];
-      k--;
+  // stable sort by abpos (ALIGN_SORT under glibc's stable qsort): bottom-up
+  // merge sort through O.tmp, or insertion sort without it
+  if (O.tmp != nullptr && nlas > 16) {
+    int *src = perm, *dst = O.tmp;
+    for (int64_t w = 1; w < nlas; w <<= 1) {
+      for (int64_t lo = 0; lo < nlas; lo += 2 * w) {
+        int64_t mid = lo + w < nlas ? lo + w : nlas;
+        int64_t hi = lo + 2 * w < nlas ? lo + 2 * w : nlas;
+        int64_t i = lo, j = mid, k = lo;
+        while (i < mid && j < hi) dst[k++] = (ov[src[j]].abpos < ov[src[i]].abpos) ? src[j++] : src[i++];
+        while (i < mid) dst[k++] = src[i++];
+        while (j < hi) dst[k++] = src[j++];
+      }
+      int *x = src;
+      src = dst;
+      dst = x;
     }
-    perm[k + 1] = x;
+    if (src != perm)
+      for (int64_t j = 0; j < nlas; j++) perm[j] = src[j];
+  } else {
+    for (int64_t j = 1; j < nlas; j++) {
+      int x = perm[j];
+      int64_t k = j - 1;
+      while (k >= 0 && ov[perm[k]].abpos > ov[x].abpos) {
+        perm[k + 1] = perm[k];
+        k--;
+      }
+      perm[k + 1] = x;
+    }
   }
   for (int64_t j = nlas - 1; j >= 0; j--) {
     Ovl &o = ov[perm[j]];
@@ -1038,10 +1059,18 @@ struct PairResult {
 // diagonal reads the bepos it holds on entry.  `lane`/`nl`: a warp runs this
 // with every lane on the same values; lane 0 writes the candidate records and
 // the lanes share the trace copies.
+//
+// [blo, bhi) limits the run to the band blocks whose first stream starts
+// there (blo and bhi must be band starts: 0, n, or an index whose band
+// differs from its predecessor's).  A block reads only its own two bands and
+// resets its chain state, so for a pair of two different contigs -- where
+// `path` carries nothing from one call to the next -- the blocks of
+// consecutive ranges can run on different warps and their candidates,
+// concatenated in range order, are exactly the whole run's.
 template <class SeedsT, class Aligner>
 PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const Seq &B, int64_t amxpos,
                       int64_t maxdag, Aligner &AL, Path &path, OvlArena &O, PairResult &R, int lane = 0,
-                      int nl = 1) {
+                      int nl = 1, int64_t blo = 0, int64_t bhi = -1) {
   const int alnMin = ALIGN_MIN - 50;
   const double alnRate = 0.3 + .05;  // ALIGN_RATE + .05
   const int64_t bmxpos = amxpos;
@@ -1054,12 +1083,15 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
   R.exit_bepos = path.bepos;
   O.nov = 0;
   if (O.pool_next == nullptr) O.nbyte = 0;
-  if (n == 0) return 0;
+  if (bhi < 0 || bhi > n) bhi = n;
+  if (blo < 0) blo = 0;
+  if (blo >= bhi) return 0;
 
-  int64_t b = 0, e = 0, m;
-  int64_t cdiag = S.band(0);
+  int64_t b = blo, e = blo, m;
+  int64_t cdiag = S.band(blo);
   while (e < n && S.band(e) == cdiag) e++;
-  int isnew = 1;
+  // a block is "new" unless the band just below it has seeds
+  int isnew = (blo == 0 || S.band(blo - 1) != cdiag - 1) ? 1 : 0;
   while (1) {
     int aux = 0;
     m = e;
@@ -1203,6 +1235,7 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
       while (e < n && S.band(e) == cdiag) e++;
       isnew = 1;
     }
+    if (b >= bhi) break;
   }
   R.exit_bepos = path.bepos;
   return 0;

@@ -77,11 +77,13 @@ struct pga_ctx {
   bool have_numeric = false;
   DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
-      cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab;
+      cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
+      ridx;
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
-  int64_t align_stats[8] = {0};    // pairs, self pairs, calls, candidates, survivors, rounds, reruns, 0
+  int64_t align_stats[8] = {0};
+  int64_t range_seeds = 0;         // pga_align_set_ranges    // pairs, self pairs, calls, candidates, survivors, rounds, reruns, 0
   bool have_align = false;
 
   // generic byte staging
@@ -549,26 +551,121 @@ void fo_ranges(int n, const std::vector<int64_t> &clen_pos, int64_t npost, const
   }
 }
 
-int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &tasks, std::vector<PairOut> &outs) {
+// Runs one launch of pair tasks and returns one PairOut per task.  With
+// `range_seeds` > 0 every pair of two different contigs with more seeds than
+// that runs as consecutive band ranges of about that many seeds on different
+// warps (its band blocks are independent), and k_finish_pairs finishes it.
+// Tasks go to the warps largest first.
+int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &tasks, std::vector<PairOut> &outs,
+                    int64_t range_seeds, long long *max_cycles) {
   outs.assign(tasks.size(), PairOut{});
   if (tasks.empty()) return PGA_OK;
-  ENSURE(ctx->tasks, sizeof(PairTask) * tasks.size());
-  ENSURE(ctx->pout, sizeof(PairOut) * tasks.size());
-  CK(cudaMemcpyAsync(ctx->tasks.p, tasks.data(), sizeof(PairTask) * tasks.size(), cudaMemcpyHostToDevice, ctx->st));
+  std::vector<PairTask> run;
+  std::vector<FinishTask> fin;
+  std::vector<int> fin_of(tasks.size(), -1), ridx;
+  std::vector<std::vector<int>> ranges;  // per finish task: its ranges' indices in `run`
+  for (size_t i = 0; i < tasks.size(); i++) {
+    PairTask t = tasks[i];
+    t.seg = -1;
+    t.slo = t.lo;
+    t.shi = t.hi;
+    int64_t n = t.hi - t.lo;
+    if (range_seeds > 0 && !t.self && n > range_seeds) {
+      FinishTask f;
+      f.comp = t.comp;
+      f.a = t.a;
+      f.b = t.b;
+      f.entry_bepos = t.entry_bepos;
+      f.nseg = (int)((n + range_seeds - 1) / range_seeds);
+      f.first = 0;
+      fin_of[i] = (int)fin.size();
+      ranges.emplace_back();
+      for (int k = 0; k < f.nseg; k++) {
+        PairTask r = t;
+        r.seg = k;
+        r.slo = t.lo + k * range_seeds;
+        r.shi = std::min(t.hi, t.lo + (k + 1) * range_seeds);
+        ranges.back().push_back((int)run.size());
+        run.push_back(r);
+      }
+      fin.push_back(f);
+    } else {
+      fin_of[i] = -2 - (int)run.size();  // whole pair at run[-2 - fin_of]
+      run.push_back(t);
+    }
+  }
+  // largest first
+  std::vector<int> order(run.size());
+  for (size_t i = 0; i < run.size(); i++) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (run[x].shi - run[x].slo) > (run[y].shi - run[y].slo);
+  });
+  std::vector<int> where(run.size());
+  std::vector<PairTask> sorted(run.size());
+  for (size_t k = 0; k < order.size(); k++) {
+    sorted[k] = run[order[k]];
+    where[order[k]] = (int)k;
+  }
+  for (size_t f = 0; f < fin.size(); f++) {
+    fin[f].first = (int)ridx.size();
+    for (int r : ranges[f]) ridx.push_back(where[r]);
+  }
+  ENSURE(ctx->tasks, sizeof(PairTask) * sorted.size());
+  ENSURE(ctx->pout, sizeof(PairOut) * sorted.size());
+  CK(cudaMemcpyAsync(ctx->tasks.p, sorted.data(), sizeof(PairTask) * sorted.size(), cudaMemcpyHostToDevice,
+                     ctx->st));
   CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
+  CK(cudaMemsetAsync(ctx->rng_next.p, 0, 8, ctx->st));
   L.tasks = P<PairTask>(ctx->tasks);
-  L.ntasks = (int)tasks.size();
+  L.ntasks = (int)sorted.size();
   L.pout = P<PairOut>(ctx->pout);
   int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
   launch_align(L, grid, ctx->st);
   LAUNCHED(1);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(outs.data(), ctx->pout.p, sizeof(PairOut) * tasks.size(), cudaMemcpyDeviceToHost, ctx->st));
+  std::vector<PairOut> fo(fin.size());
+  if (!fin.empty()) {
+    ENSURE(ctx->ftasks, sizeof(FinishTask) * fin.size());
+    ENSURE(ctx->fout, sizeof(PairOut) * fin.size());
+    ENSURE(ctx->ridx, sizeof(int) * ridx.size());
+    CK(cudaMemcpyAsync(ctx->ftasks.p, fin.data(), sizeof(FinishTask) * fin.size(), cudaMemcpyHostToDevice,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->ridx.p, ridx.data(), sizeof(int) * ridx.size(), cudaMemcpyHostToDevice, ctx->st));
+    AlignLaunch F = L;
+    F.ftasks = P<FinishTask>(ctx->ftasks);
+    F.nftasks = (int)fin.size();
+    F.range_idx = P<int>(ctx->ridx);
+    F.range_out = P<PairOut>(ctx->pout);
+    F.pout = P<PairOut>(ctx->fout);
+    launch_finish(F, grid, ctx->st);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(fo.data(), ctx->fout.p, sizeof(PairOut) * fin.size(), cudaMemcpyDeviceToHost, ctx->st));
+  }
+  std::vector<PairOut> ro(sorted.size());
+  CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * sorted.size(), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
-  for (size_t i = 0; i < outs.size(); i++)
-    if (outs[i].err)
+  for (size_t k = 0; k < sorted.size(); k++) {
+    if (max_cycles) *max_cycles = std::max(*max_cycles, ro[k].cycles);
+    if (ro[k].err)
       return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
-                  tasks[i].a, tasks[i].b, tasks[i].comp ? "C" : "N", outs[i].err);
+                  sorted[k].a, sorted[k].b, sorted[k].comp ? "C" : "N", ro[k].err);
+  }
+  for (size_t f = 0; f < fin.size(); f++)
+    if (fo[f].err)
+      return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)", fin[f].a,
+                  fin[f].b, fin[f].comp ? "C" : "N", fo[f].err);
+  for (size_t i = 0; i < tasks.size(); i++) {
+    if (fin_of[i] >= 0) {
+      const int f = fin_of[i];
+      outs[i] = fo[f];
+      long long c = 0;
+      for (int r : ranges[f]) c += ro[where[r]].cycles;
+      outs[i].cycles = c + fo[f].cycles;  // the pair's warp-cycles, all ranges and the finish
+    } else {
+      outs[i] = ro[where[-2 - fin_of[i]]];
+    }
+  }
   return PGA_OK;
 }
 
@@ -667,9 +764,11 @@ int run_align(pga_ctx *ctx) {
       t.b = ab[2 * p + 1];
       t.self = (comp == 0 && t.a == t.b);
       t.entry_bepos = 0;
-      t.pad = 0;
+      t.seg = -1;
       t.lo = st[p];
       t.hi = (p + 1 < np) ? st[p + 1] : n;
+      t.slo = t.lo;
+      t.shi = t.hi;
       pairs[comp].push_back(t);
     }
   }
@@ -705,7 +804,10 @@ int run_align(pga_ctx *ctx) {
   ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
   ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
   ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * L.ovl_cap);
-  ENSURE(ctx->perm, sizeof(int) * (size_t)L.nwarps * L.ovl_cap);
+  ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * L.ovl_cap);
+  L.rng_cap = (int64_t)1 << 22;     // 4M candidates of band ranges
+  ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)L.rng_cap);
+  ENSURE(ctx->rng_next, 64);
   ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)L.cell_cap);
   ENSURE(ctx->cand, (size_t)L.cand_cap);
   ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)L.rec_cap);
@@ -731,6 +833,8 @@ int run_align(pga_ctx *ctx) {
   L.rec_next = P<unsigned long long>(ctx->rec_next);
   L.out_bytes = P<uint8_t>(ctx->outb);
   L.out_next = P<unsigned long long>(ctx->out_next);
+  L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
+  L.rng_next = P<unsigned long long>(ctx->rng_next);
 
   // 5. launch 1: every pair that does not read a leftover value (all C pairs,
   // every N pair of two different contigs), largest first
@@ -743,14 +847,19 @@ int run_align(pga_ctx *ctx) {
     }
   std::stable_sort(first.begin(), first.end(),
                    [](const PairTask &x, const PairTask &y) { return (x.hi - x.lo) > (y.hi - y.lo); });
+  // pairs above range_seeds run as band ranges: about 8 tasks per warp
+  int64_t first_seeds = 0;
+  for (auto &t : first) first_seeds += t.hi - t.lo;
+  const int64_t range_seeds = ctx->range_seeds < 0    ? 0
+                              : ctx->range_seeds > 0 ? ctx->range_seeds
+                                                     : std::max<int64_t>(512, first_seeds / (8 * L.nwarps));
   std::vector<PairOut> out1;
-  int r = align_run_tasks(ctx, L, first, out1);
+  long long maxcyc = 0, sumcyc = 0;
+  int r = align_run_tasks(ctx, L, first, out1, range_seeds, &maxcyc);
   if (r) return r;
   int64_t calls = 0;
-  long long maxcyc = 0, sumcyc = 0;
   for (auto &o : out1) {
     calls += o.calls;
-    maxcyc = std::max(maxcyc, o.cycles);
     sumcyc += o.cycles;
   }
 
@@ -854,7 +963,7 @@ int run_align(pga_ctx *ctx) {
       if (batch.empty()) break;
       nrounds++;
       std::vector<PairOut> ob;
-      r = align_run_tasks(ctx, L, batch, ob);
+      r = align_run_tasks(ctx, L, batch, ob, 0, &maxcyc);
       if (r) return r;
       for (size_t i = 0; i < batch.size(); i++) {
         size_t q = bq[i];
@@ -862,7 +971,6 @@ int run_align(pga_ctx *ctx) {
         int x = F.pos[batch[i].a];
         S[x] = ob[i].calls > 0 ? 3 + (int64_t)ob[i].exit_bepos : 2;
         calls += ob[i].calls;
-        maxcyc = std::max(maxcyc, ob[i].cycles);
         sumcyc += ob[i].cycles;
       }
     }
@@ -949,7 +1057,8 @@ void pga_ctx_destroy(pga_ctx *ctx) {
   DBuf *abufs[] = {&ctx->pk, &ctx->poff, &ctx->pwords, &ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout,
                    &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
-                   &ctx->pidx, &ctx->pstart, &ctx->pab};
+                   &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
+                   &ctx->fout, &ctx->ridx};
   for (DBuf *b : abufs)
     if (b->p) cudaFree(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
@@ -1451,6 +1560,12 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
   }
   if (trace_off) memcpy(trace_off, ctx->h_toff.data(), sizeof(int64_t) * (n + 1));
   if (trace && !ctx->h_trace.empty()) memcpy(trace, ctx->h_trace.data(), ctx->h_trace.size());
+  return PGA_OK;
+}
+
+int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds) {
+  if (!ctx || range_seeds < -1) return PGA_ERR_ARG;
+  ctx->range_seeds = range_seeds;
   return PGA_OK;
 }
 

@@ -67,6 +67,9 @@ _SIGS = {
     "pga_align": (C.c_int, [vp, C.POINTER(C.c_int64)]),
     "pga_align_copy": (C.c_int, [vp, vp, vp, vp]),
     "pga_align_stats": (C.c_int, [vp, vp]),
+    "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
+    "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
+                                            C.c_int, vp, vp, vp]),
 }
 
 _LIB = None
@@ -280,6 +283,10 @@ class Device:
         self._ck(self.L.pga_align(self.h, C.byref(n)), "align")
         self.nalign = n.value
         return n.value
+
+    def set_ranges(self, range_seeds: int) -> None:
+        """Band-range size for large pairs (0 automatic, -1 never split)."""
+        self._ck(self.L.pga_align_set_ranges(self.h, int(range_seeds)), "align_set_ranges")
 
     def alignments(self):
         """(records (n, 9) int32: aread abpos aepos bread bbpos bepos comp diffs tlen,

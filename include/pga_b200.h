@@ -141,6 +141,15 @@ int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4);
  * needed.  *nalign = surviving alignments. */
 int pga_align(pga_ctx *ctx, int64_t *nalign);
 
+/* How pga_align spreads large pairs of two different contigs over warps: it
+ * cuts such a pair into ranges of about range_seeds seeds at band
+ * boundaries, aligns the ranges on different warps (a pair's band blocks are
+ * independent) and finishes the pair from the ranges' candidates in order;
+ * the result is the same for every setting.  0 (default): automatic; -1: never
+ * split; n > 0: ranges of n seeds.  No counterpart in the reference (one
+ * thread runs each pair there). */
+int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
+
 /* The alignments in la_sort order: per alignment 9 ints (aread abpos aepos
  * bread bbpos bepos comp diffs tlen), trace_off (nalign+1) and the trace
  * bytes (uint8 pairs: differences, b-delta per 100-base A interval, as
@@ -148,8 +157,8 @@ int pga_align(pga_ctx *ctx, int64_t *nalign);
 int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *trace);
 
 /* [0] pairs [1] self pairs [2] Local_Alignment calls [3] SM cycles of the
- * longest pair [4] alignments [5] self-pair rounds [6] SM cycles of all pairs
- * [7] 0 */
+ * longest warp task (a pair, or a band range of a large pair) [4] alignments
+ * [5] self-pair rounds [6] SM cycles of all tasks [7] 0 */
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
 
 /* ---- seed diagonal sort without device allocation ---------------------------- */

@@ -20,11 +20,17 @@ extern "C" {
 // output order: aread bread comp abpos aepos bbpos bepos diffs tlen
 // followed by the trace bytes in `tr`.  Also per pair: anchor, partner,
 // calls, exit bepos (pairs_out, 4 ints per pair).
+//
+// split > 0 runs every pair of two different contigs the way the GPU runs a
+// large one: as consecutive seed ranges of `split` seeds, each moved forward
+// to the next band start, aligned separately and their candidates
+// concatenated in range order before the pair's sort / elimination step; the
+// pair's exit bepos is the last range's with a call.
 int aht_align_unit(const uint8_t *bps, int ncontig, const int64_t *clen, const int64_t *boff, const float *freq,
                    const uint8_t *rec, const int64_t *panel_off, int swide, int dbyte, int ctgb, int comp,
                    const int *self_entry, int vcap, int64_t cell_cap, int64_t ovl_cap,
                    int *rows, int64_t row_cap, int64_t *nrows, uint8_t *tr, int64_t tr_cap, int64_t *ntr,
-                   int *pairs_out, int64_t pair_cap, int64_t *npairs) {
+                   int *pairs_out, int64_t pair_cap, int64_t *npairs, int64_t split) {
   int64_t maxctg = 0;
   for (int i = 0; i < ncontig; i++) maxctg = clen[i] > maxctg ? clen[i] : maxctg;
   std::vector<int16_t> score(32768), table(32768);
@@ -54,13 +60,23 @@ int aht_align_unit(const uint8_t *bps, int ncontig, const int64_t *clen, const i
   W.err = 0;
   OvlArena O;
   std::vector<Ovl> ovl(ovl_cap);
-  std::vector<int> perm(ovl_cap);
+  std::vector<int> perm(ovl_cap), tmp(ovl_cap);
   int64_t bcap = 64 * (maxctg / 100 + 4) + (1 << 20);
   std::vector<uint8_t> bytes(bcap);
-  O.ovl = ovl.data(); O.perm = perm.data(); O.ovl_cap = ovl_cap; O.bytes = bytes.data(); O.byte_cap = bcap;
+  O.ovl = ovl.data(); O.perm = perm.data(); O.tmp = tmp.data(); O.ovl_cap = ovl_cap; O.bytes = bytes.data();
+  O.byte_cap = bcap;
   O.err = 0;
   O.pool_next = nullptr;
   O.pool_cap = 0;
+  // one range's candidates when split > 0
+  OvlArena G;
+  std::vector<Ovl> govl(split > 0 ? ovl_cap : 1);
+  std::vector<uint8_t> gbytes(split > 0 ? bcap : 1);
+  G.ovl = govl.data(); G.perm = nullptr; G.tmp = nullptr; G.ovl_cap = split > 0 ? ovl_cap : 0;
+  G.bytes = gbytes.data(); G.byte_cap = split > 0 ? bcap : 0;
+  G.err = 0;
+  G.pool_next = nullptr;
+  G.pool_cap = 0;
   Path path;
   memset(&path, 0, sizeof(path));
   *nrows = 0; *ntr = 0; *npairs = 0;
@@ -96,7 +112,35 @@ int aht_align_unit(const uint8_t *bps, int ncontig, const int64_t *clen, const i
       Seq B{fwd[jc].data() + 1, (int)clen[jc]};
       PairResult R;
       ScalarAligner AL{W, spec};
-      if (align_pair(S, comp != 0, self, A, B, maxctg, 2 * maxctg, AL, path, O, R)) return 100 + (W.err | O.err);
+      if (split <= 0 || self) {
+        if (align_pair(S, comp != 0, self, A, B, maxctg, 2 * maxctg, AL, path, O, R)) return 100 + (W.err | O.err);
+      } else {
+        const int64_t n = S.n;
+        auto band_start = [&](int64_t x) {
+          while (x < n && x > 0 && S.band(x) == S.band(x - 1)) x++;
+          return x < n ? x : n;
+        };
+        O.nov = 0;
+        O.nbyte = 0;
+        R.calls = 0;
+        R.exit_bepos = path.bepos;
+        for (int64_t lo = 0; lo < n; lo += split) {
+          int64_t blo = band_start(lo), bhi = band_start(lo + split < n ? lo + split : n);
+          PairResult Rg;
+          if (align_pair(S, comp != 0, false, A, B, maxctg, 2 * maxctg, AL, path, G, Rg, 0, 1, blo, bhi))
+            return 100 + (W.err | G.err);
+          if (O.nov + G.nov > O.ovl_cap || O.nbyte + G.nbyte > O.byte_cap) return 300;
+          for (int64_t q = 0; q < G.nov; q++) {
+            Ovl o = G.ovl[q];
+            memcpy(O.bytes + O.nbyte, G.bytes + o.toff, o.tlen);
+            o.toff = O.nbyte;
+            O.nbyte += o.tlen;
+            O.ovl[O.nov++] = o;
+          }
+          R.calls += Rg.calls;
+          if (Rg.calls > 0) R.exit_bepos = Rg.exit_bepos;
+        }
+      }
       finish_pair(O);
       if (O.err) return 200 + O.err;
       if (*npairs < pair_cap) {

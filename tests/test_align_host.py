@@ -29,12 +29,12 @@ def aht():
     L = C.CDLL(so)
     vp, i64, ci = C.c_void_p, C.c_int64, C.c_int
     L.aht_align_unit.argtypes = [vp, ci, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp, ci, i64, i64, vp, i64, vp, vp,
-                                 i64, vp, vp, i64, vp]
+                                 i64, vp, vp, i64, vp, i64]
     L.aht_align_unit.restype = ci
     return L
 
 
-def run_unit(L, cs, arr, off, dig, comp, self_entry=None):
+def run_unit(L, cs, arr, off, dig, comp, self_entry=None, split=0):
     rows = np.zeros((400000, 9), np.int32)
     tr = np.zeros(64_000_000, np.uint8)
     pairs = np.zeros((200000, 4), np.int32)
@@ -45,7 +45,7 @@ def run_unit(L, cs, arr, off, dig, comp, self_entry=None):
                           dig["swide"], dig["dbyte"], dig["ctgb"], comp,
                           se.ctypes.data if se is not None else None, 8192, 50_000_000, 1_000_000,
                           rows.ctypes.data, len(rows), C.byref(nr), tr.ctypes.data, len(tr), C.byref(nt),
-                          pairs.ctypes.data, len(pairs), C.byref(npair))
+                          pairs.ctypes.data, len(pairs), C.byref(npair), split)
     assert rc == 0, rc
     out, o = [], 0
     for r in rows[: nr.value]:
@@ -181,3 +181,24 @@ def test_host_aligner_matches_reference(oracle, aht, case):
            if l.strip()]
     assert len(mine) == dig["aln"]["count"]
     assert mine == ref
+
+
+@pytest.mark.parametrize("case", ["small_s002", "chromset_s0005", "edge_mix", "small_full"])
+def test_host_block_ranges_compose(oracle, aht, case):
+    """Splitting each pair of two different contigs into consecutive band
+    ranges (as the GPU does with large pairs) and concatenating the ranges'
+    candidates gives the whole-pair run's output, record for record and in
+    the same order, and the same calls and exit bepos per pair."""
+    cs, dig = load_case(case)
+    posb, ctgb = dig["posb"], dig["ctgb"]
+    srt = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    ent, cum, _ = oracle.build_adapter(srt, posb, ctgb)
+    ns, css, _, _ = oracle.merge(ent, cum, posb, ctgb, 10, cs.ncontig)
+    for comp, seeds in ((0, ns), (1, css)):
+        arr, off = oracle.reimport_sort(seeds, posb, ctgb, comp, cs.ncontig, cs.maxctg, dig["dbyte"])
+        whole, pw = run_unit(aht, cs, arr, off, dig, comp)
+        for split in (1, 13, 200):
+            part, pp = run_unit(aht, cs, arr, off, dig, comp, split=split)
+            assert len(part) == len(whole)
+            assert part == whole, (comp, split)
+            assert np.array_equal(pp, pw), (comp, split)

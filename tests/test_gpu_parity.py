@@ -149,9 +149,32 @@ def test_alignments_match_reference(dev, case):
     dev.gdb_load(cs)
     dev.index_build(want_entries=False)
     dev.merge(dig["freq_cutoff"])
+    dev.set_ranges(0)
     n = dev.align()
     recs, toff, tr = dev.alignments()
     mine = _aln_norm(alignment_lines(recs, toff, tr))
     ref = _aln_norm(gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n"))
     assert n == dig["aln"]["count"]
     assert mine == ref
+
+
+@pytest.mark.parametrize("case", ["chromset_s0005", "small_full"])
+def test_alignments_independent_of_band_ranges(dev, case):
+    """Large pairs cut into band ranges on many warps (down to one band per
+    range) give the same alignments as whole pairs on one warp each."""
+    from distributedpanga_b200.pipeline import alignment_lines
+    cs, dig = load_case(case)
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=False)
+    dev.merge(dig["freq_cutoff"])
+    got = {}
+    try:
+        for r in (-1, 1, 64):
+            dev.set_ranges(r)
+            dev.align()
+            got[r] = alignment_lines(*dev.alignments())
+    finally:
+        dev.set_ranges(0)
+    assert len(got[-1]) == dig["aln"]["count"]
+    assert got[1] == got[-1]
+    assert got[64] == got[-1]
