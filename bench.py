@@ -350,8 +350,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
                    "pairs": astats["pairs"], "self_pairs": astats["self_pairs"],
                    "local_alignment_calls": astats["calls"], "alignments": astats["alignments"],
-                   "longest_pair_ms_at_max_clock": astats["max_pair_cycles"] / 1965e3,
-                   "all_pairs_warp_s_at_max_clock": astats["all_pair_cycles"] / 1965e6,
+                   "longest_warp_task_ms_at_max_clock": astats["max_task_cycles"] / 1965e3,
+                   "longest_warp_task_calls": astats["max_task_calls"],
+                   "all_tasks_warp_s_at_max_clock": astats["all_task_cycles"] / 1965e6,
                    "aligned_bases": aligned_bases,
                    "record_bytes": rsize, "swide": swide,
                    "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),

@@ -82,8 +82,9 @@ struct pga_ctx {
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
-  int64_t align_stats[8] = {0};
-  int64_t range_seeds = 0;         // pga_align_set_ranges    // pairs, self pairs, calls, candidates, survivors, rounds, reruns, 0
+  int64_t align_stats[8] = {0};    // pga_align_stats
+  int64_t range_seeds = 0;         // pga_align_set_ranges
+  unsigned long long rec_used = 0, out_used = 0;  // survivors so far in recs / outb
   bool have_align = false;
 
   // generic byte staging
@@ -121,6 +122,29 @@ int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
     cudaGetLastError();
     return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
   }
+  b.cap = bytes;
+  return PGA_OK;
+}
+
+// Grows b to `bytes`, keeping its first `keep` bytes.
+int grow_keep(pga_ctx *ctx, DBuf &b, size_t bytes, size_t keep) {
+  if (b.cap >= bytes) return PGA_OK;
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  if (keep > 0) {
+    e = cudaMemcpyAsync(p, b.p, keep, cudaMemcpyDeviceToDevice, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) {
+      cudaFree(p);
+      return fail(ctx, PGA_ERR_CUDA, "grow copy: %s", cudaGetErrorString(e));
+    }
+  }
+  if (b.p) cudaFree(b.p);
+  b.p = p;
   b.cap = bytes;
   return PGA_OK;
 }
@@ -557,7 +581,7 @@ void fo_ranges(int n, const std::vector<int64_t> &clen_pos, int64_t npost, const
 // warps (its band blocks are independent), and k_finish_pairs finishes it.
 // Tasks go to the warps largest first.
 int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &tasks, std::vector<PairOut> &outs,
-                    int64_t range_seeds, long long *max_cycles) {
+                    int64_t range_seeds, long long *max_cycles, int64_t *max_task_calls) {
   outs.assign(tasks.size(), PairOut{});
   if (tasks.empty()) return PGA_OK;
   std::vector<PairTask> run;
@@ -594,11 +618,12 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
       run.push_back(t);
     }
   }
-  // largest first
+  // largest pair first, a pair's ranges in order (a large pair's ranges each
+  // tend to re-extend its longest alignments, so they start early)
   std::vector<int> order(run.size());
   for (size_t i = 0; i < run.size(); i++) order[i] = (int)i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return (run[x].shi - run[x].slo) > (run[y].shi - run[y].slo);
+    return (run[x].hi - run[x].lo) > (run[y].hi - run[y].lo);
   });
   std::vector<int> where(run.size());
   std::vector<PairTask> sorted(run.size());
@@ -614,16 +639,6 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
   ENSURE(ctx->pout, sizeof(PairOut) * sorted.size());
   CK(cudaMemcpyAsync(ctx->tasks.p, sorted.data(), sizeof(PairTask) * sorted.size(), cudaMemcpyHostToDevice,
                      ctx->st));
-  CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
-  CK(cudaMemsetAsync(ctx->rng_next.p, 0, 8, ctx->st));
-  L.tasks = P<PairTask>(ctx->tasks);
-  L.ntasks = (int)sorted.size();
-  L.pout = P<PairOut>(ctx->pout);
-  int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
-  launch_align(L, grid, ctx->st);
-  LAUNCHED(1);
-  CK(cudaGetLastError());
-  std::vector<PairOut> fo(fin.size());
   if (!fin.empty()) {
     ENSURE(ctx->ftasks, sizeof(FinishTask) * fin.size());
     ENSURE(ctx->fout, sizeof(PairOut) * fin.size());
@@ -631,30 +646,111 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
     CK(cudaMemcpyAsync(ctx->ftasks.p, fin.data(), sizeof(FinishTask) * fin.size(), cudaMemcpyHostToDevice,
                        ctx->st));
     CK(cudaMemcpyAsync(ctx->ridx.p, ridx.data(), sizeof(int) * ridx.size(), cudaMemcpyHostToDevice, ctx->st));
-    AlignLaunch F = L;
-    F.ftasks = P<FinishTask>(ctx->ftasks);
-    F.nftasks = (int)fin.size();
-    F.range_idx = P<int>(ctx->ridx);
-    F.range_out = P<PairOut>(ctx->pout);
-    F.pout = P<PairOut>(ctx->fout);
-    launch_finish(F, grid, ctx->st);
+  }
+  std::vector<PairOut> fo(fin.size()), ro(sorted.size());
+  const int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
+  for (int attempt = 0;; attempt++) {
+    // pebbles and candidate traces live for one launch; survivors accumulate
+    CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
+    CK(cudaMemsetAsync(ctx->rng_next.p, 0, 8, ctx->st));
+    CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
+    CK(cudaMemsetAsync(ctx->cand_next.p, 0, 8, ctx->st));
+    CK(cudaMemcpyAsync(ctx->rec_next.p, &ctx->rec_used, 8, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->out_next.p, &ctx->out_used, 8, cudaMemcpyHostToDevice, ctx->st));
+    L.tasks = P<PairTask>(ctx->tasks);
+    L.ntasks = (int)sorted.size();
+    L.pout = P<PairOut>(ctx->pout);
+    launch_align(L, grid, ctx->st);
     LAUNCHED(1);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(fo.data(), ctx->fout.p, sizeof(PairOut) * fin.size(), cudaMemcpyDeviceToHost, ctx->st));
-  }
-  std::vector<PairOut> ro(sorted.size());
-  CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * sorted.size(), cudaMemcpyDeviceToHost, ctx->st));
-  CK(cudaStreamSynchronize(ctx->st));
-  for (size_t k = 0; k < sorted.size(); k++) {
-    if (max_cycles) *max_cycles = std::max(*max_cycles, ro[k].cycles);
-    if (ro[k].err)
+    if (!fin.empty()) {
+      AlignLaunch F = L;
+      F.ftasks = P<FinishTask>(ctx->ftasks);
+      F.nftasks = (int)fin.size();
+      F.range_idx = P<int>(ctx->ridx);
+      F.range_out = P<PairOut>(ctx->pout);
+      F.pout = P<PairOut>(ctx->fout);
+      launch_finish(F, grid, ctx->st);
+      LAUNCHED(1);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(fo.data(), ctx->fout.p, sizeof(PairOut) * fin.size(), cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * sorted.size(), cudaMemcpyDeviceToHost, ctx->st));
+    unsigned long long used[2] = {0, 0};
+    CK(cudaMemcpyAsync(&used[0], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&used[1], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    int errs = 0, bad = -1, badf = -1;
+    for (size_t k = 0; k < sorted.size(); k++)
+      if (ro[k].err) {
+        errs |= ro[k].err;
+        if (bad < 0) bad = (int)k;
+      }
+    for (size_t f = 0; f < fin.size(); f++)
+      if (fo[f].err) {
+        errs |= fo[f].err;
+        if (badf < 0) badf = (int)f;
+      }
+    if (errs == 0) {
+      ctx->rec_used = used[0];
+      ctx->out_used = used[1];
+      break;
+    }
+    // grow what overflowed and run the launch again
+    bool grown = false;
+    if (attempt < 6) {
+      int r = PGA_OK;
+      if (errs & aln::ALN_ERR_CELLS) {
+        r = r ? r : ensure(ctx, ctx->cells, 2 * ctx->cells.cap);
+        L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
+        L.cells = P<aln::Pebble>(ctx->cells);
+        grown = true;
+      }
+      if (errs & aln::ALN_ERR_TRACE) {
+        r = r ? r : ensure(ctx, ctx->cand, 2 * ctx->cand.cap);
+        L.cand_cap = (int64_t)ctx->cand.cap;
+        L.cand_bytes = P<uint8_t>(ctx->cand);
+        grown = true;
+      }
+      if (errs & 0x800) {
+        r = r ? r : ensure(ctx, ctx->rng_ovl, 2 * ctx->rng_ovl.cap);
+        L.rng_cap = (int64_t)(ctx->rng_ovl.cap / sizeof(aln::Ovl));
+        L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
+        grown = true;
+      }
+      if (errs & 0x400) {
+        r = r ? r : grow_keep(ctx, ctx->recs, 2 * ctx->recs.cap, sizeof(AlnRec) * ctx->rec_used);
+        r = r ? r : grow_keep(ctx, ctx->outb, 2 * ctx->outb.cap, ctx->out_used);
+        L.rec_cap = (int64_t)(ctx->recs.cap / sizeof(AlnRec));
+        L.out_cap = (int64_t)ctx->outb.cap;
+        L.recs = P<AlnRec>(ctx->recs);
+        L.out_bytes = P<uint8_t>(ctx->outb);
+        grown = true;
+      }
+      if ((errs & 0x1000) || ((errs & aln::ALN_ERR_OVLS) && !(errs & (0x400 | 0x800)))) {
+        int64_t oc = 2 * L.ovl_cap;
+        r = r ? r : ensure(ctx, ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * oc);
+        r = r ? r : ensure(ctx, ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * oc);
+        L.ovl_cap = oc;
+        L.ovl = P<aln::Ovl>(ctx->ovl);
+        L.perm = P<int>(ctx->perm);
+        grown = true;
+      }
+      if (r) return r;
+    }
+    if (!grown) {
+      if (bad >= 0)
+        return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
+                    sorted[bad].a, sorted[bad].b, sorted[bad].comp ? "C" : "N", ro[bad].err);
       return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
-                  sorted[k].a, sorted[k].b, sorted[k].comp ? "C" : "N", ro[k].err);
+                  fin[badf].a, fin[badf].b, fin[badf].comp ? "C" : "N", fo[badf].err);
+    }
   }
-  for (size_t f = 0; f < fin.size(); f++)
-    if (fo[f].err)
-      return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)", fin[f].a,
-                  fin[f].b, fin[f].comp ? "C" : "N", fo[f].err);
+  for (size_t k = 0; k < sorted.size(); k++)
+    if (ro[k].cycles > *max_cycles) {
+      *max_cycles = ro[k].cycles;
+      *max_task_calls = ro[k].calls;
+    }
   for (size_t i = 0; i < tasks.size(); i++) {
     if (fin_of[i] >= 0) {
       const int f = fin_of[i];
@@ -795,31 +891,32 @@ int run_align(pga_ctx *ctx) {
   L.nwarps = 148 * 16;
   L.vcap = 8192;
   L.point_cap = 4 * (maxctg / 100 + 4) + 64;
-  L.ovl_cap = 16384;
-  L.cell_cap = (int64_t)1 << 30;   // 16 GB of pebbles
-  L.cand_cap = (int64_t)4 << 30;   // 4 GB of candidate traces
-  L.rec_cap = (int64_t)1 << 24;    // 16M surviving alignments
-  L.out_cap = (int64_t)2 << 30;    // 2 GB of surviving traces
+  // Pools sized from the sequence total; align_run_tasks grows one that
+  // overflows and reruns the launch.  Buffers keep their size across calls.
+  int64_t seqtot = 0;
+  for (int c = 0; c < nc; c++) seqtot += ctx->clen[c];
   ENSURE(ctx->task_next, 64);
   ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
   ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
-  ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * L.ovl_cap);
-  ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * L.ovl_cap);
-  L.rng_cap = (int64_t)1 << 22;     // 4M candidates of band ranges
-  ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)L.rng_cap);
+  ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * 16384);
+  ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * 16384);
+  ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)std::max<int64_t>(1 << 18, seqtot / 256));
+  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)std::max<int64_t>(1 << 24, 4 * seqtot));
+  ENSURE(ctx->cand, (size_t)std::max<int64_t>(64 << 20, 2 * seqtot));
+  ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)std::max<int64_t>(1 << 20, seqtot / 256));
+  ENSURE(ctx->outb, (size_t)std::max<int64_t>(64 << 20, seqtot / 8));
+  L.ovl_cap = (int64_t)(ctx->ovl.cap / (sizeof(aln::Ovl) * L.nwarps));
+  L.rng_cap = (int64_t)(ctx->rng_ovl.cap / sizeof(aln::Ovl));
+  L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
+  L.cand_cap = (int64_t)ctx->cand.cap;
+  L.rec_cap = (int64_t)(ctx->recs.cap / sizeof(AlnRec));
+  L.out_cap = (int64_t)ctx->outb.cap;
   ENSURE(ctx->rng_next, 64);
-  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)L.cell_cap);
-  ENSURE(ctx->cand, (size_t)L.cand_cap);
-  ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)L.rec_cap);
-  ENSURE(ctx->outb, (size_t)L.out_cap);
   ENSURE(ctx->cell_next, 64);
   ENSURE(ctx->cand_next, 64);
   ENSURE(ctx->rec_next, 64);
   ENSURE(ctx->out_next, 64);
-  CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
-  CK(cudaMemsetAsync(ctx->cand_next.p, 0, 8, ctx->st));
-  CK(cudaMemsetAsync(ctx->rec_next.p, 0, 8, ctx->st));
-  CK(cudaMemsetAsync(ctx->out_next.p, 0, 8, ctx->st));
+  ctx->rec_used = ctx->out_used = 0;
   L.next_task = P<unsigned>(ctx->task_next);
   L.wave = P<int>(ctx->wave);
   L.points = P<uint16_t>(ctx->points);
@@ -847,15 +944,16 @@ int run_align(pga_ctx *ctx) {
     }
   std::stable_sort(first.begin(), first.end(),
                    [](const PairTask &x, const PairTask &y) { return (x.hi - x.lo) > (y.hi - y.lo); });
-  // pairs above range_seeds run as band ranges: about 8 tasks per warp
+  // pairs above range_seeds run as band ranges: about 32 tasks per warp
   int64_t first_seeds = 0;
   for (auto &t : first) first_seeds += t.hi - t.lo;
   const int64_t range_seeds = ctx->range_seeds < 0    ? 0
                               : ctx->range_seeds > 0 ? ctx->range_seeds
-                                                     : std::max<int64_t>(512, first_seeds / (8 * L.nwarps));
+                                                     : std::max<int64_t>(256, first_seeds / (32 * L.nwarps));
   std::vector<PairOut> out1;
   long long maxcyc = 0, sumcyc = 0;
-  int r = align_run_tasks(ctx, L, first, out1, range_seeds, &maxcyc);
+  int64_t maxcalls = 0;
+  int r = align_run_tasks(ctx, L, first, out1, range_seeds, &maxcyc, &maxcalls);
   if (r) return r;
   int64_t calls = 0;
   for (auto &o : out1) {
@@ -963,7 +1061,7 @@ int run_align(pga_ctx *ctx) {
       if (batch.empty()) break;
       nrounds++;
       std::vector<PairOut> ob;
-      r = align_run_tasks(ctx, L, batch, ob, 0, &maxcyc);
+      r = align_run_tasks(ctx, L, batch, ob, 0, &maxcyc, &maxcalls);
       if (r) return r;
       for (size_t i = 0; i < batch.size(); i++) {
         size_t q = bq[i];
@@ -1018,6 +1116,7 @@ int run_align(pga_ctx *ctx) {
   ctx->align_stats[4] = (int64_t)nrec;
   ctx->align_stats[5] = nrounds;
   ctx->align_stats[6] = sumcyc;
+  ctx->align_stats[7] = maxcalls;
   ctx->have_align = true;
   return PGA_OK;
 }

@@ -304,7 +304,8 @@ class Device:
         a = np.zeros(8, dtype=np.int64)
         self._ck(self.L.pga_align_stats(self.h, a.ctypes.data_as(vp)), "align_stats")
         return {"pairs": int(a[0]), "self_pairs": int(a[1]), "calls": int(a[2]), "alignments": int(a[4]),
-                "self_rounds": int(a[5]), "max_pair_cycles": int(a[3]), "all_pair_cycles": int(a[6])}
+                "self_rounds": int(a[5]), "max_task_cycles": int(a[3]), "all_task_cycles": int(a[6]),
+                "max_task_calls": int(a[7])}
 
 
 def alignment_lines(recs, toff, tr):

@@ -158,7 +158,8 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
 
 /* [0] pairs [1] self pairs [2] Local_Alignment calls [3] SM cycles of the
  * longest warp task (a pair, or a band range of a large pair) [4] alignments
- * [5] self-pair rounds [6] SM cycles of all tasks [7] 0 */
+ * [5] self-pair rounds [6] SM cycles of all tasks [7] Local_Alignment calls
+ * of the longest task */
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
 
 /* ---- seed diagonal sort without device allocation ---------------------------- */
