@@ -16,6 +16,11 @@ namespace pga {
 
 using namespace aln;
 
+// A pair's seeds as its sorted keys, read by a whole warp: band scans test
+// 32 keys per step, and a Cursor holds a window of 32 decoded seeds (one per
+// lane) that the lane-uniform chain driver reads with shuffles, so a stream
+// costs one coalesced load per 32 seeds.  All lanes call every method with
+// the same arguments.
 struct KeySeeds {
   const U128 *k;
   int64_t n;
@@ -24,6 +29,50 @@ struct KeySeeds {
   __device__ int64_t band(int64_t i) const { return (int64_t)key_bits(k[i], L.off_band, L.off_j - L.off_band); }
   __device__ int lcp(int64_t i) const { return (int)key_bits(k[i], 0, 6); }
   __device__ int dlow(int64_t i) const { return (int)key_bits(k[i], L.off_dlow, 6); }
+  __device__ int64_t band_end(int64_t i, int64_t b) const {
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = i; base < n; base += 32) {
+      int64_t j = base + lane;
+      bool stop = j < n && band(j) != b;
+      unsigned msk = __ballot_sync(FULL, stop);
+      if (msk) return base + __ffs(msk) - 1;
+    }
+    return n;
+  }
+  struct Cursor {
+    const KeySeeds *S;
+    int64_t wb;        // window start: this lane holds seed wb + lane
+    uint32_t a;        // its antidiagonal (DBYTE <= 4 bytes)
+    int ld;            // its lcp | dlow << 8
+    __device__ void fill(int64_t i) {
+      wb = i;
+      int64_t j = i + (threadIdx.x & 31);
+      a = 0;
+      ld = 0;
+      if (j < S->n) {
+        U128 key = S->k[j];
+        a = (uint32_t)key_bits(key, S->L.off_anti, S->L.off_band - S->L.off_anti);
+        ld = (int)key_bits(key, 0, 6) | ((int)key_bits(key, S->L.off_dlow, 6) << 8);
+      }
+    }
+    __device__ int at(int64_t i) {
+      if ((uint64_t)(i - wb) >= 32) fill(i);
+      return (int)(i - wb);
+    }
+    __device__ int64_t anti(int64_t i) {
+      int q = at(i);
+      return (int64_t)__shfl_sync(FULL, a, q);
+    }
+    __device__ int lcp(int64_t i) {
+      int q = at(i);
+      return __shfl_sync(FULL, ld, q) & 0xff;
+    }
+    __device__ int dlow(int64_t i) {
+      int q = at(i);
+      return __shfl_sync(FULL, ld, q) >> 8;
+    }
+  };
+  __device__ Cursor cursor() const { return Cursor{this, -64, 0, 0}; }
 };
 
 struct WarpAligner {

@@ -1021,7 +1021,9 @@ PGA_HD void finish_pair(OvlArena &O) {
 }
 
 // Seeds of one (anchor, partner) pair in diagonal-sort order, decoded into
-// arrays (host harness).  Any type with the same accessors works.
+// arrays (host harness).  Any type with the same interface works: band(i),
+// band_end(i, band) = the first index >= i whose band differs (or n), and a
+// Cursor reading anti / lcp / dlow of a stream that mostly moves forward.
 struct PairSeeds {
   const int64_t *anti_;
   const int64_t *band_;
@@ -1032,6 +1034,17 @@ struct PairSeeds {
   PGA_HD int64_t band(int64_t i) const { return band_[i]; }
   PGA_HD int lcp(int64_t i) const { return lcp_[i]; }
   PGA_HD int dlow(int64_t i) const { return dlow_[i]; }
+  PGA_HD int64_t band_end(int64_t i, int64_t b) const {
+    while (i < n && band_[i] == b) i++;
+    return i;
+  }
+  struct Cursor {
+    const PairSeeds *S;
+    PGA_HD int64_t anti(int64_t i) { return S->anti_[i]; }
+    PGA_HD int lcp(int64_t i) { return S->lcp_[i]; }
+    PGA_HD int dlow(int64_t i) { return S->dlow_[i]; }
+  };
+  PGA_HD Cursor cursor() const { return Cursor{this}; }
 };
 
 // The scalar aligner: Local_Alignment on one thread.
@@ -1089,43 +1102,42 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
 
   int64_t b = blo, e = blo, m;
   int64_t cdiag = S.band(blo);
-  while (e < n && S.band(e) == cdiag) e++;
+  e = S.band_end(e, cdiag);
+  // the two streams of a block: band cdiag from b, band cdiag+1 from m
+  typename SeedsT::Cursor C1 = S.cursor(), C2 = S.cursor();
   // a block is "new" unless the band just below it has seeds
   int isnew = (blo == 0 || S.band(blo - 1) != cdiag - 1) ? 1 : 0;
   while (1) {
-    int aux = 0;
     m = e;
-    while (e < n && S.band(e) == cdiag + 1) {
-      e++;
-      aux = 1;
-    }
+    e = S.band_end(e, cdiag + 1);
+    int aux = e > m ? 1 : 0;
     if (isnew || aux) {
       int go = 1, lcp, wch = 0, mix = 0, dgmin = 2 * BUCK_WIDTH, dgmax = 0, dg = 0;
       int64_t cov = 0, ahgh = -CHAIN_BREAK, alow, amid, alast = -1, anti;
       int64_t s = b, t = m;
-      int64_t ipost = S.anti(s);
-      int64_t apost = aux ? S.anti(t) : MAX_I64;
+      int64_t ipost = C1.anti(s);
+      int64_t apost = aux ? C2.anti(t) : MAX_I64;
       alow = apost < ipost ? apost : ipost;
       while (go) {
         if (apost < ipost) {
-          lcp = S.lcp(t);
-          dg = S.dlow(t) + BUCK_WIDTH;
+          lcp = C2.lcp(t);
+          dg = C2.dlow(t) + BUCK_WIDTH;
           anti = apost;
           t += 1;
-          apost = (t >= e) ? MAX_I64 : S.anti(t);
+          apost = (t >= e) ? MAX_I64 : C2.anti(t);
           wch = 0x2;
         } else {
           // s == m is one past the first stream: the reference reads that
           // record's lcp and diagonal (unused: go becomes 0 below)
-          lcp = (s < n) ? S.lcp(s) : 0;
-          dg = (s < n) ? S.dlow(s) : 0;
+          lcp = (s < n) ? C1.lcp(s) : 0;
+          dg = (s < n) ? C1.dlow(s) : 0;
           anti = ipost;
           s += 1;
           if (s >= m) {
             if (s > m) go = 0;
             else ipost = MAX_I64;
           } else
-            ipost = S.anti(s);
+            ipost = C1.anti(s);
           wch = 0x1;
         }
         lcp <<= 1;
@@ -1232,7 +1244,7 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
     } else {
       b = e;
       cdiag = S.band(e);
-      while (e < n && S.band(e) == cdiag) e++;
+      e = S.band_end(e, cdiag);
       isnew = 1;
     }
     if (b >= bhi) break;

@@ -205,6 +205,398 @@ __device__ __forceinline__ void history_run(uint64_t &b, int &m, int r) {
   b = r >= 64 ? ~0ull : ((b << r) | ((1ull << r) - 1));
 }
 
+// ---------------------------------------------------------------------------
+// One wave of forward_wave / reverse_wave after its boundary diagonals are
+// set: every diagonal of [low, hgh] computed from the previous wave's buffer
+// (cur) into the other buffer, in the reference's visit order (forward:
+// k = hgh..low, reverse: k = low..hgh).
+//
+// Each lane takes up to WJ consecutive diagonals of the visit order (lane 0
+// the first), so a wave of up to 32*WJ diagonals is one pass: the lane's
+// loads and snakes are independent and run side by side, and the visit-order
+// scans are a lane-local pass plus one warp scan.  Wider waves take several
+// passes, carried in visit order.
+// ---------------------------------------------------------------------------
+constexpr int WJ = 4;
+
+// What a one-pass sweep leaves in registers for wave_prune.
+struct WaveSlice {
+  int c[WJ];
+  int k0;       // the lane's first diagonal
+  int nact;     // its diagonals
+  bool single;  // one pass covered [low, hgh]
+};
+
+// Lockstep snakes of a lane's diagonals: forward along A.pf / B.pf from
+// (x, x-k), reverse along A.pr / B.pr from (A.len-x, B.len-y); stops and
+// sentinel hits as snake_fwd / snake_rev.
+template <bool FWD, int J>
+__device__ __forceinline__ void lane_snakes(const Seq &A, const Seq &B, int nact, const int *k, int *x, int *run,
+                                            int *hb, int *hA) {
+  int oa[J], ob[J], mx[J], t[J];
+  bool go[J];
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    go[j] = false;
+    hb[j] = hA[j] = 0;
+    t[j] = 0;
+    mx[j] = 0;
+    oa[j] = ob[j] = 0;
+    if (j < nact) {
+      int xx = x[j], y = xx - k[j];
+      if (FWD) {
+        if (y < 0 || y > B.len) hb[j] = 1;
+        else if (xx < 0 || xx > A.len) hA[j] = 1;
+        else {
+          int ra = A.len - xx, rb = B.len - y;
+          mx[j] = ra < rb ? ra : rb;
+          oa[j] = xx;
+          ob[j] = y;
+          go[j] = mx[j] > 0;
+        }
+      } else {
+        if (y <= 0 || y >= B.len + 1) hb[j] = 1;
+        else if (xx <= 0 || xx > A.len) hA[j] = 1;
+        else {
+          mx[j] = xx < y ? xx : y;
+          oa[j] = A.len - xx;
+          ob[j] = B.len - y;
+          go[j] = mx[j] > 0;
+        }
+      }
+    }
+  }
+  const uint64_t *pa = FWD ? A.pf : A.pr, *pb = FWD ? B.pf : B.pr;
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < J; j++) any |= go[j];
+  while (any) {
+    any = false;
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+      if (go[j]) {
+        uint64_t d = bases32(pa, oa[j] + t[j]) ^ bases32(pb, ob[j] + t[j]);
+        int chunk = mx[j] - t[j] < 32 ? mx[j] - t[j] : 32;
+        int lead = d ? (__clzll(d) >> 1) : 32;
+        if (lead < chunk) {
+          t[j] += lead;
+          go[j] = false;
+        } else {
+          t[j] += chunk;
+          go[j] = t[j] < mx[j];
+        }
+        any |= go[j];
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    if (j < nact && !hb[j] && !hA[j]) {
+      if (t[j] == mx[j]) {
+        int xx = x[j], y = xx - k[j];
+        int ra = FWD ? A.len - xx : xx, rb = FWD ? B.len - y : y;
+        if (rb <= ra) hb[j] = 1;
+        else hA[j] = 1;
+      }
+      x[j] = FWD ? x[j] + t[j] : x[j] - t[j];
+    }
+    run[j] = t[j];
+  }
+}
+
+// v[j] for a per-lane index j < J, without local memory
+template <int J>
+__device__ __forceinline__ int pick(const int *v, int j) {
+  int r = v[0];
+#pragma unroll
+  for (int q = 1; q < J; q++)
+    if (j == q) r = v[q];
+  return r;
+}
+
+// One pass of a wave over visit positions [p0, p0 + 32*J): lane l takes
+// positions p0 + l*J .. p0 + l*J + J-1.  carry is the running best before
+// the pass.
+template <bool FWD, int J>
+__device__ __forceinline__ int wave_pass(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
+                                         int hgh, int w, int p0, int dif, int cur, int &carry, int &besta,
+                                         int &bestx, int &lasta, int &trima, int &trimx, int &trimd, int &trimha,
+                                         int &more, int &aclip, int &bclip, WaveSlice &WS) {
+  const int lane = threadIdx.x & 31;
+  const int vmask = W.vcap - 1;
+  const int tspace = spec.trace_space;
+  const int PATH_AVE = spec.ave_path;
+  const int16_t *SCORE = spec.score;
+  const int16_t *TABLE = spec.table;
+  const int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur], *HMo = W.HM[cur];
+  const uint64_t *To = W.T[cur];
+  int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1], *HMn = W.HM[cur ^ 1];
+  uint64_t *Tn = W.T[cur ^ 1];
+  int *NA = W.NA;
+  Pebble *cells = W.pool.cells;
+  const int pl = p0 + lane * J;
+  int nact = w - pl;
+  if (nact > J) nact = J;
+  if (nact < 0) nact = 0;
+  const int k0 = FWD ? hgh - pl : low + pl;
+  int k[J], c[J], x[J], m[J], ha[J], hm[J], nak[J], run[J], hb[J], hA[J], npb[J];
+  uint64_t b[J];
+  // previous wave around the lane's diagonals: forward nv[i] = V[k0+1-i],
+  // reverse nv[i] = V[k0-1+i]
+  int nv[J + 2];
+#pragma unroll
+  for (int i = 0; i < J + 2; i++) {
+    nv[i] = 0;
+    if (nact > 0 && i < nact + 2) nv[i] = Vo[(FWD ? k0 + 1 - i : k0 - 1 + i) & vmask];
+  }
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    k[j] = FWD ? k0 - j : k0 + j;
+    c[j] = x[j] = m[j] = hm[j] = nak[j] = npb[j] = 0;
+    ha[j] = -1;
+    b[j] = 0;
+    if (j < nact) {
+      int src, sk;
+      if (FWD) {
+        int ap = nv[j], ac = nv[j + 1], am = nv[j + 2];
+        if (ac < am) src = (am < ap) ? 1 : -1;
+        else src = (ac < ap) ? 1 : 0;
+        c[j] = src == 1 ? ap + 1 : (src == -1 ? am + 1 : ac + 2);
+      } else {
+        int am = nv[j], ac = nv[j + 1], ap = nv[j + 2];
+        if (ac > ap) src = (ap > am) ? -1 : 1;
+        else src = (ac > am) ? -1 : 0;
+        c[j] = src == -1 ? am - 1 : (src == 1 ? ap - 1 : ac - 2);
+      }
+      sk = k[j] + src;
+      bool dflt = FWD ? (src == 1 && k[j] == hgh) : (src == -1 && k[j] == low);
+      if (dflt) {
+        m[j] = PATH_LEN;
+        b[j] = PATH_INT;
+      } else {
+        int si = sk & vmask;
+        m[j] = Mo[si];
+        b[j] = To[si];
+        ha[j] = HAo[si];
+        hm[j] = HMo[si];
+      }
+      nak[j] = NA[k[j] & vmask];
+      if ((b[j] & PATH_TOP) != 0) m[j] -= 1;
+      b[j] <<= 1;
+      x[j] = (c[j] + k[j]) >> 1;
+    }
+  }
+  lane_snakes<FWD, J>(A, B, nact, k, x, run, hb, hA);
+  int npl = 0;
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    if (j < nact) {
+      history_run(b[j], m[j], run[j]);
+      c[j] = (x[j] << 1) - k[j];
+      int hq = hm[j];
+      if (FWD) {
+        for (int q = nak[j]; x[j] >= q; q += tspace)
+          if (hq < q) {
+            npb[j]++;
+            hq = q;
+          }
+      } else {
+        for (int q = nak[j]; x[j] <= q; q -= tspace)
+          if (hq > q) {
+            npb[j]++;
+            hq = q;
+          }
+      }
+      npl += npb[j];
+    }
+  }
+  // pebble slots in visit order
+  int off, tot;
+  if (__ballot_sync(FULL, npl > 1) == 0) {
+    uint32_t one = __ballot_sync(FULL, npl == 1);
+    off = __popc(one & ((1u << lane) - 1));
+    tot = __popc(one);
+  } else {
+    off = warp_excl_sum(npl, lane);
+    tot = warp_sum(npl);
+  }
+  int64_t pb0 = warp_pebbles(W, tot);
+  if (pb0 < 0) return 1;
+  int64_t s = pb0 + off;
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    if (j < nact) {
+      if (FWD) {
+        while (x[j] >= nak[j]) {
+          if (hm[j] < nak[j]) {
+            cells[s] = {ha[j], k[j], dif, nak[j]};
+            ha[j] = (int)s;
+            hm[j] = nak[j];
+            s += 1;
+          }
+          nak[j] += tspace;
+        }
+      } else {
+        while (x[j] <= nak[j]) {
+          if (hm[j] > nak[j]) {
+            cells[s] = {ha[j], k[j], dif, nak[j]};
+            ha[j] = (int)s;
+            hm[j] = nak[j];
+            s += 1;
+          }
+          nak[j] -= tspace;
+        }
+      }
+      int vi = k[j] & vmask;
+      NA[vi] = nak[j];
+      Vn[vi] = c[j];
+      Tn[vi] = b[j];
+      Mn[vi] = m[j];
+      HAn[vi] = ha[j];
+      HMn[vi] = hm[j];
+    }
+  }
+  // clips: bclip from the first visited diagonal that met B's end, aclip
+  // from the last visited that met A's end
+  int fb = -1, la = -1;
+#pragma unroll
+  for (int j = J - 1; j >= 0; j--)
+    if (j < nact && hb[j]) fb = j;
+#pragma unroll
+  for (int j = 0; j < J; j++)
+    if (j < nact && hA[j]) la = j;
+  uint32_t bbl = __ballot_sync(FULL, fb >= 0), bal = __ballot_sync(FULL, la >= 0);
+  if (bbl) {
+    more = 0;
+    int L = __ffs(bbl) - 1;
+    int kk = __shfl_sync(FULL, FWD ? k0 - fb : k0 + fb, L);
+    if (FWD ? (bclip < kk) : (bclip > kk)) bclip = kk;
+  }
+  if (bal) {
+    more = 0;
+    int L = last_lane(bal);
+    aclip = __shfl_sync(FULL, FWD ? k0 - la : k0 + la, L);
+  }
+  // records: c beyond the running best (max forward, min reverse) in visit order
+  int agg = FWD ? -2147483647 : 2147483647;
+#pragma unroll
+  for (int j = 0; j < J; j++)
+    if (j < nact) agg = FWD ? max(agg, c[j]) : min(agg, c[j]);
+  int pm = FWD ? warp_excl_max(agg, lane, carry) : warp_excl_min(agg, lane, carry);
+  int lr = -1, lp = -1, lt = -1;
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    if (j < nact) {
+      bool rec = FWD ? c[j] > pm : c[j] < pm;
+      if (rec) {
+        pm = c[j];
+        lr = j;
+        if (m[j] >= PATH_AVE) {
+          lp = j;
+          if (TABLE[b[j] & TRIM_MASK] >= 0 && TABLE[(b[j] >> TRIM_LEN) & TRIM_MASK] + SCORE[b[j] & TRIM_MASK] >= 0)
+            lt = j;
+        }
+      }
+    }
+  }
+  uint32_t rb = __ballot_sync(FULL, lr >= 0);
+  if (rb) {
+    int L = last_lane(rb);
+    carry = __shfl_sync(FULL, pick<J>(c, lr), L);
+    besta = carry;
+    bestx = __shfl_sync(FULL, pick<J>(x, lr), L);
+    uint32_t pab = __ballot_sync(FULL, lp >= 0);
+    if (pab) {
+      lasta = __shfl_sync(FULL, pick<J>(c, lp), last_lane(pab));
+      uint32_t trb = __ballot_sync(FULL, lt >= 0);
+      if (trb) {
+        int T2 = last_lane(trb);
+        trima = __shfl_sync(FULL, pick<J>(c, lt), T2);
+        trimx = __shfl_sync(FULL, pick<J>(x, lt), T2);
+        trimd = dif;
+        trimha = __shfl_sync(FULL, pick<J>(ha, lt), T2);
+      }
+    }
+  }
+  if (WS.single) {
+#pragma unroll
+    for (int j = 0; j < J; j++) WS.c[j] = c[j];
+    WS.k0 = k0;
+    WS.nact = nact;
+  }
+  return 0;
+}
+
+// The whole wave: one pass of single diagonals when it is at most 32 wide,
+// else passes of WJ diagonals per lane.
+template <bool FWD>
+__device__ __forceinline__ int wave_sweep(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
+                                          int hgh, int dif, int cur, int &besta, int &bestx, int &lasta, int &trima,
+                                          int &trimx, int &trimd, int &trimha, int &more, int &aclip, int &bclip,
+                                          WaveSlice &WS) {
+  const int w = hgh - low + 1;
+  WS.single = w <= 32 * WJ;
+  WS.nact = 0;
+  WS.k0 = 0;
+  int carry = besta;
+  if (w <= 32)
+    return wave_pass<FWD, 1>(W, spec, A, B, low, hgh, w, 0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
+                             trimd, trimha, more, aclip, bclip, WS);
+  for (int p0 = 0; p0 < w; p0 += 32 * WJ)
+    if (wave_pass<FWD, WJ>(W, spec, A, B, low, hgh, w, p0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
+                           trimd, trimha, more, aclip, bclip, WS))
+      return 1;
+  return 0;
+}
+
+// WAVE_LAG pruning of [low, hgh] (already clipped) on the wave just made:
+// hgh becomes the largest and low the smallest diagonal within WAVE_LAG of
+// the best antidiagonal, or hgh = low - 1 when none is (the reference's
+// loop from either end).  V is the new wave's buffer.
+template <bool FWD>
+__device__ __forceinline__ void wave_prune(const WarpWork &W, const int *V, int besta, int &low, int &hgh,
+                                           const WaveSlice &WS) {
+  if (hgh < low) return;
+  const int vmask = W.vcap - 1;
+  const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+  if (WS.single) {
+    int kmax = -2147483647, kmin = 2147483647;
+#pragma unroll
+    for (int j = 0; j < WJ; j++) {
+      int k = FWD ? WS.k0 - j : WS.k0 + j;
+      if (j < WS.nact && k >= low && k <= hgh && (FWD ? WS.c[j] >= n : WS.c[j] <= n)) {
+        kmax = max(kmax, k);
+        kmin = min(kmin, k);
+      }
+    }
+    kmax = __reduce_max_sync(FULL, kmax);
+    kmin = __reduce_min_sync(FULL, kmin);
+    if (kmin <= kmax) {
+      hgh = kmax;
+      low = kmin;
+    } else
+      hgh = low - 1;
+    return;
+  }
+  if (FWD) {
+    while (hgh >= low)
+      if (V[hgh & vmask] < n)
+        hgh -= 1;
+      else {
+        while (V[low & vmask] < n) low += 1;
+        break;
+      }
+  } else {
+    while (hgh >= low)
+      if (V[hgh & vmask] > n)
+        hgh -= 1;
+      else {
+        while (V[low & vmask] > n) low += 1;
+        break;
+      }
+  }
+}
+
 #define WVI(k) ((k) & vmask)
 
 // ---------------------------------------------------------------------------
@@ -220,9 +612,6 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   int *NA = W.NA;
   Pebble *cells = W.pool.cells;
   const int tspace = spec.trace_space;
-  const int PATH_AVE = spec.ave_path;
-  const int16_t *SCORE = spec.score;
-  const int16_t *TABLE = spec.table;
 
   int hgh = maxd, low = *mind, dif = 0;
   int besta, bestx, trima, trimx, trimd, trimha, morea, morex, mored, moreha, more, morem, lasta;
@@ -346,12 +735,9 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.err |= ALN_ERR_VCAP;
       return 1;
     }
-    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur], *HMo = W.HM[cur];
-    uint64_t *To = W.T[cur];
-    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1], *HMn = W.HM[cur ^ 1];
-    uint64_t *Tn = W.T[cur ^ 1];
-    // boundary diagonals on the previous wave's buffer (lane 0; visible after syncwarp)
-    bool top_default = false;
+    int *Vo = W.V[cur];
+    // boundary diagonals on the previous wave's buffer (lane 0; visible after
+    // syncwarp); k = hgh+1 carries T = PATH_INT, M = PATH_LEN, HA = -1
     if (low >= minp) {
       if (lane == 0) {
         NA[WVI(low)] = NA[WVI(low + 1)];
@@ -370,104 +756,12 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       Vo[WVI(hgh + 1)] = -1;
       Vo[WVI(low - 1)] = -1;
     }
-    top_default = true;  // k = hgh+1 carries T = PATH_INT, M = PATH_LEN, HA = -1
     dif += 1;
     __syncwarp();
-    int carry = besta;
-    for (int base = hgh; base >= low; base -= 32) {
-      int k = base - lane;
-      bool act = k >= low;
-      int x = 0, c = 0, m = 0, ha = -1, hm = 0, hb = 0, hA = 0, npb = 0, nak = 0;
-      uint64_t b = 0;
-      if (act) {
-        int vi = WVI(k);
-        int ap = Vo[WVI(k + 1)], ac = Vo[vi], am = Vo[WVI(k - 1)];
-        int src;  // 1: k+1, 0: k, -1: k-1
-        if (ac < am)
-          src = (am < ap) ? 1 : -1;
-        else
-          src = (ac < ap) ? 1 : 0;
-        int sk = k + src;
-        c = src == 1 ? ap + 1 : (src == -1 ? am + 1 : ac + 2);
-        if (src == 1 && k == hgh && top_default) {
-          m = PATH_LEN; b = PATH_INT; ha = -1;
-        } else {
-          int si = WVI(sk);
-          m = Mo[si]; b = To[si]; ha = HAo[si]; hm = HMo[si];
-        }
-        if ((b & PATH_TOP) != 0) m -= 1;
-        b <<= 1;
-        x = (c + k) >> 1;
-        int x0 = x;
-        x = snake_fwd(A, B, x, k, &hb, &hA);
-        history_run(b, m, x - x0);
-        c = (x << 1) - k;
-        nak = NA[vi];
-        int hq = hm;
-        for (int q = nak; x >= q; q += tspace)
-          if (hq < q) {
-            npb++;
-            hq = q;  // the new pebble's mark
-          }
-      }
-      int off = warp_excl_sum(npb, lane);
-      int tot = warp_sum(npb);
-      int64_t pb0 = warp_pebbles(W, tot);
-      if (pb0 < 0) return 1;
-      if (act) {
-        int vi = WVI(k);
-        int64_t s = pb0 + off;
-        while (x >= nak) {
-          if (hm < nak) {
-            cells[s] = {ha, k, dif, nak};
-            ha = (int)s;
-            hm = nak;
-            s += 1;
-          }
-          nak += tspace;
-        }
-        NA[vi] = nak;
-        Vn[vi] = c;
-        Tn[vi] = b;
-        Mn[vi] = m;
-        HAn[vi] = ha;
-        HMn[vi] = hm;
-      }
-      uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
-      if (bb) {
-        more = 0;
-        int kk = base - (__ffs(bb) - 1);
-        if (bclip < kk) bclip = kk;
-      }
-      if (ba) {
-        more = 0;
-        aclip = base - last_lane(ba);
-      }
-      int pm = warp_excl_max(act ? c : -2147483647, lane, carry);
-      bool rec = act && c > pm;
-      uint32_t rb = __ballot_sync(FULL, rec);
-      if (rb) {
-        int L = last_lane(rb);
-        carry = __shfl_sync(FULL, c, L);
-        besta = carry;
-        bestx = __shfl_sync(FULL, x, L);
-        bool pa = rec && m >= PATH_AVE;
-        uint32_t pab = __ballot_sync(FULL, pa);
-        if (pab) {
-          lasta = __shfl_sync(FULL, c, last_lane(pab));
-          bool tr = pa && TABLE[b & TRIM_MASK] >= 0 &&
-                    TABLE[(b >> TRIM_LEN) & TRIM_MASK] + SCORE[b & TRIM_MASK] >= 0;
-          uint32_t trb = __ballot_sync(FULL, tr);
-          if (trb) {
-            int T2 = last_lane(trb);
-            trima = __shfl_sync(FULL, c, T2);
-            trimx = __shfl_sync(FULL, x, T2);
-            trimd = dif;
-            trimha = __shfl_sync(FULL, ha, T2);
-          }
-        }
-      }
-    }
+    WaveSlice WS;
+    if (wave_sweep<true>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
+                         aclip, bclip, WS))
+      return 1;
     cur ^= 1;
     __syncwarp();
     int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
@@ -496,15 +790,7 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       aclip = I32MAX;
       bclip = -I32MAX;
     }
-    int n = besta - WAVE_LAG;
-    while (hgh >= low)
-      if (V[WVI(hgh)] < n)
-        hgh -= 1;
-      else {
-        while (V[WVI(low)] < n) low += 1;
-        break;
-      }
-    // copy the surviving diagonals' NA-independent state is already in the new buffer
+    wave_prune<true>(W, V, besta, low, hgh, WS);
   }
   __syncwarp();
 
@@ -602,9 +888,6 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
   int *NA = W.NA;
   Pebble *cells = W.pool.cells;
   const int tspace = spec.trace_space;
-  const int PATH_AVE = spec.ave_path;
-  const int16_t *SCORE = spec.score;
-  const int16_t *TABLE = spec.table;
 
   int hgh = maxd, low = mind, dif = 0;
   int besta, bestx, trima, trimx, trimd, trimha, morea, morex, mored, moreha, more, morem, lasta;
@@ -726,10 +1009,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       W.err |= ALN_ERR_VCAP;
       return 1;
     }
-    int *Vo = W.V[cur], *Mo = W.M[cur], *HAo = W.HA[cur], *HMo = W.HM[cur];
-    uint64_t *To = W.T[cur];
-    int *Vn = W.V[cur ^ 1], *Mn = W.M[cur ^ 1], *HAn = W.HA[cur ^ 1], *HMn = W.HM[cur ^ 1];
-    uint64_t *Tn = W.T[cur ^ 1];
+    int *Vo = W.V[cur];
     if (low >= minp) {
       if (lane == 0) {
         NA[WVI(low)] = NA[WVI(low + 1)];
@@ -750,101 +1030,10 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     }
     dif += 1;
     __syncwarp();
-    int carry = besta;
-    for (int base = low; base <= hgh; base += 32) {
-      int k = base + lane;
-      bool act = k <= hgh;
-      int x = 0, c = 0, m = 0, ha = -1, hm = 0, hb = 0, hA = 0, npb = 0, nak = 0;
-      uint64_t b = 0;
-      if (act) {
-        int vi = WVI(k);
-        int am = Vo[WVI(k - 1)], ac = Vo[vi], ap = Vo[WVI(k + 1)];
-        int src;  // -1: k-1 (the previous visit), 0: k, 1: k+1
-        if (ac > ap)
-          src = (ap > am) ? -1 : 1;
-        else
-          src = (ac > am) ? -1 : 0;
-        int sk = k + src;
-        c = src == -1 ? am - 1 : (src == 1 ? ap - 1 : ac - 2);
-        if (src == -1 && k == low) {
-          m = PATH_LEN; b = PATH_INT; ha = -1;
-        } else {
-          int si = WVI(sk);
-          m = Mo[si]; b = To[si]; ha = HAo[si]; hm = HMo[si];
-        }
-        if ((b & PATH_TOP) != 0) m -= 1;
-        b <<= 1;
-        x = (c + k) >> 1;
-        int x0 = x;
-        x = snake_rev(A, B, x, k, &hb, &hA);
-        history_run(b, m, x0 - x);
-        c = (x << 1) - k;
-        nak = NA[vi];
-        int hq = hm;
-        for (int q = nak; x <= q; q -= tspace)
-          if (hq > q) {
-            npb++;
-            hq = q;
-          }
-      }
-      int off = warp_excl_sum(npb, lane);
-      int tot = warp_sum(npb);
-      int64_t pb0 = warp_pebbles(W, tot);
-      if (pb0 < 0) return 1;
-      if (act) {
-        int vi = WVI(k);
-        int64_t s = pb0 + off;
-        while (x <= nak) {
-          if (hm > nak) {
-            cells[s] = {ha, k, dif, nak};
-            ha = (int)s;
-            hm = nak;
-            s += 1;
-          }
-          nak -= tspace;
-        }
-        NA[vi] = nak;
-        Vn[vi] = c;
-        Tn[vi] = b;
-        Mn[vi] = m;
-        HAn[vi] = ha;
-        HMn[vi] = hm;
-      }
-      uint32_t bb = __ballot_sync(FULL, act && hb), ba = __ballot_sync(FULL, act && hA);
-      if (bb) {
-        more = 0;
-        int kk = base + (__ffs(bb) - 1);
-        if (bclip > kk) bclip = kk;
-      }
-      if (ba) {
-        more = 0;
-        aclip = base + last_lane(ba);
-      }
-      int pm = warp_excl_min(act ? c : 2147483647, lane, carry);
-      bool rec = act && c < pm;
-      uint32_t rb = __ballot_sync(FULL, rec);
-      if (rb) {
-        int L = last_lane(rb);
-        carry = __shfl_sync(FULL, c, L);
-        besta = carry;
-        bestx = __shfl_sync(FULL, x, L);
-        bool pa = rec && m >= PATH_AVE;
-        uint32_t pab = __ballot_sync(FULL, pa);
-        if (pab) {
-          lasta = __shfl_sync(FULL, c, last_lane(pab));
-          bool tr = pa && TABLE[b & TRIM_MASK] >= 0 &&
-                    TABLE[(b >> TRIM_LEN) & TRIM_MASK] + SCORE[b & TRIM_MASK] >= 0;
-          uint32_t trb = __ballot_sync(FULL, tr);
-          if (trb) {
-            int T2 = last_lane(trb);
-            trima = __shfl_sync(FULL, c, T2);
-            trimx = __shfl_sync(FULL, x, T2);
-            trimd = dif;
-            trimha = __shfl_sync(FULL, ha, T2);
-          }
-        }
-      }
-    }
+    WaveSlice WS;
+    if (wave_sweep<false>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
+                          aclip, bclip, WS))
+      return 1;
     cur ^= 1;
     __syncwarp();
     int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
@@ -873,14 +1062,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
       aclip = -I32MAX;
       bclip = I32MAX;
     }
-    int n = besta + WAVE_LAG;
-    while (hgh >= low)
-      if (V[WVI(hgh)] > n)
-        hgh -= 1;
-      else {
-        while (V[WVI(low)] > n) low += 1;
-        break;
-      }
+    wave_prune<false>(W, V, besta, low, hgh, WS);
   }
   __syncwarp();
 

@@ -700,8 +700,10 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
     bool grown = false;
     if (attempt < 6) {
       int r = PGA_OK;
-      if (errs & aln::ALN_ERR_CELLS) {
-        r = r ? r : ensure(ctx, ctx->cells, 2 * ctx->cells.cap);
+      // pebble numbers are int: at most 2^31 - 1 pebbles
+      const size_t max_cells = sizeof(aln::Pebble) * (size_t)0x7fffffff;
+      if ((errs & aln::ALN_ERR_CELLS) && ctx->cells.cap < max_cells) {
+        r = r ? r : ensure(ctx, ctx->cells, std::min(2 * ctx->cells.cap, max_cells));
         L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
         L.cells = P<aln::Pebble>(ctx->cells);
         grown = true;
