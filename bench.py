@@ -286,6 +286,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     dev.enable_timing(False)
 
     astats = dev.align_stats()
+    atimes = dev.align_times()
     recs, toff, tr = dev.alignments()
     aligned_bases = int((recs[:, 2] - recs[:, 1]).sum()) if len(recs) else 0
 
@@ -358,6 +359,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "stage_ms": st,
+        "align_ms": atimes,
         "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
                                                "k_lcp, k_entries, k_prefix_table)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

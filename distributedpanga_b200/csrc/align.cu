@@ -16,15 +16,47 @@ namespace pga {
 
 using namespace aln;
 
+// One seed of a merged band block, staged in shared memory.
+struct BlockSeed {
+  int64_t anti;
+  int lcp2, dgw;  // 2*lcp; low diagonal bits (+BUCK_WIDTH in stream 2) | stream << 16
+};
+
+// 64-bit exclusive running max in lane order, seeded with init.
+__device__ __forceinline__ int64_t warp_excl_max64(int64_t v, int lane, int64_t init) {
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= o) x = x > y ? x : y;
+  }
+  int64_t ex = __shfl_up_sync(FULL, x, 1);
+  if (lane == 0) ex = init;
+  return ex > init ? ex : init;
+}
+
+// Number of the 32 sorted values held one per lane (xo) below v (strictly,
+// or not above it with `le`).
+__device__ __forceinline__ int warp_count_below(int64_t xo, int64_t v, bool le) {
+  int c = 0;
+#pragma unroll
+  for (int st = 16; st > 0; st >>= 1) {
+    int64_t y = __shfl_sync(FULL, xo, c + st - 1);
+    if (le ? (y <= v) : (y < v)) c += st;
+  }
+  int64_t y = __shfl_sync(FULL, xo, c);
+  if (c < 32 && (le ? (y <= v) : (y < v))) c += 1;
+  return c;
+}
+
 // A pair's seeds as its sorted keys, read by a whole warp: band scans test
-// 32 keys per step, and a Cursor holds a window of 32 decoded seeds (one per
-// lane) that the lane-uniform chain driver reads with shuffles, so a stream
-// costs one coalesced load per 32 seeds.  All lanes call every method with
-// the same arguments.
+// 32 keys per step, and a block's chains are found 32 merged seeds at a time
+// (scan_block).  All lanes call every method with the same arguments.
 struct KeySeeds {
   const U128 *k;
   int64_t n;
   SeedKeyLayout L;
+  BlockSeed *sh;  // 32 slots of this warp's shared memory
   __device__ int64_t anti(int64_t i) const { return (int64_t)key_bits(k[i], L.off_anti, L.off_band - L.off_anti); }
   __device__ int64_t band(int64_t i) const { return (int64_t)key_bits(k[i], L.off_band, L.off_j - L.off_band); }
   __device__ int lcp(int64_t i) const { return (int)key_bits(k[i], 0, 6); }
@@ -39,40 +71,113 @@ struct KeySeeds {
     }
     return n;
   }
-  struct Cursor {
-    const KeySeeds *S;
-    int64_t wb;        // window start: this lane holds seed wb + lane
-    uint32_t a;        // its antidiagonal (DBYTE <= 4 bytes)
-    int ld;            // its lcp | dlow << 8
-    __device__ void fill(int64_t i) {
-      wb = i;
-      int64_t j = i + (threadIdx.x & 31);
-      a = 0;
-      ld = 0;
-      if (j < S->n) {
-        U128 key = S->k[j];
-        a = (uint32_t)key_bits(key, S->L.off_anti, S->L.off_band - S->L.off_anti);
-        ld = (int)key_bits(key, 0, 6) | ((int)key_bits(key, S->L.off_dlow, 6) << 8);
+
+  // The chains of the block [b, m) + [m, e) exactly as scan_block_scalar
+  // finds them.  Per step each lane loads the next seed of both streams; a
+  // seed's place in the merged order is its index plus the number of the
+  // other stream's window seeds before it (stream 1 first on ties), and the
+  // first 32 places form the step.  With P the running maximum of chain ends
+  // (seeded with -CHAIN_BREAK), seed i opens a chain iff
+  // anti_i >= P_before_i + CHAIN_BREAK, and adds
+  // max(0, end_i - max(anti_i, P_before_i)) to its chain's coverage -- the
+  // scalar loop's union length, since P_before_i is its chain's high end.
+  template <class Sink>
+  __device__ int scan_block(int64_t b, int64_t m, int64_t e, Sink &K) const {
+    const int lane = threadIdx.x & 31;
+    int64_t P = -CHAIN_BREAK;  // highest chain end so far
+    bool open = false;         // a chain is open (the first seed always opens one)
+    int64_t cov = 0, alow = 0;
+    int mix = 0, dgmin = 0, dgmax = 0;
+    int64_t s = b, t = m;
+    while (s < m || t < e) {
+      int64_t i1 = s + lane, i2 = t + lane;
+      int64_t a1 = MAX_I64, a2 = MAX_I64;
+      int l1 = 0, l2 = 0, d1 = 0, d2 = 0;
+      if (i1 < m) {
+        U128 key = k[i1];
+        a1 = (int64_t)key_bits(key, L.off_anti, L.off_band - L.off_anti);
+        l1 = (int)key_bits(key, 0, 6);
+        d1 = (int)key_bits(key, L.off_dlow, 6);
       }
+      if (i2 < e) {
+        U128 key = k[i2];
+        a2 = (int64_t)key_bits(key, L.off_anti, L.off_band - L.off_anti);
+        l2 = (int)key_bits(key, 0, 6);
+        d2 = (int)key_bits(key, L.off_dlow, 6);
+      }
+      int take1, take2;
+      int64_t anti;
+      int lcp2, dg, wch;
+      int cnt;
+      if (t >= e) {
+        // stream 1 alone
+        take1 = (m - s) < 32 ? (int)(m - s) : 32;
+        take2 = 0;
+        cnt = take1;
+        anti = a1;
+        lcp2 = l1 << 1;
+        dg = d1;
+        wch = 1;
+      } else {
+        int r1 = lane + warp_count_below(a2, a1, false);
+        int r2 = lane + warp_count_below(a1, a2, true);
+        bool g1 = i1 < m && r1 < 32, g2 = i2 < e && r2 < 32;
+        take1 = __popc(__ballot_sync(FULL, g1));
+        take2 = __popc(__ballot_sync(FULL, g2));
+        cnt = take1 + take2;
+        if (g1) sh[r1] = BlockSeed{a1, l1 << 1, d1 | (1 << 16)};
+        if (g2) sh[r2] = BlockSeed{a2, l2 << 1, (d2 + BUCK_WIDTH) | (2 << 16)};
+        __syncwarp();
+        BlockSeed q = sh[lane];
+        __syncwarp();
+        anti = q.anti;
+        lcp2 = q.lcp2;
+        dg = q.dgw & 0xffff;
+        wch = q.dgw >> 16;
+      }
+      const bool valid = lane < cnt;
+      const int64_t end = valid ? anti + lcp2 : -MAX_I64;
+      const int64_t pb = warp_excl_max64(end, lane, P);  // P before this seed
+      const bool brk = valid && anti >= pb + CHAIN_BREAK;
+      int64_t hi = pb > anti ? pb : anti;
+      const int add = valid ? (end > hi ? (int)(end - hi) : 0) : 0;
+      uint32_t bm = __ballot_sync(FULL, brk);
+      int lo = 0;
+      while (true) {
+        // seeds [lo, stop) continue the open chain
+        int stop = bm ? __ffs(bm) - 1 : cnt;
+        if (stop > lo) {
+          bool in = lane >= lo && lane < stop;
+          cov += __reduce_add_sync(FULL, in ? add : 0);
+          mix |= (int)__reduce_or_sync(FULL, in ? (unsigned)wch : 0u);
+          dgmin = min(dgmin, __reduce_min_sync(FULL, in ? dg : 2147483647));
+          dgmax = max(dgmax, __reduce_max_sync(FULL, in ? dg : -2147483647));
+        }
+        if (!bm) break;
+        // seed `stop` ends the open chain and opens the next
+        const int64_t ahgh = __shfl_sync(FULL, pb, stop);
+        if (open && K.chain(cov, mix, dgmin, dgmax, alow, ahgh)) return 1;
+        open = true;
+        cov = __shfl_sync(FULL, add, stop);
+        mix = __shfl_sync(FULL, wch, stop);
+        dgmin = dgmax = __shfl_sync(FULL, dg, stop);
+        alow = __shfl_sync(FULL, anti, stop);
+        lo = stop + 1;
+        bm &= bm - 1;
+      }
+      int64_t em = end;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        int64_t y = __shfl_xor_sync(FULL, em, o);
+        em = em > y ? em : y;
+      }
+      if (em > P) P = em;
+      s += take1;
+      t += take2;
     }
-    __device__ int at(int64_t i) {
-      if ((uint64_t)(i - wb) >= 32) fill(i);
-      return (int)(i - wb);
-    }
-    __device__ int64_t anti(int64_t i) {
-      int q = at(i);
-      return (int64_t)__shfl_sync(FULL, a, q);
-    }
-    __device__ int lcp(int64_t i) {
-      int q = at(i);
-      return __shfl_sync(FULL, ld, q) & 0xff;
-    }
-    __device__ int dlow(int64_t i) {
-      int q = at(i);
-      return __shfl_sync(FULL, ld, q) >> 8;
-    }
-  };
-  __device__ Cursor cursor() const { return Cursor{this, -64, 0, 0}; }
+    if (open) return K.chain(cov, mix, dgmin, dgmax, alow, P);
+    return 0;
+  }
 };
 
 struct WarpAligner {
@@ -182,6 +287,7 @@ __device__ void finish_and_emit(const AlignLaunch &P, OvlArena &O, int a, int b,
 
 __global__ void __launch_bounds__(ALIGN_THREADS)
 k_align_pairs(AlignLaunch P) {
+  __shared__ BlockSeed s_block[ALIGN_THREADS / 32][32];
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
   if (wid >= P.nwarps) return;
@@ -224,7 +330,7 @@ k_align_pairs(AlignLaunch P) {
     W.err = 0;
     O.err = 0;
     const SeedKeyLayout &L = tk.comp ? P.layC : P.layN;
-    KeySeeds S{(tk.comp ? P.keysC : P.keysN) + tk.lo, tk.hi - tk.lo, L};
+    KeySeeds S{(tk.comp ? P.keysC : P.keysN) + tk.lo, tk.hi - tk.lo, L, s_block[threadIdx.x >> 5]};
     const uint8_t *abuf = tk.comp ? P.rc : P.fwd;
     Seq A{abuf + P.soff[tk.a], (int)P.clen[tk.a]};
     Seq B{P.fwd + P.soff[tk.b], (int)P.clen[tk.b]};

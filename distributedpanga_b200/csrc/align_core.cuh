@@ -1020,10 +1020,171 @@ PGA_HD void finish_pair(OvlArena &O) {
   }
 }
 
+struct PairResult {
+  int calls;       // real Local_Alignment calls (Pair_Calls)
+  int exit_bepos;  // path.bepos when the pair finished (Pair_Bepos)
+  int64_t nhit, nlas;
+};
+
+// What align_contigs does when a chain of a band block ends
+// (src/fastga_pipeline.c:656-760): the hit test, then Local_Alignment calls
+// along the chain's antidiagonal span, each result that is long and good
+// enough kept as a candidate.  cdiag, isnew and alast are the block's; a
+// chain is (cov, mix, dgmin, dgmax) relative to the block and its
+// antidiagonal span [alow, ahgh].
+template <class Aligner>
+struct ChainSink {
+  bool comp, self;
+  const Seq &A, &B;
+  Aligner &AL;
+  Path &path;
+  OvlArena &O;
+  PairResult &R;
+  int lane, nl;
+  int64_t bmxpos, mlen, doffset, aoffset;
+  int64_t cdiag;
+  int isnew;
+  int64_t alast;
+
+  PGA_HD int chain(int64_t cov, int mix, int dgmin, int dgmax, int64_t alow, int64_t ahgh) {
+    const int alnMin = ALIGN_MIN - 50;
+    const double alnRate = 0.3 + .05;  // ALIGN_RATE + .05
+    if (!(cov >= CHAIN_MIN && (mix != 1 || isnew))) return 0;
+    R.nhit += 1;
+    dgmin += (int)(cdiag << BUCK_SHIFT);
+    dgmax += (int)(cdiag << BUCK_SHIFT);
+    if (comp) {
+      dgmin += (int)doffset;
+      dgmax += (int)doffset;
+      alow += aoffset;
+      ahgh += aoffset;
+    } else {
+      dgmin -= (int)bmxpos;
+      dgmax -= (int)bmxpos;
+    }
+    if (ahgh <= alast) return 0;
+    if (alow < alast) alow = alast;
+    ahgh -= BUCK_ANTI;
+    int64_t amid;
+    do {
+      amid = alow + BUCK_ANTI;
+      if (amid > ahgh) {
+        amid = ahgh;
+        if (amid + dgmin < 0) {
+          dgmin = (int)-amid;
+          if (dgmin > dgmax) break;
+        }
+      }
+      int called = 0;
+      if (self) {
+        if (dgmin > 0) {
+          if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, dgmin - 1, -1)) return 1;
+          called = 1;
+        } else if (dgmax < 0) {
+          if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, -1, -(dgmax + 1))) return 1;
+          called = 1;
+        } else
+          path.abpos = path.aepos = 0;
+      } else {
+        if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, -1, -1)) return 1;
+        called = 1;
+      }
+      R.calls += called;
+      int rlen = path.aepos - path.abpos;
+      if (rlen >= alnMin && alnRate * rlen >= path.diffs) {
+        if (O.nov >= O.ovl_cap) {
+          O.err |= ALN_ERR_OVLS;
+          return 1;
+        }
+        if (!O.reserve(path.tlen, nl > 1)) {
+          O.err |= ALN_ERR_TRACE;
+          return 1;
+        }
+        if (lane == 0) {
+          Ovl &c = O.ovl[O.nov];
+          c.abpos = path.abpos;
+          c.aepos = path.aepos;
+          c.bbpos = path.bbpos;
+          c.bepos = path.bepos;
+          c.diffs = path.diffs;
+          c.tlen = path.tlen;
+          c.flags = 0;
+          c.toff = O.nbyte;
+        }
+        O.nov++;
+        const uint16_t *tr = AL.points() + path.trace_off;  // Compress_TraceTo8
+        for (int q = lane; q < path.tlen; q += nl) O.bytes[O.nbyte + q] = (uint8_t)tr[q];
+        O.nbyte += path.tlen;
+        R.nlas += 1;
+      }
+      int64_t eant = comp ? mlen - (path.abpos + path.bbpos) : (int64_t)path.aepos + path.bepos;
+      if (eant <= alow) alow = amid;
+      else alow = eant;
+    } while (alow < ahgh);
+    alast = alow;
+    return 0;
+  }
+};
+
+// One band block (src/fastga_pipeline.c:620-770), one seed at a time: the
+// seeds of band cdiag ([b, m), stream 1) and cdiag+1 ([m, e), stream 2)
+// merged by antidiagonal (stream 1 first on ties), cut into chains where a
+// seed starts CHAIN_BREAK or more past the highest chain end so far.  A
+// chain's coverage is the union length of its [anti, anti + 2 lcp) spans,
+// mix the streams it draws on, dgmin / dgmax the extremes of its seeds'
+// low diagonal bits (+BUCK_WIDTH in stream 2).
+template <class Cursor, class Sink>
+PGA_HD int scan_block_scalar(Cursor &C1, Cursor &C2, int64_t b, int64_t m, int64_t e, Sink &K) {
+  int mix = 0, dgmin = 2 * BUCK_WIDTH, dgmax = 0;
+  int64_t cov = 0, ahgh = -CHAIN_BREAK, alow = 0;
+  int64_t s = b, t = m;
+  int64_t ipost = C1.anti(s);
+  int64_t apost = t < e ? C2.anti(t) : MAX_I64;
+  while (s < m || t < e) {
+    int lcp, dg, wch;
+    int64_t anti;
+    if (apost < ipost) {
+      lcp = C2.lcp(t);
+      dg = C2.dlow(t) + BUCK_WIDTH;
+      anti = apost;
+      t += 1;
+      apost = (t >= e) ? MAX_I64 : C2.anti(t);
+      wch = 0x2;
+    } else {
+      lcp = C1.lcp(s);
+      dg = C1.dlow(s);
+      anti = ipost;
+      s += 1;
+      ipost = (s >= m) ? MAX_I64 : C1.anti(s);
+      wch = 0x1;
+    }
+    lcp <<= 1;
+    if (anti < ahgh + CHAIN_BREAK) {
+      int64_t cps = anti + lcp;
+      if (cps > ahgh) {
+        if (anti >= ahgh) cov += lcp;
+        else cov += cps - ahgh;
+        ahgh = cps;
+      }
+      mix |= wch;
+      if (dg < dgmin) dgmin = dg;
+      else if (dg > dgmax) dgmax = dg;
+    } else {
+      if (K.chain(cov, mix, dgmin, dgmax, alow, ahgh)) return 1;
+      cov = lcp;
+      ahgh = anti + lcp;
+      mix = wch;
+      alow = anti;
+      dgmin = dgmax = dg;
+    }
+  }
+  return K.chain(cov, mix, dgmin, dgmax, alow, ahgh);
+}
+
 // Seeds of one (anchor, partner) pair in diagonal-sort order, decoded into
 // arrays (host harness).  Any type with the same interface works: band(i),
-// band_end(i, band) = the first index >= i whose band differs (or n), and a
-// Cursor reading anti / lcp / dlow of a stream that mostly moves forward.
+// band_end(i, band) = the first index >= i whose band differs (or n), and
+// scan_block(b, m, e, sink), which runs a block's chains into the sink.
 struct PairSeeds {
   const int64_t *anti_;
   const int64_t *band_;
@@ -1044,7 +1205,11 @@ struct PairSeeds {
     PGA_HD int lcp(int64_t i) { return S->lcp_[i]; }
     PGA_HD int dlow(int64_t i) { return S->dlow_[i]; }
   };
-  PGA_HD Cursor cursor() const { return Cursor{this}; }
+  template <class Sink>
+  PGA_HD int scan_block(int64_t b, int64_t m, int64_t e, Sink &K) const {
+    Cursor C1{this}, C2{this};
+    return scan_block_scalar(C1, C2, b, m, e, K);
+  }
 };
 
 // The scalar aligner: Local_Alignment on one thread.
@@ -1057,12 +1222,6 @@ struct ScalarAligner {
   }
   PGA_HD const uint16_t *points() const { return W.points; }
   PGA_HD int err() const { return W.err; }
-};
-
-struct PairResult {
-  int calls;       // real Local_Alignment calls (Pair_Calls)
-  int exit_bepos;  // path.bepos when the pair finished (Pair_Bepos)
-  int64_t nhit, nlas;
 };
 
 // align_contigs (src/fastga_pipeline.c:576-813) for one pair, leaving the
@@ -1084,12 +1243,8 @@ template <class SeedsT, class Aligner>
 PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const Seq &B, int64_t amxpos,
                       int64_t maxdag, Aligner &AL, Path &path, OvlArena &O, PairResult &R, int lane = 0,
                       int nl = 1, int64_t blo = 0, int64_t bhi = -1) {
-  const int alnMin = ALIGN_MIN - 50;
-  const double alnRate = 0.3 + .05;  // ALIGN_RATE + .05
-  const int64_t bmxpos = amxpos;
   const int64_t n = S.n;
-  const int64_t alen = A.len, blen = B.len, mlen = alen + blen;
-  const int64_t doffset = alen - maxdag, aoffset = alen - amxpos;
+  const int64_t alen = A.len, blen = B.len;
   R.calls = 0;
   R.nhit = 0;
   R.nlas = 0;
@@ -1100,141 +1255,23 @@ PGA_HD int align_pair(const SeedsT &S, bool comp, bool self, const Seq &A, const
   if (blo < 0) blo = 0;
   if (blo >= bhi) return 0;
 
+  ChainSink<Aligner> K{comp, self, A, B, AL, path, O, R, lane, nl,
+                       amxpos, alen + blen, alen - maxdag, alen - amxpos, 0, 0, -1};
   int64_t b = blo, e = blo, m;
   int64_t cdiag = S.band(blo);
   e = S.band_end(e, cdiag);
-  // the two streams of a block: band cdiag from b, band cdiag+1 from m
-  typename SeedsT::Cursor C1 = S.cursor(), C2 = S.cursor();
   // a block is "new" unless the band just below it has seeds
   int isnew = (blo == 0 || S.band(blo - 1) != cdiag - 1) ? 1 : 0;
   while (1) {
+    // the block of band cdiag ([b, m)) and cdiag+1 ([m, e))
     m = e;
     e = S.band_end(e, cdiag + 1);
     int aux = e > m ? 1 : 0;
     if (isnew || aux) {
-      int go = 1, lcp, wch = 0, mix = 0, dgmin = 2 * BUCK_WIDTH, dgmax = 0, dg = 0;
-      int64_t cov = 0, ahgh = -CHAIN_BREAK, alow, amid, alast = -1, anti;
-      int64_t s = b, t = m;
-      int64_t ipost = C1.anti(s);
-      int64_t apost = aux ? C2.anti(t) : MAX_I64;
-      alow = apost < ipost ? apost : ipost;
-      while (go) {
-        if (apost < ipost) {
-          lcp = C2.lcp(t);
-          dg = C2.dlow(t) + BUCK_WIDTH;
-          anti = apost;
-          t += 1;
-          apost = (t >= e) ? MAX_I64 : C2.anti(t);
-          wch = 0x2;
-        } else {
-          // s == m is one past the first stream: the reference reads that
-          // record's lcp and diagonal (unused: go becomes 0 below)
-          lcp = (s < n) ? C1.lcp(s) : 0;
-          dg = (s < n) ? C1.dlow(s) : 0;
-          anti = ipost;
-          s += 1;
-          if (s >= m) {
-            if (s > m) go = 0;
-            else ipost = MAX_I64;
-          } else
-            ipost = C1.anti(s);
-          wch = 0x1;
-        }
-        lcp <<= 1;
-        if (anti < ahgh + CHAIN_BREAK) {
-          int64_t cps = anti + lcp;
-          if (cps > ahgh) {
-            if (anti >= ahgh) cov += lcp;
-            else cov += cps - ahgh;
-            ahgh = cps;
-          }
-          mix |= wch;
-          if (dg < dgmin) dgmin = dg;
-          else if (dg > dgmax) dgmax = dg;
-        } else {
-          if (cov >= CHAIN_MIN && (mix != 1 || isnew)) {
-            R.nhit += 1;
-            dgmin += (int)(cdiag << BUCK_SHIFT);
-            dgmax += (int)(cdiag << BUCK_SHIFT);
-            if (comp) {
-              dgmin += (int)doffset;
-              dgmax += (int)doffset;
-              alow += aoffset;
-              ahgh += aoffset;
-            } else {
-              dgmin -= (int)bmxpos;
-              dgmax -= (int)bmxpos;
-            }
-            if (ahgh > alast) {
-              if (alow < alast) alow = alast;
-              ahgh -= BUCK_ANTI;
-              do {
-                amid = alow + BUCK_ANTI;
-                if (amid > ahgh) {
-                  amid = ahgh;
-                  if (amid + dgmin < 0) {
-                    dgmin = (int)-amid;
-                    if (dgmin > dgmax) break;
-                  }
-                }
-                int called = 0;
-                if (self) {
-                  if (dgmin > 0) {
-                    if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, dgmin - 1, -1)) return 1;
-                    called = 1;
-                  } else if (dgmax < 0) {
-                    if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, -1, -(dgmax + 1))) return 1;
-                    called = 1;
-                  } else
-                    path.abpos = path.aepos = 0;
-                } else {
-                  if (AL.call(A, B, comp, path, dgmin, dgmax, (int)amid, -1, -1)) return 1;
-                  called = 1;
-                }
-                R.calls += called;
-                int rlen = path.aepos - path.abpos;
-                if (rlen >= alnMin && alnRate * rlen >= path.diffs) {
-                  if (O.nov >= O.ovl_cap) {
-                    O.err |= ALN_ERR_OVLS;
-                    return 1;
-                  }
-                  if (!O.reserve(path.tlen, nl > 1)) {
-                    O.err |= ALN_ERR_TRACE;
-                    return 1;
-                  }
-                  if (lane == 0) {
-                    Ovl &c = O.ovl[O.nov];
-                    c.abpos = path.abpos;
-                    c.aepos = path.aepos;
-                    c.bbpos = path.bbpos;
-                    c.bepos = path.bepos;
-                    c.diffs = path.diffs;
-                    c.tlen = path.tlen;
-                    c.flags = 0;
-                    c.toff = O.nbyte;
-                  }
-                  O.nov++;
-                  const uint16_t *tr = AL.points() + path.trace_off;  // Compress_TraceTo8
-                  for (int q = lane; q < path.tlen; q += nl) O.bytes[O.nbyte + q] = (uint8_t)tr[q];
-                  O.nbyte += path.tlen;
-                  R.nlas += 1;
-                }
-                int64_t eant = comp ? mlen - (path.abpos + path.bbpos) : (int64_t)path.aepos + path.bepos;
-                if (eant <= alow) alow = amid;
-                else alow = eant;
-              } while (alow < ahgh);
-              alast = alow;
-            }
-          }
-          if (go) {
-            cov = lcp;
-            ahgh = anti + lcp;
-            mix = wch;
-            alow = anti;
-            dgmin = dgmax = dg;
-          }
-        }
-      }
+      K.cdiag = cdiag;
+      K.isnew = isnew;
+      K.alast = -1;
+      if (S.scan_block(b, m, e, K)) return 1;
     }
     if (e >= n) break;
     if (aux) {

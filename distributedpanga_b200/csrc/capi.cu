@@ -2,6 +2,7 @@
 // points declared in include/pga_b200.h.
 #include <algorithm>
 #include <cstdarg>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -83,6 +84,7 @@ struct pga_ctx {
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
   int64_t align_stats[8] = {0};    // pga_align_stats
+  float align_ms[4] = {0};         // pga_align_times
   int64_t range_seeds = 0;         // pga_align_set_ranges
   unsigned long long rec_used = 0, out_used = 0;  // survivors so far in recs / outb
   bool have_align = false;
@@ -767,7 +769,12 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
   return PGA_OK;
 }
 
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 int run_align(pga_ctx *ctx) {
+  const double t_start = now_ms();
   const int nc = ctx->ncontig;
   int64_t maxctg = ctx->maxctg;
   // 1. the two units must be diagonal-sorted
@@ -952,6 +959,7 @@ int run_align(pga_ctx *ctx) {
   const int64_t range_seeds = ctx->range_seeds < 0    ? 0
                               : ctx->range_seeds > 0 ? ctx->range_seeds
                                                      : std::max<int64_t>(256, first_seeds / (32 * L.nwarps));
+  const double t_launch = now_ms();
   std::vector<PairOut> out1;
   long long maxcyc = 0, sumcyc = 0;
   int64_t maxcalls = 0;
@@ -963,6 +971,7 @@ int run_align(pga_ctx *ctx) {
     sumcyc += o.cycles;
   }
 
+  const double t_self = now_ms();
   // 6. self pairs: entry values by FastGA's order (src/fastga_order.c)
   int64_t nrounds = 0;
   if (!self_idx.empty()) {
@@ -1078,6 +1087,7 @@ int run_align(pga_ctx *ctx) {
       if (!done[q]) return fail(ctx, PGA_ERR_ARG, "self pairs that cannot be resolved");
   }
 
+  const double t_order = now_ms();
   // 7. survivors in la_sort order: (aread, abpos, bread, comp), ties in the
   // pair's own output order (src/fastga_pipeline.c:1500-1515)
   unsigned long long nrec = 0, nbytes = 0;
@@ -1119,6 +1129,11 @@ int run_align(pga_ctx *ctx) {
   ctx->align_stats[5] = nrounds;
   ctx->align_stats[6] = sumcyc;
   ctx->align_stats[7] = maxcalls;
+  const double t_end = now_ms();
+  ctx->align_ms[0] = (float)(t_launch - t_start);
+  ctx->align_ms[1] = (float)(t_self - t_launch);
+  ctx->align_ms[2] = (float)(t_order - t_self);
+  ctx->align_ms[3] = (float)(t_end - t_order);
   ctx->have_align = true;
   return PGA_OK;
 }
@@ -1661,6 +1676,12 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
   }
   if (trace_off) memcpy(trace_off, ctx->h_toff.data(), sizeof(int64_t) * (n + 1));
   if (trace && !ctx->h_trace.empty()) memcpy(trace, ctx->h_trace.data(), ctx->h_trace.size());
+  return PGA_OK;
+}
+
+int pga_align_times(const pga_ctx *ctx, float *ms4) {
+  if (!ctx || !ms4) return PGA_ERR_ARG;
+  for (int i = 0; i < 4; i++) ms4[i] = ctx->align_ms[i];
   return PGA_OK;
 }
 

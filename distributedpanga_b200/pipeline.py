@@ -68,6 +68,7 @@ _SIGS = {
     "pga_align_copy": (C.c_int, [vp, vp, vp, vp]),
     "pga_align_stats": (C.c_int, [vp, vp]),
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
+    "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
 }
@@ -283,6 +284,12 @@ class Device:
         self._ck(self.L.pga_align(self.h, C.byref(n)), "align")
         self.nalign = n.value
         return n.value
+
+    def align_times(self) -> dict:
+        """Host wall-clock split of the last align() in ms."""
+        a = (C.c_float * 4)()
+        self._ck(self.L.pga_align_times(self.h, a), "align_times")
+        return {"setup": a[0], "pairs": a[1], "self_pairs": a[2], "order": a[3]}
 
     def set_ranges(self, range_seeds: int) -> None:
         """Band-range size for large pairs (0 automatic, -1 never split)."""

@@ -162,6 +162,13 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
  * of the longest task */
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
 
+/* Host wall-clock split of the last pga_align, in ms: [0] set-up (diagonal
+ * sort if needed, sequences, pair lists) [1] pairs of two contigs and all C
+ * pairs (one launch plus the band-range finish) [2] self pairs (rounds of
+ * FastGA's order) [3] la_sort order and read-back.  No counterpart in the
+ * reference. */
+int pga_align_times(const pga_ctx *ctx, float *ms4);
+
 /* ---- seed diagonal sort without device allocation ---------------------------- */
 
 /* No counterpart in the reference: the reference runs on the host and never
