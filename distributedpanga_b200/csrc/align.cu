@@ -370,10 +370,14 @@ k_align_pairs(AlignLaunch P) {
         po.nsurv = (int)O.nov;
         po.rec_off = (int64_t)g0;
       }
-    } else if (rc == 0) {
-      finish_and_emit(P, O, tk.a, tk.b, tk.comp, po, lane);
     }
     po.cycles = clock64() - t0;
+    if (tk.seg >= 0) {
+      if (lane == 0) P.rout[tk.seg] = po;
+    } else if (rc == 0) {
+      finish_and_emit(P, O, tk.a, tk.b, tk.comp, po, lane);
+      po.cycles = clock64() - t0;
+    }
     if (lane == 0) P.pout[t] = po;
     __syncwarp();
   }
@@ -402,7 +406,7 @@ k_finish_pairs(AlignLaunch P) {
     O.nov = 0;
     O.err = 0;
     for (int k = 0; k < ft.nseg; k++) {
-      const PairOut ro = P.range_out[P.range_idx[ft.first + k]];
+      const PairOut ro = P.rout[P.range_idx[ft.first + k]];
       po.calls += ro.calls;
       if (ro.calls > 0) po.exit_bepos = ro.exit_bepos;
       if (O.nov + ro.nsurv > O.ovl_cap) {
@@ -545,6 +549,34 @@ void launch_align(const AlignLaunch &P, int grid, cudaStream_t st) {
 
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st) {
   k_finish_pairs<<<grid, ALIGN_THREADS, 0, st>>>(P);
+}
+
+// For each self pair [lo, hi) of the N unit: the first seed whose band is
+// >= cd_lo and the first whose band is > cd_hi (relative to lo).  The band
+// blocks between are the only ones whose diagonal span can hold diagonal 0.
+__global__ void k_self_bounds(const U128 *__restrict__ keys, SeedKeyLayout L, const int64_t *__restrict__ lohi,
+                              int npair, int64_t cd_lo, int64_t cd_hi, int64_t *__restrict__ x12) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npair) return;
+  const int64_t lo = lohi[2 * q], hi = lohi[2 * q + 1];
+  for (int w = 0; w < 2; w++) {
+    // first index in [lo, hi) with band > lim (lim = cd_lo - 1, then cd_hi)
+    const int64_t lim = w == 0 ? cd_lo - 1 : cd_hi;
+    int64_t a = lo, b = hi;
+    while (a < b) {
+      int64_t mid = a + (b - a) / 2;
+      int64_t band = (int64_t)key_bits(keys[mid], L.off_band, L.off_j - L.off_band);
+      if (band > lim) b = mid;
+      else a = mid + 1;
+    }
+    x12[2 * q + w] = a - lo;
+  }
+}
+
+void launch_self_bounds(const U128 *keys, SeedKeyLayout L, const int64_t *lohi, int npair, int64_t cd_lo,
+                        int64_t cd_hi, int64_t *x12, cudaStream_t st) {
+  if (npair <= 0) return;
+  k_self_bounds<<<(npair + 127) / 128, 128, 0, st>>>(keys, L, lohi, npair, cd_lo, cd_hi, x12);
 }
 
 void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,

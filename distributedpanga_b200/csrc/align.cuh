@@ -12,11 +12,11 @@ constexpr int ALIGN_THREADS = 128;  // 4 warps per CTA, one pair per warp at a t
 constexpr int WAVE_INTS = 13;       // per diagonal slot: V,M,HA,HM x2, NA, T x2 (uint64)
 
 // One (anchor, partner) pair of a unit: seeds [lo, hi) of the unit's sorted
-// keys.  seg < 0: the whole pair, finished by the same warp.  seg >= 0: one
-// band range of a large pair of two different contigs: the band blocks
-// whose first stream starts in [slo, shi), both moved forward to the next
-// band start; its candidates go to the range store and k_finish_pairs
-// finishes the pair.
+// keys.  seg < 0: the whole pair, finished by the same warp.  seg >= 0: band
+// range number seg of a pair run in ranges: the band blocks whose first
+// stream starts in [slo, shi), both moved forward to the next band start;
+// its candidates go to the range store, its PairOut to rout[seg], and
+// k_finish_pairs finishes the pair later.
 struct PairTask {
   int comp, a, b, self, entry_bepos, seg;
   int64_t lo, hi, slo, shi;
@@ -30,8 +30,8 @@ struct PairOut {
   long long cycles;  // SM clock cycles the warp spent on the task
 };
 
-// A pair split into ranges: its ranges' PairOut indices are
-// range_idx[first .. first + nseg).
+// A pair run in ranges: its ranges, in order, are range_idx[first ..
+// first + nseg).
 struct FinishTask {
   int comp, a, b, entry_bepos, first, nseg;
 };
@@ -70,10 +70,10 @@ struct AlignLaunch {
   aln::Ovl *rng_ovl;                 // range store: candidates of range tasks
   unsigned long long *rng_next;
   int64_t rng_cap;
+  PairOut *rout;                     // per range number
   const FinishTask *ftasks;          // k_finish_pairs
   int nftasks;
   const int *range_idx;
-  const PairOut *range_out;
   uint8_t *cand_bytes;
   unsigned long long *cand_next;
   int64_t cand_cap;
@@ -88,6 +88,8 @@ struct AlignLaunch {
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);
+void launch_self_bounds(const U128 *keys, SeedKeyLayout L, const int64_t *lohi, int npair, int64_t cd_lo,
+                        int64_t cd_hi, int64_t *x12, cudaStream_t st);
 void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *boff, int ncontig,
                         unsigned long long *cnt, cudaStream_t st);
 void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff, const int64_t *soff, int ncontig,

@@ -79,14 +79,17 @@ struct pga_ctx {
   DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
-      ridx;
+      ridx, rout, selfb;
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
   int64_t align_stats[8] = {0};    // pga_align_stats
   float align_ms[4] = {0};         // pga_align_times
   int64_t range_seeds = 0;         // pga_align_set_ranges
-  unsigned long long rec_used = 0, out_used = 0;  // survivors so far in recs / outb
+  // pool use over the launches of one pga_align: candidate trace bytes,
+  // range candidates, survivors, survivor trace bytes
+  unsigned long long cand_used = 0, rng_used = 0, rec_used = 0, out_used = 0;
+  unsigned long long counters[4] = {0, 0, 0, 0};  // staging for the device counters
   bool have_align = false;
 
   // generic byte staging
@@ -577,125 +580,109 @@ void fo_ranges(int n, const std::vector<int64_t> &clen_pos, int64_t npost, const
   }
 }
 
-// Runs one launch of pair tasks and returns one PairOut per task.  With
-// `range_seeds` > 0 every pair of two different contigs with more seeds than
-// that runs as consecutive band ranges of about that many seeds on different
-// warps (its band blocks are independent), and k_finish_pairs finishes it.
-// Tasks go to the warps largest first.
-int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &tasks, std::vector<PairOut> &outs,
-                    int64_t range_seeds, long long *max_cycles, int64_t *max_task_calls) {
-  outs.assign(tasks.size(), PairOut{});
-  if (tasks.empty()) return PGA_OK;
-  std::vector<PairTask> run;
-  std::vector<FinishTask> fin;
-  std::vector<int> fin_of(tasks.size(), -1), ridx;
-  std::vector<std::vector<int>> ranges;  // per finish task: its ranges' indices in `run`
-  for (size_t i = 0; i < tasks.size(); i++) {
-    PairTask t = tasks[i];
-    t.seg = -1;
-    t.slo = t.lo;
-    t.shi = t.hi;
-    int64_t n = t.hi - t.lo;
-    if (range_seeds > 0 && !t.self && n > range_seeds) {
-      FinishTask f;
-      f.comp = t.comp;
-      f.a = t.a;
-      f.b = t.b;
-      f.entry_bepos = t.entry_bepos;
-      f.nseg = (int)((n + range_seeds - 1) / range_seeds);
-      f.first = 0;
-      fin_of[i] = (int)fin.size();
-      ranges.emplace_back();
-      for (int k = 0; k < f.nseg; k++) {
-        PairTask r = t;
-        r.seg = k;
-        r.slo = t.lo + k * range_seeds;
-        r.shi = std::min(t.hi, t.lo + (k + 1) * range_seeds);
-        ranges.back().push_back((int)run.size());
-        run.push_back(r);
-      }
-      fin.push_back(f);
-    } else {
-      fin_of[i] = -2 - (int)run.size();  // whole pair at run[-2 - fin_of]
-      run.push_back(t);
-    }
-  }
-  // largest pair first, a pair's ranges in order (a large pair's ranges each
-  // tend to re-extend its longest alignments, so they start early)
-  std::vector<int> order(run.size());
-  for (size_t i = 0; i < run.size(); i++) order[i] = (int)i;
+// What one launch runs: tasks (whole pairs or band ranges, any order) and
+// then the pairs to finish from their ranges (k_finish_pairs), each listing
+// its range numbers, in order, at ridx[first .. first + nseg).
+struct LaunchPlan {
+  std::vector<PairTask> tasks;
+  std::vector<FinishTask> fins;
+  std::vector<int> ridx;
+};
+
+// Runs a plan: the tasks go to the warps largest pair first.  tout: one
+// PairOut per task (plan order), fout: one per finished pair; rout_h (one
+// per range number) is refreshed.  Pebbles live for one launch; candidate
+// traces, range candidates and survivors accumulate over the launches of one
+// pga_align.  A pool that overflows is grown (keeping what earlier launches
+// left in it) and the launch runs again from the same counters.
+int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vector<PairOut> &tout,
+                 std::vector<PairOut> &fout, std::vector<PairOut> &rout_h, long long *max_cycles,
+                 int64_t *max_task_calls) {
+  const size_t nt = plan.tasks.size(), nf = plan.fins.size();
+  tout.assign(nt, PairOut{});
+  fout.assign(nf, PairOut{});
+  if (nt == 0 && nf == 0) return PGA_OK;
+  std::vector<int> order(nt);
+  for (size_t i = 0; i < nt; i++) order[i] = (int)i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return (run[x].hi - run[x].lo) > (run[y].hi - run[y].lo);
+    return (plan.tasks[x].hi - plan.tasks[x].lo) > (plan.tasks[y].hi - plan.tasks[y].lo);
   });
-  std::vector<int> where(run.size());
-  std::vector<PairTask> sorted(run.size());
-  for (size_t k = 0; k < order.size(); k++) {
-    sorted[k] = run[order[k]];
-    where[order[k]] = (int)k;
+  std::vector<PairTask> sorted(nt);
+  for (size_t k = 0; k < nt; k++) sorted[k] = plan.tasks[order[k]];
+  if (nt) {
+    ENSURE(ctx->tasks, sizeof(PairTask) * nt);
+    ENSURE(ctx->pout, sizeof(PairOut) * nt);
+    CK(cudaMemcpyAsync(ctx->tasks.p, sorted.data(), sizeof(PairTask) * nt, cudaMemcpyHostToDevice, ctx->st));
   }
-  for (size_t f = 0; f < fin.size(); f++) {
-    fin[f].first = (int)ridx.size();
-    for (int r : ranges[f]) ridx.push_back(where[r]);
+  if (nf) {
+    ENSURE(ctx->ftasks, sizeof(FinishTask) * nf);
+    ENSURE(ctx->fout, sizeof(PairOut) * nf);
+    ENSURE(ctx->ridx, sizeof(int) * (plan.ridx.size() + 1));
+    CK(cudaMemcpyAsync(ctx->ftasks.p, plan.fins.data(), sizeof(FinishTask) * nf, cudaMemcpyHostToDevice, ctx->st));
+    if (!plan.ridx.empty())
+      CK(cudaMemcpyAsync(ctx->ridx.p, plan.ridx.data(), sizeof(int) * plan.ridx.size(), cudaMemcpyHostToDevice,
+                         ctx->st));
   }
-  ENSURE(ctx->tasks, sizeof(PairTask) * sorted.size());
-  ENSURE(ctx->pout, sizeof(PairOut) * sorted.size());
-  CK(cudaMemcpyAsync(ctx->tasks.p, sorted.data(), sizeof(PairTask) * sorted.size(), cudaMemcpyHostToDevice,
-                     ctx->st));
-  if (!fin.empty()) {
-    ENSURE(ctx->ftasks, sizeof(FinishTask) * fin.size());
-    ENSURE(ctx->fout, sizeof(PairOut) * fin.size());
-    ENSURE(ctx->ridx, sizeof(int) * ridx.size());
-    CK(cudaMemcpyAsync(ctx->ftasks.p, fin.data(), sizeof(FinishTask) * fin.size(), cudaMemcpyHostToDevice,
-                       ctx->st));
-    CK(cudaMemcpyAsync(ctx->ridx.p, ridx.data(), sizeof(int) * ridx.size(), cudaMemcpyHostToDevice, ctx->st));
-  }
-  std::vector<PairOut> fo(fin.size()), ro(sorted.size());
+  std::vector<PairOut> ro(nt);
   const int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
+  const unsigned long long base[4] = {ctx->cand_used, ctx->rng_used, ctx->rec_used, ctx->out_used};
   for (int attempt = 0;; attempt++) {
-    // pebbles and candidate traces live for one launch; survivors accumulate
+    ctx->counters[0] = base[0];
+    ctx->counters[1] = base[1];
+    ctx->counters[2] = base[2];
+    ctx->counters[3] = base[3];
     CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
-    CK(cudaMemsetAsync(ctx->rng_next.p, 0, 8, ctx->st));
     CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
-    CK(cudaMemsetAsync(ctx->cand_next.p, 0, 8, ctx->st));
-    CK(cudaMemcpyAsync(ctx->rec_next.p, &ctx->rec_used, 8, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->out_next.p, &ctx->out_used, 8, cudaMemcpyHostToDevice, ctx->st));
-    L.tasks = P<PairTask>(ctx->tasks);
-    L.ntasks = (int)sorted.size();
-    L.pout = P<PairOut>(ctx->pout);
-    launch_align(L, grid, ctx->st);
-    LAUNCHED(1);
-    CK(cudaGetLastError());
-    if (!fin.empty()) {
+    CK(cudaMemcpyAsync(ctx->cand_next.p, &ctx->counters[0], 8, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->rng_next.p, &ctx->counters[1], 8, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->rec_next.p, &ctx->counters[2], 8, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->out_next.p, &ctx->counters[3], 8, cudaMemcpyHostToDevice, ctx->st));
+    L.rout = P<PairOut>(ctx->rout);
+    if (nt) {
+      L.tasks = P<PairTask>(ctx->tasks);
+      L.ntasks = (int)nt;
+      L.pout = P<PairOut>(ctx->pout);
+      launch_align(L, grid, ctx->st);
+      LAUNCHED(1);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * nt, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    if (nf) {
       AlignLaunch F = L;
       F.ftasks = P<FinishTask>(ctx->ftasks);
-      F.nftasks = (int)fin.size();
+      F.nftasks = (int)nf;
       F.range_idx = P<int>(ctx->ridx);
-      F.range_out = P<PairOut>(ctx->pout);
       F.pout = P<PairOut>(ctx->fout);
       launch_finish(F, grid, ctx->st);
       LAUNCHED(1);
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(fo.data(), ctx->fout.p, sizeof(PairOut) * fin.size(), cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(fout.data(), ctx->fout.p, sizeof(PairOut) * nf, cudaMemcpyDeviceToHost, ctx->st));
     }
-    CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * sorted.size(), cudaMemcpyDeviceToHost, ctx->st));
-    unsigned long long used[2] = {0, 0};
-    CK(cudaMemcpyAsync(&used[0], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(&used[1], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    if (!rout_h.empty())
+      CK(cudaMemcpyAsync(rout_h.data(), ctx->rout.p, sizeof(PairOut) * rout_h.size(), cudaMemcpyDeviceToHost,
+                         ctx->st));
+    unsigned long long used[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(&used[0], ctx->cand_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&used[1], ctx->rng_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&used[2], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&used[3], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     int errs = 0, bad = -1, badf = -1;
-    for (size_t k = 0; k < sorted.size(); k++)
+    for (size_t k = 0; k < nt; k++)
       if (ro[k].err) {
         errs |= ro[k].err;
         if (bad < 0) bad = (int)k;
       }
-    for (size_t f = 0; f < fin.size(); f++)
-      if (fo[f].err) {
-        errs |= fo[f].err;
+    for (size_t f = 0; f < nf; f++)
+      if (fout[f].err) {
+        errs |= fout[f].err;
         if (badf < 0) badf = (int)f;
       }
     if (errs == 0) {
-      ctx->rec_used = used[0];
-      ctx->out_used = used[1];
+      ctx->cand_used = used[0];
+      ctx->rng_used = used[1];
+      ctx->rec_used = used[2];
+      ctx->out_used = used[3];
       break;
     }
     // grow what overflowed and run the launch again
@@ -711,20 +698,20 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
         grown = true;
       }
       if (errs & aln::ALN_ERR_TRACE) {
-        r = r ? r : ensure(ctx, ctx->cand, 2 * ctx->cand.cap);
+        r = r ? r : grow_keep(ctx, ctx->cand, 2 * ctx->cand.cap, base[0]);
         L.cand_cap = (int64_t)ctx->cand.cap;
         L.cand_bytes = P<uint8_t>(ctx->cand);
         grown = true;
       }
       if (errs & 0x800) {
-        r = r ? r : ensure(ctx, ctx->rng_ovl, 2 * ctx->rng_ovl.cap);
+        r = r ? r : grow_keep(ctx, ctx->rng_ovl, 2 * ctx->rng_ovl.cap, sizeof(aln::Ovl) * base[1]);
         L.rng_cap = (int64_t)(ctx->rng_ovl.cap / sizeof(aln::Ovl));
         L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
         grown = true;
       }
       if (errs & 0x400) {
-        r = r ? r : grow_keep(ctx, ctx->recs, 2 * ctx->recs.cap, sizeof(AlnRec) * ctx->rec_used);
-        r = r ? r : grow_keep(ctx, ctx->outb, 2 * ctx->outb.cap, ctx->out_used);
+        r = r ? r : grow_keep(ctx, ctx->recs, 2 * ctx->recs.cap, sizeof(AlnRec) * base[2]);
+        r = r ? r : grow_keep(ctx, ctx->outb, 2 * ctx->outb.cap, base[3]);
         L.rec_cap = (int64_t)(ctx->recs.cap / sizeof(AlnRec));
         L.out_cap = (int64_t)ctx->outb.cap;
         L.recs = P<AlnRec>(ctx->recs);
@@ -747,26 +734,29 @@ int align_run_tasks(pga_ctx *ctx, AlignLaunch &L, const std::vector<PairTask> &t
         return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
                     sorted[bad].a, sorted[bad].b, sorted[bad].comp ? "C" : "N", ro[bad].err);
       return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
-                  fin[badf].a, fin[badf].b, fin[badf].comp ? "C" : "N", fo[badf].err);
+                  plan.fins[badf].a, plan.fins[badf].b, plan.fins[badf].comp ? "C" : "N", fout[badf].err);
     }
   }
-  for (size_t k = 0; k < sorted.size(); k++)
+  for (size_t k = 0; k < nt; k++) {
+    tout[order[k]] = ro[k];
     if (ro[k].cycles > *max_cycles) {
       *max_cycles = ro[k].cycles;
       *max_task_calls = ro[k].calls;
     }
-  for (size_t i = 0; i < tasks.size(); i++) {
-    if (fin_of[i] >= 0) {
-      const int f = fin_of[i];
-      outs[i] = fo[f];
-      long long c = 0;
-      for (int r : ranges[f]) c += ro[where[r]].cycles;
-      outs[i].cycles = c + fo[f].cycles;  // the pair's warp-cycles, all ranges and the finish
-    } else {
-      outs[i] = ro[where[-2 - fin_of[i]]];
-    }
   }
   return PGA_OK;
+}
+
+// Calls and exit bepos of a pair run as ranges: the sum, and the last range
+// (in order) that called, else `entry`.
+void combine_ranges(const std::vector<PairOut> &rout_h, const std::vector<int> &ids, int *calls, int *exit_bepos,
+                    int entry) {
+  *calls = 0;
+  *exit_bepos = entry;
+  for (int id : ids) {
+    *calls += rout_h[id].calls;
+    if (rout_h[id].calls > 0) *exit_bepos = rout_h[id].exit_bepos;
+  }
 }
 
 double now_ms() {
@@ -925,7 +915,7 @@ int run_align(pga_ctx *ctx) {
   ENSURE(ctx->cand_next, 64);
   ENSURE(ctx->rec_next, 64);
   ENSURE(ctx->out_next, 64);
-  ctx->rec_used = ctx->out_used = 0;
+  ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
   L.next_task = P<unsigned>(ctx->task_next);
   L.wave = P<int>(ctx->wave);
   L.points = P<uint16_t>(ctx->points);
@@ -942,8 +932,15 @@ int run_align(pga_ctx *ctx) {
   L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
   L.rng_next = P<unsigned long long>(ctx->rng_next);
 
-  // 5. launch 1: every pair that does not read a leftover value (all C pairs,
-  // every N pair of two different contigs), largest first
+  // 5. Plan.  Pairs of two different contigs (all C pairs, every N pair of
+  // two contigs) run in the first launch, large ones as band ranges finished
+  // right after.  A self pair reads what the previous pair left in `path`
+  // only in a chain that straddles diagonal 0, i.e. only in its band blocks
+  // whose diagonal span holds 0 (bands cd_lo..cd_hi); its blocks below and
+  // above that run as ranges in the first launch too, and its middle part
+  // runs in rounds of FastGA's order, entered with the bepos of the last call
+  // below it (or, if none, the order's value).  With ranges off, self pairs
+  // run whole in the rounds.
   std::vector<PairTask> first;
   std::vector<int> self_idx;
   for (int comp = 0; comp < 2; comp++)
@@ -951,30 +948,115 @@ int run_align(pga_ctx *ctx) {
       if (pairs[comp][i].self) self_idx.push_back((int)i);
       else first.push_back(pairs[comp][i]);
     }
-  std::stable_sort(first.begin(), first.end(),
-                   [](const PairTask &x, const PairTask &y) { return (x.hi - x.lo) > (y.hi - y.lo); });
-  // pairs above range_seeds run as band ranges: about 32 tasks per warp
-  int64_t first_seeds = 0;
-  for (auto &t : first) first_seeds += t.hi - t.lo;
-  const int64_t range_seeds = ctx->range_seeds < 0    ? 0
-                              : ctx->range_seeds > 0 ? ctx->range_seeds
-                                                     : std::max<int64_t>(256, first_seeds / (32 * L.nwarps));
+  int64_t all_seeds = 0;
+  for (int comp = 0; comp < 2; comp++)
+    for (auto &t : pairs[comp]) all_seeds += t.hi - t.lo;
+  // about 32 tasks per warp
+  const int64_t RS = ctx->range_seeds < 0    ? 0
+                     : ctx->range_seeds > 0 ? ctx->range_seeds
+                                            : std::max<int64_t>(256, all_seeds / (32 * L.nwarps));
+  const int nself = (int)self_idx.size();
+  std::vector<int64_t> x12(2 * (size_t)nself, 0);
+  if (RS > 0 && nself > 0) {
+    const int64_t bmx = maxctg, num = bmx - 127;
+    const int64_t cd_lo = num >= 0 ? (num + 63) / 64 : -((-num) / 64), cd_hi = bmx / 64;
+    std::vector<int64_t> lohi(2 * (size_t)nself);
+    for (int q = 0; q < nself; q++) {
+      lohi[2 * q] = pairs[0][self_idx[q]].lo;
+      lohi[2 * q + 1] = pairs[0][self_idx[q]].hi;
+    }
+    ENSURE(ctx->selfb, sizeof(int64_t) * 4 * (size_t)nself);
+    int64_t *dlohi = P<int64_t>(ctx->selfb), *dx12 = dlohi + 2 * nself;
+    CK(cudaMemcpyAsync(dlohi, lohi.data(), sizeof(int64_t) * 2 * nself, cudaMemcpyHostToDevice, ctx->st));
+    launch_self_bounds(ctx->sorted[0], ctx->lay[0], dlohi, nself, cd_lo, cd_hi, dx12, ctx->st);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(x12.data(), dx12, sizeof(int64_t) * 2 * nself, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  int nranges = 0;
+  // ranges of about RS seeds covering seeds [x0, x1) of pair t (x1 a band start)
+  auto add_ranges = [&](const PairTask &t, int64_t x0, int64_t x1, std::vector<int> &ids,
+                        std::vector<PairTask> &dst) {
+    const int64_t step = RS > 0 ? RS : x1 - x0;
+    for (int64_t x = x0; x < x1; x += step) {
+      PairTask r = t;
+      r.entry_bepos = 0;
+      r.seg = nranges++;
+      r.slo = x;
+      r.shi = std::min(x1, x + step);
+      ids.push_back(r.seg);
+      dst.push_back(r);
+    }
+  };
+  LaunchPlan P1;
+  std::vector<int> first_task(first.size(), -1), first_fin(first.size(), -1);
+  std::vector<std::vector<int>> first_ids(first.size());
+  for (size_t i = 0; i < first.size(); i++) {
+    PairTask t = first[i];
+    if (RS > 0 && t.hi - t.lo > RS) {
+      add_ranges(t, t.lo, t.hi, first_ids[i], P1.tasks);
+      FinishTask f{t.comp, t.a, t.b, 0, (int)P1.ridx.size(), (int)first_ids[i].size()};
+      P1.ridx.insert(P1.ridx.end(), first_ids[i].begin(), first_ids[i].end());
+      first_fin[i] = (int)P1.fins.size();
+      P1.fins.push_back(f);
+    } else {
+      first_task[i] = (int)P1.tasks.size();
+      P1.tasks.push_back(t);
+    }
+  }
+  struct SelfPlan {
+    std::vector<int> pre, post;
+    int diag = -1;  // range number of the middle part (RS > 0)
+    bool whole = false;
+  };
+  std::vector<SelfPlan> sp(nself);
+  std::vector<PairTask> diag_task(nself);
+  for (int q = 0; q < nself; q++) {
+    const PairTask &t = pairs[0][self_idx[q]];
+    if (RS <= 0) {
+      sp[q].whole = true;
+      diag_task[q] = t;
+      continue;
+    }
+    const int64_t x1 = t.lo + x12[2 * q], x2 = t.lo + x12[2 * q + 1];
+    add_ranges(t, t.lo, x1, sp[q].pre, P1.tasks);
+    add_ranges(t, x2, t.hi, sp[q].post, P1.tasks);
+    if (x2 > x1) {
+      PairTask d = t;
+      d.seg = sp[q].diag = nranges++;
+      d.slo = x1;
+      d.shi = x2;
+      diag_task[q] = d;
+    }
+  }
+  ENSURE(ctx->rout, sizeof(PairOut) * (size_t)(nranges + 1));
+  std::vector<PairOut> rout_h(nranges);
+
   const double t_launch = now_ms();
-  std::vector<PairOut> out1;
   long long maxcyc = 0, sumcyc = 0;
-  int64_t maxcalls = 0;
-  int r = align_run_tasks(ctx, L, first, out1, range_seeds, &maxcyc, &maxcalls);
+  int64_t maxcalls = 0, calls = 0;
+  std::vector<PairOut> tout, fout;
+  int r = align_launch(ctx, L, P1, tout, fout, rout_h, &maxcyc, &maxcalls);
   if (r) return r;
-  int64_t calls = 0;
-  for (auto &o : out1) {
-    calls += o.calls;
-    sumcyc += o.cycles;
+  std::vector<PairOut> out1(first.size());
+  for (size_t i = 0; i < first.size(); i++) {
+    if (first_task[i] >= 0) {
+      out1[i] = tout[first_task[i]];
+    } else {
+      out1[i] = fout[first_fin[i]];
+      long long c = 0;
+      for (int id : first_ids[i]) c += rout_h[id].cycles;
+      out1[i].cycles = c + fout[first_fin[i]].cycles;
+    }
+    calls += out1[i].calls;
+    sumcyc += out1[i].cycles;
   }
 
   const double t_self = now_ms();
   // 6. self pairs: entry values by FastGA's order (src/fastga_order.c)
   int64_t nrounds = 0;
-  if (!self_idx.empty()) {
+  if (nself > 0) {
     FastgaOrder F;
     F.n = nc;
     F.at.resize(nc);
@@ -1009,11 +1091,44 @@ int run_align(pga_ctx *ctx) {
     const int UNSET_MAIN = 32767;
     auto unset = [&](int rs) { return rs == 0 ? UNSET_MAIN : 0; };
     std::vector<int64_t> S(nc, 0);  // 0 none, 1 pending, 2 no call, 3+bepos called
-    std::vector<int> val(self_idx.size(), 0), state(self_idx.size(), 0);  // 0 undetermined, 1 known
-    for (size_t q = 0; q < self_idx.size(); q++) {
+    std::vector<int> val(nself, 0), state(nself, 0);  // 0 undetermined, 1 known
+    std::vector<char> done(nself, 0);
+    // the ranges of self pair q in order, with its middle part's
+    auto self_ids = [&](int q) {
+      std::vector<int> ids = sp[q].pre;
+      if (sp[q].diag >= 0) ids.push_back(sp[q].diag);
+      ids.insert(ids.end(), sp[q].post.begin(), sp[q].post.end());
+      return ids;
+    };
+    LaunchPlan pending;  // self pairs to finish in the next launch
+    std::vector<int> pending_q;
+    for (int q = 0; q < nself; q++) {
       const PairTask &t = pairs[0][self_idx[q]];
       int x = F.pos[t.a];
       S[x] = 1;
+      if (!sp[q].whole) {
+        int pc, pe;
+        combine_ranges(rout_h, sp[q].pre, &pc, &pe, 0);
+        if (pc > 0 || sp[q].diag < 0) {
+          // entered after a call of its own, or with no middle part: its
+          // result does not depend on the order's value
+          val[q] = pe;
+          state[q] = 1;
+          if (sp[q].diag < 0) {
+            std::vector<int> ids = self_ids(q);
+            int c, e;
+            combine_ranges(rout_h, ids, &c, &e, 0);
+            S[x] = c > 0 ? 3 + (int64_t)e : 2;
+            calls += c;
+            for (int id : ids) sumcyc += rout_h[id].cycles;
+            done[q] = 1;
+            FinishTask f{0, t.a, t.b, 0, (int)pending.ridx.size(), (int)ids.size()};
+            pending.ridx.insert(pending.ridx.end(), ids.begin(), ids.end());
+            pending.fins.push_back(f);
+          }
+          continue;
+        }
+      }
       auto &e = earlier[x];
       std::sort(e.begin(), e.end(), [](const std::pair<int, int> &u, const std::pair<int, int> &v) {
         return u.first > v.first;  // nearest (latest) earlier partner first
@@ -1031,11 +1146,11 @@ int run_align(pga_ctx *ctx) {
         state[q] = 1;
       }
     }
-    std::vector<char> done(self_idx.size(), 0);
     while (true) {
-      std::vector<PairTask> batch;
-      std::vector<size_t> bq;
-      for (size_t q = 0; q < self_idx.size(); q++) {
+      LaunchPlan plan = pending;
+      pending = LaunchPlan();
+      std::vector<int> bq;
+      for (int q = 0; q < nself; q++) {
         if (done[q]) continue;
         if (!state[q]) {
           // fo_from_rows (src/fastga_order_core.c:167-192)
@@ -1064,26 +1179,40 @@ int run_align(pga_ctx *ctx) {
           val[q] = known ? bep : unset(rs);
           state[q] = 1;
         }
-        PairTask t = pairs[0][self_idx[q]];
-        t.entry_bepos = val[q];
-        batch.push_back(t);
+        PairTask d = diag_task[q];
+        d.entry_bepos = val[q];
+        plan.tasks.push_back(d);
         bq.push_back(q);
+        if (!sp[q].whole) {
+          std::vector<int> ids = self_ids(q);
+          FinishTask f{0, d.a, d.b, 0, (int)plan.ridx.size(), (int)ids.size()};
+          plan.ridx.insert(plan.ridx.end(), ids.begin(), ids.end());
+          plan.fins.push_back(f);
+        }
       }
-      if (batch.empty()) break;
-      nrounds++;
-      std::vector<PairOut> ob;
-      r = align_run_tasks(ctx, L, batch, ob, 0, &maxcyc, &maxcalls);
+      if (plan.tasks.empty() && plan.fins.empty()) break;
+      if (!plan.tasks.empty()) nrounds++;
+      r = align_launch(ctx, L, plan, tout, fout, rout_h, &maxcyc, &maxcalls);
       if (r) return r;
-      for (size_t i = 0; i < batch.size(); i++) {
-        size_t q = bq[i];
+      for (size_t i = 0; i < bq.size(); i++) {
+        const int q = bq[i];
         done[q] = 1;
-        int x = F.pos[batch[i].a];
-        S[x] = ob[i].calls > 0 ? 3 + (int64_t)ob[i].exit_bepos : 2;
-        calls += ob[i].calls;
-        sumcyc += ob[i].cycles;
+        int x = F.pos[pairs[0][self_idx[q]].a];
+        int c, e;
+        if (sp[q].whole) {
+          c = tout[i].calls;
+          e = tout[i].exit_bepos;
+          sumcyc += tout[i].cycles;
+        } else {
+          std::vector<int> ids = self_ids(q);
+          combine_ranges(rout_h, ids, &c, &e, val[q]);
+          for (int id : ids) sumcyc += rout_h[id].cycles;
+        }
+        S[x] = c > 0 ? 3 + (int64_t)e : 2;
+        calls += c;
       }
     }
-    for (size_t q = 0; q < self_idx.size(); q++)
+    for (int q = 0; q < nself; q++)
       if (!done[q]) return fail(ctx, PGA_ERR_ARG, "self pairs that cannot be resolved");
   }
 
@@ -1174,7 +1303,7 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
-                   &ctx->fout, &ctx->ridx};
+                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb};
   for (DBuf *b : abufs)
     if (b->p) cudaFree(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
