@@ -597,6 +597,378 @@ __device__ __forceinline__ void wave_prune(const WarpWork &W, const int *V, int 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident waves.  While a wave is at most 32 diagonals wide (and
+// the previous one was not empty) diagonal k lives in lane k mod 32: its
+// antidiagonal, match count, match history, head pebble, head mark and next
+// trace mark stay in registers, the previous wave's neighbours come by
+// shuffle, and the visit-order questions (pebble slots, records, clips,
+// pruning) are answered with ballots rotated into visit order and warp
+// reductions.  NA is also written through to memory; the other fields go to
+// the memory ring only when a wider wave hands over to wave_sweep.
+// ---------------------------------------------------------------------------
+struct RegWave {
+  int V, M, HA, HM, NA;
+  uint64_t T;
+};
+
+// Visit position of lane l's diagonal (forward: hgh first, reverse: low first).
+template <bool FWD>
+__device__ __forceinline__ int reg_pos(int l, int low, int hgh) {
+  return FWD ? ((hgh - l) & 31) : ((l - low) & 31);
+}
+template <bool FWD>
+__device__ __forceinline__ int reg_lane(int p, int low, int hgh) {
+  return FWD ? ((hgh - p) & 31) : ((low + p) & 31);
+}
+// A lane mask reordered so that bit p is the lane at visit position p.
+template <bool FWD>
+__device__ __forceinline__ uint32_t reg_posmask(uint32_t m, int low, int hgh) {
+  return FWD ? __brev(__funnelshift_l(m, m, 31 - (hgh & 31))) : __funnelshift_r(m, m, low & 31);
+}
+
+// Memory ring (buffer cur) -> registers for the diagonals of [plow, phgh].
+__device__ __forceinline__ void reg_load(const WarpWork &W, int cur, int plow, int phgh, RegWave &R) {
+  const int lane = threadIdx.x & 31, vmask = W.vcap - 1;
+  const int k = plow + ((lane - plow) & 31);
+  if (k <= phgh) {
+    const int vi = k & vmask;
+    R.V = W.V[cur][vi];
+    R.M = W.M[cur][vi];
+    R.T = W.T[cur][vi];
+    R.HA = W.HA[cur][vi];
+    R.HM = W.HM[cur][vi];
+    R.NA = W.NA[vi];
+  }
+}
+
+// Registers -> memory ring (buffer cur) for the diagonals of [plow, phgh].
+__device__ __forceinline__ void reg_store(WarpWork &W, int cur, int plow, int phgh, const RegWave &R) {
+  const int lane = threadIdx.x & 31, vmask = W.vcap - 1;
+  const int k = plow + ((lane - plow) & 31);
+  if (k <= phgh) {
+    const int vi = k & vmask;
+    W.V[cur][vi] = R.V;
+    W.M[cur][vi] = R.M;
+    W.T[cur][vi] = R.T;
+    W.HA[cur][vi] = R.HA;
+    W.HM[cur][vi] = R.HM;
+    W.NA[vi] = R.NA;
+  }
+}
+
+// One wave in registers: [low, hgh] (at most 32 wide) from the previous
+// wave [plow, phgh] (not empty, inside [low-1, hgh+1]).  Same results as
+// wave_sweep; fills WS for wave_prune.
+template <bool FWD>
+__device__ __forceinline__ int reg_wave(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
+                                        int hgh, int plow, int phgh, int dif, RegWave &R, int &besta, int &bestx,
+                                        int &lasta, int &trima, int &trimx, int &trimd, int &trimha, int &more,
+                                        int &aclip, int &bclip, WaveSlice &WS) {
+  const int lane = threadIdx.x & 31;
+  const int vmask = W.vcap - 1;
+  const int tspace = spec.trace_space;
+  const int BV = FWD ? -1 : I32MAX;
+  const int k = low + ((lane - low) & 31);
+  const bool act = k <= hgh;
+  // the previous wave at k+1, k, k-1
+  const int vp = __shfl_sync(FULL, R.V, (lane + 1) & 31), vm = __shfl_sync(FULL, R.V, (lane - 1) & 31);
+  const int ap = (k + 1 >= plow && k + 1 <= phgh) ? vp : BV;
+  const int ac = (k >= plow && k <= phgh) ? R.V : BV;
+  const int am = (k - 1 >= plow && k - 1 <= phgh) ? vm : BV;
+  int src, c;
+  if (FWD) {
+    if (ac < am) src = (am < ap) ? 1 : -1;
+    else src = (ac < ap) ? 1 : 0;
+    c = src == 1 ? ap + 1 : (src == -1 ? am + 1 : ac + 2);
+  } else {
+    if (ac > ap) src = (ap > am) ? -1 : 1;
+    else src = (ac > am) ? -1 : 0;
+    c = src == -1 ? am - 1 : (src == 1 ? ap - 1 : ac - 2);
+  }
+  const int sl = (k + src) & 31;
+  const int sM = __shfl_sync(FULL, R.M, sl), sHA = __shfl_sync(FULL, R.HA, sl), sHM = __shfl_sync(FULL, R.HM, sl);
+  const uint64_t sT = __shfl_sync(FULL, R.T, sl);
+  // next trace mark: a new bottom diagonal copies the one above it, a new top
+  // diagonal the one below it
+  const int nlo = __shfl_sync(FULL, R.NA, plow & 31), nhi = __shfl_sync(FULL, R.NA, phgh & 31);
+  const bool dflt = FWD ? (src == 1 && k == hgh) : (src == -1 && k == low);
+  int m = dflt ? PATH_LEN : sM;
+  uint64_t b = dflt ? PATH_INT : sT;
+  int ha = dflt ? -1 : sHA, hm = dflt ? 0 : sHM;
+  int nak = (k >= plow && k <= phgh) ? R.NA : (k < plow ? nlo : nhi);
+  if ((b & PATH_TOP) != 0) m -= 1;
+  b <<= 1;
+  int x = (c + k) >> 1;
+  int kk[1] = {k}, xx[1] = {x}, run[1], hb[1], hA[1];
+  lane_snakes<FWD, 1>(A, B, act ? 1 : 0, kk, xx, run, hb, hA);
+  x = xx[0];
+  int npb = 0;
+  if (act) {
+    history_run(b, m, run[0]);
+    c = (x << 1) - k;
+    int hq = hm;
+    if (FWD) {
+      for (int q = nak; x >= q; q += tspace)
+        if (hq < q) {
+          npb++;
+          hq = q;
+        }
+    } else {
+      for (int q = nak; x <= q; q -= tspace)
+        if (hq > q) {
+          npb++;
+          hq = q;
+        }
+    }
+  }
+  // trim test of this diagonal's history (used if it is a record)
+  bool tr = false;
+  if (act && m >= spec.ave_path)
+    tr = spec.table[b & TRIM_MASK] >= 0 &&
+         spec.table[(b >> TRIM_LEN) & TRIM_MASK] + spec.score[b & TRIM_MASK] >= 0;
+  // pebble slots in visit order
+  const int pos = reg_pos<FWD>(lane, low, hgh);
+  int off, tot;
+  if (__ballot_sync(FULL, npb > 1) == 0) {
+    uint32_t one = reg_posmask<FWD>(__ballot_sync(FULL, npb == 1), low, hgh);
+    off = __popc(one & ((1u << pos) - 1));
+    tot = __popc(one);
+  } else {
+    // visit-order exclusive sum over positions
+    int xsum = npb;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int y = __shfl_sync(FULL, xsum, reg_lane<FWD>(pos - d, low, hgh));
+      if (pos >= d) xsum += y;
+    }
+    off = xsum - npb;
+    tot = __reduce_add_sync(FULL, npb);
+  }
+  int64_t pb0 = warp_pebbles(W, tot);
+  if (pb0 < 0) return 1;
+  if (act) {
+    int64_t s = pb0 + off;
+    Pebble *cells = W.pool.cells;
+    if (FWD) {
+      while (x >= nak) {
+        if (hm < nak) {
+          cells[s] = {ha, k, dif, nak};
+          ha = (int)s;
+          hm = nak;
+          s += 1;
+        }
+        nak += tspace;
+      }
+    } else {
+      while (x <= nak) {
+        if (hm > nak) {
+          cells[s] = {ha, k, dif, nak};
+          ha = (int)s;
+          hm = nak;
+          s += 1;
+        }
+        nak -= tspace;
+      }
+    }
+    W.NA[k & vmask] = nak;
+    R.V = c;
+    R.M = m;
+    R.T = b;
+    R.HA = ha;
+    R.HM = hm;
+    R.NA = nak;
+  }
+  // clips: bclip from the first visited diagonal that met B's end, aclip
+  // from the last visited that met A's end
+  const uint32_t hbm = reg_posmask<FWD>(__ballot_sync(FULL, act && hb[0]), low, hgh);
+  const uint32_t ham = reg_posmask<FWD>(__ballot_sync(FULL, act && hA[0]), low, hgh);
+  if (hbm) {
+    more = 0;
+    const int p = __ffs(hbm) - 1;
+    const int kb = FWD ? hgh - p : low + p;
+    if (FWD ? (bclip < kb) : (bclip > kb)) bclip = kb;
+  }
+  if (ham) {
+    more = 0;
+    const int p = 31 - __clz(ham);
+    aclip = FWD ? hgh - p : low + p;
+  }
+  // records: c beyond the running best in visit order.  The last record is
+  // the first diagonal reaching the wave's best; the one before it the first
+  // reaching the best of the earlier positions, and so on.
+  const int carry = besta;
+  const int cv = act ? c : (FWD ? -2147483647 : 2147483647);
+  int best = FWD ? __reduce_max_sync(FULL, cv) : __reduce_min_sync(FULL, cv);
+  if (FWD ? best > carry : best < carry) {
+    const int fl = (m >= spec.ave_path ? 1 : 0) | (tr ? 2 : 0);
+    int limit = 32;  // positions below this are still candidates
+    int lp = -1, lt = -1;
+    bool first = true;
+    while (true) {
+      const uint32_t eq = reg_posmask<FWD>(__ballot_sync(FULL, act && c == best && pos < limit), low, hgh);
+      const int p = __ffs(eq) - 1;
+      const int L = reg_lane<FWD>(p, low, hgh);
+      if (first) {
+        besta = best;
+        bestx = __shfl_sync(FULL, x, L);
+        first = false;
+      }
+      const int f = __shfl_sync(FULL, fl, L);
+      if (lp < 0 && (f & 1)) lp = L;
+      if (f & 2) {
+        lt = L;
+        break;
+      }
+      limit = p;
+      const int cv2 = (act && pos < limit) ? c : (FWD ? -2147483647 : 2147483647);
+      best = FWD ? __reduce_max_sync(FULL, cv2) : __reduce_min_sync(FULL, cv2);
+      if (!(FWD ? best > carry : best < carry)) break;
+    }
+    if (lp >= 0) lasta = __shfl_sync(FULL, c, lp);
+    if (lt >= 0) {
+      trima = __shfl_sync(FULL, c, lt);
+      trimx = __shfl_sync(FULL, x, lt);
+      trimd = dif;
+      trimha = __shfl_sync(FULL, ha, lt);
+    }
+  }
+  WS.single = true;
+  WS.c[0] = c;
+  WS.k0 = k;
+  WS.nact = act ? 1 : 0;
+  return 0;
+}
+
+// The wave loop of forward_wave (FWD) or reverse_wave after the 0-wave:
+// grow the band, compute the wave, clip at sequence ends, prune.  Waves of
+// at most 32 diagonals run in registers (reg_wave), wider ones through the
+// memory ring (wave_sweep).
+template <bool FWD>
+__device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B,
+                                         const uint8_t *aseq, const uint8_t *bseq, int minp, int maxp, int &low,
+                                         int &hgh, int &dif, int &cur, int &besta, int &bestx, int &lasta,
+                                         int &trima, int &trimx, int &trimd, int &trimha, int &more, int &aclip,
+                                         int &bclip, int &morem, int &morea, int &morex, int &mored, int &moreha,
+                                         int max_waves) {
+  const int lane = threadIdx.x & 31;
+  const int vmask = W.vcap - 1;
+  const int BV = FWD ? -1 : I32MAX;
+  int *NA = W.NA;
+  RegWave R;
+  R.V = BV;
+  R.M = R.HA = R.HM = R.NA = 0;
+  R.T = 0;
+  bool regmode = false;
+  while (more && (FWD ? lasta >= besta - TRIM_MLAG : lasta <= besta + TRIM_MLAG)) {
+    if (dif > max_waves) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
+    const int plow = low, phgh = hgh;
+    low -= 1;
+    hgh += 1;
+    if (hgh - low + 3 > W.vcap) {
+      W.err |= ALN_ERR_VCAP;
+      return 1;
+    }
+    const bool grow_lo = low >= minp, grow_hi = hgh <= maxp;
+    if (!grow_lo) low += 1;
+    if (!grow_hi) hgh -= 1;
+    const bool use_reg = phgh >= plow && hgh - low + 1 <= 32;
+    WaveSlice WS;
+    if (use_reg) {
+      if (!regmode) {
+        reg_load(W, cur, plow, phgh, R);
+        regmode = true;
+      }
+      dif += 1;
+      if (reg_wave<FWD>(W, spec, A, B, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
+                        trimha, more, aclip, bclip, WS))
+        return 1;
+    } else {
+      if (regmode) {
+        reg_store(W, cur, plow, phgh, R);
+        regmode = false;
+        __syncwarp();
+      }
+      // boundary diagonals on the previous wave's buffer (lane 0; visible
+      // after syncwarp); the diagonal past the top carries T = PATH_INT,
+      // M = PATH_LEN, HA = -1
+      int *Vo = W.V[cur];
+      if (lane == 0) {
+        if (grow_lo) {
+          NA[low & vmask] = NA[(low + 1) & vmask];
+          Vo[low & vmask] = BV;
+        }
+        if (grow_hi) {
+          NA[hgh & vmask] = NA[(hgh - 1) & vmask];
+          Vo[hgh & vmask] = BV;
+        }
+        Vo[(hgh + 1) & vmask] = BV;
+        Vo[(low - 1) & vmask] = BV;
+      }
+      dif += 1;
+      __syncwarp();
+      if (wave_sweep<FWD>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
+                          aclip, bclip, WS))
+        return 1;
+      cur ^= 1;
+      __syncwarp();
+    }
+    if (more == 0) {
+      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
+      // state of a diagonal of the wave just made
+      auto at = [&](int kq, int &vq, int &mq, int &haq) {
+        if (regmode) {
+          vq = __shfl_sync(FULL, R.V, kq & 31);
+          mq = __shfl_sync(FULL, R.M, kq & 31);
+          haq = __shfl_sync(FULL, R.HA, kq & 31);
+        } else {
+          vq = W.V[cur][kq & vmask];
+          mq = W.M[cur][kq & vmask];
+          haq = W.HA[cur][kq & vmask];
+        }
+      };
+      // FWD: the top side meets A's end (aclip), the bottom B's (bclip);
+      // reverse: the bottom meets A's start, the top B's
+      const bool cut_a = FWD ? hgh >= aclip : low <= aclip;
+      if (cut_a) {
+        if (FWD) hgh = aclip - 1;
+        else low = aclip + 1;
+        int vq, mq, haq;
+        at(aclip, vq, mq, haq);
+        if (morem <= mq) {
+          morem = mq;
+          morea = vq;
+          morex = (morea + aclip) >> 1;
+          mored = dif;
+          moreha = haq;
+        }
+      }
+      const bool cut_b = FWD ? low <= bclip : hgh >= bclip;
+      if (cut_b) {
+        if (FWD) low = bclip + 1;
+        else hgh = bclip - 1;
+        int vq, mq, haq;
+        at(bclip, vq, mq, haq);
+        if (morem <= mq) {
+          morem = mq;
+          morea = vq;
+          morex = (morea + bclip) >> 1;
+          mored = dif;
+          moreha = haq;
+        }
+      }
+      aclip = FWD ? I32MAX : -I32MAX;
+      bclip = FWD ? -I32MAX : I32MAX;
+    }
+    wave_prune<FWD>(W, W.V[cur], besta, low, hgh, WS);
+  }
+  __syncwarp();
+  return 0;
+}
+
 #define WVI(k) ((k) & vmask)
 
 // ---------------------------------------------------------------------------
@@ -724,74 +1096,9 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     }
   }
 
-  while (more && lasta >= besta - TRIM_MLAG) {
-    if (dif > max_waves) {
-      W.err |= ALN_ERR_VCAP;
-      return 1;
-    }
-    low -= 1;
-    hgh += 1;
-    if (hgh - low + 3 > W.vcap) {
-      W.err |= ALN_ERR_VCAP;
-      return 1;
-    }
-    int *Vo = W.V[cur];
-    // boundary diagonals on the previous wave's buffer (lane 0; visible after
-    // syncwarp); k = hgh+1 carries T = PATH_INT, M = PATH_LEN, HA = -1
-    if (low >= minp) {
-      if (lane == 0) {
-        NA[WVI(low)] = NA[WVI(low + 1)];
-        Vo[WVI(low)] = -1;
-      }
-    } else
-      low += 1;
-    if (hgh <= maxp) {
-      if (lane == 0) {
-        NA[WVI(hgh)] = NA[WVI(hgh - 1)];
-        Vo[WVI(hgh)] = -1;
-      }
-    } else
-      hgh -= 1;
-    if (lane == 0) {
-      Vo[WVI(hgh + 1)] = -1;
-      Vo[WVI(low - 1)] = -1;
-    }
-    dif += 1;
-    __syncwarp();
-    WaveSlice WS;
-    if (wave_sweep<true>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
-                         aclip, bclip, WS))
-      return 1;
-    cur ^= 1;
-    __syncwarp();
-    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
-    if (more == 0) {
-      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
-      if (hgh >= aclip) {
-        hgh = aclip - 1;
-        if (morem <= M[WVI(aclip)]) {
-          morem = M[WVI(aclip)];
-          morea = V[WVI(aclip)];
-          morex = (morea + aclip) >> 1;
-          mored = dif;
-          moreha = HA[WVI(aclip)];
-        }
-      }
-      if (low <= bclip) {
-        low = bclip + 1;
-        if (morem <= M[WVI(bclip)]) {
-          morem = M[WVI(bclip)];
-          morea = V[WVI(bclip)];
-          morex = (morea + bclip) >> 1;
-          mored = dif;
-          moreha = HA[WVI(bclip)];
-        }
-      }
-      aclip = I32MAX;
-      bclip = -I32MAX;
-    }
-    wave_prune<true>(W, V, besta, low, hgh, WS);
-  }
+  if (wave_loop<true>(W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx,
+                      trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
+    return 1;
   __syncwarp();
 
   // trace-back (lane-uniform sequential code; only lane 0 writes)
@@ -998,72 +1305,9 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     }
   }
 
-  while (more && lasta <= besta + TRIM_MLAG) {
-    if (dif > max_waves) {
-      W.err |= ALN_ERR_VCAP;
-      return 1;
-    }
-    low -= 1;
-    hgh += 1;
-    if (hgh - low + 3 > W.vcap) {
-      W.err |= ALN_ERR_VCAP;
-      return 1;
-    }
-    int *Vo = W.V[cur];
-    if (low >= minp) {
-      if (lane == 0) {
-        NA[WVI(low)] = NA[WVI(low + 1)];
-        Vo[WVI(low)] = I32MAX;
-      }
-    } else
-      low += 1;
-    if (hgh <= maxp) {
-      if (lane == 0) {
-        NA[WVI(hgh)] = NA[WVI(hgh - 1)];
-        Vo[WVI(hgh)] = I32MAX;
-      }
-    } else
-      hgh -= 1;
-    if (lane == 0) {
-      Vo[WVI(hgh + 1)] = I32MAX;
-      Vo[WVI(low - 1)] = I32MAX;
-    }
-    dif += 1;
-    __syncwarp();
-    WaveSlice WS;
-    if (wave_sweep<false>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
-                          aclip, bclip, WS))
-      return 1;
-    cur ^= 1;
-    __syncwarp();
-    int *V = W.V[cur], *M = W.M[cur], *HA = W.HA[cur];
-    if (more == 0) {
-      if (bseq[besta - bestx] != 4 && aseq[bestx] != 4) more = 1;
-      if (low <= aclip) {
-        low = aclip + 1;
-        if (morem <= M[WVI(aclip)]) {
-          morem = M[WVI(aclip)];
-          morea = V[WVI(aclip)];
-          morex = (morea + aclip) >> 1;
-          mored = dif;
-          moreha = HA[WVI(aclip)];
-        }
-      }
-      if (hgh >= bclip) {
-        hgh = bclip - 1;
-        if (morem <= M[WVI(bclip)]) {
-          morem = M[WVI(bclip)];
-          morea = V[WVI(bclip)];
-          morex = (morea + bclip) >> 1;
-          mored = dif;
-          moreha = HA[WVI(bclip)];
-        }
-      }
-      aclip = -I32MAX;
-      bclip = I32MAX;
-    }
-    wave_prune<false>(W, V, besta, low, hgh, WS);
-  }
+  if (wave_loop<false>(W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima,
+                       trimx, trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
+    return 1;
   __syncwarp();
 
   {
