@@ -235,7 +235,47 @@ def run_reference(args, rank: int) -> None:
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": "chromset generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    emit(rank, line)
+
+
+# ---- ranks ---------------------------------------------------------------------------
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+
+
+def max_over_ranks(vals, world: int, device: str):
+    """Element-wise maximum of `vals` over all ranks (the slowest rank's times)."""
+    if world <= 1:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def emit(rank: int, line: dict) -> None:
+    """Rank 0 prints the one JSON line."""
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def align_roofline(work: dict, align_ms: float) -> dict:
+    """The aligner is integer-issue bound: its work in cells (one diagonal
+    updated in one wave step) per second, with the SM issue utilisation of
+    k_align_pairs from the committed ncu summary when there is one."""
+    out = {"bound": "issue", "unit": "cells/s", "cells": work["cells"], "waves": work["waves"],
+           "calls": work["calls"], "warp_tasks": work["tasks"],
+           "achieved": work["cells"] / (align_ms / 1000.0) if align_ms > 0 else None,
+           "issue_util": None}
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_align_pairs_issue.json")) as f:
+            out["issue_util"] = json.load(f).get("sm_issue_active_pct_of_active_cycles")
+    except Exception:
+        pass
+    return out
 
 
 # ---- GPU arm ---------------------------------------------------------------------
@@ -261,8 +301,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    barrier(world)
     clocks = ClockSampler(local_rank)
     clocks.start()
     l0 = dev.launches()
@@ -273,6 +312,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
+    barrier(world)
     ms = ev0.elapsed_time(ev1) / args.steps
     launches = (dev.launches() - l0) // args.steps
     clk = clocks.stop()
@@ -287,6 +327,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     astats = dev.align_stats()
     atimes = dev.align_times()
+    awork = dev.align_work()
     recs, toff, tr = dev.alignments()
     aligned_bases = int((recs[:, 2] - recs[:, 1]).sum()) if len(recs) else 0
 
@@ -315,10 +356,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             e2e_ms.append(t0.elapsed_time(t1))
     e2e_ms_step = statistics.median(e2e_ms)
 
-    t = torch.tensor([ms, e2e_ms_step], device="cuda", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms, e2e_ms_step = float(t[0]), float(t[1])
+    ms, e2e_ms_step = max_over_ranks([ms, e2e_ms_step], world, "cuda")
     mbp = cs.seqtot / 1e6
     value = world * mbp / (ms / 1000.0)
     e2e = world * mbp / (e2e_ms_step / 1000.0)
@@ -360,6 +398,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "stage_ms": st,
         "align_ms": atimes,
+        "align_roofline": align_roofline(awork, st["align"]),
         "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
                                                "k_lcp, k_entries, k_prefix_table)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -370,7 +409,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "gpu_launches": int(launches),
         "clocks": clk,
     }
-    print(json.dumps(line))
+    emit(rank, line)
 
 
 def main():

@@ -318,6 +318,7 @@ k_align_pairs(AlignLaunch P) {
   W.pool.next = P.cell_next;
   W.pool.cap = P.cell_cap;
   W.chunk_next = W.chunk_end = 0;
+  W.waves = W.cells = 0;
 
   OvlArena O = warp_arena(P, wid);
 
@@ -353,6 +354,9 @@ k_align_pairs(AlignLaunch P) {
     int rc = align_pair(S, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane, 32, blo, bhi);
     __syncwarp();
     PairOut po;
+    po.waves = W.waves;
+    po.cells = W.cells;
+    W.waves = W.cells = 0;
     po.calls = R.calls;
     po.exit_bepos = R.exit_bepos;
     po.nsurv = 0;
@@ -398,6 +402,7 @@ k_finish_pairs(AlignLaunch P) {
     const FinishTask ft = P.ftasks[t];
     long long t0 = clock64();
     PairOut po;
+    po.waves = po.cells = 0;
     po.calls = 0;
     po.exit_bepos = ft.entry_bepos;
     po.nsurv = 0;

@@ -27,7 +27,8 @@ struct PairTask {
 struct PairOut {
   int calls, exit_bepos, nsurv, err;
   int64_t rec_off;
-  long long cycles;  // SM clock cycles the warp spent on the task
+  long long cycles;     // SM clock cycles the warp spent on the task
+  int64_t waves, cells;  // wave steps of its Local_Alignment calls, and their diagonals
 };
 
 // A pair run in ranges: its ranges, in order, are range_idx[first ..

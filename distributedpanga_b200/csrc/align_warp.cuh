@@ -45,6 +45,7 @@ struct WarpWork {
   PebblePool pool;
   int64_t chunk_next, chunk_end;  // this warp's current pebble chunk (lane-uniform)
   int err;
+  int64_t waves, cells;  // waves after the 0-wave, and their diagonals (lane-uniform counts)
 };
 
 constexpr int PEBBLE_CHUNK = 4096;
@@ -876,6 +877,8 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
     if (!grow_lo) low += 1;
     if (!grow_hi) hgh -= 1;
     const bool use_reg = phgh >= plow && hgh - low + 1 <= 32;
+    W.waves += 1;
+    W.cells += hgh >= low ? hgh - low + 1 : 0;
     WaveSlice WS;
     if (use_reg) {
       if (!regmode) {

@@ -85,6 +85,7 @@ struct pga_ctx {
   std::vector<int64_t> h_toff;     // offsets into h_trace
   int64_t align_stats[8] = {0};    // pga_align_stats
   float align_ms[4] = {0};         // pga_align_times
+  int64_t align_work[4] = {0};     // pga_align_work
   int64_t range_seeds = 0;         // pga_align_set_ranges
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
@@ -739,6 +740,9 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
   }
   for (size_t k = 0; k < nt; k++) {
     tout[order[k]] = ro[k];
+    ctx->align_work[0] += ro[k].waves;
+    ctx->align_work[1] += ro[k].cells;
+    ctx->align_work[3] += 1;
     if (ro[k].cycles > *max_cycles) {
       *max_cycles = ro[k].cycles;
       *max_task_calls = ro[k].calls;
@@ -916,6 +920,7 @@ int run_align(pga_ctx *ctx) {
   ENSURE(ctx->rec_next, 64);
   ENSURE(ctx->out_next, 64);
   ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
+  for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
   L.next_task = P<unsigned>(ctx->task_next);
   L.wave = P<int>(ctx->wave);
   L.points = P<uint16_t>(ctx->points);
@@ -1258,6 +1263,7 @@ int run_align(pga_ctx *ctx) {
   ctx->align_stats[5] = nrounds;
   ctx->align_stats[6] = sumcyc;
   ctx->align_stats[7] = maxcalls;
+  ctx->align_work[2] = calls;
   const double t_end = now_ms();
   ctx->align_ms[0] = (float)(t_launch - t_start);
   ctx->align_ms[1] = (float)(t_self - t_launch);
@@ -1805,6 +1811,12 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
   }
   if (trace_off) memcpy(trace_off, ctx->h_toff.data(), sizeof(int64_t) * (n + 1));
   if (trace && !ctx->h_trace.empty()) memcpy(trace, ctx->h_trace.data(), ctx->h_trace.size());
+  return PGA_OK;
+}
+
+int pga_align_work(const pga_ctx *ctx, int64_t *work4) {
+  if (!ctx || !work4) return PGA_ERR_ARG;
+  for (int i = 0; i < 4; i++) work4[i] = ctx->align_work[i];
   return PGA_OK;
 }
 

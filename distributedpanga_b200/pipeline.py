@@ -69,6 +69,7 @@ _SIGS = {
     "pga_align_stats": (C.c_int, [vp, vp]),
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "pga_align_work": (C.c_int, [vp, vp]),
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
 }
@@ -290,6 +291,12 @@ class Device:
         a = (C.c_float * 4)()
         self._ck(self.L.pga_align_times(self.h, a), "align_times")
         return {"setup": a[0], "pairs": a[1], "self_pairs": a[2], "order": a[3]}
+
+    def align_work(self) -> dict:
+        """Wave steps, diagonal updates (cells), calls and warp tasks of the last align()."""
+        a = np.zeros(4, dtype=np.int64)
+        self._ck(self.L.pga_align_work(self.h, a.ctypes.data_as(vp)), "align_work")
+        return {"waves": int(a[0]), "cells": int(a[1]), "calls": int(a[2]), "tasks": int(a[3])}
 
     def set_ranges(self, range_seeds: int) -> None:
         """Band-range size for large pairs (0 automatic, -1 never split)."""

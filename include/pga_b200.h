@@ -169,6 +169,12 @@ int pga_align_stats(const pga_ctx *ctx, int64_t *stats8);
  * reference. */
 int pga_align_times(const pga_ctx *ctx, float *ms4);
 
+/* Work of the last pga_align: [0] wave steps of all Local_Alignment calls
+ * (after each call's first wave), [1] their diagonal updates ("cells", the
+ * unit of forward_wave / reverse_wave, lib/align.c:639-753), [2]
+ * Local_Alignment calls, [3] warp tasks.  No counterpart in the reference. */
+int pga_align_work(const pga_ctx *ctx, int64_t *work4);
+
 /* ---- seed diagonal sort without device allocation ---------------------------- */
 
 /* No counterpart in the reference: the reference runs on the host and never
