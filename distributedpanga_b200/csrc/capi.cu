@@ -1832,6 +1832,32 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds) {
   return PGA_OK;
 }
 
+int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, const char *version,
+                         const char *command, const char *db_name, const char *cwd, int nscaff,
+                         const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
+                         const int64_t *contig_sbeg) {
+  if (!ctx || !ctx->have_align) return PGA_ERR_ARG;
+  if (nscaff > 0 && scaff_fctg && scaff_fctg[nscaff] > ctx->ncontig) return PGA_ERR_ARG;
+  const int64_t n = (int64_t)ctx->h_recs.size();
+  std::vector<int32_t> r9(9 * (size_t)n);
+  for (int64_t i = 0; i < n; i++) {
+    const AlnRec &a = ctx->h_recs[i];
+    int32_t *r = r9.data() + 9 * i;
+    r[0] = a.aread;
+    r[1] = a.abpos;
+    r[2] = a.aepos;
+    r[3] = a.bread;
+    r[4] = a.bbpos;
+    r[5] = a.bepos;
+    r[6] = a.comp;
+    r[7] = a.diffs;
+    r[8] = a.tlen;
+  }
+  return pga_write_1aln(path, program, version, command, db_name, cwd, aln::TSPACE, nscaff, scaff_name, scaff_len,
+                        scaff_fctg, contig_sbeg, ctx->clen.data(), n, r9.data(), ctx->h_toff.data(),
+                        ctx->h_trace.data());
+}
+
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8) {
   if (!ctx || !stats8) return PGA_ERR_ARG;
   for (int i = 0; i < 8; i++) stats8[i] = ctx->align_stats[i];

@@ -70,6 +70,10 @@ _SIGS = {
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
+    "pga_write_1aln": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                 C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
+    "pga_align_write_1aln": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                       C.c_char_p, C.c_int, vp, vp, vp, vp]),
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
 }
@@ -292,6 +296,15 @@ class Device:
         self._ck(self.L.pga_align_times(self.h, a), "align_times")
         return {"setup": a[0], "pairs": a[1], "self_pairs": a[2], "order": a[3]}
 
+    def write_1aln(self, path, skeleton=None, db_name="", cwd=None, command="distributedpanga_b200"):
+        """The last align()'s alignments as a .1aln file."""
+        sk = skeleton or Skeleton.per_contig(self.cs.clen)
+        names = sk.c_names()
+        self._ck(self.L.pga_align_write_1aln(self.h, path.encode(), _PROG, _VERSION, command.encode(),
+                                             db_name.encode(), cwd.encode() if cwd else None, len(sk.names), names,
+                                             sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp),
+                                             sk.sbeg.ctypes.data_as(vp)), "align_write_1aln")
+
     def align_work(self) -> dict:
         """Wave steps, diagonal updates (cells), calls and warp tasks of the last align()."""
         a = np.zeros(4, dtype=np.int64)
@@ -320,6 +333,56 @@ class Device:
         return {"pairs": int(a[0]), "self_pairs": int(a[1]), "calls": int(a[2]), "alignments": int(a[4]),
                 "self_rounds": int(a[5]), "max_task_cycles": int(a[3]), "all_task_cycles": int(a[6]),
                 "max_task_calls": int(a[7])}
+
+
+class Skeleton:
+    """The GDB skeleton of a .1aln file: scaffold names and lengths, and
+    where each contig sits (contigs of scaffold s are fctg[s]..fctg[s+1]-1,
+    contig c at sbeg[c] within its scaffold).  One contig per scaffold when
+    built from plain contig lengths."""
+
+    def __init__(self, names, scaff_len, fctg, sbeg):
+        self.names = [n.encode() if isinstance(n, str) else bytes(n) for n in names]
+        self.scaff_len = np.ascontiguousarray(scaff_len, dtype=np.int64)
+        self.fctg = np.ascontiguousarray(fctg, dtype=np.int32)
+        self.sbeg = np.ascontiguousarray(sbeg, dtype=np.int64)
+
+    @classmethod
+    def per_contig(cls, clen, names=None):
+        clen = np.asarray(clen, dtype=np.int64)
+        n = len(clen)
+        names = names if names is not None else ["ctg%d" % i for i in range(n)]
+        return cls(names, clen, np.arange(n + 1, dtype=np.int32), np.zeros(n, dtype=np.int64))
+
+    def c_names(self):
+        arr = (C.c_char_p * max(1, len(self.names)))(*self.names)
+        return arr
+
+
+_PROG = b"distributedpanga_b200"
+_VERSION = b"0.1"
+
+
+def write_1aln(path, recs, toff, trace, contig_len, skeleton=None, db_name="", cwd=None,
+               command="distributedpanga_b200", tspace=100):
+    """Writes alignments (as Device.alignments() returns them) as a .1aln file
+    (la_merge's output, src/fastga_pipeline.c:1616-1656)."""
+    L = load_library()
+    contig_len = np.ascontiguousarray(contig_len, dtype=np.int64)
+    sk = skeleton or Skeleton.per_contig(contig_len)
+    recs = np.ascontiguousarray(recs, dtype=np.int32)
+    toff = np.ascontiguousarray(toff, dtype=np.int64)
+    trace = np.ascontiguousarray(trace, dtype=np.uint8)
+    if trace.size == 0:
+        trace = np.zeros(1, dtype=np.uint8)
+    names = sk.c_names()
+    rc = L.pga_write_1aln(path.encode(), _PROG, _VERSION, command.encode(), db_name.encode(),
+                          cwd.encode() if cwd else None, int(tspace), len(sk.names), names,
+                          sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp), sk.sbeg.ctypes.data_as(vp),
+                          contig_len.ctypes.data_as(vp), int(len(recs)), recs.ctypes.data_as(vp),
+                          toff.ctypes.data_as(vp), trace.ctypes.data_as(vp))
+    if rc != 0:
+        raise PgaError("write_1aln(%s): status %d" % (path, rc))
 
 
 def alignment_lines(recs, toff, tr):

@@ -175,6 +175,31 @@ int pga_align_times(const pga_ctx *ctx, float *ms4);
  * Local_Alignment calls, [3] warp tasks.  No counterpart in the reference. */
 int pga_align_work(const pga_ctx *ctx, int64_t *work4);
 
+/* ---- the .1aln file ------------------------------------------------------------ */
+
+/* la_merge's output file (src/fastga_pipeline.c:1616-1656: open_Aln_Write,
+ * Write_Skeleton, Write_Aln_Overlap, Write_Aln_Trace; lib/alncode.c:239-305,
+ * lib/GDB.c:2059-2086), as an ASCII ONE file of type "aln" that ONE readers
+ * (open_Aln_Read, ALNtoPAF) read like the reference's binary one: header with
+ * provenance (program, version, command, date), references db_name (1) and
+ * cwd (3, may be NULL), the trace spacing, the GDB skeleton (per scaffold
+ * its name, then G gap / C contig lengths; contigs of scaffold s are
+ * [scaff_fctg[s], scaff_fctg[s+1]), at contig_sbeg within the scaffold), then
+ * the alignments as pga_align_copy gives them: recs9 (aread abpos aepos
+ * bread bbpos bepos comp diffs tlen), trace_off, trace.  Host only. */
+int pga_write_1aln(const char *path, const char *program, const char *version, const char *command,
+                   const char *db_name, const char *cwd, int tspace, int nscaff, const char *const *scaff_name,
+                   const int64_t *scaff_len, const int32_t *scaff_fctg, const int64_t *contig_sbeg,
+                   const int64_t *contig_len, int64_t nalign, const int32_t *recs9, const int64_t *trace_off,
+                   const uint8_t *trace);
+
+/* The same for the alignments of the last pga_align, with the loaded
+ * contigs' lengths. */
+int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, const char *version,
+                         const char *command, const char *db_name, const char *cwd, int nscaff,
+                         const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
+                         const int64_t *contig_sbeg);
+
 /* ---- seed diagonal sort without device allocation ---------------------------- */
 
 /* No counterpart in the reference: the reference runs on the host and never

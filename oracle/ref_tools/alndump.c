@@ -1,14 +1,16 @@
-/* alndump <file.1aln>
+/* alndump [-s] <file.1aln>
  *
  * Prints the alignment record stream of a .1aln file, one alignment per line:
  *   aread abpos aepos bread bbpos bepos comp diffs ; T b-deltas ; X diffs
  * read with the reference's own reader (open_Aln_Read / Read_Aln_Overlap /
- * Read_Aln_Trace, lib/alncode.c:59-190).  The provenance, references and GDB
- * skeleton (which carry a timestamp and paths) are not printed.  Compiled
- * only into oracle/_ref.  Test infrastructure.
+ * Read_Aln_Trace, lib/alncode.c:59-190).  The provenance and references
+ * (which carry a timestamp and paths) are not printed; with -s the GDB
+ * skeleton is, first, one line per S (scaffold name), G (gap) and C (contig
+ * length) record.  Compiled only into oracle/_ref.  Test infrastructure.
  */
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 #include "GDB.h"
 #include "align.h"
 #include "alncode.h"
@@ -23,14 +25,29 @@ int main(int argc, char *argv[])
 
   Prog_Name    = "alndump";
   Command_Line = "alndump";
+  int skel = 0;
+  if (argc == 3 && strcmp(argv[1], "-s") == 0)
+    { skel = 1;
+      argv += 1;
+      argc -= 1;
+    }
   if (argc != 2)
-    { fprintf(stderr, "usage: alndump <file.1aln>\n");
+    { fprintf(stderr, "usage: alndump [-s] <file.1aln>\n");
       return 1;
     }
   of = open_Aln_Read(argv[1], 1, &novl, &tspace, &db1, &db2, &cpath);
   if (of == NULL)
     { fprintf(stderr, "alndump: cannot open %s\n", argv[1]);
       return 1;
+    }
+  if (skel)
+    { while (of->lineType != 'A')          /* print the GDB skeleton */
+        { if (of->lineType == 'S')
+            printf("S %.*s\n", (int) oneLen(of), oneString(of));
+          else if (of->lineType == 'G' || of->lineType == 'C')
+            printf("%c %lld\n", of->lineType, (long long) oneInt(of, 0));
+          if (!oneReadLine(of)) break;
+        }
     }
   while (of->lineType == 'g')              /* skip the GDB skeleton */
     { Skip_Skeleton(of);

@@ -178,3 +178,30 @@ def test_alignments_independent_of_band_ranges(dev, case):
     assert len(got[-1]) == dig["aln"]["count"]
     assert got[1] == got[-1]
     assert got[64] == got[-1]
+
+
+@pytest.mark.parametrize("case", ["small_s002", "edge_mix"])
+def test_1aln_file_matches_reference(dev, case):
+    """The GPU path's .1aln file, read by the reference's own reader, is the
+    reference's record stream."""
+    import gzip
+    import os
+    import subprocess
+    import tempfile
+    from conftest import GOLDEN, ROOT
+    alndump = os.path.join(ROOT, "oracle", "_ref", "alndump")
+    if not os.path.exists(alndump):
+        pytest.skip("oracle/_ref not built")
+    cs, dig = load_case(case)
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=False)
+    dev.merge(dig["freq_cutoff"])
+    dev.align()
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "out.1aln")
+        dev.write_1aln(p, db_name="g.1gdb", cwd=d)
+        out = subprocess.run([alndump, p], check=True, capture_output=True, text=True).stdout
+    mine = [" ".join(l.split()) for l in out.split("\n") if l.strip() and not l.startswith("#")]
+    ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n")
+           if l.strip()]
+    assert mine == ref
