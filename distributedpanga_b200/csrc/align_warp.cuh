@@ -305,6 +305,81 @@ __device__ __forceinline__ void lane_snakes(const Seq &A, const Seq &B, int nact
   }
 }
 
+// 32 bases of a packed sequence from a 2-bit shift sh (0..62) into words
+// (w0, w1): w0 << sh with w1's top bits shifted in, no branch on sh == 0.
+__device__ __forceinline__ uint64_t join32(uint64_t w0, uint64_t w1, int sh) {
+  return (w0 << sh) | ((w1 >> 1) >> (63 - sh));
+}
+
+// The snake of one diagonal (the one-diagonal-per-lane case of
+// lane_snakes): the same stops and sentinel hits, 64 bases per round from
+// three words of each packed sequence loaded together.  The third word may
+// lie past this sequence's copy (its bases are beyond mx and never count);
+// the packed buffer has spare words at its end.
+template <bool FWD>
+__device__ __forceinline__ void snake1(const Seq &A, const Seq &B, bool act, int k, int &x, int &run, int &hb,
+                                       int &hA) {
+  hb = hA = 0;
+  run = 0;
+  if (!act) return;
+  const int y = x - k;
+  int oa, ob, mx;
+  const uint64_t *pa, *pb;
+  if (FWD) {
+    if (y < 0 || y > B.len) {
+      hb = 1;
+      return;
+    }
+    if (x < 0 || x > A.len) {
+      hA = 1;
+      return;
+    }
+    const int ra = A.len - x, rb = B.len - y;
+    mx = ra < rb ? ra : rb;
+    oa = x;
+    ob = y;
+    pa = A.pf;
+    pb = B.pf;
+  } else {
+    if (y <= 0 || y >= B.len + 1) {
+      hb = 1;
+      return;
+    }
+    if (x <= 0 || x > A.len) {
+      hA = 1;
+      return;
+    }
+    mx = x < y ? x : y;
+    oa = A.len - x;
+    ob = B.len - y;
+    pa = A.pr;
+    pb = B.pr;
+  }
+  int t = 0;
+  while (t < mx) {
+    const int qa = oa + t, qb = ob + t;
+    const uint64_t *ua = pa + (qa >> 5), *ub = pb + (qb >> 5);
+    const int sa = (qa & 31) << 1, sb = (qb & 31) << 1;
+    const uint64_t a0 = ua[0], a1 = ua[1], a2 = ua[2], b0 = ub[0], b1 = ub[1], b2 = ub[2];
+    const uint64_t d0 = join32(a0, a1, sa) ^ join32(b0, b1, sb);
+    const uint64_t d1 = join32(a1, a2, sa) ^ join32(b1, b2, sb);
+    const int lead = d0 ? (__clzll(d0) >> 1) : 32 + (d1 ? (__clzll(d1) >> 1) : 32);
+    const int chunk = mx - t < 64 ? mx - t : 64;
+    if (lead < chunk) {
+      t += lead;
+      break;
+    }
+    t += chunk;
+  }
+  if (t == mx) {
+    const int ra = FWD ? A.len - x : x, rb = FWD ? B.len - y : y;
+    if (rb <= ra) hb = 1;
+    else hA = 1;
+  }
+  x = FWD ? x + t : x - t;
+  run = t;
+}
+
 // v[j] for a per-lane index j < J, without local memory
 template <int J>
 __device__ __forceinline__ int pick(const int *v, int j) {
@@ -613,6 +688,38 @@ struct RegWave {
   uint64_t T;
 };
 
+// What a register wave needs of WarpWork, held in the wave loop's registers
+// (WarpWork itself lives in addressable memory).
+struct RegCtx {
+  int vmask;
+  int *NA;
+  Pebble *cells;
+  unsigned long long *pool_next;
+  int64_t pool_cap;
+  int64_t chunk_next, chunk_end;  // the warp's current pebble chunk
+  int err;
+};
+
+// warp_pebbles on a RegCtx.
+__device__ __forceinline__ int64_t reg_pebbles(RegCtx &X, int cnt) {
+  if (cnt == 0) return 0;
+  if (X.chunk_next + cnt > X.chunk_end) {
+    int64_t want = cnt > PEBBLE_CHUNK ? cnt : PEBBLE_CHUNK;
+    unsigned long long base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(X.pool_next, (unsigned long long)want);
+    base = __shfl_sync(FULL, base, 0);
+    if ((int64_t)base + want > X.pool_cap) {
+      X.err |= ALN_ERR_CELLS;
+      return -1;
+    }
+    X.chunk_next = (int64_t)base;
+    X.chunk_end = (int64_t)base + want;
+  }
+  int64_t s = X.chunk_next;
+  X.chunk_next += cnt;
+  return s;
+}
+
 // Visit position of lane l's diagonal (forward: hgh first, reverse: low first).
 template <bool FWD>
 __device__ __forceinline__ int reg_pos(int l, int low, int hgh) {
@@ -662,12 +769,12 @@ __device__ __forceinline__ void reg_store(WarpWork &W, int cur, int plow, int ph
 // wave [plow, phgh] (not empty, inside [low-1, hgh+1]).  Same results as
 // wave_sweep; fills WS for wave_prune.
 template <bool FWD>
-__device__ __forceinline__ int reg_wave(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
+__device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
                                         int hgh, int plow, int phgh, int dif, RegWave &R, int &besta, int &bestx,
                                         int &lasta, int &trima, int &trimx, int &trimd, int &trimha, int &more,
                                         int &aclip, int &bclip, WaveSlice &WS) {
   const int lane = threadIdx.x & 31;
-  const int vmask = W.vcap - 1;
+  const int vmask = X.vmask;
   const int tspace = spec.trace_space;
   const int BV = FWD ? -1 : I32MAX;
   const int k = low + ((lane - low) & 31);
@@ -701,9 +808,8 @@ __device__ __forceinline__ int reg_wave(WarpWork &W, const AlignSpec &spec, cons
   if ((b & PATH_TOP) != 0) m -= 1;
   b <<= 1;
   int x = (c + k) >> 1;
-  int kk[1] = {k}, xx[1] = {x}, run[1], hb[1], hA[1];
-  lane_snakes<FWD, 1>(A, B, act ? 1 : 0, kk, xx, run, hb, hA);
-  x = xx[0];
+  int run[1], hb[1], hA[1];
+  snake1<FWD>(A, B, act, k, x, run[0], hb[0], hA[0]);
   int npb = 0;
   if (act) {
     history_run(b, m, run[0]);
@@ -746,11 +852,11 @@ __device__ __forceinline__ int reg_wave(WarpWork &W, const AlignSpec &spec, cons
     off = xsum - npb;
     tot = __reduce_add_sync(FULL, npb);
   }
-  int64_t pb0 = warp_pebbles(W, tot);
+  int64_t pb0 = reg_pebbles(X, tot);
   if (pb0 < 0) return 1;
   if (act) {
     int64_t s = pb0 + off;
-    Pebble *cells = W.pool.cells;
+    Pebble *cells = X.cells;
     if (FWD) {
       while (x >= nak) {
         if (hm < nak) {
@@ -772,7 +878,7 @@ __device__ __forceinline__ int reg_wave(WarpWork &W, const AlignSpec &spec, cons
         nak -= tspace;
       }
     }
-    W.NA[k & vmask] = nak;
+    X.NA[k & vmask] = nak;
     R.V = c;
     R.M = m;
     R.T = b;
@@ -861,24 +967,38 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
   R.M = R.HA = R.HM = R.NA = 0;
   R.T = 0;
   bool regmode = false;
+  RegCtx X{vmask, W.NA, W.pool.cells, W.pool.next, W.pool.cap, W.chunk_next, W.chunk_end, 0};
+  int64_t nwaves = 0, ncells = 0;
+  // back to WarpWork: the pebble chunk, counts and errors
+  auto sync = [&]() {
+    W.chunk_next = X.chunk_next;
+    W.chunk_end = X.chunk_end;
+    W.err |= X.err;
+    W.waves += nwaves;
+    W.cells += ncells;
+    nwaves = ncells = 0;
+    X.err = 0;
+  };
   while (more && (FWD ? lasta >= besta - TRIM_MLAG : lasta <= besta + TRIM_MLAG)) {
     if (dif > max_waves) {
-      W.err |= ALN_ERR_VCAP;
+      X.err |= ALN_ERR_VCAP;
+      sync();
       return 1;
     }
     const int plow = low, phgh = hgh;
     low -= 1;
     hgh += 1;
-    if (hgh - low + 3 > W.vcap) {
-      W.err |= ALN_ERR_VCAP;
+    if (hgh - low + 3 > vmask + 1) {
+      X.err |= ALN_ERR_VCAP;
+      sync();
       return 1;
     }
     const bool grow_lo = low >= minp, grow_hi = hgh <= maxp;
     if (!grow_lo) low += 1;
     if (!grow_hi) hgh -= 1;
     const bool use_reg = phgh >= plow && hgh - low + 1 <= 32;
-    W.waves += 1;
-    W.cells += hgh >= low ? hgh - low + 1 : 0;
+    nwaves += 1;
+    ncells += hgh >= low ? hgh - low + 1 : 0;
     WaveSlice WS;
     if (use_reg) {
       if (!regmode) {
@@ -886,10 +1006,13 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
         regmode = true;
       }
       dif += 1;
-      if (reg_wave<FWD>(W, spec, A, B, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
-                        trimha, more, aclip, bclip, WS))
+      if (reg_wave<FWD>(X, spec, A, B, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
+                        trimha, more, aclip, bclip, WS)) {
+        sync();
         return 1;
+      }
     } else {
+      sync();
       if (regmode) {
         reg_store(W, cur, plow, phgh, R);
         regmode = false;
@@ -916,6 +1039,8 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
       if (wave_sweep<FWD>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
                           aclip, bclip, WS))
         return 1;
+      X.chunk_next = W.chunk_next;
+      X.chunk_end = W.chunk_end;
       cur ^= 1;
       __syncwarp();
     }
@@ -968,6 +1093,7 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
     }
     wave_prune<FWD>(W, W.V[cur], besta, low, hgh, WS);
   }
+  sync();
   __syncwarp();
   return 0;
 }
