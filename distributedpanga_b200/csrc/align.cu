@@ -207,16 +207,37 @@ __device__ OvlArena warp_arena(const AlignLaunch &P, int64_t wid) {
 }
 
 // First index >= x in [x, hi) whose band differs from its predecessor's
-// (x itself when x == 0), else hi; warp-wide.
+// (x itself when x == 0), else hi; warp-wide.  Bands never decrease within
+// a pair, so this is the first index whose band exceeds band(x-1): a search
+// that probes 32 points per step (ballot) and ends with one linear step of
+// 32, so a range that starts inside a long band does not walk its seeds.
 __device__ int64_t next_band_start(const KeySeeds &S, int64_t x, int64_t hi, int lane) {
   if (x <= 0) return 0;
-  for (int64_t base = x; base < hi; base += 32) {
-    int64_t i = base + lane;
-    bool f = i < hi && S.band(i) != S.band(i - 1);
-    unsigned m = __ballot_sync(FULL, f);
-    if (m) return base + __ffs(m) - 1;
+  if (x >= hi) return hi;
+  const int64_t b = S.band(x - 1);
+  int64_t lo = x, h = hi;  // the answer lies in [lo, h], h meaning none below h
+  while (h - lo > 32) {
+    const int64_t span = h - lo;
+    const int64_t p = lo + (span * (lane + 1)) / 33;  // increasing in lane, inside [lo, h)
+    const unsigned m = __ballot_sync(FULL, S.band(p) > b);
+    if (m) {
+      const int f = __ffs(m) - 1;
+      const int64_t pf = lo + (span * (f + 1)) / 33;
+      const int64_t before = f > 0 ? lo + (span * f) / 33 : lo - 1;  // last probe known not past b
+      lo = before + 1;
+      h = pf;  // band(pf) > b: the answer is at most pf
+      if (h - lo <= 32) {
+        const int64_t q = lo + lane;
+        const unsigned m2 = __ballot_sync(FULL, q < h && S.band(q) > b);
+        return m2 ? lo + __ffs(m2) - 1 : h;
+      }
+    } else {
+      lo = lo + (span * 32) / 33 + 1;
+    }
   }
-  return hi;
+  const int64_t q = lo + lane;
+  const unsigned m = __ballot_sync(FULL, q < h && S.band(q) > b);
+  return m ? lo + __ffs(m) - 1 : h;
 }
 
 // The sort / elimination step of a pair whose candidates are in O, then its

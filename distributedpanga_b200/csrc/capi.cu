@@ -956,10 +956,11 @@ int run_align(pga_ctx *ctx) {
   int64_t all_seeds = 0;
   for (int comp = 0; comp < 2; comp++)
     for (auto &t : pairs[comp]) all_seeds += t.hi - t.lo;
-  // about 32 tasks per warp
+  // about 160 tasks per warp: short enough that a long alignment's band
+  // blocks spread over warps, long enough to keep the per-task cost small
   const int64_t RS = ctx->range_seeds < 0    ? 0
                      : ctx->range_seeds > 0 ? ctx->range_seeds
-                                            : std::max<int64_t>(256, all_seeds / (32 * L.nwarps));
+                                            : std::max<int64_t>(256, all_seeds / (160 * L.nwarps));
   const int nself = (int)self_idx.size();
   std::vector<int64_t> x12(2 * (size_t)nself, 0);
   if (RS > 0 && nself > 0) {
