@@ -191,6 +191,58 @@ struct WarpAligner {
   __device__ int err() const { return W.err; }
 };
 
+__device__ AlignSpec launch_spec(const AlignLaunch &P) {
+  AlignSpec spec;
+  spec.trace_space = TSPACE;
+  spec.ave_path = P.ave_path;
+  spec.reach = 0;
+  spec.score = P.score;
+  spec.table = P.table;
+  return spec;
+}
+
+// Warp wid's wave buffers, trace points and pebble pool.
+__device__ WarpWork warp_work(const AlignLaunch &P, int64_t wid) {
+  WarpWork W;
+  int *wb = P.wave + wid * (int64_t)P.vcap * WAVE_INTS;
+  W.V[0] = wb;
+  W.V[1] = wb + P.vcap;
+  W.M[0] = wb + 2 * P.vcap;
+  W.M[1] = wb + 3 * P.vcap;
+  W.HA[0] = wb + 4 * P.vcap;
+  W.HA[1] = wb + 5 * P.vcap;
+  W.NA = wb + 6 * P.vcap;
+  W.HM[0] = wb + 7 * P.vcap;
+  W.HM[1] = wb + 8 * P.vcap;
+  W.T[0] = (uint64_t *)(wb + 9 * P.vcap);
+  W.T[1] = (uint64_t *)(wb + 11 * P.vcap);
+  W.vcap = P.vcap;
+  W.points = P.points + wid * P.point_cap;
+  W.point_cap = P.point_cap;
+  W.pool.cells = P.cells;
+  W.pool.next = P.cell_next;
+  W.pool.cap = P.cell_cap;
+  W.chunk_next = W.chunk_end = 0;
+  W.waves = W.cells = 0;
+  return W;
+}
+
+// Sequences of contig c as a Local_Alignment operand: A is complemented
+// when comp (the reverse-complement copies), B never.
+__device__ Seq contig_seq(const AlignLaunch &P, int c, bool as_a, bool comp) {
+  const uint8_t *buf = (as_a && comp) ? P.rc : P.fwd;
+  Seq S{buf + P.soff[c], (int)P.clen[c]};
+  const uint64_t *base = P.pk + P.poff[c] * 4;
+  if (as_a) {
+    S.pf = base + (comp ? 2 : 0) * P.pwords[c];
+    S.pr = base + (comp ? 3 : 1) * P.pwords[c];
+  } else {
+    S.pf = base;
+    S.pr = base + P.pwords[c];
+  }
+  return S;
+}
+
 __device__ OvlArena warp_arena(const AlignLaunch &P, int64_t wid) {
   OvlArena O;
   O.ovl = P.ovl + wid * P.ovl_cap;
@@ -312,34 +364,8 @@ k_align_pairs(AlignLaunch P) {
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
   if (wid >= P.nwarps) return;
-  AlignSpec spec;
-  spec.trace_space = TSPACE;
-  spec.ave_path = P.ave_path;
-  spec.reach = 0;
-  spec.score = P.score;
-  spec.table = P.table;
-
-  WarpWork W;
-  int *wb = P.wave + wid * (int64_t)P.vcap * WAVE_INTS;
-  W.V[0] = wb;
-  W.V[1] = wb + P.vcap;
-  W.M[0] = wb + 2 * P.vcap;
-  W.M[1] = wb + 3 * P.vcap;
-  W.HA[0] = wb + 4 * P.vcap;
-  W.HA[1] = wb + 5 * P.vcap;
-  W.NA = wb + 6 * P.vcap;
-  W.HM[0] = wb + 7 * P.vcap;
-  W.HM[1] = wb + 8 * P.vcap;
-  W.T[0] = (uint64_t *)(wb + 9 * P.vcap);
-  W.T[1] = (uint64_t *)(wb + 11 * P.vcap);
-  W.vcap = P.vcap;
-  W.points = P.points + wid * P.point_cap;
-  W.point_cap = P.point_cap;
-  W.pool.cells = P.cells;
-  W.pool.next = P.cell_next;
-  W.pool.cap = P.cell_cap;
-  W.chunk_next = W.chunk_end = 0;
-  W.waves = W.cells = 0;
+  const AlignSpec spec = launch_spec(P);
+  WarpWork W = warp_work(P, wid);
 
   OvlArena O = warp_arena(P, wid);
 
@@ -353,13 +379,8 @@ k_align_pairs(AlignLaunch P) {
     O.err = 0;
     const SeedKeyLayout &L = tk.comp ? P.layC : P.layN;
     KeySeeds S{(tk.comp ? P.keysC : P.keysN) + tk.lo, tk.hi - tk.lo, L, s_block[threadIdx.x >> 5]};
-    const uint8_t *abuf = tk.comp ? P.rc : P.fwd;
-    Seq A{abuf + P.soff[tk.a], (int)P.clen[tk.a]};
-    Seq B{P.fwd + P.soff[tk.b], (int)P.clen[tk.b]};
-    A.pf = P.pk + P.poff[tk.a] * 4 + (tk.comp ? 2 : 0) * P.pwords[tk.a];
-    A.pr = P.pk + P.poff[tk.a] * 4 + (tk.comp ? 3 : 1) * P.pwords[tk.a];
-    B.pf = P.pk + P.poff[tk.b] * 4;
-    B.pr = P.pk + P.poff[tk.b] * 4 + P.pwords[tk.b];
+    const Seq A = contig_seq(P, tk.a, true, tk.comp != 0);
+    const Seq B = contig_seq(P, tk.b, false, false);
     long long t0 = clock64();
     Path path;
     path.tlen = path.diffs = path.abpos = path.bbpos = path.aepos = 0;
@@ -448,6 +469,62 @@ k_finish_pairs(AlignLaunch P) {
     if (lane == 0) P.pout[t] = po;
     __syncwarp();
   }
+}
+
+// Local_Alignment on request lists (pga_local_alignment): warps take
+// requests in turn (a b comp low hgh anti lbord hbord); each writes its path
+// (abpos aepos bbpos bepos diffs tlen status) and copies its tlen uint16
+// trace values into a shared pool.
+__global__ void __launch_bounds__(ALIGN_THREADS)
+k_local_batch(AlignLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
+  if (wid >= P.nwarps) return;
+  const AlignSpec spec = launch_spec(P);
+  WarpWork W = warp_work(P, wid);
+  while (true) {
+    unsigned long long r = 0;
+    if (lane == 0) r = atomicAdd(P.lreq_next, 1ull);
+    r = __shfl_sync(FULL, r, 0);
+    if ((int64_t)r >= P.nlreq) break;
+    const int32_t *q = P.lreq + 8 * r;
+    const bool comp = q[2] != 0;
+    const Seq A = contig_seq(P, q[0], true, comp);
+    const Seq B = contig_seq(P, q[1], false, false);
+    W.err = 0;
+    Path path;
+    path.tlen = path.diffs = path.abpos = path.bbpos = path.aepos = path.bepos = 0;
+    path.trace_off = 0;
+    int status = local_alignment_w(W, spec, A, B, comp, path, q[3], q[4], q[5], q[6], q[7]) ? (W.err | 0x100) : 0;
+    int64_t off = -1;
+    if (status == 0 && path.tlen > 0) {
+      unsigned long long o = 0;
+      if (lane == 0) o = atomicAdd(P.ltrace_next, (unsigned long long)path.tlen);
+      o = __shfl_sync(FULL, o, 0);
+      if ((int64_t)o + path.tlen > P.ltrace_cap) {
+        status = ALN_ERR_TRACE | 0x200;
+      } else {
+        off = (int64_t)o;
+        for (int k = lane; k < path.tlen; k += 32) P.ltrace[off + k] = W.points[path.trace_off + k];
+      }
+    }
+    if (lane == 0) {
+      int32_t *o7 = P.lpath + 7 * r;
+      o7[0] = path.abpos;
+      o7[1] = path.aepos;
+      o7[2] = path.bbpos;
+      o7[3] = path.bepos;
+      o7[4] = path.diffs;
+      o7[5] = status ? 0 : path.tlen;
+      o7[6] = status;
+      P.ltoff[r] = off;
+    }
+    __syncwarp();
+  }
+}
+
+void launch_local_batch(const AlignLaunch &P, int grid, cudaStream_t st) {
+  k_local_batch<<<grid, ALIGN_THREADS, 0, st>>>(P);
 }
 
 // NUMERIC copies of every contig, each between sentinel bytes (value 4):

@@ -72,6 +72,14 @@ struct AlignLaunch {
   unsigned long long *rng_next;
   int64_t rng_cap;
   PairOut *rout;                     // per range number
+  const int32_t *lreq;               // k_local_batch: 8 ints per request
+  int64_t nlreq;
+  unsigned long long *lreq_next;
+  int32_t *lpath;                    // 7 ints per request
+  int64_t *ltoff;                    // trace offset per request (-1: none)
+  uint16_t *ltrace;
+  unsigned long long *ltrace_next;
+  int64_t ltrace_cap;
   const FinishTask *ftasks;          // k_finish_pairs
   int nftasks;
   const int *range_idx;
@@ -89,6 +97,7 @@ struct AlignLaunch {
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);
+void launch_local_batch(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_self_bounds(const U128 *keys, SeedKeyLayout L, const int64_t *lohi, int npair, int64_t cd_lo,
                         int64_t cd_hi, int64_t *x12, cudaStream_t st);
 void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *boff, int ncontig,

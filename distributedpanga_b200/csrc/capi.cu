@@ -86,6 +86,12 @@ struct pga_ctx {
   int64_t align_stats[8] = {0};    // pga_align_stats
   float align_ms[4] = {0};         // pga_align_times
   int64_t align_work[4] = {0};     // pga_align_work
+  // pga_local_alignment: requests, paths, trace pool
+  DBuf lreq, lpath, ltoff, ltrace, lnext;
+  std::vector<int32_t> h_lpath;    // 7 ints per request
+  std::vector<int64_t> h_ltoff;    // trace offsets in request order (n + 1)
+  std::vector<uint16_t> h_ltrace;
+  bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
@@ -763,23 +769,10 @@ void combine_ranges(const std::vector<PairOut> &rout_h, const std::vector<int> &
   }
 }
 
-double now_ms() {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
-int run_align(pga_ctx *ctx) {
-  const double t_start = now_ms();
+// NUMERIC (with sentinels) and 2-bit packed copies of every contig, the base
+// frequencies if not given, and the scoring tables (New_Align_Spec).
+int prepare_sequences(pga_ctx *ctx, int *ave_path) {
   const int nc = ctx->ncontig;
-  int64_t maxctg = ctx->maxctg;
-  // 1. the two units must be diagonal-sorted
-  for (int comp = 0; comp < 2; comp++)
-    if (!ctx->have_diag[comp]) {
-      int64_t cnt;
-      int sw;
-      int r = pga_diag_sort(ctx, comp, &sw, &cnt);
-      if (r) return r;
-    }
-  // 2. NUMERIC sequences and base frequencies
   if (!ctx->have_numeric) {
     std::vector<int64_t> so(nc + 1);
     int64_t o = 1;
@@ -825,10 +818,100 @@ int run_align(pga_ctx *ctx) {
     ctx->have_numeric = true;
   }
   std::vector<int16_t> tab(2 * 32768);
-  int ave_path = aln::build_align_spec(ctx->base_freq, tab.data(), tab.data() + 32768);
+  *ave_path = aln::build_align_spec(ctx->base_freq, tab.data(), tab.data() + 32768);
   ENSURE(ctx->spec_tab, sizeof(int16_t) * tab.size());
   CK(cudaMemcpyAsync(ctx->spec_tab.p, tab.data(), sizeof(int16_t) * tab.size(), cudaMemcpyHostToDevice, ctx->st));
 
+  return PGA_OK;
+}
+
+// The aligner's launch description and work spaces (pools sized from the
+// input; align_launch grows one that overflows).
+int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
+  memset(&L, 0, sizeof(L));
+  L.keysN = ctx->sorted[0];
+  L.keysC = ctx->sorted[1];
+  L.layN = ctx->lay[0];
+  L.layC = ctx->lay[1];
+  L.fwd = P<uint8_t>(ctx->numf);
+  L.rc = P<uint8_t>(ctx->numr);
+  L.soff = P<int64_t>(ctx->soff);
+  L.clen = P<int64_t>(ctx->dclen);
+  L.pk = P<uint64_t>(ctx->pk);
+  L.poff = P<int64_t>(ctx->poff);
+  L.pwords = P<int64_t>(ctx->pwords);
+  L.score = P<int16_t>(ctx->spec_tab);
+  L.table = P<int16_t>(ctx->spec_tab) + 32768;
+  L.ave_path = ave_path;
+  L.amxpos = ctx->maxctg;
+  L.maxdag = 2 * ctx->maxctg;
+  L.nwarps = 148 * 16;
+  L.vcap = 8192;
+  L.point_cap = 4 * (ctx->maxctg / 100 + 4) + 64;
+  // Pools sized from the sequence total; align_run_tasks grows one that
+  // overflows and reruns the launch.  Buffers keep their size across calls.
+  int64_t seqtot = 0;
+  for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
+  ENSURE(ctx->task_next, 64);
+  ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
+  ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
+  ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * 16384);
+  ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * 16384);
+  ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)std::max<int64_t>(1 << 18, seqtot / 256));
+  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)std::max<int64_t>(1 << 24, 4 * seqtot));
+  ENSURE(ctx->cand, (size_t)std::max<int64_t>(64 << 20, 2 * seqtot));
+  ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)std::max<int64_t>(1 << 20, seqtot / 256));
+  ENSURE(ctx->outb, (size_t)std::max<int64_t>(64 << 20, seqtot / 8));
+  L.ovl_cap = (int64_t)(ctx->ovl.cap / (sizeof(aln::Ovl) * L.nwarps));
+  L.rng_cap = (int64_t)(ctx->rng_ovl.cap / sizeof(aln::Ovl));
+  L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
+  L.cand_cap = (int64_t)ctx->cand.cap;
+  L.rec_cap = (int64_t)(ctx->recs.cap / sizeof(AlnRec));
+  L.out_cap = (int64_t)ctx->outb.cap;
+  ENSURE(ctx->rng_next, 64);
+  ENSURE(ctx->cell_next, 64);
+  ENSURE(ctx->cand_next, 64);
+  ENSURE(ctx->rec_next, 64);
+  ENSURE(ctx->out_next, 64);
+  L.next_task = P<unsigned>(ctx->task_next);
+  L.wave = P<int>(ctx->wave);
+  L.points = P<uint16_t>(ctx->points);
+  L.ovl = P<aln::Ovl>(ctx->ovl);
+  L.perm = P<int>(ctx->perm);
+  L.cells = P<aln::Pebble>(ctx->cells);
+  L.cell_next = P<unsigned long long>(ctx->cell_next);
+  L.cand_bytes = P<uint8_t>(ctx->cand);
+  L.cand_next = P<unsigned long long>(ctx->cand_next);
+  L.recs = P<AlnRec>(ctx->recs);
+  L.rec_next = P<unsigned long long>(ctx->rec_next);
+  L.out_bytes = P<uint8_t>(ctx->outb);
+  L.out_next = P<unsigned long long>(ctx->out_next);
+  L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
+  L.rng_next = P<unsigned long long>(ctx->rng_next);
+
+  return PGA_OK;
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int run_align(pga_ctx *ctx) {
+  const double t_start = now_ms();
+  const int nc = ctx->ncontig;
+  int64_t maxctg = ctx->maxctg;
+  // 1. the two units must be diagonal-sorted
+  for (int comp = 0; comp < 2; comp++)
+    if (!ctx->have_diag[comp]) {
+      int64_t cnt;
+      int sw;
+      int r = pga_diag_sort(ctx, comp, &sw, &cnt);
+      if (r) return r;
+    }
+  // 2. NUMERIC and packed sequences, base frequencies, scoring tables
+  int ave_path = 0;
+  int r0 = prepare_sequences(ctx, &ave_path);
+  if (r0) return r0;
   // 3. pair lists of both units
   std::vector<PairTask> pairs[2];
   for (int comp = 0; comp < 2; comp++) {
@@ -874,68 +957,10 @@ int run_align(pga_ctx *ctx) {
 
   // 4. work spaces
   AlignLaunch L;
-  memset(&L, 0, sizeof(L));
-  L.keysN = ctx->sorted[0];
-  L.keysC = ctx->sorted[1];
-  L.layN = ctx->lay[0];
-  L.layC = ctx->lay[1];
-  L.fwd = P<uint8_t>(ctx->numf);
-  L.rc = P<uint8_t>(ctx->numr);
-  L.soff = P<int64_t>(ctx->soff);
-  L.clen = P<int64_t>(ctx->dclen);
-  L.pk = P<uint64_t>(ctx->pk);
-  L.poff = P<int64_t>(ctx->poff);
-  L.pwords = P<int64_t>(ctx->pwords);
-  L.score = P<int16_t>(ctx->spec_tab);
-  L.table = P<int16_t>(ctx->spec_tab) + 32768;
-  L.ave_path = ave_path;
-  L.amxpos = maxctg;
-  L.maxdag = 2 * maxctg;
-  L.nwarps = 148 * 16;
-  L.vcap = 8192;
-  L.point_cap = 4 * (maxctg / 100 + 4) + 64;
-  // Pools sized from the sequence total; align_run_tasks grows one that
-  // overflows and reruns the launch.  Buffers keep their size across calls.
-  int64_t seqtot = 0;
-  for (int c = 0; c < nc; c++) seqtot += ctx->clen[c];
-  ENSURE(ctx->task_next, 64);
-  ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
-  ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
-  ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * 16384);
-  ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * 16384);
-  ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)std::max<int64_t>(1 << 18, seqtot / 256));
-  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)std::max<int64_t>(1 << 24, 4 * seqtot));
-  ENSURE(ctx->cand, (size_t)std::max<int64_t>(64 << 20, 2 * seqtot));
-  ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)std::max<int64_t>(1 << 20, seqtot / 256));
-  ENSURE(ctx->outb, (size_t)std::max<int64_t>(64 << 20, seqtot / 8));
-  L.ovl_cap = (int64_t)(ctx->ovl.cap / (sizeof(aln::Ovl) * L.nwarps));
-  L.rng_cap = (int64_t)(ctx->rng_ovl.cap / sizeof(aln::Ovl));
-  L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
-  L.cand_cap = (int64_t)ctx->cand.cap;
-  L.rec_cap = (int64_t)(ctx->recs.cap / sizeof(AlnRec));
-  L.out_cap = (int64_t)ctx->outb.cap;
-  ENSURE(ctx->rng_next, 64);
-  ENSURE(ctx->cell_next, 64);
-  ENSURE(ctx->cand_next, 64);
-  ENSURE(ctx->rec_next, 64);
-  ENSURE(ctx->out_next, 64);
+  r0 = prepare_workspace(ctx, L, ave_path);
+  if (r0) return r0;
   ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
   for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
-  L.next_task = P<unsigned>(ctx->task_next);
-  L.wave = P<int>(ctx->wave);
-  L.points = P<uint16_t>(ctx->points);
-  L.ovl = P<aln::Ovl>(ctx->ovl);
-  L.perm = P<int>(ctx->perm);
-  L.cells = P<aln::Pebble>(ctx->cells);
-  L.cell_next = P<unsigned long long>(ctx->cell_next);
-  L.cand_bytes = P<uint8_t>(ctx->cand);
-  L.cand_next = P<unsigned long long>(ctx->cand_next);
-  L.recs = P<AlnRec>(ctx->recs);
-  L.rec_next = P<unsigned long long>(ctx->rec_next);
-  L.out_bytes = P<uint8_t>(ctx->outb);
-  L.out_next = P<unsigned long long>(ctx->out_next);
-  L.rng_ovl = P<aln::Ovl>(ctx->rng_ovl);
-  L.rng_next = P<unsigned long long>(ctx->rng_next);
 
   // 5. Plan.  Pairs of two different contigs (all C pairs, every N pair of
   // two contigs) run in the first launch, large ones as band ranges finished
@@ -1310,7 +1335,8 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
-                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb};
+                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb, &ctx->lreq, &ctx->lpath, &ctx->ltoff,
+                   &ctx->ltrace, &ctx->lnext};
   for (DBuf *b : abufs)
     if (b->p) cudaFree(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
@@ -1812,6 +1838,106 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
   }
   if (trace_off) memcpy(trace_off, ctx->h_toff.data(), sizeof(int64_t) * (n + 1));
   if (trace && !ctx->h_trace.empty()) memcpy(trace, ctx->h_trace.data(), ctx->h_trace.size());
+  return PGA_OK;
+}
+
+int pga_local_alignment(pga_ctx *ctx, int64_t n, const int32_t *req8, int64_t *ntrace) {
+  if (!ctx || !ctx->have_gdb || n < 0 || (n > 0 && !req8)) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  ctx->have_local = false;
+  for (int64_t i = 0; i < n; i++) {
+    const int32_t *q = req8 + 8 * i;
+    if (q[0] < 0 || q[0] >= ctx->ncontig || q[1] < 0 || q[1] >= ctx->ncontig || (q[2] != 0 && q[2] != 1))
+      return fail(ctx, PGA_ERR_ARG, "request %lld: contigs or orientation out of range", (long long)i);
+    const int64_t alen = ctx->clen[q[0]], blen = ctx->clen[q[1]];
+    // the band's start points ((anti+k)/2, (anti-k)/2) must lie in the contigs
+    bool in = q[3] <= q[4] && q[4] - q[3] <= 8000;
+    for (int e = 3; e <= 4 && in; e++) {
+      const int64_t x = ((int64_t)q[5] + q[e]) >> 1, y = x - q[e];
+      in = x >= 0 && x <= alen && y >= 0 && y <= blen;
+    }
+    if (!in)
+      return fail(ctx, PGA_ERR_ARG, "request %lld: band [%d,%d] at antidiagonal %d starts outside the contigs",
+                  (long long)i, q[3], q[4], q[5]);
+  }
+  int ave_path = 0;
+  int r = prepare_sequences(ctx, &ave_path);
+  if (r) return r;
+  AlignLaunch L;
+  r = prepare_workspace(ctx, L, ave_path);
+  if (r) return r;
+  ENSURE(ctx->lreq, sizeof(int32_t) * 8 * (size_t)(n + 1));
+  ENSURE(ctx->lpath, sizeof(int32_t) * 7 * (size_t)(n + 1));
+  ENSURE(ctx->ltoff, sizeof(int64_t) * (size_t)(n + 1));
+  ENSURE(ctx->lnext, 64);
+  int64_t tcap = 0;  // trace values: at most 2 per 100 A-bases + 4 per request
+  for (int64_t i = 0; i < n; i++) tcap += 2 * (ctx->clen[req8[8 * i]] / 100 + 2);
+  ENSURE(ctx->ltrace, sizeof(uint16_t) * (size_t)(tcap + 1));
+  if (n > 0)
+    CK(cudaMemcpyAsync(ctx->lreq.p, req8, sizeof(int32_t) * 8 * n, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(ctx->lnext.p, 0, 16, ctx->st));
+  CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
+  L.lreq = P<int32_t>(ctx->lreq);
+  L.nlreq = n;
+  L.lreq_next = P<unsigned long long>(ctx->lnext);
+  L.lpath = P<int32_t>(ctx->lpath);
+  L.ltoff = P<int64_t>(ctx->ltoff);
+  L.ltrace = P<uint16_t>(ctx->ltrace);
+  L.ltrace_next = P<unsigned long long>(ctx->lnext) + 1;
+  L.ltrace_cap = tcap;
+  std::vector<int32_t> path(7 * (size_t)n);
+  std::vector<int64_t> toff(n);
+  for (int attempt = 0;; attempt++) {
+    if (n > 0) {
+      const int grid = (int)((L.nwarps * 32 + ALIGN_THREADS - 1) / ALIGN_THREADS);
+      launch_local_batch(L, grid, ctx->st);
+      LAUNCHED(1);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(path.data(), ctx->lpath.p, sizeof(int32_t) * 7 * n, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(toff.data(), ctx->ltoff.p, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    int cells_full = 0;
+    for (int64_t i = 0; i < n; i++)
+      if (path[7 * i + 6] & aln::ALN_ERR_CELLS) cells_full = 1;
+    const size_t max_cells = sizeof(aln::Pebble) * (size_t)0x7fffffff;
+    if (!cells_full || attempt >= 6 || ctx->cells.cap >= max_cells) break;
+    // grow the pebble pool and run again
+    r = ensure(ctx, ctx->cells, std::min(2 * ctx->cells.cap, max_cells));
+    if (r) return r;
+    L.cell_cap = (int64_t)(ctx->cells.cap / sizeof(aln::Pebble));
+    L.cells = P<aln::Pebble>(ctx->cells);
+    CK(cudaMemsetAsync(ctx->lnext.p, 0, 16, ctx->st));
+    CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
+  }
+  // traces in request order
+  ctx->h_lpath = path;
+  ctx->h_ltoff.assign(n + 1, 0);
+  int64_t tot = 0;
+  for (int64_t i = 0; i < n; i++) {
+    ctx->h_ltoff[i] = tot;
+    tot += path[7 * i + 5];
+  }
+  ctx->h_ltoff[n] = tot;
+  std::vector<uint16_t> pool(tcap + 1);
+  if (tcap > 0)
+    CK(cudaMemcpyAsync(pool.data(), ctx->ltrace.p, sizeof(uint16_t) * tcap, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->h_ltrace.assign(tot, 0);
+  for (int64_t i = 0; i < n; i++)
+    if (path[7 * i + 5] > 0)
+      memcpy(ctx->h_ltrace.data() + ctx->h_ltoff[i], pool.data() + toff[i], sizeof(uint16_t) * path[7 * i + 5]);
+  ctx->have_local = true;
+  if (ntrace) *ntrace = tot;
+  return PGA_OK;
+}
+
+int pga_local_alignment_copy(pga_ctx *ctx, int32_t *path7, int64_t *trace_off, uint16_t *trace) {
+  if (!ctx || !ctx->have_local) return PGA_ERR_ARG;
+  const size_t n = ctx->h_ltoff.size() - 1;
+  if (path7 && n) memcpy(path7, ctx->h_lpath.data(), sizeof(int32_t) * 7 * n);
+  if (trace_off) memcpy(trace_off, ctx->h_ltoff.data(), sizeof(int64_t) * (n + 1));
+  if (trace && !ctx->h_ltrace.empty()) memcpy(trace, ctx->h_ltrace.data(), sizeof(uint16_t) * ctx->h_ltrace.size());
   return PGA_OK;
 }
 

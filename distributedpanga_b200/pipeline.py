@@ -70,6 +70,8 @@ _SIGS = {
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
+    "pga_local_alignment": (C.c_int, [vp, C.c_int64, vp, C.POINTER(C.c_int64)]),
+    "pga_local_alignment_copy": (C.c_int, [vp, vp, vp, vp]),
     "pga_write_1aln": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                  C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
     "pga_align_write_1aln": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
@@ -304,6 +306,23 @@ class Device:
                                              db_name.encode(), cwd.encode() if cwd else None, len(sk.names), names,
                                              sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp),
                                              sk.sbeg.ctypes.data_as(vp)), "align_write_1aln")
+
+    def local_alignment(self, requests):
+        """Local_Alignment for each request row (a, b, comp, low, hgh, anti,
+        lbord, hbord) on the loaded contigs.  Returns (paths (n, 7) int32:
+        abpos aepos bbpos bepos diffs tlen status, trace offsets (n+1), trace
+        uint16 values)."""
+        req = np.ascontiguousarray(requests, dtype=np.int32).reshape(-1, 8)
+        n = len(req)
+        nt = C.c_int64()
+        self._ck(self.L.pga_local_alignment(self.h, n, req.ctypes.data_as(vp) if n else None, C.byref(nt)),
+                 "local_alignment")
+        path = np.zeros((n, 7), dtype=np.int32)
+        toff = np.zeros(n + 1, dtype=np.int64)
+        tr = np.zeros(max(1, nt.value), dtype=np.uint16)
+        self._ck(self.L.pga_local_alignment_copy(self.h, path.ctypes.data_as(vp), toff.ctypes.data_as(vp),
+                                                 tr.ctypes.data_as(vp)), "local_alignment_copy")
+        return path, toff, tr[: nt.value]
 
     def align_work(self) -> dict:
         """Wave steps, diagonal updates (cells), calls and warp tasks of the last align()."""

@@ -175,6 +175,27 @@ int pga_align_times(const pga_ctx *ctx, float *ms4);
  * Local_Alignment calls, [3] warp tasks.  No counterpart in the reference. */
 int pga_align_work(const pga_ctx *ctx, int64_t *work4);
 
+/* ---- Local_Alignment on request lists -------------------------------------------- */
+
+/* Local_Alignment (lib/align.c:1423-1576) for n independent requests on the
+ * loaded contigs, as align_contigs calls it (src/fastga_pipeline.c:720-775):
+ * request i is 8 ints "a b comp low hgh anti lbord hbord" -- contig a
+ * (reverse-complemented when comp) against contig b, diagonal band [low, hgh]
+ * at antidiagonal anti, borders lbord / hbord (-1 = none); the band's start
+ * points ((anti+k)/2, (anti-k)/2) must lie in the contigs (PGA_ERR_ARG
+ * otherwise: the reference reads outside its buffers there).  Trace spacing 100;
+ * the scoring tables follow the GDB's base frequencies (pga_gdb_set_freq) as
+ * New_Align_Spec(0.7, 100, freq, 0).  One warp per request.  *ntrace = total
+ * trace values of the results. */
+int pga_local_alignment(pga_ctx *ctx, int64_t n, const int32_t *req8, int64_t *ntrace);
+
+/* The results of the last pga_local_alignment, in request order: path7 (7
+ * ints each: abpos aepos bbpos bepos diffs tlen status, status 0 or a work
+ * space overflow code), trace_off (n+1), trace (the tlen uint16 values of
+ * each path: diffs, b-delta per trace interval, as Local_Alignment leaves
+ * them before Compress_TraceTo8). */
+int pga_local_alignment_copy(pga_ctx *ctx, int32_t *path7, int64_t *trace_off, uint16_t *trace);
+
 /* ---- the .1aln file ------------------------------------------------------------ */
 
 /* la_merge's output file (src/fastga_pipeline.c:1616-1656: open_Aln_Write,
