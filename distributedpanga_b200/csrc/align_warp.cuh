@@ -968,7 +968,10 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
   R.T = 0;
   bool regmode = false;
   RegCtx X{vmask, W.NA, W.pool.cells, W.pool.next, W.pool.cap, W.chunk_next, W.chunk_end, 0};
-  int64_t nwaves = 0, ncells = 0;
+  int nwaves = 0, ncells = 0;
+  // the register waves' read-only inputs, held in this loop's registers
+  const AlignSpec rspec = spec;
+  const Seq rA = A, rB = B;
   // back to WarpWork: the pebble chunk, counts and errors
   auto sync = [&]() {
     W.chunk_next = X.chunk_next;
@@ -1006,7 +1009,7 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
         regmode = true;
       }
       dif += 1;
-      if (reg_wave<FWD>(X, spec, A, B, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
+      if (reg_wave<FWD>(X, rspec, rA, rB, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
                         trimha, more, aclip, bclip, WS)) {
         sync();
         return 1;
@@ -1091,7 +1094,21 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
       aclip = FWD ? I32MAX : -I32MAX;
       bclip = FWD ? -I32MAX : I32MAX;
     }
-    wave_prune<FWD>(W, W.V[cur], besta, low, hgh, WS);
+    if (regmode) {
+      // WAVE_LAG pruning of a register wave: its one diagonal per lane
+      if (hgh >= low) {
+        const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
+        const bool pass = WS.nact && WS.k0 >= low && WS.k0 <= hgh && (FWD ? WS.c[0] >= n : WS.c[0] <= n);
+        const int kmax = __reduce_max_sync(FULL, pass ? WS.k0 : -2147483647);
+        const int kmin = __reduce_min_sync(FULL, pass ? WS.k0 : 2147483647);
+        if (kmin <= kmax) {
+          hgh = kmax;
+          low = kmin;
+        } else
+          hgh = low - 1;
+      }
+    } else
+      wave_prune<FWD>(W, W.V[cur], besta, low, hgh, WS);
   }
   sync();
   __syncwarp();

@@ -596,7 +596,7 @@ struct LaunchPlan {
   std::vector<int> ridx;
 };
 
-// Runs a plan: the tasks go to the warps largest pair first.  tout: one
+// Runs a plan: the warps take the tasks in plan order.  tout: one
 // PairOut per task (plan order), fout: one per finished pair; rout_h (one
 // per range number) is refreshed.  Pebbles live for one launch; candidate
 // traces, range candidates and survivors accumulate over the launches of one
@@ -609,13 +609,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
   tout.assign(nt, PairOut{});
   fout.assign(nf, PairOut{});
   if (nt == 0 && nf == 0) return PGA_OK;
-  std::vector<int> order(nt);
-  for (size_t i = 0; i < nt; i++) order[i] = (int)i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return (plan.tasks[x].hi - plan.tasks[x].lo) > (plan.tasks[y].hi - plan.tasks[y].lo);
-  });
-  std::vector<PairTask> sorted(nt);
-  for (size_t k = 0; k < nt; k++) sorted[k] = plan.tasks[order[k]];
+  const std::vector<PairTask> &sorted = plan.tasks;  // the warps take them in this order
   if (nt) {
     ENSURE(ctx->tasks, sizeof(PairTask) * nt);
     ENSURE(ctx->pout, sizeof(PairOut) * nt);
@@ -745,7 +739,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     }
   }
   for (size_t k = 0; k < nt; k++) {
-    tout[order[k]] = ro[k];
+    tout[k] = ro[k];
     ctx->align_work[0] += ro[k].waves;
     ctx->align_work[1] += ro[k].cells;
     ctx->align_work[3] += 1;
@@ -1023,19 +1017,6 @@ int run_align(pga_ctx *ctx) {
   LaunchPlan P1;
   std::vector<int> first_task(first.size(), -1), first_fin(first.size(), -1);
   std::vector<std::vector<int>> first_ids(first.size());
-  for (size_t i = 0; i < first.size(); i++) {
-    PairTask t = first[i];
-    if (RS > 0 && t.hi - t.lo > RS) {
-      add_ranges(t, t.lo, t.hi, first_ids[i], P1.tasks);
-      FinishTask f{t.comp, t.a, t.b, 0, (int)P1.ridx.size(), (int)first_ids[i].size()};
-      P1.ridx.insert(P1.ridx.end(), first_ids[i].begin(), first_ids[i].end());
-      first_fin[i] = (int)P1.fins.size();
-      P1.fins.push_back(f);
-    } else {
-      first_task[i] = (int)P1.tasks.size();
-      P1.tasks.push_back(t);
-    }
-  }
   struct SelfPlan {
     std::vector<int> pre, post;
     int diag = -1;  // range number of the middle part (RS > 0)
@@ -1043,6 +1024,41 @@ int run_align(pga_ctx *ctx) {
   };
   std::vector<SelfPlan> sp(nself);
   std::vector<PairTask> diag_task(nself);
+  // The launch's tasks, largest pair first (a large pair's ranges each tend
+  // to re-extend its longest alignments, so they start early): pairs of two
+  // contigs (id >= 0) and the outer parts of self pairs (id = -1 - q).
+  std::vector<std::pair<int64_t, int>> src;
+  for (size_t i = 0; i < first.size(); i++) src.push_back({first[i].hi - first[i].lo, (int)i});
+  if (RS > 0)
+    for (int q = 0; q < nself; q++) {
+      const PairTask &t = pairs[0][self_idx[q]];
+      src.push_back({t.hi - t.lo, -1 - q});
+    }
+  std::stable_sort(src.begin(), src.end(), [](const std::pair<int64_t, int> &x, const std::pair<int64_t, int> &y) {
+    return x.first > y.first;
+  });
+  for (const auto &s : src) {
+    if (s.second >= 0) {
+      const size_t i = (size_t)s.second;
+      PairTask t = first[i];
+      if (RS > 0 && t.hi - t.lo > RS) {
+        add_ranges(t, t.lo, t.hi, first_ids[i], P1.tasks);
+        FinishTask f{t.comp, t.a, t.b, 0, (int)P1.ridx.size(), (int)first_ids[i].size()};
+        P1.ridx.insert(P1.ridx.end(), first_ids[i].begin(), first_ids[i].end());
+        first_fin[i] = (int)P1.fins.size();
+        P1.fins.push_back(f);
+      } else {
+        first_task[i] = (int)P1.tasks.size();
+        P1.tasks.push_back(t);
+      }
+    } else {
+      const int q = -1 - s.second;
+      const PairTask &t = pairs[0][self_idx[q]];
+      const int64_t x1 = t.lo + x12[2 * q], x2 = t.lo + x12[2 * q + 1];
+      add_ranges(t, t.lo, x1, sp[q].pre, P1.tasks);
+      add_ranges(t, x2, t.hi, sp[q].post, P1.tasks);
+    }
+  }
   for (int q = 0; q < nself; q++) {
     const PairTask &t = pairs[0][self_idx[q]];
     if (RS <= 0) {
@@ -1051,8 +1067,6 @@ int run_align(pga_ctx *ctx) {
       continue;
     }
     const int64_t x1 = t.lo + x12[2 * q], x2 = t.lo + x12[2 * q + 1];
-    add_ranges(t, t.lo, x1, sp[q].pre, P1.tasks);
-    add_ranges(t, x2, t.hi, sp[q].post, P1.tasks);
     if (x2 > x1) {
       PairTask d = t;
       d.seg = sp[q].diag = nranges++;
