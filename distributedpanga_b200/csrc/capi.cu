@@ -1037,6 +1037,12 @@ int run_align(pga_ctx *ctx) {
   std::stable_sort(src.begin(), src.end(), [](const std::pair<int64_t, int> &x, const std::pair<int64_t, int> &y) {
     return x.first > y.first;
   });
+  {
+    size_t est = 2 * (size_t)nself + 1;
+    for (const auto &s : src) est += RS > 0 ? (size_t)(s.first / RS + 2) : 1;
+    P1.tasks.reserve(est);
+    P1.ridx.reserve(est);
+  }
   for (const auto &s : src) {
     if (s.second >= 0) {
       const size_t i = (size_t)s.second;
