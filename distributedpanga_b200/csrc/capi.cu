@@ -18,6 +18,7 @@
 #include "seeds.cuh"
 #include "align.cuh"
 #include "align_spec.h"
+#include "ingest.cuh"
 #include "../../include/pga_b200.h"
 
 using namespace pga;
@@ -48,7 +49,17 @@ struct pga_ctx {
   bool have_gdb = false;
   int ncontig = 0;
   int64_t maxctg = 0;
+  int64_t bps_bytes = 0;
   std::vector<int64_t> clen, boff;
+  // GDB ingest (pga_gdb_ingest_fasta): the scaffold side of the GDB
+  bool have_scaffolds = false;
+  std::vector<int64_t> h_sbeg, h_scf4;   // per contig sbeg; per scaffold {fctg, ectg, slen, hoff}
+  std::vector<int32_t> h_scaf;           // per contig
+  std::vector<char> h_headers;
+  int64_t base_count[4] = {0, 0, 0, 0};
+  DBuf fa_text, fa_mask, fa_seq, fa_cnt, fa_tmp, fa_tot, fa_status, fa_hdr, fa_hbytes, fa_runs, fa_ctg;
+  cudaEvent_t fa_ev[3] = {nullptr, nullptr, nullptr};  // upload start, parse start, parse end
+  float ingest_ms[2] = {0, 0};                        // pga_gdb_ingest_times
   int posb = 0, ctgb = 0, rsize = 0;
   DBuf bps, dclen, dboff, tile_ctg, tile_j0;
   int ntiles = 0;
@@ -1364,13 +1375,16 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                   &ctx->qbig, &ctx->qcount, &ctx->maxrun, &ctx->u64tmp, &ctx->blk_n, &ctx->blk_c,
                   &ctx->blk_tmp, &ctx->seed[0], &ctx->seed[1], &ctx->keys[0], &ctx->keys[1],
                   &ctx->keys_alt, &ctx->rhist, &ctx->rscan, &ctx->panel[0], &ctx->panel[1], &ctx->io,
-                  &ctx->io2};
+                  &ctx->io2, &ctx->fa_text, &ctx->fa_mask, &ctx->fa_seq, &ctx->fa_cnt, &ctx->fa_tmp,
+                  &ctx->fa_tot, &ctx->fa_status, &ctx->fa_hdr, &ctx->fa_hbytes, &ctx->fa_runs, &ctx->fa_ctg};
   for (DBuf *b : bufs)
     if (b->p) cudaFree(b->p);
   for (int s = 0; s < ST_N; s++) {
     cudaEventDestroy(ctx->ev[s][0]);
     cudaEventDestroy(ctx->ev[s][1]);
   }
+  for (cudaEvent_t e : ctx->fa_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -1409,12 +1423,13 @@ int pga_stage_times(const pga_ctx *cctx, float *ms9) {
   return PGA_OK;
 }
 
-int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int ncontig, const int64_t *clen,
-                 const int64_t *boff) {
-  if (!ctx || ncontig < 0 || (ncontig > 0 && (!clen || !boff)) || bps_bytes < 0) return PGA_ERR_ARG;
-  if (ncontig >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%d contigs: at most 32767 supported", ncontig);
-  CK(cudaSetDevice(ctx->device));
+namespace {
+
+// Contig table of a GDB whose sequence image is already on the device:
+// validation, record sizing and the extraction tiles.
+int gdb_tables(pga_ctx *ctx, int ncontig, const int64_t *clen, const int64_t *boff, int64_t bps_bytes) {
   ctx->ncontig = ncontig;
+  ctx->bps_bytes = bps_bytes;
   ctx->clen.assign(clen, clen + ncontig);
   ctx->boff.assign(boff, boff + ncontig);
   ctx->maxctg = 0;
@@ -1429,14 +1444,6 @@ int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int nconti
   ctx->ctgb = bytes_inclusive(2 * (int64_t)ncontig - 1);
   if (ctx->ctgb < 1) ctx->ctgb = 1;
   ctx->rsize = 12 + ctx->posb + ctx->ctgb;
-  ENSURE(ctx->bps, (size_t)bps_bytes + 16);
-  ENSURE(ctx->dclen, sizeof(int64_t) * (ncontig + 1));
-  ENSURE(ctx->dboff, sizeof(int64_t) * (ncontig + 1));
-  if (bps_bytes > 0) CK(cudaMemcpyAsync(ctx->bps.p, bps, bps_bytes, cudaMemcpyHostToDevice, ctx->st));
-  if (ncontig > 0) {
-    CK(cudaMemcpyAsync(ctx->dclen.p, clen, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->dboff.p, boff, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
-  }
   std::vector<int64_t> tj;
   ctx->h_tile_ctg.clear();
   for (int r = 0; r < ncontig; r++) {
@@ -1456,13 +1463,282 @@ int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int nconti
     CK(cudaMemcpyAsync(ctx->tile_j0.p, tj.data(), sizeof(int64_t) * ctx->ntiles, cudaMemcpyHostToDevice, ctx->st));
   }
   CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+// A new GDB invalidates everything computed from the previous one.
+void gdb_reset(pga_ctx *ctx) {
+  ctx->have_gdb = false;
+  ctx->have_scaffolds = false;
   ctx->freq_set = false;
-  ctx->have_gdb = true;
   ctx->have_index = false;
   ctx->have_seeds = false;
   ctx->have_numeric = false;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
   ctx->have_align = false;
+}
+
+}  // namespace
+
+int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int ncontig, const int64_t *clen,
+                 const int64_t *boff) {
+  if (!ctx || ncontig < 0 || (ncontig > 0 && (!clen || !boff)) || bps_bytes < 0) return PGA_ERR_ARG;
+  if (ncontig >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%d contigs: at most 32767 supported", ncontig);
+  CK(cudaSetDevice(ctx->device));
+  gdb_reset(ctx);
+  ENSURE(ctx->bps, (size_t)bps_bytes + 16);
+  ENSURE(ctx->dclen, sizeof(int64_t) * (ncontig + 1));
+  ENSURE(ctx->dboff, sizeof(int64_t) * (ncontig + 1));
+  if (bps_bytes > 0) CK(cudaMemcpyAsync(ctx->bps.p, bps, bps_bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (ncontig > 0) {
+    CK(cudaMemcpyAsync(ctx->dclen.p, clen, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->dboff.p, boff, sizeof(int64_t) * ncontig, cudaMemcpyHostToDevice, ctx->st));
+  }
+  int r = gdb_tables(ctx, ncontig, clen, boff, bps_bytes);
+  if (r != PGA_OK) return r;
+  ctx->have_gdb = true;
+  return PGA_OK;
+}
+
+namespace {
+
+// Queues a copy of `count` values of `size` bytes at device address `src`
+// into `dst` (stream order).
+int fetch_n(pga_ctx *ctx, void *dst, const void *src, int64_t count, size_t size) {
+  if (count <= 0) return PGA_OK;
+  CK(cudaMemcpyAsync(dst, src, size * count, cudaMemcpyDeviceToHost, ctx->st));
+  return PGA_OK;
+}
+#define fetch(ctx, dst, src, count) fetch_n((ctx), (dst), (src), (count), sizeof(*(dst)))
+
+#define TRY(x)                  \
+  do {                          \
+    int _r = (x);               \
+    if (_r != PGA_OK) return _r; \
+  } while (0)
+
+// The device half of pga_gdb_ingest_fasta: text already in ctx->fa_text.
+int ingest_device(pga_ctx *ctx, int64_t n, int nthr, int64_t *sizes6) {
+  cudaStream_t st = ctx->st;
+  const int64_t nt = (n + FA_TILE - 1) / FA_TILE;
+  unsigned long long *status;
+  int64_t *tot;
+  ENSURE(ctx->fa_status, sizeof(unsigned long long) * (FA_NSTATUS + 256));
+  ENSURE(ctx->fa_tot, sizeof(int64_t) * 8);
+  ENSURE(ctx->fa_cnt, sizeof(int64_t) * 2 * (nt + 1));
+  ENSURE(ctx->fa_tmp, sizeof(int64_t) * scan_tmp_elems(nt));
+  status = P<unsigned long long>(ctx->fa_status);
+  tot = P<int64_t>(ctx->fa_tot);
+  int64_t *cnt = P<int64_t>(ctx->fa_cnt), *cnt2 = cnt + (nt + 1);
+  const uint8_t *text = P<uint8_t>(ctx->fa_text);
+  int64_t h[8];
+  unsigned long long hs[FA_NSTATUS + 256];
+
+  // headers
+  CK(fa_init_status(status, st));
+  CK(fa_count_headers(text, n, cnt, status, st));
+  CK(exclusive_scan<int64_t>(cnt, cnt, nt, P<int64_t>(ctx->fa_tmp), tot + 0, st));
+  LAUNCHED(5);
+  TRY(fetch(ctx, h, tot, 1));
+  TRY(fetch(ctx, hs, status, FA_NSTATUS));
+  CK(cudaStreamSynchronize(st));
+  if (hs[FA_BAD] != ~0ull)
+    return fail(ctx, PGA_ERR_ARG, "byte %llu of the text is NUL or not ASCII", hs[FA_BAD]);
+  const int64_t nh64 = h[0];
+  if (nh64 >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%lld scaffolds: at most 32767 supported", (long long)nh64);
+  const int nh = (int)nh64;
+  // per scaffold: hstart hend htext hlen1 hoff sstart(+1) trail scf4(4)
+  ENSURE(ctx->fa_hdr, sizeof(int64_t) * 11 * (nh + 1));
+  int64_t *hstart = P<int64_t>(ctx->fa_hdr), *hend = hstart + (nh + 1), *htext = hend + (nh + 1),
+          *hlen1 = htext + (nh + 1), *hoff = hlen1 + (nh + 1), *sstart = hoff + (nh + 1),
+          *trail = sstart + (nh + 1), *scf4 = trail + (nh + 1);
+  ENSURE(ctx->fa_mask, sizeof(uint32_t) * ((n + 31) / 32 + 4));
+  uint32_t *mask = P<uint32_t>(ctx->fa_mask);
+  CK(fa_write_headers(text, n, cnt, hstart, st));
+  CK(fa_header_lines(text, hstart, nh, hend, htext, hlen1, st));
+  ENSURE(ctx->fa_tmp, sizeof(int64_t) * std::max(scan_tmp_elems(nt), scan_tmp_elems(nh)));
+  CK(exclusive_scan<int64_t>(hlen1, hoff, nh, P<int64_t>(ctx->fa_tmp), tot + 1, st));
+  CK(cudaMemsetAsync(mask, 0, sizeof(uint32_t) * ((n + 31) / 32 + 4), st));
+  CK(fa_paint_headers(hstart, hend, nh, mask, st));
+  // sequence characters; their total is sstart[nh]
+  CK(fa_count_seq(text, n, mask, cnt, st));
+  CK(exclusive_scan<int64_t>(cnt, cnt, nt, P<int64_t>(ctx->fa_tmp), sstart + nh, st));
+  CK(cudaMemsetAsync(trail, 0, sizeof(int64_t) * (nh + 1), st));
+  LAUNCHED(10);
+  TRY(fetch(ctx, h + 1, tot + 1, 1));
+  TRY(fetch(ctx, h + 2, sstart + nh, 1));
+  CK(cudaStreamSynchronize(st));
+  const int64_t hdrtot = h[1], G = h[2];
+  if (G == 0) return fail(ctx, PGA_ERR_ARG, "missing sequence entry for scaffold 0");
+  ENSURE(ctx->fa_hbytes, (size_t)hdrtot + 16);
+  ENSURE(ctx->fa_seq, (size_t)G + 64);
+  uint8_t *seq = P<uint8_t>(ctx->fa_seq);
+  CK(fa_copy_headers(text, htext, hlen1, hoff, nh, P<char>(ctx->fa_hbytes), st));
+  CK(cudaMemsetAsync(seq + G, 0, 64, st));
+  CK(fa_write_seq(text, n, mask, cnt, hend, nh, seq, sstart, status, st));
+  CK(fa_flag_scaffolds(seq, sstart, nh, status, st));
+  // N runs
+  const int64_t gt = (G + FA_TILE - 1) / FA_TILE;
+  ENSURE(ctx->fa_cnt, sizeof(int64_t) * 2 * (std::max(nt, gt) + 1));
+  cnt = P<int64_t>(ctx->fa_cnt);
+  cnt2 = cnt + (gt + 1);
+  ENSURE(ctx->fa_tmp, sizeof(int64_t) * std::max(scan_tmp_elems(gt), scan_tmp_elems(nh)));
+  CK(fa_count_runs(seq, G, cnt, cnt2, st));
+  CK(exclusive_scan<int64_t>(cnt, cnt, gt, P<int64_t>(ctx->fa_tmp), tot + 2, st));
+  CK(exclusive_scan<int64_t>(cnt2, cnt2, gt, P<int64_t>(ctx->fa_tmp), tot + 3, st));
+  LAUNCHED(10);
+  TRY(fetch(ctx, h + 3, tot + 2, 2));
+  TRY(fetch(ctx, hs, status, FA_NSTATUS));
+  CK(cudaStreamSynchronize(st));
+  if (hs[FA_EMPTY] != ~0ull)
+    return fail(ctx, PGA_ERR_ARG, "missing sequence entry for scaffold %llu", hs[FA_EMPTY]);
+  const int64_t R = h[3];
+  if (h[4] != R) return fail(ctx, PGA_ERR_CUDA, "ingest: %lld run starts but %lld run ends", (long long)R,
+                              (long long)h[4]);
+  // per run: rs re is_split sr ; rscaf (int32)
+  ENSURE(ctx->fa_runs, sizeof(int64_t) * 4 * (R + 1) + sizeof(int32_t) * (R + 1));
+  int64_t *rs = P<int64_t>(ctx->fa_runs), *re = rs + (R + 1), *isp = re + (R + 1), *sr = isp + (R + 1);
+  int32_t *rscaf = (int32_t *)(sr + (R + 1));
+  ENSURE(ctx->fa_tmp, sizeof(int64_t) * std::max(scan_tmp_elems(R), scan_tmp_elems(nh)));
+  if (R > 0) {
+    CK(fa_write_runs(seq, G, cnt, cnt2, rs, re, st));
+    CK(fa_classify_runs(rs, re, R, sstart, nh, nthr, isp, rscaf, trail, status, st));
+    LAUNCHED(5);
+  }
+  CK(exclusive_scan<int64_t>(isp, sr, R, P<int64_t>(ctx->fa_tmp), tot + 4, st));
+  TRY(fetch(ctx, h + 5, tot + 4, 1));
+  TRY(fetch(ctx, hs, status, FA_NSTATUS));
+  CK(cudaStreamSynchronize(st));
+  if (hs[FA_ALLN] != ~0ull)
+    return fail(ctx, PGA_ERR_ARG, "missing sequence entry for scaffold %llu (all N)", hs[FA_ALLN]);
+  const int64_t nsplit = h[5], nc64 = nh + nsplit;
+  if (nc64 >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%lld contigs: at most 32767 supported", (long long)nc64);
+  const int nc = (int)nc64;
+  // contigs: cstart cend sbeg ; cscaf (int32); clen and boff go to the GDB's own arrays
+  ENSURE(ctx->fa_ctg, sizeof(int64_t) * 3 * (nc + 1) + sizeof(int32_t) * (nc + 1));
+  int64_t *cstart = P<int64_t>(ctx->fa_ctg), *cend = cstart + (nc + 1), *sbeg = cend + (nc + 1);
+  int32_t *cscaf = (int32_t *)(sbeg + (nc + 1));
+  ENSURE(ctx->dclen, sizeof(int64_t) * (nc + 1));
+  ENSURE(ctx->dboff, sizeof(int64_t) * (nc + 1));
+  ENSURE(ctx->fa_tmp, sizeof(int64_t) * std::max(scan_tmp_elems(R), scan_tmp_elems(nc)));
+  int64_t *dclen = P<int64_t>(ctx->dclen), *dboff = P<int64_t>(ctx->dboff);
+  CK(fa_scaffolds(sstart, nh, rs, R, sr, nsplit, trail, hoff, scf4, cstart, cend, cscaf, st));
+  if (R > 0) {
+    CK(fa_splits(rs, re, R, isp, sr, rscaf, cstart, cend, cscaf, st));
+    LAUNCHED(1);
+  }
+  CK(fa_contigs(nc, cstart, cend, cscaf, sstart, dclen, sbeg, dboff, status, st));
+  CK(exclusive_scan<int64_t>(dboff, dboff, nc, P<int64_t>(ctx->fa_tmp), dboff + nc, st));
+  LAUNCHED(5);
+  TRY(fetch(ctx, h + 6, dboff + nc, 1));
+  CK(cudaStreamSynchronize(st));
+  const int64_t nbps = h[6];
+  ENSURE(ctx->bps, (size_t)((nbps + 3) / 4 * 4) + 16);
+  CK(fa_pack(seq, nc, dboff, cstart, dclen, P<uint8_t>(ctx->bps), st));
+  CK(cudaEventRecord(ctx->fa_ev[2], st));
+  LAUNCHED(1);
+
+  // host tables
+  std::vector<int64_t> clen(nc), boff(nc);
+  ctx->h_sbeg.resize(nc);
+  ctx->h_scaf.resize(nc);
+  ctx->h_scf4.resize(4 * (size_t)nh);
+  ctx->h_headers.resize(hdrtot);
+  TRY(fetch(ctx, clen.data(), dclen, nc));
+  TRY(fetch(ctx, boff.data(), dboff, nc));
+  TRY(fetch(ctx, ctx->h_sbeg.data(), sbeg, nc));
+  TRY(fetch(ctx, ctx->h_scaf.data(), cscaf, nc));
+  TRY(fetch(ctx, ctx->h_scf4.data(), scf4, 4 * (int64_t)nh));
+  TRY(fetch(ctx, ctx->h_headers.data(), ctx->fa_hbytes.p, hdrtot));
+  TRY(fetch(ctx, hs, status, FA_NSTATUS + 256));
+  CK(cudaStreamSynchronize(st));
+  for (int v = 0; v < 4; v++) {
+    unsigned long long c = 0;
+    for (int b = 0; b < 64; b++) c += hs[FA_NSTATUS + 4 * b + v];
+    ctx->base_count[v] = (int64_t)c;
+  }
+  ctx->base_count[0] += (int64_t)hs[FA_FILL];
+  TRY(gdb_tables(ctx, nc, clen.data(), boff.data(), nbps));
+  const int64_t seqtot = ctx->base_count[0] + ctx->base_count[1] + ctx->base_count[2] + ctx->base_count[3];
+  // GDB.freq as Create_GDB sets it (lib/GDB.c:1083-1086)
+  for (int v = 0; v < 4; v++) ctx->base_freq[v] = (float)((1. * ctx->base_count[v]) / seqtot);
+  ctx->freq_set = true;
+  if (sizes6) {
+    sizes6[0] = nh;
+    sizes6[1] = nc;
+    sizes6[2] = nbps;
+    sizes6[3] = hdrtot;
+    sizes6[4] = (int64_t)hs[FA_MAXCTG];
+    sizes6[5] = seqtot;
+  }
+  return PGA_OK;
+}
+
+}  // namespace
+
+int pga_gdb_ingest_fasta(pga_ctx *ctx, const char *text, int64_t nbytes, int nthr, int64_t *sizes6) {
+  if (!ctx || nbytes < 0 || (nbytes > 0 && !text)) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  gdb_reset(ctx);
+  if (nbytes == 0) return fail(ctx, PGA_ERR_ARG, "input is empty");
+  if (text[0] != '>') return fail(ctx, PGA_ERR_ARG, "first header is missing");
+  if (text[nbytes - 1] != '\n') return fail(ctx, PGA_ERR_ARG, "last line does not end with new-line");
+  for (cudaEvent_t &e : ctx->fa_ev)
+    if (!e) CK(cudaEventCreate(&e));
+  ENSURE(ctx->fa_text, (size_t)nbytes + 64);
+  CK(cudaEventRecord(ctx->fa_ev[0], ctx->st));
+  CK(cudaMemcpyAsync(ctx->fa_text.p, text, nbytes, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(P<uint8_t>(ctx->fa_text) + nbytes, 0, 64, ctx->st));
+  CK(cudaEventRecord(ctx->fa_ev[1], ctx->st));
+  int r = ingest_device(ctx, nbytes, nthr, sizes6);
+  if (r != PGA_OK) return r;
+  CK(cudaEventElapsedTime(&ctx->ingest_ms[0], ctx->fa_ev[0], ctx->fa_ev[1]));
+  CK(cudaEventElapsedTime(&ctx->ingest_ms[1], ctx->fa_ev[1], ctx->fa_ev[2]));
+  ctx->have_gdb = true;
+  ctx->have_scaffolds = true;
+  return PGA_OK;
+}
+
+int pga_gdb_ingest_times(const pga_ctx *ctx, float *ms2) {
+  if (!ctx || !ms2 || !ctx->have_scaffolds) return PGA_ERR_ARG;
+  ms2[0] = ctx->ingest_ms[0];
+  ms2[1] = ctx->ingest_ms[1];
+  return PGA_OK;
+}
+
+int pga_gdb_copy(pga_ctx *ctx, uint8_t *bps, int64_t *contigs4, int64_t *scaffolds4, char *headers,
+                 int64_t *counts4) {
+  if (!ctx || !ctx->have_scaffolds) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (bps && ctx->bps_bytes > 0) {
+    CK(cudaMemcpyAsync(bps, ctx->bps.p, ctx->bps_bytes, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  if (contigs4)
+    for (int c = 0; c < ctx->ncontig; c++) {
+      contigs4[4 * c + 0] = ctx->clen[c];
+      contigs4[4 * c + 1] = ctx->boff[c];
+      contigs4[4 * c + 2] = ctx->h_sbeg[c];
+      contigs4[4 * c + 3] = ctx->h_scaf[c];
+    }
+  if (scaffolds4) std::copy(ctx->h_scf4.begin(), ctx->h_scf4.end(), scaffolds4);
+  if (headers) std::copy(ctx->h_headers.begin(), ctx->h_headers.end(), headers);
+  if (counts4)
+    for (int v = 0; v < 4; v++) counts4[v] = ctx->base_count[v];
+  return PGA_OK;
+}
+
+int pga_gdb_write(pga_ctx *ctx, const char *tpath, const char *program, const char *version, const char *command,
+                  const char *srcpath) {
+  if (!ctx || !ctx->have_scaffolds || !tpath || !program || !version || !command || !srcpath) return PGA_ERR_ARG;
+  std::vector<uint8_t> bps(ctx->bps_bytes);
+  std::vector<int64_t> ctg(4 * (size_t)ctx->ncontig);
+  int r = pga_gdb_copy(ctx, bps.data(), ctg.data(), nullptr, nullptr, nullptr);
+  if (r != PGA_OK) return r;
+  r = pga_write_1gdb(tpath, program, version, command, srcpath, ctx->base_freq, (int)(ctx->h_scf4.size() / 4),
+                     ctx->h_scf4.data(), ctx->h_headers.data(), (int64_t)ctx->h_headers.size(), ctx->ncontig,
+                     ctg.data(), bps.data(), ctx->bps_bytes);
+  if (r != PGA_OK) return fail(ctx, r, "cannot write %s or its .bps", tpath);
   return PGA_OK;
 }
 

@@ -78,6 +78,12 @@ _SIGS = {
                                        C.c_char_p, C.c_int, vp, vp, vp, vp]),
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
+    "pga_gdb_ingest_fasta": (C.c_int, [vp, C.c_char_p, C.c_int64, C.c_int, vp]),
+    "pga_gdb_copy": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "pga_gdb_ingest_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "pga_gdb_write": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    "pga_write_1gdb": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, vp, C.c_int, vp,
+                                 vp, C.c_int64, C.c_int, vp, vp, C.c_int64]),
 }
 
 _LIB = None
@@ -176,6 +182,51 @@ class Device:
                                      np.ascontiguousarray(cs.clen, dtype=np.int64),
                                      np.ascontiguousarray(cs.boff, dtype=np.int64)), "gdb_load")
         self.cs = cs
+
+    def gdb_ingest_fasta(self, text, nthr: int = 0, nbytes: int | None = None, tables: bool = True):
+        """Create_GDB (lib/GDB.c:442) of a FASTA text, parsed on the device;
+        the result becomes this context's GDB (as gdb_load would leave it).
+        `text` is bytes, or a host address with `nbytes` (pinned memory
+        uploads fastest).  Returns the GdbTables, or with tables=False only
+        the sizes {nscaff, ncontig, bps bytes, header bytes, maxctg, seqtot}."""
+        if isinstance(text, int):
+            ptr, n = C.cast(text, C.c_char_p), int(nbytes)
+        else:
+            text = bytes(text)
+            ptr, n = text, len(text)
+        sizes = np.zeros(6, dtype=np.int64)
+        self._ck(self.L.pga_gdb_ingest_fasta(self.h, ptr, n, int(nthr), sizes.ctypes.data_as(vp)),
+                 "gdb_ingest_fasta")
+        self.cs = None
+        if not tables:
+            return sizes
+        t = self.gdb_tables(sizes)
+        self.cs = _gdb.ContigSet(bps=t.bps, clen=t.contigs[:, 0].copy(), boff=t.contigs[:, 1].copy(),
+                                 freq=t.freq)
+        return t
+
+    def gdb_tables(self, sizes) -> "GdbTables":
+        nscaff, ncontig, nbps, hdrtot = (int(x) for x in sizes[:4])
+        bps = np.zeros(max(nbps, 1), dtype=np.uint8)
+        ctg = np.zeros((ncontig, 4), dtype=np.int64)
+        scf = np.zeros((nscaff, 4), dtype=np.int64)
+        hdr = np.zeros(max(hdrtot, 1), dtype=np.uint8)
+        cnt = np.zeros(4, dtype=np.int64)
+        self._ck(self.L.pga_gdb_copy(self.h, bps.ctypes.data_as(vp), ctg.ctypes.data_as(vp),
+                                     scf.ctypes.data_as(vp), hdr.ctypes.data_as(vp), cnt.ctypes.data_as(vp)),
+                 "gdb_copy")
+        return GdbTables(bps=bps[:nbps], contigs=ctg, scaffolds=scf, headers=hdr[:hdrtot].tobytes(), count=cnt,
+                         maxctg=int(sizes[4]))
+
+    def gdb_ingest_times(self) -> dict:
+        a = (C.c_float * 2)()
+        self._ck(self.L.pga_gdb_ingest_times(self.h, a), "gdb_ingest_times")
+        return {"upload_ms": float(a[0]), "parse_ms": float(a[1])}
+
+    def gdb_write(self, tpath: str, srcpath: str, command: str = "distributedpanga_b200"):
+        """Write_GDB (lib/GDB.c:1519) of the ingested GDB: tpath and its .bps."""
+        self._ck(self.L.pga_gdb_write(self.h, tpath.encode(), _PROG, _VERSION, command.encode(),
+                                      srcpath.encode()), "gdb_write")
 
     def record_sizing(self):
         a, b, c = C.c_int(), C.c_int(), C.c_int()
@@ -352,6 +403,37 @@ class Device:
         return {"pairs": int(a[0]), "self_pairs": int(a[1]), "calls": int(a[2]), "alignments": int(a[4]),
                 "self_rounds": int(a[5]), "max_task_cycles": int(a[3]), "all_task_cycles": int(a[6]),
                 "max_task_calls": int(a[7])}
+
+
+class GdbTables:
+    """A GDB as Create_GDB builds it (lib/GDB.h:28-70): the .bps image,
+    contigs rows {clen, boff, sbeg, scaf}, scaffolds rows {fctg, ectg, slen,
+    hoff}, the header block (names ended by NUL) and the base counts."""
+
+    def __init__(self, bps, contigs, scaffolds, headers, count, maxctg):
+        self.bps = bps
+        self.contigs = contigs
+        self.scaffolds = scaffolds
+        self.headers = headers
+        self.count = count
+        self.maxctg = maxctg
+
+    @property
+    def seqtot(self) -> int:
+        return int(self.count.sum())
+
+    @property
+    def freq(self) -> np.ndarray:
+        """GDB.freq (lib/GDB.c:1083-1086)."""
+        return (self.count / max(1, self.seqtot)).astype(np.float32)
+
+    @property
+    def names(self) -> list:
+        return [self.headers[h:self.headers.index(b"\0", h)] for h in self.scaffolds[:, 3]]
+
+    def skeleton(self) -> "Skeleton":
+        fctg = np.append(self.scaffolds[:, 0], self.scaffolds[-1, 1] if len(self.scaffolds) else 0)
+        return Skeleton(self.names, self.scaffolds[:, 2], fctg, self.contigs[:, 2])
 
 
 class Skeleton:

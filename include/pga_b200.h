@@ -65,6 +65,47 @@ int         pga_stage_times(const pga_ctx *ctx, float *ms9);
 int pga_gdb_load(pga_ctx *ctx, const uint8_t *bps, int64_t bps_bytes, int ncontig,
                  const int64_t *clen, const int64_t *boff);
 
+/* Create_GDB (lib/GDB.c:442) on a FASTA text in host memory, parsed on the
+ * device: the reader of lib/GDB.c:771-1057 with gap threshold `nthr` (the
+ * reference's own callers pass 0: every N run followed by a base splits a
+ * contig; a run shorter than nthr is otherwise filled with A's).  The result
+ * is the context's GDB, as pga_gdb_load would leave it, with its base
+ * frequencies set as Create_GDB sets GDB.freq (lib/GDB.c:1083-1086).
+ * sizes6 (may be NULL) = {nscaff, ncontig, .bps bytes, header bytes,
+ * maxctg, seqtot}.  The reference's errors are PGA_ERR_ARG with its message:
+ * an empty text, a first line without '>', a last line without '\n', a
+ * scaffold without sequence; NUL or non-ASCII bytes are refused too.  At
+ * most 32767 contigs (PGA_ERR_LIMIT).  Soft masks (lower case, an ANO
+ * argument of Create_GDB) are not produced. */
+int pga_gdb_ingest_fasta(pga_ctx *ctx, const char *text, int64_t nbytes, int nthr, int64_t *sizes6);
+
+/* The GDB made by pga_gdb_ingest_fasta, each array optional (NULL):
+ * bps (sizes6[2] bytes), contigs4 (ncontig x {clen, boff, sbeg, scaf},
+ * GDB_CONTIG lib/GDB.h:28-34), scaffolds4 (nscaff x {fctg, ectg, slen, hoff},
+ * GDB_SCAFFOLD lib/GDB.h:36-41), headers (sizes6[3] bytes: each scaffold's
+ * name ended by '\0', at hoff), counts4 (bases A C G T; filled gap bases
+ * count as A). */
+int pga_gdb_copy(pga_ctx *ctx, uint8_t *bps, int64_t *contigs4, int64_t *scaffolds4, char *headers,
+                 int64_t *counts4);
+
+/* Device times of the last pga_gdb_ingest_fasta, ms2 = {text upload, parse
+ * (every kernel from the first header scan to the packed image)}. */
+int pga_gdb_ingest_times(const pga_ctx *ctx, float *ms2);
+
+/* Write_GDB (lib/GDB.c:1519) of the GDB made by pga_gdb_ingest_fasta:
+ * tpath (<dir>/<root>.1gdb) and its hidden <dir>/.<root>.bps.  The .1gdb is
+ * written in ONE's ASCII encoding; the reference's Read_GDB (lib/GDB.c:1171)
+ * reads it.  srcpath is the FASTA's path as recorded in the file. */
+int pga_gdb_write(pga_ctx *ctx, const char *tpath, const char *program, const char *version, const char *command,
+                  const char *srcpath);
+
+/* The writer behind pga_gdb_write, on host tables laid out as pga_gdb_copy's;
+ * freq4 as GDB.freq.  Needs no device. */
+int pga_write_1gdb(const char *tpath, const char *program, const char *version, const char *command,
+                   const char *srcpath, const float *freq4, int nscaff, const int64_t *scaffolds4,
+                   const char *headers, int64_t hdrtot, int ncontig, const int64_t *contigs4,
+                   const uint8_t *bps, int64_t bps_bytes);
+
 /* Record sizing of the loaded GDB (compute_record_sizing, src/record.c:18). */
 int pga_record_sizing(const pga_ctx *ctx, int *position_bytes, int *contig_strand_bytes,
                       int *record_size);

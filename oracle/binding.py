@@ -48,6 +48,9 @@ def lib():
         L.orc_reimport_sort.restype = C.c_int
         L.orc_reimport_sort.argtypes = [u8p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                         C.c_int, u8p, i64p]
+        L.orc_fasta_gdb.restype = C.c_int
+        L.orc_fasta_gdb.argtypes = [C.c_char_p, C.c_int64, C.c_int, i64p, C.c_int64, i64p, C.c_int64,
+                                    u8p, C.c_int64, u8p, C.c_int64, i64p, i64p, C.c_char_p, C.c_int]
         _LIB = L
     return _LIB
 
@@ -123,8 +126,58 @@ def ref_available() -> bool:
                for x in ("pga-mpi-merge", "fa2gdb", "gdbdump", "GIXmake_dump", "ALNtoPAF"))
 
 
-def ref_make_gdb(fasta: str, stem: str) -> None:
-    subprocess.run([os.path.join(REF_DIR, "fa2gdb"), fasta, stem + ".1gdb"], check=True)
+def fasta_gdb(text: bytes, nthr: int = 0) -> dict:
+    """Create_GDB's FASTA reader on `text` (orc_fasta_gdb).  Raises ValueError
+    with the reader's message for an input it rejects."""
+    n = len(text)
+    cap = n + 2
+    scf = np.zeros(4 * cap, np.int64)
+    ctg = np.zeros(4 * cap, np.int64)
+    hdr = np.zeros(cap, np.uint8)
+    bps = np.zeros(cap, np.uint8)
+    sizes = np.zeros(6, np.int64)
+    count = np.zeros(4, np.int64)
+    err = C.create_string_buffer(256)
+    r = lib().orc_fasta_gdb(text, n, nthr, scf, cap, ctg, cap, hdr, cap, bps, cap, sizes, count, err, 256)
+    if r == -1:
+        raise ValueError(err.value.decode())
+    if r != 0:
+        raise RuntimeError("orc_fasta_gdb: capacity")
+    nscaff, ncontig, nbps, hdrtot, maxctg, seqtot = (int(x) for x in sizes)
+    return {"nscaff": nscaff, "ncontig": ncontig, "maxctg": maxctg, "seqtot": seqtot,
+            "scaffolds": scf[:4 * nscaff].reshape(-1, 4).copy(),
+            "contigs": ctg[:4 * ncontig].reshape(-1, 4).copy(),
+            "headers": hdr[:hdrtot].tobytes(), "bps": bps[:nbps].copy(), "count": count.copy()}
+
+
+def ref_make_gdb(fasta: str, stem: str, nthr: int | None = None) -> None:
+    cmd = [os.path.join(REF_DIR, "fa2gdb"), fasta, stem + ".1gdb"]
+    if nthr is not None:
+        cmd.append(str(nthr))
+    subprocess.run(cmd, check=True, capture_output=True)
+
+
+def ref_gdb_tables(stem: str) -> dict:
+    """The GDB as the reference reads it back (gdbdump -s): contig rows
+    (clen, boff, sbeg, scaf), scaffold rows (fctg, ectg, slen, hoff), the
+    headers, the frequencies as floats and the .bps bytes."""
+    out = subprocess.run([os.path.join(REF_DIR, "gdbdump"), "-s", stem], check=True,
+                         capture_output=True).stdout.decode("latin-1").split("\n")
+    head = out[0].split()
+    ncontig = int(head[0])
+    ctg = np.array([list(map(int, l.split())) for l in out[1:1 + ncontig]], np.int64).reshape(-1, 4)
+    nscaff, hdrtot = (int(x) for x in out[1 + ncontig].split())
+    scf, names = [], []
+    for l in out[2 + ncontig:2 + ncontig + nscaff]:
+        f = l.split(" ", 4)
+        scf.append([int(x) for x in f[:4]])
+        names.append(f[4] if len(f) > 4 else "")
+    with open(head[7], "rb") as f:
+        bps = np.frombuffer(f.read(), np.uint8)
+    return {"ncontig": ncontig, "maxctg": int(head[1]), "seqtot": int(head[2]),
+            "freq": np.array([float(x) for x in head[3:7]], np.float32),
+            "contigs": ctg, "scaffolds": np.array(scf, np.int64).reshape(-1, 4),
+            "names": names, "hdrtot": hdrtot, "bps": bps}
 
 
 def ref_gdbdump(stem: str):

@@ -372,3 +372,191 @@ int orc_reimport_sort(const uint8_t *seeds, int64_t len, int posb, int ctgb, int
     }
   return swide;
 }
+
+/* ---- Create_GDB's FASTA reader ------------------------------------------ */
+
+/* Base value of a sequence character (lib/GDB.c:350-367): A/a 0, C/c 1,
+ * G/g 2, T/t 3, N/n 4 (not a base), every other character 0. */
+static int fa_value(int c)
+{ switch (c)
+    { case 'C': case 'c': return 1;
+      case 'G': case 'g': return 2;
+      case 'T': case 't': return 3;
+      case 'N': case 'n': return 4;
+      default:            return 0;
+    }
+}
+
+static int fa_isspace(int c)
+{ return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+
+typedef struct
+  { int64_t *ctg4, ctg_cap, ncontig;
+    uint8_t *bps;
+    int64_t  bps_cap, boff;     /* bytes written so far */
+    int      m;                 /* bits used in the partial byte */
+    uint8_t  byte;
+    int64_t  count[4];
+    int64_t  maxctg;
+    int      over;
+  } FaState;
+
+/* Appends base v to the current contig's bytes (lib/GDB.c:960-977). */
+static void fa_put(FaState *F, int v)
+{ F->byte |= (uint8_t) (v << F->m);
+  if (F->m == 6)
+    { if (F->boff < F->bps_cap) F->bps[F->boff] = F->byte; else F->over = 1;
+      F->boff += 1;
+      F->m = 0;
+      F->byte = 0;
+    }
+  else
+    F->m += 2;
+  F->count[v] += 1;
+}
+
+/* Ends the current contig: flushes its partial byte and records it
+ * (lib/GDB.c:897-956). */
+static void fa_close(FaState *F, int64_t clen, int64_t sbeg, int64_t bpos, int64_t scaf)
+{ if (F->m > 0)
+    { if (F->boff < F->bps_cap) F->bps[F->boff] = F->byte; else F->over = 1;
+      F->boff += 1;
+    }
+  F->byte = 0;
+  F->m = 0;
+  if (F->ncontig < F->ctg_cap)
+    { int64_t *c = F->ctg4 + 4 * F->ncontig;
+      c[0] = clen;
+      c[1] = bpos;
+      c[2] = sbeg;
+      c[3] = scaf;
+    }
+  else
+    F->over = 1;
+  F->ncontig += 1;
+  if (clen > F->maxctg) F->maxctg = clen;
+}
+
+/* The reader works line by line as read_line (lib/GDB.c:372-439) does: a line
+ * must end with a new-line.  Within a scaffold the N runs of its lines join
+ * into one run across line ends (lib/GDB.c:850-876): a run of length L that
+ * is followed by a base is a gap, filled with L A's when L < nthr
+ * (lib/GDB.c:879-897) and otherwise ending the current contig
+ * (lib/GDB.c:898-956), so a scaffold that opens with such a run has an
+ * empty first contig; the run that ends a scaffold is dropped
+ * (lib/GDB.c:853-857, lib/GDB.c:870-874, lib/GDB.c:947-950).  A scaffold
+ * without any base is an error (lib/GDB.c:1039-1043).  NUL and non-ASCII
+ * bytes, which the reference does not read as characters, are refused. */
+int orc_fasta_gdb(const char *text, int64_t n, int nthr,
+                  int64_t *scf4, int64_t scf_cap, int64_t *ctg4, int64_t ctg_cap,
+                  char *hdr, int64_t hdr_cap, uint8_t *bps, int64_t bps_cap,
+                  int64_t *sizes6, int64_t *count4, char *err, int errlen)
+{ FaState F;
+  int64_t pos, nscaff, hdrtot, i;
+  int     over;
+
+  memset(&F, 0, sizeof(F));
+  F.ctg4 = ctg4;
+  F.ctg_cap = ctg_cap;
+  F.bps = bps;
+  F.bps_cap = bps_cap;
+  nscaff = 0;
+  hdrtot = 0;
+  over = 0;
+  if (err && errlen > 0) err[0] = '\0';
+
+  if (n <= 0)
+    { if (err) snprintf(err, errlen, "input is empty");
+      return -1;
+    }
+  for (i = 0; i < n; i++)
+    if (text[i] == 0 || (uint8_t) text[i] >= 128)
+      { if (err) snprintf(err, errlen, "byte %lld is NUL or not ASCII", (long long) i);
+        return -1;
+      }
+  if (text[n - 1] != '\n')
+    { if (err) snprintf(err, errlen, "last line does not end with new-line");
+      return -1;
+    }
+  if (text[0] != '>')
+    { if (err) snprintf(err, errlen, "first header is missing");
+      return -1;
+    }
+
+  pos = 0;
+  while (pos < n)
+    { /* header line: text after '>' and any white space (lib/GDB.c:815-834) */
+      int64_t e = pos;
+      int64_t s, len, clen, spos, bpos, pend;
+      while (text[e] != '\n') e += 1;
+      len = e - pos;
+      for (s = 1; s < len; s++)
+        if (!fa_isspace(text[pos + s])) break;
+      if (nscaff < scf_cap)
+        { scf4[4 * nscaff + 0] = F.ncontig;
+          scf4[4 * nscaff + 3] = hdrtot;
+        }
+      else
+        over = 1;
+      if (hdrtot + (len - s) + 1 <= hdr_cap)
+        { memcpy(hdr + hdrtot, text + pos + s, (size_t) (len - s));
+          hdr[hdrtot + len - s] = '\0';
+        }
+      else
+        over = 1;
+      hdrtot += len - s + 1;
+      pos = e + 1;
+
+      /* sequence lines up to the next header or the end */
+      clen = 0;
+      spos = 0;
+      bpos = F.boff;
+      pend = 0;
+      while (pos < n && text[pos] != '>')
+        { for (; text[pos] != '\n'; pos++)
+            { int v = fa_value(text[pos]);
+              if (v == 4)
+                { pend += 1;
+                  continue;
+                }
+              if (pend > 0)
+                { if (pend < nthr)
+                    { int64_t x;
+                      for (x = 0; x < pend; x++) fa_put(&F, 0);
+                      clen += pend;
+                    }
+                  else
+                    { fa_close(&F, clen, spos, bpos, nscaff);
+                      spos += clen + pend;
+                      bpos = F.boff;
+                      clen = 0;
+                    }
+                  pend = 0;
+                }
+              fa_put(&F, v);
+              clen += 1;
+            }
+          pos += 1;
+        }
+      fa_close(&F, clen, spos, bpos, nscaff);
+      spos += clen;
+      if (spos == 0)
+        { if (err) snprintf(err, errlen, "scaffold %lld has no sequence", (long long) nscaff);
+          return -1;
+        }
+      if (nscaff < scf_cap)
+        { scf4[4 * nscaff + 1] = F.ncontig;
+          scf4[4 * nscaff + 2] = spos;
+        }
+      nscaff += 1;
+    }
+
+  sizes6[0] = nscaff;
+  sizes6[1] = F.ncontig;
+  sizes6[2] = F.boff;
+  sizes6[3] = hdrtot;
+  sizes6[4] = F.maxctg;
+  sizes6[5] = F.count[0] + F.count[1] + F.count[2] + F.count[3];
+  for (i = 0; i < 4; i++) count4[i] = F.count[i];
+  return (over || F.over) ? -2 : 0;
+}

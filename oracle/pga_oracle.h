@@ -1,6 +1,6 @@
 /* CPU restatement of DistributedPanGA's FastGA alignment path, stages
  * extract -> index sort + LCP -> k-mer table view -> adaptamer seed merge ->
- * seed reimport + diagonal sort.
+ * seed reimport + diagonal sort, and of the GDB's FASTA reader.
  *
  * TEST INFRASTRUCTURE ONLY.  This is the oracle the CUDA path is checked
  * against; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
@@ -81,6 +81,22 @@ int orc_reimport_sort(const uint8_t *seeds, int64_t len, int posb, int ctgb, int
 /* swide and DBYTE for a contig set (src/pga-mpi-merge.c:415-425,
  * src/fastga_pipeline.c:1736). */
 void orc_diag_sizing(int64_t maxctg, int ctgb, int *dbyte, int *swide);
+
+/* Create_GDB's FASTA reader (lib/GDB.c:771-1057, base table lib/GDB.c:350-367)
+ * on an in-memory text, with nthr as given (the reference's own callers pass
+ * 0, lib/GDB.c:1662):
+ *   scf4  nscaff x {fctg, ectg, slen, hoff}   (GDB_SCAFFOLD, lib/GDB.h:36-43)
+ *   ctg4  ncontig x {clen, boff, sbeg, scaf}  (GDB_CONTIG, lib/GDB.h:28-34)
+ *   hdr   the header bytes, each ended by '\0'
+ *   bps   the 2-bit image, LSB-first, each contig from a fresh byte
+ *   sizes {nscaff, ncontig, bps bytes, hdrtot, maxctg, seqtot}
+ *   count bases per value A C G T (filled gap bases count as A)
+ * Returns 0; -1 for an input the reference rejects or cannot read (message in
+ * err); -2 when a capacity is too small. */
+int orc_fasta_gdb(const char *text, int64_t n, int nthr,
+                  int64_t *scf4, int64_t scf_cap, int64_t *ctg4, int64_t ctg_cap,
+                  char *hdr, int64_t hdr_cap, uint8_t *bps, int64_t bps_cap,
+                  int64_t *sizes6, int64_t *count4, char *err, int errlen);
 
 #ifdef __cplusplus
 }
