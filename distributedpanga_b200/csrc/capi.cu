@@ -66,7 +66,7 @@ struct pga_ctx {
   std::vector<int32_t> h_tile_ctg;
 
   // index
-  DBuf hist, start, scan_tmp, rec, rec2, lcp, ent, cum, qmed, qbig, qcount, maxrun, u64tmp;
+  DBuf hist, start, scan_tmp, rec, rec2, lcp, ent, cum, qmed, qbig, qcount, maxrun, u64tmp, coarse;
   int64_t nrec = 0;
   bool have_index = false, have_entries = false;
   int64_t largest = 0;
@@ -219,6 +219,16 @@ int bitlen(uint64_t v) {
 
 // ---- index stages ---------------------------------------------------------
 
+int sort_queued(pga_ctx *ctx);
+
+// Prefixes per k_bucket_rank CTA: a power of two giving about BK_CAP/4
+// records per CTA on average.
+int bucket_run(const pga_ctx *ctx) {
+  int bpc = 1;
+  while (bpc < 4096 && (double)ctx->nrec * (bpc * 2) / NPREFIX <= BK_CAP / 4) bpc *= 2;
+  return bpc;
+}
+
 // Buckets are already scattered by prefix into ctx->rec; `start` holds the
 // exclusive scan (NPREFIX+1 entries).  Sort each bucket.
 int sort_buckets(pga_ctx *ctx) {
@@ -226,15 +236,19 @@ int sort_buckets(pga_ctx *ctx) {
   ENSURE(ctx->qbig, sizeof(uint32_t) * NPREFIX);
   ENSURE(ctx->qcount, sizeof(uint32_t) * 4);
   CK(cudaMemsetAsync(ctx->qcount.p, 0, sizeof(uint32_t) * 4, ctx->st));
-  // prefixes per CTA: a power of two giving about BK_CAP/4 records per CTA on average
-  int bpc = 1;
-  while (bpc < 4096 && (double)ctx->nrec * (bpc * 2) / NPREFIX <= BK_CAP / 4) bpc *= 2;
+  const int bpc = bucket_run(ctx);
   CK(cudaFuncSetAttribute(k_bucket_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, BK_CAP * (int)sizeof(Rec)));
   k_bucket_rank<<<NPREFIX / bpc, BK_THREADS, BK_CAP * sizeof(Rec), ctx->st>>>(
       P<Rec>(ctx->rec), P<uint32_t>(ctx->start), bpc, BK_CAP, P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
       P<uint32_t>(ctx->qcount));
   LAUNCHED(1);
   CK(cudaGetLastError());
+  return sort_queued(ctx);
+}
+
+// The buckets k_bucket_rank / k_big_digit queued: one CTA each up to
+// BK_MEDIUM records, the global bitonic network beyond.
+int sort_queued(pga_ctx *ctx) {
   uint32_t q[4];
   CK(cudaMemcpyAsync(q, ctx->qcount.p, sizeof(q), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
@@ -1375,7 +1389,7 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                   &ctx->qbig, &ctx->qcount, &ctx->maxrun, &ctx->u64tmp, &ctx->blk_n, &ctx->blk_c,
                   &ctx->blk_tmp, &ctx->seed[0], &ctx->seed[1], &ctx->keys[0], &ctx->keys[1],
                   &ctx->keys_alt, &ctx->rhist, &ctx->rscan, &ctx->panel[0], &ctx->panel[1], &ctx->io,
-                  &ctx->io2, &ctx->fa_text, &ctx->fa_mask, &ctx->fa_seq, &ctx->fa_cnt, &ctx->fa_tmp,
+                  &ctx->io2, &ctx->coarse, &ctx->fa_text, &ctx->fa_mask, &ctx->fa_seq, &ctx->fa_cnt, &ctx->fa_tmp,
                   &ctx->fa_tot, &ctx->fa_status, &ctx->fa_hdr, &ctx->fa_hbytes, &ctx->fa_runs, &ctx->fa_ctg};
   for (DBuf *b : bufs)
     if (b->p) cudaFree(b->p);
@@ -1997,40 +2011,81 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb,
 int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
-  ENSURE(ctx->hist, sizeof(uint32_t) * (NPREFIX + 1));
+  ENSURE(ctx->hist, sizeof(uint32_t) * (NDIGIT + 1));
   ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
+  // digit starts (NDIGIT + 1), digit cursors (NDIGIT + 1), digits above DS_CAP
+  // (NDIGIT) and above DS_CAP_MID (NDIGIT)
+  ENSURE(ctx->coarse, sizeof(uint32_t) * (4 * (size_t)NDIGIT + 2));
+  uint32_t *dstart = P<uint32_t>(ctx->coarse), *dcur = dstart + (NDIGIT + 1), *qdig = dcur + (NDIGIT + 1),
+           *qdig2 = qdig + NDIGIT;
+  uint32_t *hist = P<uint32_t>(ctx->hist), *start = P<uint32_t>(ctx->start);
   const uint8_t *bps = P<uint8_t>(ctx->bps);
   const int64_t *cl = P<int64_t>(ctx->dclen), *bo = P<int64_t>(ctx->dboff);
   const int32_t *tc = P<int32_t>(ctx->tile_ctg);
   const int64_t *tj = P<int64_t>(ctx->tile_j0);
   stage_begin(ctx, ST_EXTRACT_HIST);
-  CK(cudaMemsetAsync(ctx->hist.p, 0, sizeof(uint32_t) * NPREFIX, ctx->st));
+  CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (NDIGIT + 1), ctx->st));
   if (ctx->ntiles > 0) {
-    launch_extract(EXT_HIST, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr,
-                   P<uint32_t>(ctx->hist), nullptr);
+    launch_extract(EXT_HIST, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr, hist,
+                   nullptr);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_HIST);
   CK(cudaGetLastError());
   stage_begin(ctx, ST_SCAN);
-  int64_t n = 0;
-  int r = scan_hist(ctx, &n);
-  if (r) return r;
+  ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(NDIGIT + 1));
+  CK(exclusive_scan<uint32_t>(hist, dstart, NDIGIT + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr, ctx->st));
+  LAUNCHED(3);
+  CK(cudaMemcpyAsync(dcur, dstart, sizeof(uint32_t) * NDIGIT, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemcpyAsync(start + NPREFIX, dstart + NDIGIT, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->st));
+  uint32_t total = 0;
+  CK(cudaMemcpyAsync(&total, dstart + NDIGIT, 4, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   stage_end(ctx, ST_SCAN);
-  r = check_records_fit(ctx, n);
+  const int64_t n = total;
+  int r = check_records_fit(ctx, n);
   if (r) return r;
   ctx->nrec = n;
   ENSURE(ctx->rec, sizeof(Rec) * (size_t)n + 16);
+  // level 1: every record into its digit's region
   stage_begin(ctx, ST_EXTRACT_SCATTER);
   if (ctx->ntiles > 0) {
-    launch_extract(EXT_SCATTER, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
-                   P<Rec>(ctx->rec), nullptr, P<uint32_t>(ctx->hist));
+    launch_extract(EXT_DIGIT, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
+                   P<Rec>(ctx->rec), nullptr, dcur);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_SCATTER);
   CK(cudaGetLastError());
+  // level 2: each digit sorted in shared memory; larger digits grouped by
+  // prefix in global memory and their buckets queued
   stage_begin(ctx, ST_BUCKET);
-  r = sort_buckets(ctx);
+  ENSURE(ctx->qmed, sizeof(uint32_t) * NPREFIX);
+  ENSURE(ctx->qbig, sizeof(uint32_t) * NPREFIX);
+  ENSURE(ctx->qcount, sizeof(uint32_t) * 8);
+  CK(cudaMemsetAsync(ctx->qcount.p, 0, sizeof(uint32_t) * 8, ctx->st));
+  uint32_t *qc = P<uint32_t>(ctx->qcount);
+  CK(launch_digit_sort(DS_CAP, NDIGIT, DS_THREADS, ctx->st, P<Rec>(ctx->rec), dstart, start, nullptr, qdig, qc + 4));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  uint32_t q[8];
+  CK(cudaMemcpyAsync(q, qc, sizeof(q), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (q[4] > 0) {
+    CK(launch_digit_sort(DS_CAP_MID, (int)q[4], DS_MID_THREADS, ctx->st, P<Rec>(ctx->rec), dstart, start, qdig,
+                         qdig2, qc + 5));
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(q, qc, sizeof(q), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  if (q[5] > 0) {
+    ENSURE(ctx->rec2, sizeof(Rec) * (size_t)n + 16);
+    k_big_digit<<<q[5], BD_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), dstart, start, qdig2, P<Rec>(ctx->rec2),
+                                                  P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig), qc);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+  }
+  r = sort_queued(ctx);
   if (r) return r;
   stage_end(ctx, ST_BUCKET);
   r = finish_index(ctx, want_entries != 0);

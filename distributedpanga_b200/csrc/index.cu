@@ -7,10 +7,13 @@
 //   run_stage2 sort + LCP  src/dsort.c:369-518, src/sort.c:38-115, lib/MSDsort.c:404-507
 //   build_kmer_adapter     src/kmer_adapter.c:6-96
 //
-// The MPI bucket exchange of run_stage2 becomes the first (24-bit prefix)
-// pass of an in-HBM MSD sort: a histogram of the prefixes, its exclusive
-// scan (which is also the k-mer table's cumulative prefix index), a scatter
-// of the records into their prefix buckets, and a per-bucket finishing sort.
+// The MPI bucket exchange of run_stage2 becomes an in-HBM MSD sort in two
+// levels: a histogram of the 18-bit digits (the first 9 bases), a scatter of
+// every record into its digit's region as it is extracted, then a sort of
+// each digit's region in shared memory that also writes the 24-bit prefix
+// table (the k-mer table's cumulative prefix index).  Records extracted from
+// the host's byte format go through the one-level path: prefix histogram,
+// scatter into the prefix buckets, per-bucket finishing sort.
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "common.cuh"
@@ -146,9 +149,9 @@ k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
             if (MODE == EXT_WRITE) {
               out[woff++] = r;
             } else if (MODE == EXT_HIST) {
-              atomicAdd(&hist[rec_prefix(r)], 1u);
-            } else {  // EXT_SCATTER
-              uint32_t slot = atomicAdd(&cursor[rec_prefix(r)], 1u);
+              atomicAdd(&hist[rec_prefix(r) >> DIGIT_SHIFT], 1u);
+            } else {  // EXT_DIGIT
+              uint32_t slot = atomicAdd(&cursor[rec_prefix(r) >> DIGIT_SHIFT], 1u);
               out[slot] = r;
             }
           }
@@ -180,8 +183,8 @@ void launch_extract(int mode, int ntiles, cudaStream_t st, const uint8_t *bps, c
                                                           offsets, out, hist, cursor);
       break;
     default:
-      k_extract<EXT_SCATTER><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
-                                                             offsets, out, hist, cursor);
+      k_extract<EXT_DIGIT><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
+                                                           offsets, out, hist, cursor);
   }
 }
 
@@ -203,6 +206,123 @@ __global__ void k_prefix_scatter(const Rec *__restrict__ in, int64_t n, uint32_t
     Rec r = in[i];
     uint32_t slot = atomicAdd(&cursor[rec_prefix(r)], 1u);
     out[slot] = r;
+  }
+}
+
+// Exclusive scan of up to 64 counts by one warp (two per lane).
+__device__ __forceinline__ void warp_scan64(const uint32_t *cnt, uint32_t *off, uint32_t total) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t c0 = cnt[2 * lane], c1 = cnt[2 * lane + 1];
+  uint32_t x = c0 + c1;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  const uint32_t pre = x - c0 - c1;
+  off[2 * lane] = pre;
+  off[2 * lane + 1] = pre + c0;
+  if (lane == 0) off[DIGIT_PREFIXES] = total;
+}
+
+template <int CAP>
+__global__ void __launch_bounds__(1024)
+k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t *__restrict__ start,
+             const uint32_t *__restrict__ list, uint32_t *__restrict__ qnext, uint32_t *__restrict__ qnext_count) {
+  extern __shared__ Rec sa[];                              // CAP records
+  uint16_t *sb = reinterpret_cast<uint16_t *>(sa + CAP);  // CAP record indices grouped by prefix
+  __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
+  static_assert(DIGIT_PREFIXES == 64, "warp_scan64 covers 64 prefixes");
+  static_assert(CAP <= 65536, "16-bit record indices");
+  const uint32_t d = list ? list[blockIdx.x] : blockIdx.x;
+  const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
+  if (m > (uint32_t)CAP) {
+    if (threadIdx.x == 0) qnext[atomicAdd(qnext_count, 1u)] = d;
+    return;
+  }
+  if (threadIdx.x < DIGIT_PREFIXES) scur[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+    const Rec r = rec[ds + i];
+    sa[i] = r;
+    atomicAdd(&scur[rec_prefix(r) & (DIGIT_PREFIXES - 1)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) warp_scan64(scur, soff, m);
+  __syncthreads();
+  if (threadIdx.x < DIGIT_PREFIXES) {
+    start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];
+    scur[threadIdx.x] = soff[threadIdx.x];
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x)
+    sb[atomicAdd(&scur[rec_prefix(sa[i]) & (DIGIT_PREFIXES - 1)], 1u)] = (uint16_t)i;
+  __syncthreads();
+  // each record's rank among its prefix bucket (records are distinct)
+  for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+    const Rec x = sa[sb[k]];
+    const uint32_t q = rec_prefix(x) & (DIGIT_PREFIXES - 1);
+    const uint32_t gs = soff[q], ge = soff[q + 1];
+    uint32_t rank = 0;
+    for (uint32_t j = gs; j < ge; j++) rank += rec_less(sa[sb[j]], x) ? 1u : 0u;
+    rec[ds + gs + rank] = x;
+  }
+}
+
+template <int CAP>
+cudaError_t launch_cap(int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart, uint32_t *start,
+                       const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count) {
+  const size_t smem = (size_t)CAP * (sizeof(Rec) + sizeof(uint16_t));
+  PGA_CUDA_TRY(cudaFuncSetAttribute(k_digit_sort<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_digit_sort<CAP><<<grid, threads, smem, st>>>(rec, dstart, start, list, qnext, qnext_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart,
+                              uint32_t *start, const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count) {
+  switch (cap) {
+    case DS_CAP: return launch_cap<DS_CAP>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count);
+    case DS_CAP_MID: return launch_cap<DS_CAP_MID>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+__global__ void __launch_bounds__(BD_THREADS)
+k_big_digit(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t *__restrict__ start,
+            const uint32_t *__restrict__ list, Rec *__restrict__ tmp_all, uint32_t *__restrict__ qmed,
+            uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount) {
+  __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
+  const uint32_t d = list[blockIdx.x];
+  const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
+  Rec *tmp = tmp_all + ds;
+  if (threadIdx.x < DIGIT_PREFIXES) scur[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS)
+    atomicAdd(&scur[rec_prefix(rec[ds + i]) & (DIGIT_PREFIXES - 1)], 1u);
+  __syncthreads();
+  if (threadIdx.x < 32) warp_scan64(scur, soff, m);
+  __syncthreads();
+  if (threadIdx.x < DIGIT_PREFIXES) {
+    start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];
+    scur[threadIdx.x] = soff[threadIdx.x];
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS) {
+    const Rec r = rec[ds + i];
+    tmp[atomicAdd(&scur[rec_prefix(r) & (DIGIT_PREFIXES - 1)], 1u)] = r;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS) rec[ds + i] = tmp[i];
+  if (threadIdx.x < DIGIT_PREFIXES) {
+    const uint32_t n = soff[threadIdx.x + 1] - soff[threadIdx.x];
+    const uint32_t p = (d << DIGIT_SHIFT) + threadIdx.x;
+    if (n > 1) {
+      if (n <= BK_MEDIUM) qmed[atomicAdd(&qcount[0], 1u)] = p;
+      else {
+        qbig[atomicAdd(&qcount[1], 1u)] = p;
+        atomicMax(&qcount[2], n);
+      }
+    }
   }
 }
 

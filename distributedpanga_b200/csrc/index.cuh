@@ -6,7 +6,23 @@
 
 namespace pga {
 
-enum { EXT_COUNT = 0, EXT_WRITE = 1, EXT_HIST = 2, EXT_SCATTER = 3 };
+enum { EXT_COUNT = 0, EXT_WRITE = 1, EXT_HIST = 2, EXT_DIGIT = 3 };
+
+// Two-level bucketing of the extracted records.  EXT_HIST counts records per
+// digit (the top DIGIT_BITS bits of the 24-bit prefix); EXT_DIGIT writes each
+// record into its digit's region -- where its prefix buckets lie in the
+// sorted index -- through one cursor per digit (the 2^18 write fronts stay
+// in L2, which merges the 16-byte writes into whole lines); k_digit_sort then
+// sorts every digit's region in shared memory and writes the prefix table.
+constexpr int DIGIT_BITS = 18;
+constexpr int DIGIT_SHIFT = 24 - DIGIT_BITS;
+constexpr int NDIGIT = 1 << DIGIT_BITS;
+constexpr int DIGIT_PREFIXES = 1 << DIGIT_SHIFT;  // 24-bit prefixes per digit
+constexpr int DS_THREADS = 256;
+constexpr int DS_CAP = 2048;                     // records a k_digit_sort CTA sorts (36 KB of shared memory)
+constexpr int DS_MID_THREADS = 1024;
+constexpr int DS_CAP_MID = 8192;                 // the same for the digits above DS_CAP (144 KB)
+constexpr int BD_THREADS = 1024;                 // k_big_digit
 
 constexpr int EXT_THREADS = 256;                   // threads per extraction CTA
 constexpr int EXT_PER = 32;                        // syncmer offsets per thread
@@ -26,6 +42,16 @@ void launch_extract(int mode, int ntiles, cudaStream_t st, const uint8_t *bps, c
                     uint32_t *counts, const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor);
 __global__ void k_prefix_hist(const Rec *rec, int64_t n, uint32_t *hist);
 __global__ void k_prefix_scatter(const Rec *in, int64_t n, uint32_t *cursor, Rec *out);
+// Sorts the region of digit d (list[blockIdx.x], or blockIdx.x when list is
+// null) in place when it holds at most cap (DS_CAP or DS_CAP_MID) records and writes start[] for its DIGIT_PREFIXES prefixes; a larger digit
+// is appended to qnext (count *qnext_count).
+cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart,
+                              uint32_t *start, const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count);
+// One CTA per digit of `list` (tmp_all: scratch as large as rec): start[]
+// for its prefixes, records grouped by prefix, buckets of more than one
+// record queued for k_bucket_medium / k_bucket_big_step.
+__global__ void k_big_digit(Rec *rec, const uint32_t *dstart, uint32_t *start, const uint32_t *list, Rec *tmp_all,
+                            uint32_t *qmed, uint32_t *qbig, uint32_t *qcount);
 __global__ void k_bucket_rank(Rec *rec, const uint32_t *start, int bpc, int cap, uint32_t *qmed,
                               uint32_t *qbig, uint32_t *qcount);
 __global__ void k_bucket_medium(Rec *rec, const uint32_t *start, const uint32_t *qmed);

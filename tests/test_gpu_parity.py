@@ -108,6 +108,30 @@ def test_degenerate_inputs(dev, oracle):
     assert np.array_equal(dev.extract_to_records(), oracle.extract(cs, posb, ctgb))
 
 
+def test_index_skewed_digits(dev, oracle):
+    """Digits (first 9 bases) of every size class of the two-level sort: a
+    poly-A run puts ~30,000 records into one digit and one prefix bucket (the
+    global path and the bitonic network), tandem copies of a 9-base unit put
+    thousands into a few digits (the 8192-record shared-memory class), random
+    sequence fills the rest.  Equal to the oracle's sorted index."""
+    from distributedpanga_b200 import gdb
+    rng = np.random.default_rng(29)
+    unit = np.array([0, 1, 2, 3, 3, 2, 1, 0, 3], np.uint8)
+    contigs = [np.zeros(30000, np.uint8), np.tile(unit, 5000),
+               np.concatenate([np.tile(unit[:5], 3000), rng.integers(0, 4, 500).astype(np.uint8)])]
+    contigs += [rng.integers(0, 4, n).astype(np.uint8) for n in (50000, 20000, 777)]
+    cs = gdb.from_contigs(contigs)
+    posb, ctgb, _ = gdb.record_sizing(cs)
+    dev.gdb_load(cs)
+    n = dev.index_build(want_entries=True)
+    want = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    assert n == want.shape[0]
+    assert np.array_equal(dev.index_records(), want)
+    ent, cum, big = dev.index_entries()
+    oent, ocum, obig = oracle.build_adapter(want, posb, ctgb)
+    assert np.array_equal(ent, oent) and np.array_equal(cum, ocum) and big == obig
+
+
 def test_sort_matches_property_at_scale(dev):
     """Size-independent properties of the index at 2 x 20 Mbp: sorted order,
     LCPs equal to the recomputed bases-in-common, prefix table consistent."""
