@@ -40,7 +40,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "aligned Mbp/s per B200 (input bases of both genomes / end-to-end seconds, plain method)"
 UNIT = "Mbp/s"
-WORKLOAD = "chromset: 2 x 100 Mbp, 40% GC, log-normal contigs (median 2 Mbp, sigma 1), 10% repeats; k=40, FREQ=10"
+WORKLOADS = {
+    "chromset": "chromset: 2 x 100 Mbp, 40% GC, log-normal contigs (median 2 Mbp, sigma 1), 10% repeats; k=40, FREQ=10",
+    "full": "full: 2 x 1 Gbp, uniform ACGT, contigs U[50, 500] kbp, 40% interspersed repeats, 3% tandem arrays, "
+            "B = A at 2% substitutions + 0.5% indels + 20 inversions; k=40, FREQ=10",
+}
+WL = {"name": "chromset"}  # the workload of this run (--workload)
 
 
 def peaks():
@@ -107,11 +112,11 @@ class ClockSampler:
 
 def make_contigs(scale: float):
     from distributedpanga_b200 import gdb, synth
-    cache = os.path.join(tempfile.gettempdir(), "pga_chromset_%g.npz" % scale)
+    cache = os.path.join(tempfile.gettempdir(), "pga_%s_%g.npz" % (WL["name"], scale))
     if os.path.exists(cache):
         z = np.load(cache)
         return gdb.ContigSet(bps=z["bps"], clen=z["clen"], boff=z["boff"], freq=z["freq"]), None
-    contigs = synth.make("chromset", scale=scale)
+    contigs = synth.make(WL["name"], scale=scale)
     cs = gdb.from_contigs(contigs)
     try:
         np.savez(cache, bps=cs.bps, clen=cs.clen, boff=cs.boff, freq=cs.freq)
@@ -120,10 +125,10 @@ def make_contigs(scale: float):
     return cs, contigs
 
 
-def index_bytes(cs, nrec: int) -> float:
+def index_bytes(cs, nrec: int, entries: bool = True) -> float:
     from distributedpanga_b200 import gdb
     posb, ctgb, rsize = gdb.record_sizing(cs)
-    ebytes = rsize - 3
+    ebytes = rsize - 3 if entries else 0
     return (cs.seqtot + 3) // 4 + 5.0 * nrec * rsize + nrec * ebytes + (1 << 27)
 
 
@@ -139,7 +144,7 @@ class ReferenceSample:
         from distributedpanga_b200 import gdb, synth
         from oracle import binding as orc
         self.tmp = tempfile.TemporaryDirectory()
-        contigs = synth.make("chromset", scale=scale)
+        contigs = synth.make(WL["name"], scale=scale)
         self.mbp = gdb.from_contigs(contigs).seqtot / 1e6
         fa = os.path.join(self.tmp.name, "s.fa")
         self.stem = os.path.join(self.tmp.name, "s")
@@ -176,7 +181,7 @@ def port_sample(scale: float):
     """The oracle's C restatement on a sample; returns (Mbp, seconds)."""
     from distributedpanga_b200 import gdb, synth
     from oracle import binding as orc
-    cs = gdb.from_contigs(synth.make("chromset", scale=scale))
+    cs = gdb.from_contigs(synth.make(WL["name"], scale=scale))
     posb, ctgb, _ = gdb.record_sizing(cs)
     dbyte, _ = gdb.diag_sizing(cs, ctgb)
     t0 = time.time()
@@ -196,14 +201,14 @@ def cpu_baseline(sample_scale: float) -> dict:
         sec = min(r.run() for _ in range(2))
         mbp = r.mbp
         return {"value": mbp / sec, "unit": UNIT, "cores": 4, "kind": "reference",
-                "sample": "chromset generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
+                "sample": WL["name"] + " generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
                           "(oracle/_ref), whole path (its TOTAL stage time: extract, sort, merge, alignments); "
                           "msd_sort uses 4 threads, the rest 1; host has %d cores" % (sample_scale, mbp, cores_total),
                 "seconds": sec}
     orc.build()
     mbp, sec = port_sample(sample_scale)
     return {"value": mbp / sec, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "chromset generator at scale %g (%.1f Mbp), oracle C restatement, 1 thread; host has %d cores"
+            "sample": WL["name"] + " generator at scale %g (%.1f Mbp), oracle C restatement, 1 thread; host has %d cores"
                       % (sample_scale, mbp, cores_total), "seconds": sec}
 
 
@@ -328,9 +333,9 @@ def run_reference(args, rank: int) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mbp / v * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "sample_scale": args.ref_scale},
+            "config": {"workload": WORKLOADS[WL["name"]], "sample_scale": args.ref_scale},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": "chromset generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)},
+                             "sample": WL["name"] + " generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     emit(rank, line)
 
@@ -389,7 +394,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     dev.gdb_load(cs)
 
     def step():
-        dev.index_build(want_entries=True)
+        dev.index_build(want_entries=not args.no_entries)
         dev.merge(10)
         dev.diag_sort(0)
         dev.diag_sort(1)
@@ -440,7 +445,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         dev.gdb_load(cs)
-        dev.index_build(want_entries=True)
+        dev.index_build(want_entries=not args.no_entries)
         dev.merge(10)
         swide, _ = dev.diag_sort(0)
         dev.diag_sort(1)
@@ -464,7 +469,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ingest = run_ingest(dev, cs, args, stream, peak, peak_kind, not args.no_cpu_baseline)
     idx_ms = sum(st[k] for k in ("extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
                                  "entries_prefix_table"))
-    ab = index_bytes(cs, nrec)
+    ab = index_bytes(cs, nrec, not args.no_entries)
     achieved = ab / (idx_ms / 1000.0) / 1e9
     traffic = None
     try:
@@ -482,8 +487,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, chromset workload)",
-        "config": {"workload": WORKLOAD, "scale": args.scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, %s workload)" % WL["name"],
+        "config": {"workload": WORKLOADS[WL["name"]], "scale": args.scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
                    "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
                    "pairs": astats["pairs"], "self_pairs": astats["self_pairs"],
                    "local_alignment_calls": astats["calls"], "alignments": astats["alignments"],
@@ -517,10 +522,18 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = 2 x 100 Mbp)")
-    ap.add_argument("--ref-scale", type=float, default=0.02, help="CPU sample scale")
+    ap.add_argument("--workload", default="chromset", choices=sorted(WORKLOADS),
+                    help="chromset (2 x 100 Mbp, the default) or full (2 x 1 Gbp)")
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the workload's full size)")
+    ap.add_argument("--ref-scale", type=float, default=None,
+                    help="CPU sample scale (default 0.02 of chromset, 0.002 of full)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-entries", action="store_true",
+                    help="do not write the reference-format k-mer table entries (saves N x E bytes of HBM)")
     args = ap.parse_args()
+    WL["name"] = args.workload
+    if args.ref_scale is None:
+        args.ref_scale = 0.02 if args.workload == "chromset" else 0.002
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

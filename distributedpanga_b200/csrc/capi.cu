@@ -75,6 +75,7 @@ struct pga_ctx {
   DBuf blk_n, blk_c, blk_tmp, seed[2];
   int64_t nseed[2] = {0, 0};
   bool have_seeds = false;
+  bool seeds_released = false;  // release_for_align freed the unsorted seeds
   int freq = 0;
 
   // diagonal sort
@@ -432,6 +433,7 @@ int run_merge(pga_ctx *ctx, int freq) {
   stage_end(ctx, ST_MERGE);
   CK(cudaGetLastError());
   ctx->have_seeds = true;
+  ctx->seeds_released = false;
   ctx->freq = freq;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
   return PGA_OK;
@@ -877,7 +879,17 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
   ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * 16384);
   ENSURE(ctx->perm, sizeof(int) * 2 * (size_t)L.nwarps * 16384);
   ENSURE(ctx->rng_ovl, sizeof(aln::Ovl) * (size_t)std::max<int64_t>(1 << 18, seqtot / 256));
-  ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)std::max<int64_t>(1 << 24, 4 * seqtot));
+  {
+    // 4 pebbles per input base to start, within what pebble numbers (int)
+    // address and a third of the free memory; an overflow grows the pool
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    int64_t want = std::max<int64_t>(1 << 24, 4 * seqtot);
+    want = std::min<int64_t>(want, 0x7fffffff);
+    const int64_t have = (int64_t)((free_b + ctx->cells.cap) / 3 / sizeof(aln::Pebble));
+    want = std::max<int64_t>(1 << 24, std::min(want, have));
+    ENSURE(ctx->cells, sizeof(aln::Pebble) * (size_t)want);
+  }
   ENSURE(ctx->cand, (size_t)std::max<int64_t>(64 << 20, 2 * seqtot));
   ENSURE(ctx->recs, sizeof(AlnRec) * (size_t)std::max<int64_t>(1 << 20, seqtot / 256));
   ENSURE(ctx->outb, (size_t)std::max<int64_t>(64 << 20, seqtot / 8));
@@ -915,6 +927,27 @@ double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Frees what the alignment no longer reads once both diagonal sorts are done
+// -- the index (records, LCPs, entries, scratch) and the unsorted seeds -- so
+// that a genome too large for all stages' buffers at once still aligns.
+// Returns whether anything was freed.
+bool release_for_align(pga_ctx *ctx) {
+  if (!ctx->have_diag[0] || !ctx->have_diag[1]) return false;
+  std::vector<DBuf *> bufs = {&ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->seed[0], &ctx->seed[1]};
+  if (ctx->sorted[0] != ctx->keys_alt.p && ctx->sorted[1] != ctx->keys_alt.p) bufs.push_back(&ctx->keys_alt);
+  bool any = false;
+  for (DBuf *b : bufs)
+    if (b->p) {
+      cudaFree(b->p);
+      b->p = nullptr;
+      b->cap = 0;
+      any = true;
+    }
+  ctx->have_index = ctx->have_entries = false;
+  ctx->seeds_released = true;
+  return any;
+}
+
 int run_align(pga_ctx *ctx) {
   const double t_start = now_ms();
   const int nc = ctx->ncontig;
@@ -927,11 +960,29 @@ int run_align(pga_ctx *ctx) {
       int r = pga_diag_sort(ctx, comp, &sw, &cnt);
       if (r) return r;
     }
+  {
+    // the aligner's sequences, pools and pair lists need about 16 bytes per
+    // input base and 8 per seed beyond the sorted seeds; make room first
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    int64_t seqtot = 0;
+    for (int c = 0; c < nc; c++) seqtot += ctx->clen[c];
+    const double need = 16.0 * seqtot + 8.0 * (ctx->nseed[0] + ctx->nseed[1]) + (8ll << 30);
+    if ((double)free_b < need) release_for_align(ctx);
+  }
   // 2. NUMERIC and packed sequences, base frequencies, scoring tables
   int ave_path = 0;
   int r0 = prepare_sequences(ctx, &ave_path);
   if (r0) return r0;
-  // 3. pair lists of both units
+  // 3. work spaces (before the pair lists: running out of memory here is
+  // cheap to recover from)
+  AlignLaunch L;
+  r0 = prepare_workspace(ctx, L, ave_path);
+  if (r0) return r0;
+  ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
+  for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
+
+  // 4. pair lists of both units
   std::vector<PairTask> pairs[2];
   for (int comp = 0; comp < 2; comp++) {
     int64_t n = ctx->nseed[comp];
@@ -973,13 +1024,6 @@ int run_align(pga_ctx *ctx) {
       pairs[comp].push_back(t);
     }
   }
-
-  // 4. work spaces
-  AlignLaunch L;
-  r0 = prepare_workspace(ctx, L, ave_path);
-  if (r0) return r0;
-  ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
-  for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
 
   // 5. Plan.  Pairs of two different contigs (all C pairs, every N pair of
   // two contigs) run in the first launch, large ones as band ranges finished
@@ -2079,9 +2123,19 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
     CK(cudaStreamSynchronize(ctx->st));
   }
   if (q[5] > 0) {
-    ENSURE(ctx->rec2, sizeof(Rec) * (size_t)n + 16);
-    k_big_digit<<<q[5], BD_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), dstart, start, qdig2, P<Rec>(ctx->rec2),
-                                                  P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig), qc);
+    // scratch for the big digits only: digit i of the list at toff[i]
+    std::vector<uint32_t> big(q[5]), hd(NDIGIT + 1);
+    CK(cudaMemcpyAsync(big.data(), qdig2, sizeof(uint32_t) * q[5], cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(hd.data(), dstart, sizeof(uint32_t) * (NDIGIT + 1), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::vector<int64_t> toff(q[5] + 1, 0);
+    for (uint32_t i = 0; i < q[5]; i++) toff[i + 1] = toff[i] + (hd[big[i] + 1] - hd[big[i]]);
+    ENSURE(ctx->rec2, sizeof(Rec) * (size_t)toff[q[5]] + 16);
+    ENSURE(ctx->u64tmp, sizeof(int64_t) * (q[5] + 1));
+    CK(cudaMemcpyAsync(ctx->u64tmp.p, toff.data(), sizeof(int64_t) * (q[5] + 1), cudaMemcpyHostToDevice, ctx->st));
+    k_big_digit<<<q[5], BD_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), dstart, start, qdig2, P<int64_t>(ctx->u64tmp),
+                                                  P<Rec>(ctx->rec2), P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
+                                                  qc);
     LAUNCHED(1);
     CK(cudaGetLastError());
   }
@@ -2132,11 +2186,13 @@ int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds) {
 
 int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck) {
   if (!ctx || !ctx->have_seeds || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
+  if (ctx->seeds_released) return fail(ctx, PGA_ERR_ARG, "seeds were freed for the alignment; run pga_merge again");
   return copy_seeds(ctx, comp, seeds, buck);
 }
 
 int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count) {
   if (!ctx || !ctx->have_seeds || !ctx->have_gdb || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
+  if (ctx->seeds_released) return fail(ctx, PGA_ERR_ARG, "seeds were freed for the alignment; run pga_merge again");
   CK(cudaSetDevice(ctx->device));
   int64_t maxdag = 2 * ctx->maxctg, cum = 1;
   int dbyte = 0;
@@ -2170,6 +2226,10 @@ int pga_align(pga_ctx *ctx, int64_t *nalign) {
   CK(cudaSetDevice(ctx->device));
   stage_begin(ctx, ST_ALIGN);
   int r = run_align(ctx);
+  if (r == PGA_ERR_NOMEM && release_for_align(ctx)) {
+    cudaGetLastError();
+    r = run_align(ctx);
+  }
   if (r) return r;
   stage_end(ctx, ST_ALIGN);
   if (nalign) *nalign = (int64_t)ctx->h_recs.size();

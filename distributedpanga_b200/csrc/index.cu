@@ -289,12 +289,12 @@ cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, R
 
 __global__ void __launch_bounds__(BD_THREADS)
 k_big_digit(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t *__restrict__ start,
-            const uint32_t *__restrict__ list, Rec *__restrict__ tmp_all, uint32_t *__restrict__ qmed,
-            uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount) {
+            const uint32_t *__restrict__ list, const int64_t *__restrict__ toff, Rec *__restrict__ tmp_all,
+            uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount) {
   __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
   const uint32_t d = list[blockIdx.x];
   const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
-  Rec *tmp = tmp_all + ds;
+  Rec *tmp = tmp_all + toff[blockIdx.x];
   if (threadIdx.x < DIGIT_PREFIXES) scur[threadIdx.x] = 0;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS)

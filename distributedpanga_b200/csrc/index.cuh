@@ -47,11 +47,11 @@ __global__ void k_prefix_scatter(const Rec *in, int64_t n, uint32_t *cursor, Rec
 // is appended to qnext (count *qnext_count).
 cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart,
                               uint32_t *start, const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count);
-// One CTA per digit of `list` (tmp_all: scratch as large as rec): start[]
-// for its prefixes, records grouped by prefix, buckets of more than one
-// record queued for k_bucket_medium / k_bucket_big_step.
-__global__ void k_big_digit(Rec *rec, const uint32_t *dstart, uint32_t *start, const uint32_t *list, Rec *tmp_all,
-                            uint32_t *qmed, uint32_t *qbig, uint32_t *qcount);
+// One CTA per digit of `list` (scratch for list[i] at tmp_all + toff[i]):
+// start[] for its prefixes, records grouped by prefix, buckets of more than
+// one record queued for k_bucket_medium / k_bucket_big_step.
+__global__ void k_big_digit(Rec *rec, const uint32_t *dstart, uint32_t *start, const uint32_t *list,
+                            const int64_t *toff, Rec *tmp_all, uint32_t *qmed, uint32_t *qbig, uint32_t *qcount);
 __global__ void k_bucket_rank(Rec *rec, const uint32_t *start, int bpc, int cap, uint32_t *qmed,
                               uint32_t *qbig, uint32_t *qcount);
 __global__ void k_bucket_medium(Rec *rec, const uint32_t *start, const uint32_t *qmed);

@@ -17,6 +17,14 @@ Workloads (sizes in bases):
   B = A at 1.5% substitutions, 0.2% indels (geometric length, mean 3),
   50 inversions and 50 translocations of U[10 kbp, 1 Mbp].
 
+* ``full`` -- two 1 Gbp genomes built as ``small``: A uniform ACGT in contigs
+  of U[50 kbp, 500 kbp], 40% of A overwritten by copies of 300 interspersed
+  repeat families (unit U[300, 6000] bp, copies 10-20% diverged from their
+  consensus) and 3% by tandem arrays (unit U[2, 200] bp, arrays of
+  U[500, 10000] bp, copies 2% diverged); B = A at 2% substitutions, indels
+  at 0.5% of positions (length U[1, 10]) and 20 inverted segments of
+  U[5 kbp, 50 kbp].
+
 ``scale`` shrinks every length of a workload (genome size, contig and SV
 lengths) by the same factor, for parity tests that must finish in seconds.
 """
@@ -169,7 +177,43 @@ def make_chromset(seed: int = 2, scale: float = 1.0) -> list:
     return split_lognormal(rng, a, med, 1.0, lo) + split_lognormal(rng, b, med, 1.0, lo)
 
 
-WORKLOADS = {"small": make_small, "chromset": make_chromset}
+def plant_tandems(rng: np.random.Generator, s: np.ndarray, fraction: float, unit_lo: int, unit_hi: int,
+                  arr_lo: int, arr_hi: int, div: float, gc: float) -> np.ndarray:
+    """Overwrites ``fraction`` of s with tandem arrays: a random unit repeated
+    to the array's length, then ``div`` of its bases substituted."""
+    out = s.copy()
+    n = len(out)
+    target = int(fraction * n)
+    covered = 0
+    while covered < target:
+        unit = random_bases(rng, int(rng.integers(unit_lo, unit_hi + 1)), gc)
+        ln = int(rng.integers(arr_lo, arr_hi + 1))
+        if ln >= n:
+            break
+        arr = substitute(rng, np.resize(unit, ln), div)
+        p = int(rng.integers(0, n - ln))
+        out[p:p + ln] = arr
+        covered += ln
+    return out
+
+
+def make_full(seed: int = 3, scale: float = 1.0) -> list:
+    """A and B of the 2 x 1 Gbp workload, as one list of contigs (A's first)."""
+    rng = np.random.default_rng(seed)
+    g = int(1_000_000_000 * scale)
+    a = random_bases(rng, g)
+    a = plant_repeats(rng, a, 0.40, 300, max(20, int(300 * min(1.0, scale * 10))),
+                      max(40, int(6000 * min(1.0, scale * 10))), 0.10, 0.20, 0.5)
+    a = plant_tandems(rng, a, 0.03, 2, 200, max(50, int(500 * min(1.0, scale * 10))),
+                      max(100, int(10_000 * min(1.0, scale * 10))), 0.02, 0.5)
+    b = substitute(rng, a, 0.02)
+    b = indels(rng, b, 0.005, lambda k: rng.integers(1, 11, size=k), 0.5)
+    b = invert(rng, b, 20, max(40, int(5_000 * scale)), max(80, int(50_000 * scale)))
+    lo, hi = max(200, int(50_000 * scale)), max(400, int(500_000 * scale))
+    return split_uniform(rng, a, lo, hi) + split_uniform(rng, b, lo, hi)
+
+
+WORKLOADS = {"small": make_small, "chromset": make_chromset, "full": make_full}
 
 
 def make(workload: str, seed: int | None = None, scale: float = 1.0) -> list:
