@@ -6,6 +6,7 @@
 //
 // Reference: search_seeds / align_contigs / Local_Alignment
 // (src/fastga_pipeline.c:576-1138, lib/align.c:1423-1576).
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "align.cuh"
@@ -358,6 +359,55 @@ __device__ void finish_and_emit(const AlignLaunch &P, OvlArena &O, int a, int b,
   po.rec_off = (int64_t)r0;
 }
 
+__device__ __forceinline__ PairTask small_task(const AlignLaunch &P, uint64_t code) {
+  const int u = (int)(code >> 63);
+  const int64_t p = (int64_t)(code & 0x7fffffffffffffffull);
+  PairTask t;
+  t.comp = u;
+  t.a = P.pab[u][2 * p];
+  t.b = P.pab[u][2 * p + 1];
+  t.self = 0;
+  t.entry_bepos = 0;
+  t.seg = -1;
+  t.lo = P.pstart[u][p];
+  t.hi = p + 1 < P.npairs[u] ? P.pstart[u][p + 1] : P.nseeds[u];
+  t.slo = t.lo;
+  t.shi = t.hi;
+  return t;
+}
+
+// A warp's running reduction of its device-planned pairs' outcomes (lane 0).
+struct SmallSums {
+  unsigned long long calls = 0, cycles = 0, maxkey = 0, err = 0, waves = 0, cells = 0, bad = ~0ull;
+  __device__ void add(const AlignLaunch &P, const PairTask &tk, const PairOut &po, unsigned t) {
+    calls += (unsigned long long)po.calls;
+    cycles += (unsigned long long)po.cycles;
+    const unsigned long long k = ((unsigned long long)po.cycles << 16) | (unsigned)min(po.calls, 65535);
+    maxkey = k > maxkey ? k : maxkey;
+    if (po.err) {
+      err |= (unsigned long long)po.err;
+      bad = t < bad ? t : bad;
+    }
+    waves += (unsigned long long)po.waves;
+    cells += (unsigned long long)po.cells;
+    if (tk.comp == 0 && po.calls > 0) {
+      const int xa = P.fo_pos[tk.a], xb = P.fo_pos[tk.b];
+      const unsigned long long key = ((unsigned long long)(xb + 1) << 32) | (uint32_t)po.exit_bepos;
+      atomicMax(&P.fo_last[xa], key);
+      if (xb < xa) atomicMax(&P.fo_earlier[xa], key);
+    }
+  }
+  __device__ void flush(const AlignLaunch &P) {
+    if (calls) atomicAdd(&P.sred[0], calls);
+    if (cycles) atomicAdd(&P.sred[1], cycles);
+    if (maxkey) atomicMax(&P.sred[2], maxkey);
+    if (err) atomicOr(&P.sred[3], err);
+    if (waves) atomicAdd(&P.sred[4], waves);
+    if (cells) atomicAdd(&P.sred[5], cells);
+    if (bad != ~0ull) atomicMin(&P.sred[6], bad);
+  }
+};
+
 __global__ void __launch_bounds__(ALIGN_THREADS)
 k_align_pairs(AlignLaunch P) {
   __shared__ BlockSeed s_block[ALIGN_THREADS / 32][32];
@@ -368,13 +418,14 @@ k_align_pairs(AlignLaunch P) {
   WarpWork W = warp_work(P, wid);
 
   OvlArena O = warp_arena(P, wid);
+  SmallSums sums;
 
   while (true) {
     unsigned t = 0;
     if (lane == 0) t = atomicAdd(P.next_task, 1u);
     t = __shfl_sync(FULL, t, 0);
-    if (t >= (unsigned)P.ntasks) break;
-    const PairTask tk = P.tasks[t];
+    if (t >= (unsigned)P.ntasks + (unsigned)P.nsmall) break;
+    const PairTask tk = t < (unsigned)P.ntasks ? P.tasks[t] : small_task(P, P.small[t - P.ntasks]);
     W.err = 0;
     O.err = 0;
     const SeedKeyLayout &L = tk.comp ? P.layC : P.layN;
@@ -424,9 +475,13 @@ k_align_pairs(AlignLaunch P) {
       finish_and_emit(P, O, tk.a, tk.b, tk.comp, po, lane);
       po.cycles = clock64() - t0;
     }
-    if (lane == 0) P.pout[t] = po;
+    if (lane == 0) {
+      if (t < (unsigned)P.ntasks) P.pout[t] = po;
+      else sums.add(P, tk, po, t);
+    }
     __syncwarp();
   }
+  if (lane == 0 && P.nsmall > 0) sums.flush(P);
 }
 
 // Finishes the pairs that ran as band ranges: gathers each pair's candidates
@@ -687,6 +742,98 @@ void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff
   if (ncontig <= 0) return;
   dim3 g(64, ncontig);
   k_numeric<<<g, 256, 0, st>>>(bps, clen, boff, soff, ncontig, fwd, rc);
+}
+
+__device__ __forceinline__ bool pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds,
+                                               int comp, int64_t rs, int64_t p, int64_t *size) {
+  const int64_t lo = pstart[p], hi = p + 1 < np ? pstart[p + 1] : nseeds;
+  *size = hi - lo;
+  return (comp == 0 && pab[2 * p] == pab[2 * p + 1]) || (rs > 0 && hi - lo > rs);
+}
+
+__global__ void k_pair_hostbound(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
+                                 int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ flag) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
+    int64_t size;
+    flag[p] = pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) ? 1u : 0u;
+  }
+}
+
+// out3 per host pair: seeds lo, hi and (anchor << 32 | partner)
+__global__ void k_pair_gather(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
+                              int64_t nseeds, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ idx,
+                              int64_t *__restrict__ out3) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[p]) continue;
+    const int64_t q = idx[p];
+    out3[3 * q] = pstart[p];
+    out3[3 * q + 1] = p + 1 < np ? pstart[p + 1] : nseeds;
+    out3[3 * q + 2] = ((int64_t)pab[2 * p] << 32) | (uint32_t)pab[2 * p + 1];
+  }
+}
+
+// Bin of a device-planned pair: larger pairs in lower bins.
+__device__ __forceinline__ uint32_t small_bin(int64_t size) {
+  return (uint32_t)(SMALL_BINS - 1) - (uint32_t)(size < SMALL_BINS - 1 ? size : SMALL_BINS - 1);
+}
+
+__global__ void k_small_hist(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
+                             int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ hist) {
+  for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = p0 + threadIdx.x;
+    int64_t size = 0;
+    const bool small = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size);
+    const uint32_t bin = small ? small_bin(size) : 0xffffffffu;
+    const unsigned same = __match_any_sync(0xffffffffu, bin);
+    if (small && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], (unsigned)__popc(same));
+  }
+}
+
+__global__ void k_small_scatter(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
+                                int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ cursor,
+                                uint64_t *__restrict__ small) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = p0 + threadIdx.x;
+    int64_t size = 0;
+    const bool small_p = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size);
+    const uint32_t bin = small_p ? small_bin(size) : 0xffffffffu;
+    const unsigned same = __match_any_sync(0xffffffffu, bin);
+    const int leader = __ffs(same) - 1;
+    uint32_t base = 0;
+    if (small_p && lane == leader) base = atomicAdd(&cursor[bin], (unsigned)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    if (small_p)
+      small[base + __popc(same & ((1u << lane) - 1u))] = ((uint64_t)comp << 63) | (uint64_t)p;
+  }
+}
+
+void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                           uint32_t *flag, cudaStream_t st) {
+  if (np <= 0) return;
+  k_pair_hostbound<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp,
+                                                                                     rs, flag);
+}
+
+void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
+                        const uint32_t *idx, int64_t *out3, cudaStream_t st) {
+  if (np <= 0) return;
+  k_pair_gather<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, flag, idx,
+                                                                                  out3);
+}
+
+void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                       uint32_t *hist, cudaStream_t st) {
+  if (np <= 0) return;
+  k_small_hist<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp, rs,
+                                                                                 hist);
+}
+
+void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                          uint32_t *cursor, uint64_t *small, cudaStream_t st) {
+  if (np <= 0) return;
+  k_small_scatter<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp,
+                                                                                     rs, cursor, small);
 }
 
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st) {

@@ -93,7 +93,36 @@ struct AlignLaunch {
   uint8_t *out_bytes;
   unsigned long long *out_next;
   int64_t out_cap;
+  // Pairs planned on the device: task t >= ntasks is pair small[t - ntasks]
+  // (bit 63 its unit, the rest its index in that unit's pair list: seeds
+  // pstart[u][p] .. pstart[u][p + 1] (or nseeds[u]), contigs pab[u][2p],
+  // pab[u][2p + 1]).  Their outcomes are reduced instead of stored:
+  // sred = {calls, cycles, max (cycles << 16 | calls), error bits, waves,
+  // cells, first failing task}; per FastGA order position of an N pair's
+  // anchor, fo_last = the largest fo key (b position + 1 << 32 | exit
+  // bepos) of its pairs that called and fo_earlier = the same over partners
+  // ordered before the anchor.
+  const uint64_t *small;
+  int nsmall;
+  const int64_t *pstart[2];
+  const int32_t *pab[2];
+  int64_t npairs[2], nseeds[2];
+  const int *fo_pos;
+  unsigned long long *sred, *fo_last, *fo_earlier;
 };
+
+// Pair lists on the device: whether the host plans pair p of a unit (a self
+// pair, or one of more than rs seeds when rs > 0), the host's list, and the
+// other pairs as `small` codes, largest first (sizes clamped to 65535).
+constexpr int SMALL_BINS = 65536;
+void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                           uint32_t *flag, cudaStream_t st);
+void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
+                        const uint32_t *idx, int64_t *out3, cudaStream_t st);
+void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                       uint32_t *hist, cudaStream_t st);
+void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
+                          uint32_t *cursor, uint64_t *small, cudaStream_t st);
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);

@@ -91,7 +91,7 @@ struct pga_ctx {
   DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
-      ridx, rout, selfb;
+      ridx, rout, selfb, pstart2, pab2, small, shist, fo_dev;
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
@@ -635,7 +635,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
   const size_t nt = plan.tasks.size(), nf = plan.fins.size();
   tout.assign(nt, PairOut{});
   fout.assign(nf, PairOut{});
-  if (nt == 0 && nf == 0) return PGA_OK;
+  if (nt == 0 && nf == 0 && L.nsmall == 0) return PGA_OK;
   const std::vector<PairTask> &sorted = plan.tasks;  // the warps take them in this order
   if (nt) {
     ENSURE(ctx->tasks, sizeof(PairTask) * nt);
@@ -666,15 +666,22 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     CK(cudaMemcpyAsync(ctx->rec_next.p, &ctx->counters[2], 8, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->out_next.p, &ctx->counters[3], 8, cudaMemcpyHostToDevice, ctx->st));
     L.rout = P<PairOut>(ctx->rout);
-    if (nt) {
+    if (L.nsmall > 0) {
+      // the device-planned pairs' reductions: sred[6] (first failing task) starts at ~0
+      CK(cudaMemsetAsync(L.sred, 0, sizeof(unsigned long long) * (8 + 2 * (size_t)ctx->ncontig), ctx->st));
+      CK(cudaMemsetAsync(L.sred + 6, 0xff, sizeof(unsigned long long), ctx->st));
+    }
+    if (nt || L.nsmall > 0) {
       L.tasks = P<PairTask>(ctx->tasks);
       L.ntasks = (int)nt;
       L.pout = P<PairOut>(ctx->pout);
       launch_align(L, grid, ctx->st);
       LAUNCHED(1);
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * nt, cudaMemcpyDeviceToHost, ctx->st));
+      if (nt) CK(cudaMemcpyAsync(ro.data(), ctx->pout.p, sizeof(PairOut) * nt, cudaMemcpyDeviceToHost, ctx->st));
     }
+    unsigned long long sred[8] = {0, 0, 0, 0, 0, 0, ~0ull, 0};
+    if (L.nsmall > 0) CK(cudaMemcpyAsync(sred, L.sred, sizeof(sred), cudaMemcpyDeviceToHost, ctx->st));
     if (nf) {
       AlignLaunch F = L;
       F.ftasks = P<FinishTask>(ctx->ftasks);
@@ -695,7 +702,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     CK(cudaMemcpyAsync(&used[2], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&used[3], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    int errs = 0, bad = -1, badf = -1;
+    int errs = (int)sred[3], bad = -1, badf = -1;
     for (size_t k = 0; k < nt; k++)
       if (ro[k].err) {
         errs |= ro[k].err;
@@ -758,6 +765,8 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
       if (r) return r;
     }
     if (!grown) {
+      if (sred[3])
+        return fail(ctx, PGA_ERR_LIMIT, "alignment of a contig pair overflowed its work space (err 0x%llx)", sred[3]);
       if (bad >= 0)
         return fail(ctx, PGA_ERR_LIMIT, "alignment of pair (%d,%d,%s) overflowed its work space (err 0x%x)",
                     sorted[bad].a, sorted[bad].b, sorted[bad].comp ? "C" : "N", ro[bad].err);
@@ -773,6 +782,18 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     if (ro[k].cycles > *max_cycles) {
       *max_cycles = ro[k].cycles;
       *max_task_calls = ro[k].calls;
+    }
+  }
+  if (L.nsmall > 0) {
+    unsigned long long sred[8];
+    CK(cudaMemcpyAsync(sred, L.sred, sizeof(sred), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->align_work[0] += (int64_t)sred[4];
+    ctx->align_work[1] += (int64_t)sred[5];
+    ctx->align_work[3] += L.nsmall;
+    if ((long long)(sred[2] >> 16) > *max_cycles) {
+      *max_cycles = (long long)(sred[2] >> 16);
+      *max_task_calls = (int64_t)(sred[2] & 0xffff);
     }
   }
   return PGA_OK;
@@ -982,8 +1003,19 @@ int run_align(pga_ctx *ctx) {
   ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
   for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
 
-  // 4. pair lists of both units
+  // 4. Pair lists of both units.  They stay on the device; only the pairs
+  // the host plans come back: self pairs (FastGA's order) and, with band
+  // ranges on, pairs of more than RS seeds.  Every other pair becomes a
+  // device task, largest first, whose outcome is reduced on the device.
+  const int64_t all_seeds = ctx->nseed[0] + ctx->nseed[1];
+  // about 160 tasks per warp: short enough that a long alignment's band
+  // blocks spread over warps, long enough to keep the per-task cost small
+  const int64_t RS = ctx->range_seeds < 0    ? 0
+                     : ctx->range_seeds > 0 ? ctx->range_seeds
+                                            : std::max<int64_t>(256, all_seeds / (160 * L.nwarps));
   std::vector<PairTask> pairs[2];
+  int64_t npairs[2] = {0, 0};
+  DBuf *dpst[2] = {&ctx->pstart, &ctx->pstart2}, *dpab[2] = {&ctx->pab, &ctx->pab2};
   for (int comp = 0; comp < 2; comp++) {
     int64_t n = ctx->nseed[comp];
     if (n == 0) continue;
@@ -999,31 +1031,95 @@ int run_align(pga_ctx *ctx) {
     uint32_t np = 0;
     CK(cudaMemcpyAsync(&np, tot, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    ENSURE(ctx->pstart, sizeof(int64_t) * (np + 1));
-    ENSURE(ctx->pab, sizeof(int32_t) * 2 * (np + 1));
+    npairs[comp] = np;
+    ENSURE(*dpst[comp], sizeof(int64_t) * (np + 1));
+    ENSURE(*dpab[comp], sizeof(int32_t) * 2 * (np + 1));
+    const int64_t *pst = P<int64_t>(*dpst[comp]);
+    const int32_t *pab = P<int32_t>(*dpab[comp]);
     launch_pair_starts(ctx->sorted[comp], n, ctx->lay[comp], P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
-                       P<int64_t>(ctx->pstart), P<int32_t>(ctx->pab), ctx->st);
-    LAUNCHED(1);
-    std::vector<int64_t> st(np);
-    std::vector<int32_t> ab(2 * np);
-    CK(cudaMemcpyAsync(st.data(), ctx->pstart.p, sizeof(int64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(ab.data(), ctx->pab.p, sizeof(int32_t) * 2 * np, cudaMemcpyDeviceToHost, ctx->st));
+                       (int64_t *)pst, (int32_t *)pab, ctx->st);
+    // the host's pairs
+    launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), ctx->st);
+    CK(exclusive_scan<uint32_t>(P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), np, P<uint32_t>(ctx->scan_tmp), tot,
+                                ctx->st));
+    LAUNCHED(5);
+    uint32_t nh = 0;
+    CK(cudaMemcpyAsync(&nh, tot, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    for (uint32_t p = 0; p < np; p++) {
+    std::vector<int64_t> h3(3 * (size_t)nh);
+    if (nh > 0) {
+      ENSURE(ctx->io2, sizeof(int64_t) * 3 * (size_t)nh);
+      launch_pair_gather(pst, pab, np, n, P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), P<int64_t>(ctx->io2),
+                         ctx->st);
+      LAUNCHED(1);
+      CK(cudaMemcpyAsync(h3.data(), ctx->io2.p, sizeof(int64_t) * 3 * nh, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+    }
+    for (uint32_t q = 0; q < nh; q++) {
       PairTask t;
       t.comp = comp;
-      t.a = ab[2 * p];
-      t.b = ab[2 * p + 1];
+      t.a = (int)(h3[3 * q + 2] >> 32);
+      t.b = (int)(uint32_t)h3[3 * q + 2];
       t.self = (comp == 0 && t.a == t.b);
       t.entry_bepos = 0;
       t.seg = -1;
-      t.lo = st[p];
-      t.hi = (p + 1 < np) ? st[p + 1] : n;
+      t.lo = h3[3 * q];
+      t.hi = h3[3 * q + 1];
       t.slo = t.lo;
       t.shi = t.hi;
       pairs[comp].push_back(t);
     }
   }
+  // the device's pairs: a counting sort by size (largest first) per unit
+  int64_t nsmall = 0;
+  {
+    int64_t cap = 0;
+    for (int comp = 0; comp < 2; comp++) cap += npairs[comp] - (int64_t)pairs[comp].size();
+    ENSURE(ctx->small, sizeof(uint64_t) * (size_t)(cap + 1));
+    ENSURE(ctx->shist, sizeof(uint32_t) * 2 * (SMALL_BINS + 1));
+    ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(SMALL_BINS + 1) + 64);
+    uint32_t *hist = P<uint32_t>(ctx->shist), *cur = hist + (SMALL_BINS + 1);
+    for (int comp = 0; comp < 2; comp++) {
+      const int64_t ns = npairs[comp] - (int64_t)pairs[comp].size();
+      if (ns <= 0) continue;
+      CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (SMALL_BINS + 1), ctx->st));
+      launch_small_hist(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
+                        hist, ctx->st);
+      CK(exclusive_scan<uint32_t>(hist, cur, SMALL_BINS + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr,
+                                  ctx->st));
+      launch_small_scatter(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
+                           cur, P<uint64_t>(ctx->small) + nsmall, ctx->st);
+      LAUNCHED(5);
+      nsmall += ns;
+    }
+    CK(cudaGetLastError());
+  }
+  if (nsmall >= (int64_t)0x7fffffff - 16)
+    return fail(ctx, PGA_ERR_LIMIT, "%lld contig pairs: at most 2^31 supported", (long long)nsmall);
+  // FastGA's order of the contigs (GIXmake's: longest first, stable)
+  FastgaOrder F;
+  F.n = nc;
+  F.at.resize(nc);
+  for (int i = 0; i < nc; i++) F.at[i] = i;
+  std::stable_sort(F.at.begin(), F.at.end(), [&](int x, int y) { return ctx->clen[x] > ctx->clen[y]; });
+  F.pos.resize(nc);
+  for (int i = 0; i < nc; i++) F.pos[F.at[i]] = i;
+  ENSURE(ctx->fo_dev, sizeof(int) * (size_t)nc + sizeof(unsigned long long) * (8 + 2 * (size_t)nc) + 16);
+  int *fo_pos = P<int>(ctx->fo_dev);
+  unsigned long long *sred = (unsigned long long *)(P<uint8_t>(ctx->fo_dev) + ((sizeof(int) * (size_t)nc + 15) & ~15));
+  CK(cudaMemcpyAsync(fo_pos, F.pos.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, ctx->st));
+  L.small = P<uint64_t>(ctx->small);
+  L.nsmall = (int)nsmall;
+  for (int u = 0; u < 2; u++) {
+    L.pstart[u] = P<int64_t>(*dpst[u]);
+    L.pab[u] = P<int32_t>(*dpab[u]);
+    L.npairs[u] = npairs[u];
+    L.nseeds[u] = ctx->nseed[u];
+  }
+  L.fo_pos = fo_pos;
+  L.sred = sred;
+  L.fo_last = sred + 8;
+  L.fo_earlier = sred + 8 + nc;
 
   // 5. Plan.  Pairs of two different contigs (all C pairs, every N pair of
   // two contigs) run in the first launch, large ones as band ranges finished
@@ -1041,14 +1137,6 @@ int run_align(pga_ctx *ctx) {
       if (pairs[comp][i].self) self_idx.push_back((int)i);
       else first.push_back(pairs[comp][i]);
     }
-  int64_t all_seeds = 0;
-  for (int comp = 0; comp < 2; comp++)
-    for (auto &t : pairs[comp]) all_seeds += t.hi - t.lo;
-  // about 160 tasks per warp: short enough that a long alignment's band
-  // blocks spread over warps, long enough to keep the per-task cost small
-  const int64_t RS = ctx->range_seeds < 0    ? 0
-                     : ctx->range_seeds > 0 ? ctx->range_seeds
-                                            : std::max<int64_t>(256, all_seeds / (160 * L.nwarps));
   const int nself = (int)self_idx.size();
   std::vector<int64_t> x12(2 * (size_t)nself, 0);
   if (RS > 0 && nself > 0) {
@@ -1159,6 +1247,23 @@ int run_align(pga_ctx *ctx) {
   std::vector<PairOut> tout, fout;
   int r = align_launch(ctx, L, P1, tout, fout, rout_h, &maxcyc, &maxcalls);
   if (r) return r;
+  // the device-planned pairs: totals and, per order position, FastGA's
+  // order keys of the N pairs among them
+  std::vector<int64_t> Lk(nc, 0), ebest(nc, 0);
+  if (L.nsmall > 0) {
+    unsigned long long red[8];
+    std::vector<unsigned long long> fo(2 * (size_t)nc);
+    CK(cudaMemcpyAsync(red, L.sred, sizeof(red), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(fo.data(), L.fo_last, sizeof(unsigned long long) * 2 * nc, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    calls += (int64_t)red[0];
+    sumcyc += (long long)red[1];
+    for (int x = 0; x < nc; x++) {
+      Lk[x] = (int64_t)fo[x];
+      ebest[x] = (int64_t)fo[nc + x];
+    }
+  }
+  L.nsmall = 0;  // the later launches run host-planned tasks only
   std::vector<PairOut> out1(first.size());
   for (size_t i = 0; i < first.size(); i++) {
     if (first_task[i] >= 0) {
@@ -1177,15 +1282,16 @@ int run_align(pga_ctx *ctx) {
   // 6. self pairs: entry values by FastGA's order (src/fastga_order.c)
   int64_t nrounds = 0;
   if (nself > 0) {
-    FastgaOrder F;
-    F.n = nc;
-    F.at.resize(nc);
-    for (int i = 0; i < nc; i++) F.at[i] = i;
-    std::stable_sort(F.at.begin(), F.at.end(), [&](int x, int y) { return ctx->clen[x] > ctx->clen[y]; });
-    F.pos.resize(nc);
-    for (int i = 0; i < nc; i++) F.pos[F.at[i]] = i;
-    std::vector<int64_t> nseeds(nc, 0);
-    for (auto &t : pairs[0]) nseeds[t.a] += t.hi - t.lo;
+    // seeds of each anchor contig in the N unit (its diagonal-sort panel)
+    std::vector<int64_t> panel(nc + 1, 0), nseeds(nc, 0);
+    ENSURE(ctx->panel[0], sizeof(int64_t) * (nc + 1));
+    k_panel_bounds<<<(nc + 1 + 255) / 256, 256, 0, ctx->st>>>(ctx->sorted[0], ctx->nseed[0], ctx->lay[0], nc,
+                                                             P<int64_t>(ctx->panel[0]));
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(panel.data(), ctx->panel[0].p, sizeof(int64_t) * (nc + 1), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int c = 0; c < nc; c++) nseeds[c] = panel[c + 1] - panel[c];
     std::vector<int64_t> clen_pos(nc), seeds_pos(nc);
     int64_t seqtot = 0;
     for (int i = 0; i < nc; i++) {
@@ -1195,18 +1301,17 @@ int run_align(pga_ctx *ctx) {
     }
     int swide = 2 * ctx->lay[0].dbyte + ctx->ctgb + 2;
     fo_ranges(nc, clen_pos, seqtot, seeds_pos, swide, 32, F.range_start);
-    // results of the N pairs of two contigs, by anchor position
-    std::vector<std::vector<std::pair<int, int>>> earlier(nc);  // per xa: (xb, answer)
-    std::vector<int64_t> Lk(nc, 0);
+    // results of the N pairs of two contigs, by anchor position: the
+    // largest key of a pair that called (Lk) and of one whose partner comes
+    // earlier in the order (ebest: the nearest earlier partner that called);
+    // the device-planned pairs' share came from their reduction
     for (size_t i = 0; i < first.size(); i++) {
       const PairTask &t = first[i];
-      if (t.comp) continue;
+      if (t.comp || out1[i].calls <= 0) continue;
       int xa = F.pos[t.a], xb = F.pos[t.b];
-      if (out1[i].calls > 0) {
-        int64_t key = fo_key(xb, out1[i].exit_bepos);
-        if (key > Lk[xa]) Lk[xa] = key;
-      }
-      if (xb < xa) earlier[xa].push_back({xb, out1[i].calls > 0 ? out1[i].exit_bepos : -2});
+      int64_t key = fo_key(xb, out1[i].exit_bepos);
+      if (key > Lk[xa]) Lk[xa] = key;
+      if (xb < xa && key > ebest[xa]) ebest[xa] = key;
     }
     const int UNSET_MAIN = 32767;
     auto unset = [&](int rs) { return rs == 0 ? UNSET_MAIN : 0; };
@@ -1249,17 +1354,9 @@ int run_align(pga_ctx *ctx) {
           continue;
         }
       }
-      auto &e = earlier[x];
-      std::sort(e.begin(), e.end(), [](const std::pair<int, int> &u, const std::pair<int, int> &v) {
-        return u.first > v.first;  // nearest (latest) earlier partner first
-      });
-      bool found = false;
-      for (auto &pr : e)
-        if (pr.second >= 0) {
-          val[q] = pr.second;
-          found = true;
-          break;
-        }
+      // nearest earlier partner that made a call (src/fastga_order_core.c:147-166)
+      const bool found = ebest[x] != 0;
+      if (found) val[q] = (int)(ebest[x] & 0xffffffffll);
       if (found) state[q] = 1;
       else if (F.range_start[x] == x) {
         val[q] = unset(F.range_start[x]);
@@ -1370,7 +1467,7 @@ int run_align(pga_ctx *ctx) {
     o += a.tlen;
   }
   ctx->h_toff[nrec] = o;
-  ctx->align_stats[0] = (int64_t)(pairs[0].size() + pairs[1].size());
+  ctx->align_stats[0] = npairs[0] + npairs[1];
   ctx->align_stats[1] = (int64_t)self_idx.size();
   ctx->align_stats[2] = calls;
   ctx->align_stats[3] = maxcyc;
@@ -1425,7 +1522,7 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
                    &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb, &ctx->lreq, &ctx->lpath, &ctx->ltoff,
-                   &ctx->ltrace, &ctx->lnext};
+                   &ctx->ltrace, &ctx->lnext, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->shist, &ctx->fo_dev};
   for (DBuf *b : abufs)
     if (b->p) cudaFree(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
