@@ -309,6 +309,32 @@ def run_ingest(dev, cs, args, stream, peak: float, peak_kind: str, cpu: bool) ->
     return out
 
 
+def run_profile_stage(args) -> None:
+    """--profile-stage: only the index build or only the GDB ingest, warmup +
+    steps times on one GPU, printing each call's device times (a small
+    program for ncu captures of one stage's kernels)."""
+    from distributedpanga_b200 import pipeline
+    cs, _ = make_contigs(args.scale)
+    dev = pipeline.Device(0)
+    if args.profile_stage == "index":
+        dev.gdb_load(cs)
+        dev.enable_timing(True)
+        for _ in range(args.warmup + args.steps):
+            n = dev.index_build(want_entries=not args.no_entries)
+            st = dev.stage_times()
+            print(json.dumps({"stage": "index", "records": n,
+                              "ms": {k: st[k] for k in ("extract_hist", "prefix_scan", "extract_scatter",
+                                                        "bucket_sort", "lcp", "entries_prefix_table")}}),
+                  flush=True)
+    else:
+        text = fasta_text(cs)
+        for _ in range(args.warmup + args.steps):
+            sizes = dev.gdb_ingest_fasta(text, 0, tables=False)
+            print(json.dumps({"stage": "ingest", "bytes": len(text), "sizes": [int(x) for x in sizes],
+                              "ms": dev.gdb_ingest_times()}), flush=True)
+    dev.close()
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -530,10 +556,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-entries", action="store_true",
                     help="do not write the reference-format k-mer table entries (saves N x E bytes of HBM)")
+    ap.add_argument("--profile-stage", choices=["index", "ingest"], default=None,
+                    help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     args = ap.parse_args()
     WL["name"] = args.workload
     if args.ref_scale is None:
         args.ref_scale = 0.02 if args.workload == "chromset" else 0.002
+    if args.profile_stage:
+        run_profile_stage(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
