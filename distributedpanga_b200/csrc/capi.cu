@@ -88,6 +88,7 @@ struct pga_ctx {
   float base_freq[4] = {.25f, .25f, .25f, .25f};
   bool freq_set = false;
   bool have_numeric = false;
+  bool in_align = false;           // pga_align / pga_local_alignment hold the alignment buffers
   DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
@@ -135,6 +136,35 @@ int fail(pga_ctx *c, int code, const char *fmt, ...) {
 
 #define LAUNCHED(k) (ctx->launches += (k))
 
+// Frees the buffers only the alignment stage uses -- sequences, pools, task
+// lists, local-alignment requests -- which the next pga_align or
+// pga_local_alignment rebuilds, so that another stage can allocate.  Not while
+// an alignment runs.  Returns whether anything was freed.
+bool shed_align_buffers(pga_ctx *ctx) {
+  if (ctx->in_align) return false;
+  DBuf *bufs[] = {&ctx->numf, &ctx->numr, &ctx->pk, &ctx->wave, &ctx->points, &ctx->cells, &ctx->ovl, &ctx->perm,
+                  &ctx->cand, &ctx->recs, &ctx->outb, &ctx->rng_ovl, &ctx->tasks, &ctx->pout, &ctx->pflag,
+                  &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->ftasks,
+                  &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace};
+  bool any = false;
+  for (DBuf *b : bufs)
+    if (b->p) {
+      cudaFree(b->p);
+      b->p = nullptr;
+      b->cap = 0;
+      any = true;
+    }
+  ctx->have_numeric = false;
+  return any;
+}
+
+// Marks an alignment call for shed_align_buffers.
+struct AlignScope {
+  pga_ctx *c;
+  explicit AlignScope(pga_ctx *x) : c(x) { c->in_align = true; }
+  ~AlignScope() { c->in_align = false; }
+};
+
 int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.cap >= bytes) return PGA_OK;
@@ -142,6 +172,10 @@ int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
   b.p = nullptr;
   b.cap = 0;
   cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess && shed_align_buffers(ctx)) {  // room held by the last alignment
+    cudaGetLastError();
+    e = cudaMalloc(&b.p, bytes);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
@@ -2321,6 +2355,7 @@ int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4) {
 int pga_align(pga_ctx *ctx, int64_t *nalign) {
   if (!ctx || !ctx->have_seeds || !ctx->have_gdb) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
+  AlignScope scope(ctx);
   stage_begin(ctx, ST_ALIGN);
   int r = run_align(ctx);
   if (r == PGA_ERR_NOMEM && release_for_align(ctx)) {
@@ -2352,6 +2387,7 @@ int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *tr
 int pga_local_alignment(pga_ctx *ctx, int64_t n, const int32_t *req8, int64_t *ntrace) {
   if (!ctx || !ctx->have_gdb || n < 0 || (n > 0 && !req8)) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
+  AlignScope scope(ctx);
   ctx->have_local = false;
   for (int64_t i = 0; i < n; i++) {
     const int32_t *q = req8 + 8 * i;

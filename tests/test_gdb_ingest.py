@@ -213,3 +213,68 @@ def test_fasta_to_alignments_on_gpu(dev, case):
            if l.strip()]
     assert n == dig["aln"]["count"]
     assert mine == ref
+
+
+def gapped_fasta(seed: int) -> bytes:
+    """The small workload at scale 0.02 (2 x 40 kbp) joined into scaffolds of
+    one to three contigs with N gaps between them (scaffold 1 and some others
+    open with N's, scaffold 2 and some others end with them), 70 bases a
+    line."""
+    from distributedpanga_b200 import synth
+    rng = np.random.default_rng(seed)
+    letters = np.frombuffer(b"ACGT", np.uint8)
+    contigs = synth.make("small", scale=0.02)
+    out, i, k = [], 0, 0
+    while i < len(contigs):
+        m = int(rng.integers(1, 4))
+        parts = []
+        if k == 1 or rng.random() < 0.2:     # an empty first contig
+            parts.append(b"N" * int(rng.integers(1, 30)))
+        for j, c in enumerate(contigs[i:i + m]):
+            if j:
+                parts.append(b"N" * int(rng.integers(1, 200)))
+            parts.append(letters[c].tobytes())
+        if k == 2 or rng.random() < 0.2:     # a dropped trailing run
+            parts.append(b"n" * int(rng.integers(1, 30)))
+        s = b"".join(parts)
+        out.append(b">scaffold_%d some text\n" % k + b"".join(s[x:x + 70] + b"\n" for x in range(0, len(s), 70)))
+        i += m
+        k += 1
+    return b"".join(out)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not all(os.path.exists(os.path.join(REF_DIR, x))
+                            for x in ("fa2gdb", "pga-mpi-merge", "GIXmake_dump", "alndump")),
+                    reason="oracle/_ref not built")
+def test_fasta_with_gaps_to_1aln_matches_reference(dev):
+    """FASTA with gapped scaffolds -> GDB -> alignments -> .1aln, every step on
+    the GPU, equal to the reference's own pipeline on the same FASTA: the
+    record stream and the GDB skeleton (scaffold names, gaps, contigs) read
+    back by the reference's ONE reader."""
+    from oracle import binding as B
+    text = gapped_fasta(7)
+    alndump = os.path.join(REF_DIR, "alndump")
+
+    def dump(path):
+        out = subprocess.run([alndump, "-s", path], check=True, capture_output=True, text=True).stdout
+        return [" ".join(l.split()) for l in out.split("\n") if l.strip() and not l.startswith("#")]
+
+    with tempfile.TemporaryDirectory() as d:
+        fa = os.path.join(d, "g.fa")
+        with open(fa, "wb") as f:
+            f.write(text)
+        B.ref_make_gdb(fa, os.path.join(d, "g"))
+        ref = dump(B.ref_run(os.path.join(d, "g"), d)["aln"])
+        t = dev.gdb_ingest_fasta(text, 0)
+        assert t.contigs.shape[0] > t.scaffolds.shape[0]      # gaps split scaffolds
+        dev.index_build(want_entries=False)
+        dev.merge(10)
+        dev.set_ranges(0)
+        dev.align()
+        p = os.path.join(d, "mine.1aln")
+        dev.write_1aln(p, skeleton=t.skeleton(), db_name="g.1gdb", cwd=d)
+        mine = dump(p)
+    assert sum(";" in l for l in ref) > 0
+    assert any(l.startswith("G ") for l in ref)
+    assert mine == ref
