@@ -777,12 +777,25 @@ __device__ __forceinline__ uint32_t small_bin(int64_t size) {
   return (uint32_t)(SMALL_BINS - 1) - (uint32_t)(size < SMALL_BINS - 1 ? size : SMALL_BINS - 1);
 }
 
+// A pair whose seeds' spans (2 lcp each) add up to less than CHAIN_MIN has
+// no chain that reaches the hit test (src/fastga_pipeline.c:656), so it makes
+// no Local_Alignment call and no alignment: it needs no task.  A pair of 8 or
+// more seeds is kept without reading them (each seed spans at least 24).
+__device__ __forceinline__ bool pair_live(const U128 *keys, int64_t lo, int64_t size) {
+  if (size >= 8) return true;
+  int sum = 0;
+  for (int64_t i = 0; i < size; i++) sum += 2 * (int)key_bits(keys[lo + i], 0, 6);
+  return sum >= CHAIN_MIN;
+}
+
 __global__ void k_small_hist(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
-                             int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ hist) {
+                             int64_t nseeds, int comp, int64_t rs, const U128 *__restrict__ keys,
+                             uint32_t *__restrict__ hist) {
   for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = p0 + threadIdx.x;
     int64_t size = 0;
-    const bool small = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size);
+    const bool small = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) &&
+                       pair_live(keys, pstart[p], size);
     const uint32_t bin = small ? small_bin(size) : 0xffffffffu;
     const unsigned same = __match_any_sync(0xffffffffu, bin);
     if (small && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], (unsigned)__popc(same));
@@ -790,13 +803,14 @@ __global__ void k_small_hist(const int64_t *__restrict__ pstart, const int32_t *
 }
 
 __global__ void k_small_scatter(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
-                                int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ cursor,
-                                uint64_t *__restrict__ small) {
+                                int64_t nseeds, int comp, int64_t rs, const U128 *__restrict__ keys,
+                                uint32_t *__restrict__ cursor, uint64_t *__restrict__ small) {
   const int lane = threadIdx.x & 31;
   for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = p0 + threadIdx.x;
     int64_t size = 0;
-    const bool small_p = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size);
+    const bool small_p = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) &&
+                         pair_live(keys, pstart[p], size);
     const uint32_t bin = small_p ? small_bin(size) : 0xffffffffu;
     const unsigned same = __match_any_sync(0xffffffffu, bin);
     const int leader = __ffs(same) - 1;
@@ -823,17 +837,17 @@ void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, i
 }
 
 void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                       uint32_t *hist, cudaStream_t st) {
+                       const U128 *keys, uint32_t *hist, cudaStream_t st) {
   if (np <= 0) return;
   k_small_hist<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp, rs,
-                                                                                 hist);
+                                                                                 keys, hist);
 }
 
 void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                          uint32_t *cursor, uint64_t *small, cudaStream_t st) {
+                          const U128 *keys, uint32_t *cursor, uint64_t *small, cudaStream_t st) {
   if (np <= 0) return;
   k_small_scatter<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp,
-                                                                                     rs, cursor, small);
+                                                                                     rs, keys, cursor, small);
 }
 
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st) {

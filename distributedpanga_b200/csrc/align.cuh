@@ -113,16 +113,17 @@ struct AlignLaunch {
 
 // Pair lists on the device: whether the host plans pair p of a unit (a self
 // pair, or one of more than rs seeds when rs > 0), the host's list, and the
-// other pairs as `small` codes, largest first (sizes clamped to 65535).
+// other pairs that can make a Local_Alignment call (their seeds' spans reach
+// CHAIN_MIN) as `small` codes, largest first (sizes clamped to 65535).
 constexpr int SMALL_BINS = 65536;
 void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
                            uint32_t *flag, cudaStream_t st);
 void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
                         const uint32_t *idx, int64_t *out3, cudaStream_t st);
 void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                       uint32_t *hist, cudaStream_t st);
+                       const U128 *keys, uint32_t *hist, cudaStream_t st);
 void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                          uint32_t *cursor, uint64_t *small, cudaStream_t st);
+                          const U128 *keys, uint32_t *cursor, uint64_t *small, cudaStream_t st);
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);

@@ -1114,15 +1114,17 @@ int run_align(pga_ctx *ctx) {
     ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(SMALL_BINS + 1) + 64);
     uint32_t *hist = P<uint32_t>(ctx->shist), *cur = hist + (SMALL_BINS + 1);
     for (int comp = 0; comp < 2; comp++) {
-      const int64_t ns = npairs[comp] - (int64_t)pairs[comp].size();
-      if (ns <= 0) continue;
+      if (npairs[comp] - (int64_t)pairs[comp].size() <= 0) continue;
       CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (SMALL_BINS + 1), ctx->st));
       launch_small_hist(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
-                        hist, ctx->st);
-      CK(exclusive_scan<uint32_t>(hist, cur, SMALL_BINS + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr,
-                                  ctx->st));
+                        ctx->sorted[comp], hist, ctx->st);
+      uint32_t *tot = P<uint32_t>(ctx->u64tmp);
+      CK(exclusive_scan<uint32_t>(hist, cur, SMALL_BINS + 1, P<uint32_t>(ctx->scan_tmp), tot, ctx->st));
+      uint32_t ns = 0;
+      CK(cudaMemcpyAsync(&ns, tot, 4, cudaMemcpyDeviceToHost, ctx->st));
       launch_small_scatter(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
-                           cur, P<uint64_t>(ctx->small) + nsmall, ctx->st);
+                           ctx->sorted[comp], cur, P<uint64_t>(ctx->small) + nsmall, ctx->st);
+      CK(cudaStreamSynchronize(ctx->st));
       LAUNCHED(5);
       nsmall += ns;
     }
