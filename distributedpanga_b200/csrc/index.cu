@@ -209,19 +209,29 @@ __global__ void k_prefix_scatter(const Rec *__restrict__ in, int64_t n, uint32_t
   }
 }
 
-// Exclusive scan of up to 64 counts by one warp (two per lane).
-__device__ __forceinline__ void warp_scan64(const uint32_t *cnt, uint32_t *off, uint32_t total) {
+// Exclusive scan of a digit's DIGIT_PREFIXES counts by one warp.
+__device__ __forceinline__ void warp_scan_prefixes(const uint32_t *cnt, uint32_t *off, uint32_t total) {
+  constexpr int PER = DIGIT_PREFIXES / 32;
+  static_assert(PER * 32 == DIGIT_PREFIXES, "a whole number of prefixes per lane");
   const int lane = threadIdx.x & 31;
-  const uint32_t c0 = cnt[2 * lane], c1 = cnt[2 * lane + 1];
-  uint32_t x = c0 + c1;
+  uint32_t c[PER], x = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    c[k] = cnt[PER * lane + k];
+    x += c[k];
+  }
+  const uint32_t own = x;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
-  const uint32_t pre = x - c0 - c1;
-  off[2 * lane] = pre;
-  off[2 * lane + 1] = pre + c0;
+  uint32_t pre = x - own;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    off[PER * lane + k] = pre;
+    pre += c[k];
+  }
   if (lane == 0) off[DIGIT_PREFIXES] = total;
 }
 
@@ -232,7 +242,6 @@ k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_
   extern __shared__ Rec sa[];                              // CAP records
   uint16_t *sb = reinterpret_cast<uint16_t *>(sa + CAP);  // CAP record indices grouped by prefix
   __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
-  static_assert(DIGIT_PREFIXES == 64, "warp_scan64 covers 64 prefixes");
   static_assert(CAP <= 65536, "16-bit record indices");
   const uint32_t d = list ? list[blockIdx.x] : blockIdx.x;
   const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
@@ -248,7 +257,7 @@ k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_
     atomicAdd(&scur[rec_prefix(r) & (DIGIT_PREFIXES - 1)], 1u);
   }
   __syncthreads();
-  if (threadIdx.x < 32) warp_scan64(scur, soff, m);
+  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m);
   __syncthreads();
   if (threadIdx.x < DIGIT_PREFIXES) {
     start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];
@@ -300,7 +309,7 @@ k_big_digit(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t
   for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS)
     atomicAdd(&scur[rec_prefix(rec[ds + i]) & (DIGIT_PREFIXES - 1)], 1u);
   __syncthreads();
-  if (threadIdx.x < 32) warp_scan64(scur, soff, m);
+  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m);
   __syncthreads();
   if (threadIdx.x < DIGIT_PREFIXES) {
     start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];

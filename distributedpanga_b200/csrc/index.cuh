@@ -14,7 +14,10 @@ enum { EXT_COUNT = 0, EXT_WRITE = 1, EXT_HIST = 2, EXT_DIGIT = 3 };
 // sorted index -- through one cursor per digit (the 2^18 write fronts stay
 // in L2, which merges the 16-byte writes into whole lines); k_digit_sort then
 // sorts every digit's region in shared memory and writes the prefix table.
-constexpr int DIGIT_BITS = 18;
+#ifndef PGA_DIGIT_BITS
+#define PGA_DIGIT_BITS 18
+#endif
+constexpr int DIGIT_BITS = PGA_DIGIT_BITS;
 constexpr int DIGIT_SHIFT = 24 - DIGIT_BITS;
 constexpr int NDIGIT = 1 << DIGIT_BITS;
 constexpr int DIGIT_PREFIXES = 1 << DIGIT_SHIFT;  // 24-bit prefixes per digit
