@@ -2281,6 +2281,37 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   return PGA_OK;
 }
 
+int pga_index_write_gix(pga_ctx *ctx, const char *stem, int nparts) {
+  if (!ctx || !stem || !ctx->have_index || !ctx->have_entries || nparts < 1 || nparts > 1024) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  // GIXmake's widths (notes/GIXmake_annotated.c:1966-1978): bytes for the
+  // longest contig's positions, and for 2 x contigs
+  auto width = [](int64_t range) {
+    int b = 0;
+    for (int64_t cum = 1; cum < range; cum *= 256) b++;
+    return b;
+  };
+  const int postb = width(ctx->maxctg), contb = width(2 * (int64_t)ctx->ncontig);
+  if (postb != ctx->posb || contb != ctx->ctgb)
+    return fail(ctx, PGA_ERR_LIMIT, "GIXmake's entry widths (%d, %d) differ from the index's (%d, %d)", postb, contb,
+                ctx->posb, ctx->ctgb);
+  const int eb = 9 + ctx->posb + ctx->ctgb;
+  std::vector<uint8_t> ent((size_t)ctx->nrec * eb + 1);
+  std::vector<int64_t> cum((size_t)1 << 24);
+  int64_t largest = 0;
+  int r = pga_index_copy_entries(ctx, ent.data(), cum.data(), &largest);
+  if (r != PGA_OK) return r;
+  // contigs longest first, ties in contig order (GIXmake's LSORT under glibc's
+  // merge sort, notes/GIXmake_annotated.c:1666-1671, 2037-2047)
+  std::vector<int32_t> order(ctx->ncontig);
+  for (int i = 0; i < ctx->ncontig; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ctx->clen[x] > ctx->clen[y]; });
+  r = pga_write_gix(stem, nparts, postb, contb, ctx->ncontig, order.data(), cum.data(), largest, ctx->nrec,
+                    ent.data());
+  if (r != PGA_OK) return fail(ctx, r, "cannot write %s.gix or its .ktab parts", stem);
+  return PGA_OK;
+}
+
 int pga_index_copy_records(pga_ctx *ctx, uint8_t *records) {
   if (!ctx || !ctx->have_index || (!records && ctx->nrec > 0)) return PGA_ERR_ARG;
   int64_t n = ctx->nrec;

@@ -79,6 +79,8 @@ _SIGS = {
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
     "pga_gdb_ingest_fasta": (C.c_int, [vp, C.c_char_p, C.c_int64, C.c_int, vp]),
+    "pga_index_write_gix": (C.c_int, [vp, C.c_char_p, C.c_int]),
+    "pga_write_gix": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int64, C.c_int64, vp]),
     "pga_gdb_copy": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "pga_gdb_ingest_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_gdb_write": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]),
@@ -227,6 +229,10 @@ class Device:
         """Write_GDB (lib/GDB.c:1519) of the ingested GDB: tpath and its .bps."""
         self._ck(self.L.pga_gdb_write(self.h, tpath.encode(), _PROG, _VERSION, command.encode(),
                                       srcpath.encode()), "gdb_write")
+
+    def index_write_gix(self, stem: str, nparts: int = 8):
+        """GIXmake's .gix + .ktab parts of the index built with entries."""
+        self._ck(self.L.pga_index_write_gix(self.h, stem.encode(), int(nparts)), "index_write_gix")
 
     def record_sizing(self):
         a, b, c = C.c_int(), C.c_int(), C.c_int()

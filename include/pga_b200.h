@@ -157,6 +157,20 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posit
  * records directly).  *count receives the record count. */
 int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count);
 int pga_index_copy_records(pga_ctx *ctx, uint8_t *records);           /* count x record_size */
+/* GIXmake's output (notes/GIXmake_annotated.c:1529-1615) from the index built
+ * with entries: <stem>.gix (header, the 2^24 cumulative prefix counts, the
+ * contigs longest first -- what src/fastga_order_core.c:11 reads) and the
+ * k-mer table in `nparts` parts <dir>/.<root>.ktab.1..nparts.  The part
+ * boundaries (whole 10-bit panels, balanced by entries) and the order of equal
+ * k-mers (by payload) are this library's; GIXmake picks both by sampling and
+ * threads.  PGA_ERR_LIMIT when GIXmake's entry widths would differ from the
+ * index's (a longest contig of exactly 256^k bases). */
+int pga_index_write_gix(pga_ctx *ctx, const char *stem, int nparts);
+/* The writer behind pga_index_write_gix, from host arrays: order[ncontig],
+ * cum[2^24] (cumulative entries per prefix), nentries entries of
+ * 9 + post_bytes + cont_bytes bytes.  Needs no device. */
+int pga_write_gix(const char *stem, int nparts, int post_bytes, int cont_bytes, int ncontig, const int32_t *order,
+                  const int64_t *cum, int64_t largest, int64_t nentries, const uint8_t *entries);
 int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t *largest_group);
 
 /* Adaptamer merge of the built index: seeds stay in HBM. */
