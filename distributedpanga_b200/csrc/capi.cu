@@ -2282,7 +2282,9 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
 }
 
 int pga_index_write_gix(pga_ctx *ctx, const char *stem, int nparts) {
-  if (!ctx || !stem || !ctx->have_index || !ctx->have_entries || nparts < 1 || nparts > 1024) return PGA_ERR_ARG;
+  if (!ctx || !stem || nparts < 1 || nparts > 1024) return PGA_ERR_ARG;
+  if (!ctx->have_index || !ctx->have_entries)
+    return fail(ctx, PGA_ERR_ARG, "no index with entries: call pga_index_build with want_entries = 1 first");
   CK(cudaSetDevice(ctx->device));
   // GIXmake's widths (notes/GIXmake_annotated.c:1966-1978): bytes for the
   // longest contig's positions, and for 2 x contigs
