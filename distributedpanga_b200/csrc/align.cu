@@ -408,8 +408,13 @@ struct SmallSums {
   }
 };
 
-__global__ void __launch_bounds__(ALIGN_THREADS)
-k_align_pairs(AlignLaunch P) {
+// The persistent alignment loop, in two builds: MINB = 1 keeps every
+// register a warp's wave loop wants (255, two CTAs per SM), for launches
+// bounded by their longest task; MINB = 3 trades spills for half as many
+// warps again (three CTAs per SM), for launches bounded by throughput (many
+// pairs).
+template <int MINB>
+__global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch P) {
   __shared__ BlockSeed s_block[ALIGN_THREADS / 32][32];
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * ALIGN_THREADS + threadIdx.x) >> 5;
@@ -483,6 +488,7 @@ k_align_pairs(AlignLaunch P) {
   }
   if (lane == 0 && P.nsmall > 0) sums.flush(P);
 }
+
 
 // Finishes the pairs that ran as band ranges: gathers each pair's candidates
 // from its ranges in range order (the order one warp running the whole pair
@@ -702,7 +708,8 @@ void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *
 }
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st) {
-  k_align_pairs<<<grid, ALIGN_THREADS, 0, st>>>(P);
+  if (P.min_blocks == 3) k_align_pairs<3><<<grid, ALIGN_THREADS, 0, st>>>(P);
+  else k_align_pairs<1><<<grid, ALIGN_THREADS, 0, st>>>(P);
 }
 
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st) {

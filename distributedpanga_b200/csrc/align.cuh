@@ -109,6 +109,8 @@ struct AlignLaunch {
   int64_t npairs[2], nseeds[2];
   const int *fo_pos;
   unsigned long long *sred, *fo_last, *fo_earlier;
+  // build of k_align_pairs: 2 (all registers) or 3 resident CTAs per SM
+  int min_blocks;
 };
 
 // Pair lists on the device: whether the host plans pair p of a unit (a self

@@ -106,6 +106,7 @@ struct pga_ctx {
   std::vector<uint16_t> h_ltrace;
   bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
+  int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2 or 3 CTAs per SM
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
   unsigned long long cand_used = 0, rng_used = 0, rec_used = 0, out_used = 0;
@@ -978,6 +979,11 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
   return PGA_OK;
 }
 
+// Pairs beyond which the alignment launch uses k_align_pairs_wide: 2 x 100 Mbp
+// (10 K pairs) is 5 % faster with <2>, 2 x 1 Gbp (101 M pairs) 19 % faster
+// with <3>.
+constexpr int64_t ALIGN_MANY_PAIRS = 1 << 20;
+
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -1153,6 +1159,9 @@ int run_align(pga_ctx *ctx) {
     L.nseeds[u] = ctx->nseed[u];
   }
   L.fo_pos = fo_pos;
+  // the launch is bounded by its longest tasks up to about a million pairs,
+  // by throughput beyond: then the build with more resident warps
+  L.min_blocks = ctx->align_build ? ctx->align_build : npairs[0] + npairs[1] > ALIGN_MANY_PAIRS ? 3 : 2;
   L.sred = sred;
   L.fo_last = sred + 8;
   L.fo_earlier = sred + 8 + nc;
@@ -2523,6 +2532,12 @@ int pga_local_alignment_copy(pga_ctx *ctx, int32_t *path7, int64_t *trace_off, u
 int pga_align_work(const pga_ctx *ctx, int64_t *work4) {
   if (!ctx || !work4) return PGA_ERR_ARG;
   for (int i = 0; i < 4; i++) work4[i] = ctx->align_work[i];
+  return PGA_OK;
+}
+
+int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
+  if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3)) return PGA_ERR_ARG;
+  ctx->align_build = ctas_per_sm;
   return PGA_OK;
 }
 

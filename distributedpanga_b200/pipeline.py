@@ -68,6 +68,7 @@ _SIGS = {
     "pga_align_copy": (C.c_int, [vp, vp, vp, vp]),
     "pga_align_stats": (C.c_int, [vp, vp]),
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
+    "pga_align_set_build": (C.c_int, [vp, C.c_int]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
     "pga_local_alignment": (C.c_int, [vp, C.c_int64, vp, C.POINTER(C.c_int64)]),
@@ -386,6 +387,10 @@ class Device:
         a = np.zeros(4, dtype=np.int64)
         self._ck(self.L.pga_align_work(self.h, a.ctypes.data_as(vp)), "align_work")
         return {"waves": int(a[0]), "cells": int(a[1]), "calls": int(a[2]), "tasks": int(a[3])}
+
+    def set_build(self, ctas_per_sm: int):
+        """Which build of the alignment kernel runs (0 automatic, 2 or 3)."""
+        self._ck(self.L.pga_align_set_build(self.h, int(ctas_per_sm)), "align_set_build")
 
     def set_ranges(self, range_seeds: int) -> None:
         """Band-range size for large pairs (0 automatic, -1 never split)."""

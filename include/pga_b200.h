@@ -205,6 +205,13 @@ int pga_align(pga_ctx *ctx, int64_t *nalign);
  * thread runs each pair there). */
 int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
 
+/* Tuning, no counterpart in the reference: which build of the alignment
+ * kernel runs -- 2 (255 registers, two CTAs per SM: best when the launch is
+ * bounded by its longest alignments) or 3 (168 registers, three CTAs per SM:
+ * best for launches of many pairs); 0 (the default) picks 3 above 2^20 pairs.
+ * The alignments are the same either way. */
+int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
+
 /* The alignments in la_sort order: per alignment 9 ints (aread abpos aepos
  * bread bbpos bepos comp diffs tlen), trace_off (nalign+1) and the trace
  * bytes (uint8 pairs: differences, b-delta per 100-base A interval, as

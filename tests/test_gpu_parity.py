@@ -204,6 +204,28 @@ def test_alignments_independent_of_band_ranges(dev, case):
     assert got[64] == got[-1]
 
 
+@pytest.mark.parametrize("case", ["chromset_s0005", "many_contigs"])
+def test_alignments_independent_of_kernel_build(dev, case):
+    """The alignment kernel's two builds (two or three CTAs per SM) give the
+    reference's alignments."""
+    import gzip
+    import os
+    from conftest import GOLDEN
+    from distributedpanga_b200.pipeline import alignment_lines
+    cs, dig = load_case(case)
+    ref = _aln_norm(gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n"))
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=False)
+    dev.merge(dig["freq_cutoff"])
+    try:
+        for build in (3, 2):
+            dev.set_build(build)
+            dev.align()
+            assert _aln_norm(alignment_lines(*dev.alignments())) == ref, build
+    finally:
+        dev.set_build(0)
+
+
 @pytest.mark.parametrize("case", ["small_s002", "edge_mix"])
 def test_1aln_file_matches_reference(dev, case):
     """The GPU path's .1aln file, read by the reference's own reader, is the
