@@ -2197,35 +2197,40 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb,
 int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
-  ENSURE(ctx->hist, sizeof(uint32_t) * (NDIGIT + 1));
+  // digit width (records ~ 0.8 per base)
+  int64_t seqtot = 0;
+  for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
+  const int dbits = digit_bits_for(seqtot - seqtot / 5), dshift = 24 - dbits;
+  const int64_t ndigit = (int64_t)1 << dbits;
+  ENSURE(ctx->hist, sizeof(uint32_t) * (ndigit + 1));
   ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
-  // digit starts (NDIGIT + 1), digit cursors (NDIGIT + 1), digits above DS_CAP
-  // (NDIGIT) and above DS_CAP_MID (NDIGIT)
-  ENSURE(ctx->coarse, sizeof(uint32_t) * (4 * (size_t)NDIGIT + 2));
-  uint32_t *dstart = P<uint32_t>(ctx->coarse), *dcur = dstart + (NDIGIT + 1), *qdig = dcur + (NDIGIT + 1),
-           *qdig2 = qdig + NDIGIT;
+  // digit starts (ndigit + 1), digit cursors (ndigit + 1), digits above DS_CAP
+  // (ndigit) and above DS_CAP_MID (ndigit)
+  ENSURE(ctx->coarse, sizeof(uint32_t) * (4 * (size_t)ndigit + 2));
+  uint32_t *dstart = P<uint32_t>(ctx->coarse), *dcur = dstart + (ndigit + 1), *qdig = dcur + (ndigit + 1),
+           *qdig2 = qdig + ndigit;
   uint32_t *hist = P<uint32_t>(ctx->hist), *start = P<uint32_t>(ctx->start);
   const uint8_t *bps = P<uint8_t>(ctx->bps);
   const int64_t *cl = P<int64_t>(ctx->dclen), *bo = P<int64_t>(ctx->dboff);
   const int32_t *tc = P<int32_t>(ctx->tile_ctg);
   const int64_t *tj = P<int64_t>(ctx->tile_j0);
   stage_begin(ctx, ST_EXTRACT_HIST);
-  CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (NDIGIT + 1), ctx->st));
+  CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (ndigit + 1), ctx->st));
   if (ctx->ntiles > 0) {
     launch_extract(EXT_HIST, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr, hist,
-                   nullptr);
+                   nullptr, dshift);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_HIST);
   CK(cudaGetLastError());
   stage_begin(ctx, ST_SCAN);
-  ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(NDIGIT + 1));
-  CK(exclusive_scan<uint32_t>(hist, dstart, NDIGIT + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr, ctx->st));
+  ENSURE(ctx->scan_tmp, sizeof(uint32_t) * scan_tmp_elems(ndigit + 1));
+  CK(exclusive_scan<uint32_t>(hist, dstart, ndigit + 1, P<uint32_t>(ctx->scan_tmp), (uint32_t *)nullptr, ctx->st));
   LAUNCHED(3);
-  CK(cudaMemcpyAsync(dcur, dstart, sizeof(uint32_t) * NDIGIT, cudaMemcpyDeviceToDevice, ctx->st));
-  CK(cudaMemcpyAsync(start + NPREFIX, dstart + NDIGIT, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemcpyAsync(dcur, dstart, sizeof(uint32_t) * ndigit, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemcpyAsync(start + NPREFIX, dstart + ndigit, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->st));
   uint32_t total = 0;
-  CK(cudaMemcpyAsync(&total, dstart + NDIGIT, 4, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(&total, dstart + ndigit, 4, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   stage_end(ctx, ST_SCAN);
   const int64_t n = total;
@@ -2237,7 +2242,7 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   stage_begin(ctx, ST_EXTRACT_SCATTER);
   if (ctx->ntiles > 0) {
     launch_extract(EXT_DIGIT, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
-                   P<Rec>(ctx->rec), nullptr, dcur);
+                   P<Rec>(ctx->rec), nullptr, dcur, dshift);
     LAUNCHED(1);
   }
   stage_end(ctx, ST_EXTRACT_SCATTER);
@@ -2250,7 +2255,8 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   ENSURE(ctx->qcount, sizeof(uint32_t) * 8);
   CK(cudaMemsetAsync(ctx->qcount.p, 0, sizeof(uint32_t) * 8, ctx->st));
   uint32_t *qc = P<uint32_t>(ctx->qcount);
-  CK(launch_digit_sort(DS_CAP, NDIGIT, DS_THREADS, ctx->st, P<Rec>(ctx->rec), dstart, start, nullptr, qdig, qc + 4));
+  CK(launch_digit_sort(DS_CAP, (int)ndigit, DS_THREADS, ctx->st, P<Rec>(ctx->rec), dstart, start, nullptr, qdig,
+                       qc + 4, dshift));
   LAUNCHED(1);
   CK(cudaGetLastError());
   uint32_t q[8];
@@ -2258,7 +2264,7 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   CK(cudaStreamSynchronize(ctx->st));
   if (q[4] > 0) {
     CK(launch_digit_sort(DS_CAP_MID, (int)q[4], DS_MID_THREADS, ctx->st, P<Rec>(ctx->rec), dstart, start, qdig,
-                         qdig2, qc + 5));
+                         qdig2, qc + 5, dshift));
     LAUNCHED(1);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(q, qc, sizeof(q), cudaMemcpyDeviceToHost, ctx->st));
@@ -2266,9 +2272,9 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   }
   if (q[5] > 0) {
     // scratch for the big digits only: digit i of the list at toff[i]
-    std::vector<uint32_t> big(q[5]), hd(NDIGIT + 1);
+    std::vector<uint32_t> big(q[5]), hd(ndigit + 1);
     CK(cudaMemcpyAsync(big.data(), qdig2, sizeof(uint32_t) * q[5], cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(hd.data(), dstart, sizeof(uint32_t) * (NDIGIT + 1), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(hd.data(), dstart, sizeof(uint32_t) * (ndigit + 1), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     std::vector<int64_t> toff(q[5] + 1, 0);
     for (uint32_t i = 0; i < q[5]; i++) toff[i + 1] = toff[i] + (hd[big[i] + 1] - hd[big[i]]);
@@ -2277,7 +2283,7 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
     CK(cudaMemcpyAsync(ctx->u64tmp.p, toff.data(), sizeof(int64_t) * (q[5] + 1), cudaMemcpyHostToDevice, ctx->st));
     k_big_digit<<<q[5], BD_THREADS, 0, ctx->st>>>(P<Rec>(ctx->rec), dstart, start, qdig2, P<int64_t>(ctx->u64tmp),
                                                   P<Rec>(ctx->rec2), P<uint32_t>(ctx->qmed), P<uint32_t>(ctx->qbig),
-                                                  qc);
+                                                  qc, dshift);
     LAUNCHED(1);
     CK(cudaGetLastError());
   }

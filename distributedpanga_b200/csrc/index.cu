@@ -8,7 +8,8 @@
 //   build_kmer_adapter     src/kmer_adapter.c:6-96
 //
 // The MPI bucket exchange of run_stage2 becomes an in-HBM MSD sort in two
-// levels: a histogram of the 18-bit digits (the first 9 bases), a scatter of
+// levels: a histogram of the digits (the first 9 bases, more for very large
+// indexes), a scatter of
 // every record into its digit's region as it is extracted, then a sort of
 // each digit's region in shared memory that also writes the 24-bit prefix
 // table (the k-mer table's cumulative prefix index).  Records extracted from
@@ -86,7 +87,7 @@ k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
           const int64_t *__restrict__ boff, const int32_t *__restrict__ tile_ctg,
           const int64_t *__restrict__ tile_j0, int ctgb, uint32_t *__restrict__ counts,
           const uint64_t *__restrict__ offsets, Rec *__restrict__ out,
-          uint32_t *__restrict__ hist, uint32_t *__restrict__ cursor) {
+          uint32_t *__restrict__ hist, uint32_t *__restrict__ cursor, int dshift) {
   __shared__ uint8_t s[EXT_SPAN];
   __shared__ uint8_t tm[256], tmrc[256];
   const int tid = threadIdx.x;
@@ -149,9 +150,9 @@ k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
             if (MODE == EXT_WRITE) {
               out[woff++] = r;
             } else if (MODE == EXT_HIST) {
-              atomicAdd(&hist[rec_prefix(r) >> DIGIT_SHIFT], 1u);
+              atomicAdd(&hist[rec_prefix(r) >> dshift], 1u);
             } else {  // EXT_DIGIT
-              uint32_t slot = atomicAdd(&cursor[rec_prefix(r) >> DIGIT_SHIFT], 1u);
+              uint32_t slot = atomicAdd(&cursor[rec_prefix(r) >> dshift], 1u);
               out[slot] = r;
             }
           }
@@ -167,24 +168,25 @@ k_extract(const uint8_t *__restrict__ bps, const int64_t *__restrict__ clen,
 
 void launch_extract(int mode, int ntiles, cudaStream_t st, const uint8_t *bps, const int64_t *clen,
                     const int64_t *boff, const int32_t *tile_ctg, const int64_t *tile_j0, int ctgb,
-                    uint32_t *counts, const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor) {
+                    uint32_t *counts, const uint64_t *offsets, Rec *out, uint32_t *hist, uint32_t *cursor,
+                    int dshift) {
   if (ntiles <= 0) return;
   switch (mode) {
     case EXT_COUNT:
       k_extract<EXT_COUNT><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
-                                                           offsets, out, hist, cursor);
+                                                           offsets, out, hist, cursor, dshift);
       break;
     case EXT_WRITE:
       k_extract<EXT_WRITE><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
-                                                           offsets, out, hist, cursor);
+                                                           offsets, out, hist, cursor, dshift);
       break;
     case EXT_HIST:
       k_extract<EXT_HIST><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
-                                                          offsets, out, hist, cursor);
+                                                          offsets, out, hist, cursor, dshift);
       break;
     default:
       k_extract<EXT_DIGIT><<<ntiles, EXT_THREADS, 0, st>>>(bps, clen, boff, tile_ctg, tile_j0, ctgb, counts,
-                                                           offsets, out, hist, cursor);
+                                                           offsets, out, hist, cursor, dshift);
   }
 }
 
@@ -209,39 +211,35 @@ __global__ void k_prefix_scatter(const Rec *__restrict__ in, int64_t n, uint32_t
   }
 }
 
-// Exclusive scan of a digit's DIGIT_PREFIXES counts by one warp.
-__device__ __forceinline__ void warp_scan_prefixes(const uint32_t *cnt, uint32_t *off, uint32_t total) {
-  constexpr int PER = DIGIT_PREFIXES / 32;
-  static_assert(PER * 32 == DIGIT_PREFIXES, "a whole number of prefixes per lane");
+// Exclusive scan of a digit's npfx (4..64) prefix counts by one warp.
+__device__ __forceinline__ void warp_scan_prefixes(const uint32_t *cnt, uint32_t *off, uint32_t total, int npfx) {
   const int lane = threadIdx.x & 31;
-  uint32_t c[PER], x = 0;
-#pragma unroll
-  for (int k = 0; k < PER; k++) {
-    c[k] = cnt[PER * lane + k];
-    x += c[k];
-  }
+  const int per = npfx > 32 ? 2 : 1;
+  const int b = lane * per;
+  const uint32_t c0 = b < npfx ? cnt[b] : 0u, c1 = per == 2 ? cnt[b + 1] : 0u;
+  uint32_t x = c0 + c1;
   const uint32_t own = x;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
-  uint32_t pre = x - own;
-#pragma unroll
-  for (int k = 0; k < PER; k++) {
-    off[PER * lane + k] = pre;
-    pre += c[k];
-  }
-  if (lane == 0) off[DIGIT_PREFIXES] = total;
+  const uint32_t pre = x - own;
+  if (b < npfx) off[b] = pre;
+  if (per == 2) off[b + 1] = pre + c0;
+  if (lane == 0) off[npfx] = total;
 }
 
 template <int CAP>
 __global__ void __launch_bounds__(1024)
 k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t *__restrict__ start,
-             const uint32_t *__restrict__ list, uint32_t *__restrict__ qnext, uint32_t *__restrict__ qnext_count) {
+             const uint32_t *__restrict__ list, uint32_t *__restrict__ qnext, uint32_t *__restrict__ qnext_count,
+             int dshift) {
+  const int npfx = 1 << dshift;
+  const uint32_t pmask = (uint32_t)npfx - 1u;
   extern __shared__ Rec sa[];                              // CAP records
   uint16_t *sb = reinterpret_cast<uint16_t *>(sa + CAP);  // CAP record indices grouped by prefix
-  __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
+  __shared__ uint32_t soff[MAX_DIGIT_PREFIXES + 1], scur[MAX_DIGIT_PREFIXES];
   static_assert(CAP <= 65536, "16-bit record indices");
   const uint32_t d = list ? list[blockIdx.x] : blockIdx.x;
   const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
@@ -249,28 +247,28 @@ k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_
     if (threadIdx.x == 0) qnext[atomicAdd(qnext_count, 1u)] = d;
     return;
   }
-  if (threadIdx.x < DIGIT_PREFIXES) scur[threadIdx.x] = 0;
+  if (threadIdx.x < npfx) scur[threadIdx.x] = 0;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
     const Rec r = rec[ds + i];
     sa[i] = r;
-    atomicAdd(&scur[rec_prefix(r) & (DIGIT_PREFIXES - 1)], 1u);
+    atomicAdd(&scur[rec_prefix(r) & pmask], 1u);
   }
   __syncthreads();
-  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m);
+  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m, npfx);
   __syncthreads();
-  if (threadIdx.x < DIGIT_PREFIXES) {
-    start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];
+  if (threadIdx.x < npfx) {
+    start[(d << dshift) + threadIdx.x] = ds + soff[threadIdx.x];
     scur[threadIdx.x] = soff[threadIdx.x];
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += blockDim.x)
-    sb[atomicAdd(&scur[rec_prefix(sa[i]) & (DIGIT_PREFIXES - 1)], 1u)] = (uint16_t)i;
+    sb[atomicAdd(&scur[rec_prefix(sa[i]) & pmask], 1u)] = (uint16_t)i;
   __syncthreads();
   // each record's rank among its prefix bucket (records are distinct)
   for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
     const Rec x = sa[sb[k]];
-    const uint32_t q = rec_prefix(x) & (DIGIT_PREFIXES - 1);
+    const uint32_t q = rec_prefix(x) & pmask;
     const uint32_t gs = soff[q], ge = soff[q + 1];
     uint32_t rank = 0;
     for (uint32_t j = gs; j < ge; j++) rank += rec_less(sa[sb[j]], x) ? 1u : 0u;
@@ -280,18 +278,19 @@ k_digit_sort(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_
 
 template <int CAP>
 cudaError_t launch_cap(int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart, uint32_t *start,
-                       const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count) {
+                       const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count, int dshift) {
   const size_t smem = (size_t)CAP * (sizeof(Rec) + sizeof(uint16_t));
   PGA_CUDA_TRY(cudaFuncSetAttribute(k_digit_sort<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_digit_sort<CAP><<<grid, threads, smem, st>>>(rec, dstart, start, list, qnext, qnext_count);
+  k_digit_sort<CAP><<<grid, threads, smem, st>>>(rec, dstart, start, list, qnext, qnext_count, dshift);
   return cudaGetLastError();
 }
 
 cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, Rec *rec, const uint32_t *dstart,
-                              uint32_t *start, const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count) {
+                              uint32_t *start, const uint32_t *list, uint32_t *qnext, uint32_t *qnext_count,
+                              int dshift) {
   switch (cap) {
-    case DS_CAP: return launch_cap<DS_CAP>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count);
-    case DS_CAP_MID: return launch_cap<DS_CAP_MID>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count);
+    case DS_CAP: return launch_cap<DS_CAP>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count, dshift);
+    case DS_CAP_MID: return launch_cap<DS_CAP_MID>(grid, threads, st, rec, dstart, start, list, qnext, qnext_count, dshift);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -299,32 +298,34 @@ cudaError_t launch_digit_sort(int cap, int grid, int threads, cudaStream_t st, R
 __global__ void __launch_bounds__(BD_THREADS)
 k_big_digit(Rec *__restrict__ rec, const uint32_t *__restrict__ dstart, uint32_t *__restrict__ start,
             const uint32_t *__restrict__ list, const int64_t *__restrict__ toff, Rec *__restrict__ tmp_all,
-            uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount) {
-  __shared__ uint32_t soff[DIGIT_PREFIXES + 1], scur[DIGIT_PREFIXES];
+            uint32_t *__restrict__ qmed, uint32_t *__restrict__ qbig, uint32_t *__restrict__ qcount, int dshift) {
+  const int npfx = 1 << dshift;
+  const uint32_t pmask = (uint32_t)npfx - 1u;
+  __shared__ uint32_t soff[MAX_DIGIT_PREFIXES + 1], scur[MAX_DIGIT_PREFIXES];
   const uint32_t d = list[blockIdx.x];
   const uint32_t ds = dstart[d], m = dstart[d + 1] - ds;
   Rec *tmp = tmp_all + toff[blockIdx.x];
-  if (threadIdx.x < DIGIT_PREFIXES) scur[threadIdx.x] = 0;
+  if (threadIdx.x < npfx) scur[threadIdx.x] = 0;
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS)
-    atomicAdd(&scur[rec_prefix(rec[ds + i]) & (DIGIT_PREFIXES - 1)], 1u);
+    atomicAdd(&scur[rec_prefix(rec[ds + i]) & pmask], 1u);
   __syncthreads();
-  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m);
+  if (threadIdx.x < 32) warp_scan_prefixes(scur, soff, m, npfx);
   __syncthreads();
-  if (threadIdx.x < DIGIT_PREFIXES) {
-    start[(d << DIGIT_SHIFT) + threadIdx.x] = ds + soff[threadIdx.x];
+  if (threadIdx.x < npfx) {
+    start[(d << dshift) + threadIdx.x] = ds + soff[threadIdx.x];
     scur[threadIdx.x] = soff[threadIdx.x];
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS) {
     const Rec r = rec[ds + i];
-    tmp[atomicAdd(&scur[rec_prefix(r) & (DIGIT_PREFIXES - 1)], 1u)] = r;
+    tmp[atomicAdd(&scur[rec_prefix(r) & pmask], 1u)] = r;
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < m; i += BD_THREADS) rec[ds + i] = tmp[i];
-  if (threadIdx.x < DIGIT_PREFIXES) {
+  if (threadIdx.x < npfx) {
     const uint32_t n = soff[threadIdx.x + 1] - soff[threadIdx.x];
-    const uint32_t p = (d << DIGIT_SHIFT) + threadIdx.x;
+    const uint32_t p = (d << dshift) + threadIdx.x;
     if (n > 1) {
       if (n <= BK_MEDIUM) qmed[atomicAdd(&qcount[0], 1u)] = p;
       else {
