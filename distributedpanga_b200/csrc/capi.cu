@@ -107,6 +107,7 @@ struct pga_ctx {
   bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
   int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2 or 3 CTAs per SM
+  int digit_bits = 0;              // pga_index_set_digit_bits: 0 by record count, else 18..22
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
   unsigned long long cand_used = 0, rng_used = 0, rec_used = 0, out_used = 0;
@@ -2200,7 +2201,7 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   // digit width (records ~ 0.8 per base)
   int64_t seqtot = 0;
   for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
-  const int dbits = digit_bits_for(seqtot - seqtot / 5), dshift = 24 - dbits;
+  const int dbits = ctx->digit_bits ? ctx->digit_bits : digit_bits_for(seqtot - seqtot / 5), dshift = 24 - dbits;
   const int64_t ndigit = (int64_t)1 << dbits;
   ENSURE(ctx->hist, sizeof(uint32_t) * (ndigit + 1));
   ENSURE(ctx->start, sizeof(uint32_t) * (NPREFIX + 1));
@@ -2544,6 +2545,12 @@ int pga_align_work(const pga_ctx *ctx, int64_t *work4) {
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
   if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3)) return PGA_ERR_ARG;
   ctx->align_build = ctas_per_sm;
+  return PGA_OK;
+}
+
+int pga_index_set_digit_bits(pga_ctx *ctx, int bits) {
+  if (!ctx || (bits != 0 && (bits < MIN_DIGIT_BITS || bits > MAX_DIGIT_BITS))) return PGA_ERR_ARG;
+  ctx->digit_bits = bits;
   return PGA_OK;
 }
 

@@ -69,6 +69,7 @@ _SIGS = {
     "pga_align_stats": (C.c_int, [vp, vp]),
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
     "pga_align_set_build": (C.c_int, [vp, C.c_int]),
+    "pga_index_set_digit_bits": (C.c_int, [vp, C.c_int]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
     "pga_local_alignment": (C.c_int, [vp, C.c_int64, vp, C.POINTER(C.c_int64)]),
@@ -391,6 +392,10 @@ class Device:
     def set_build(self, ctas_per_sm: int):
         """Which build of the alignment kernel runs (0 automatic, 2 or 3)."""
         self._ck(self.L.pga_align_set_build(self.h, int(ctas_per_sm)), "align_set_build")
+
+    def set_digit_bits(self, bits: int) -> None:
+        """Width of the index sort's first-level digit (0 automatic, 18..22)."""
+        self._ck(self.L.pga_index_set_digit_bits(self.h, int(bits)), "index_set_digit_bits")
 
     def set_ranges(self, range_seeds: int) -> None:
         """Band-range size for large pairs (0 automatic, -1 never split)."""

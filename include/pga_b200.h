@@ -212,6 +212,12 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
  * The alignments are the same either way. */
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
 
+/* Tuning, no counterpart in the reference: the width in bits (18..22) of the
+ * first-level digit of pga_index_build's two-level sort; 0 (the default)
+ * takes 18 unless digits would then average more than 8192 records.  The
+ * index is the same for every width. */
+int pga_index_set_digit_bits(pga_ctx *ctx, int bits);
+
 /* The alignments in la_sort order: per alignment 9 ints (aread abpos aepos
  * bread bbpos bepos comp diffs tlen), trace_off (nalign+1) and the trace
  * bytes (uint8 pairs: differences, b-delta per 100-base A interval, as

@@ -108,12 +108,14 @@ def test_degenerate_inputs(dev, oracle):
     assert np.array_equal(dev.extract_to_records(), oracle.extract(cs, posb, ctgb))
 
 
-def test_index_skewed_digits(dev, oracle):
-    """Digits (first 9 bases) of every size class of the two-level sort: a
-    poly-A run puts ~30,000 records into one digit and one prefix bucket (the
-    global path and the bitonic network), tandem copies of a 9-base unit put
-    thousands into a few digits (the 8192-record shared-memory class), random
-    sequence fills the rest.  Equal to the oracle's sorted index."""
+@pytest.mark.parametrize("bits", [0, 19, 20, 22])
+def test_index_skewed_digits(dev, oracle, bits):
+    """Digits (the first 9 to 11 bases) of every size class of the two-level
+    sort: a poly-A run puts ~30,000 records into one digit and one prefix
+    bucket (the global path and the bitonic network), tandem copies of a
+    9-base unit put thousands into a few digits (the 8192-record shared-memory
+    class), random sequence fills the rest.  Equal to the oracle's sorted
+    index at the automatic width and at forced wider ones."""
     from distributedpanga_b200 import gdb
     rng = np.random.default_rng(29)
     unit = np.array([0, 1, 2, 3, 3, 2, 1, 0, 3], np.uint8)
@@ -123,7 +125,11 @@ def test_index_skewed_digits(dev, oracle):
     cs = gdb.from_contigs(contigs)
     posb, ctgb, _ = gdb.record_sizing(cs)
     dev.gdb_load(cs)
-    n = dev.index_build(want_entries=True)
+    dev.set_digit_bits(bits)
+    try:
+        n = dev.index_build(want_entries=True)
+    finally:
+        dev.set_digit_bits(0)
     want = oracle.sort_records(oracle.extract(cs, posb, ctgb))
     assert n == want.shape[0]
     assert np.array_equal(dev.index_records(), want)
