@@ -57,6 +57,7 @@ struct pga_ctx {
   std::vector<int32_t> h_scaf;           // per contig
   std::vector<char> h_headers;
   int64_t base_count[4] = {0, 0, 0, 0};
+  int ingest_nthr = 0;                   // the gap threshold the GDB was read with
   DBuf fa_text, fa_mask, fa_seq, fa_cnt, fa_tmp, fa_tot, fa_status, fa_hdr, fa_hbytes, fa_runs, fa_ctg;
   cudaEvent_t fa_ev[3] = {nullptr, nullptr, nullptr};  // upload start, parse start, parse end
   float ingest_ms[2] = {0, 0};                        // pga_gdb_ingest_times
@@ -116,6 +117,20 @@ struct pga_ctx {
 
   // generic byte staging
   DBuf io, io2;
+};
+
+// A resident target (pga_target_create): an ingested GDB and its sorted index,
+// moved out of a context and kept on the device, read-only, for the requests
+// of pga_serve_load on any context of the same device.
+struct pga_target {
+  int device = 0;
+  int ncontig = 0, ctgb = 1, nthr = 0;
+  int64_t bps_bytes = 0, nrec = 0;
+  std::vector<int64_t> clen, boff, sbeg, scf4;
+  std::vector<int32_t> scaf;
+  std::vector<char> headers;
+  int64_t base_count[4] = {0, 0, 0, 0};
+  DBuf bps, rec, start;  // sequence image, sorted records, prefix table (NPREFIX + 1)
 };
 
 namespace {
@@ -217,6 +232,8 @@ int grow_keep(pga_ctx *ctx, DBuf &b, size_t bytes, size_t keep) {
 
 template <typename T>
 T *P(DBuf &b) { return (T *)b.p; }
+template <typename T>
+const T *P(const DBuf &b) { return (const T *)b.p; }
 
 int grid_for(int64_t n, int threads, int cap = 148 * 32) {
   int64_t g = (n + threads - 1) / threads;
@@ -1897,6 +1914,7 @@ int pga_gdb_ingest_fasta(pga_ctx *ctx, const char *text, int64_t nbytes, int nth
   CK(cudaEventElapsedTime(&ctx->ingest_ms[1], ctx->fa_ev[1], ctx->fa_ev[2]));
   ctx->have_gdb = true;
   ctx->have_scaffolds = true;
+  ctx->ingest_nthr = nthr;
   return PGA_OK;
 }
 
@@ -2195,12 +2213,12 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb,
   return copy_diag(ctx, comp, ncontig, out, panel_off);
 }
 
-int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
-  if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
-  CK(cudaSetDevice(ctx->device));
-  // digit width (records ~ 0.8 per base)
-  int64_t seqtot = 0;
-  for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
+namespace {
+
+// The two-level sort of the records of extraction tiles [tile0, tile0 +
+// ntiles) into ctx->rec, with the prefix table (start) of those records;
+// seqtot (the tiles' bases) sizes the digit.
+int sort_tiles(pga_ctx *ctx, int tile0, int ntiles, int64_t seqtot) {
   const int dbits = ctx->digit_bits ? ctx->digit_bits : digit_bits_for(seqtot - seqtot / 5), dshift = 24 - dbits;
   const int64_t ndigit = (int64_t)1 << dbits;
   ENSURE(ctx->hist, sizeof(uint32_t) * (ndigit + 1));
@@ -2213,12 +2231,12 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   uint32_t *hist = P<uint32_t>(ctx->hist), *start = P<uint32_t>(ctx->start);
   const uint8_t *bps = P<uint8_t>(ctx->bps);
   const int64_t *cl = P<int64_t>(ctx->dclen), *bo = P<int64_t>(ctx->dboff);
-  const int32_t *tc = P<int32_t>(ctx->tile_ctg);
-  const int64_t *tj = P<int64_t>(ctx->tile_j0);
+  const int32_t *tc = P<int32_t>(ctx->tile_ctg) + tile0;
+  const int64_t *tj = P<int64_t>(ctx->tile_j0) + tile0;
   stage_begin(ctx, ST_EXTRACT_HIST);
   CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (ndigit + 1), ctx->st));
-  if (ctx->ntiles > 0) {
-    launch_extract(EXT_HIST, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr, hist,
+  if (ntiles > 0) {
+    launch_extract(EXT_HIST, ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr, nullptr, hist,
                    nullptr, dshift);
     LAUNCHED(1);
   }
@@ -2241,8 +2259,8 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   ENSURE(ctx->rec, sizeof(Rec) * (size_t)n + 16);
   // level 1: every record into its digit's region
   stage_begin(ctx, ST_EXTRACT_SCATTER);
-  if (ctx->ntiles > 0) {
-    launch_extract(EXT_DIGIT, ctx->ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
+  if (ntiles > 0) {
+    launch_extract(EXT_DIGIT, ntiles, ctx->st, bps, cl, bo, tc, tj, ctx->ctgb, nullptr, nullptr,
                    P<Rec>(ctx->rec), nullptr, dcur, dshift);
     LAUNCHED(1);
   }
@@ -2291,8 +2309,167 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   r = sort_queued(ctx);
   if (r) return r;
   stage_end(ctx, ST_BUCKET);
+  return PGA_OK;
+}
+
+}  // namespace
+
+int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
+  if (!ctx || !ctx->have_gdb) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  // digit width (records ~ 0.8 per base)
+  int64_t seqtot = 0;
+  for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
+  int r = sort_tiles(ctx, 0, ctx->ntiles, seqtot);
+  if (r) return r;
   r = finish_index(ctx, want_entries != 0);
   if (r) return r;
+  if (count) *count = ctx->nrec;
+  return PGA_OK;
+}
+
+int pga_target_create(pga_ctx *ctx, pga_target **out) {
+  if (!ctx || !out) return PGA_ERR_ARG;
+  *out = nullptr;
+  if (!ctx->have_scaffolds || !ctx->have_index)
+    return fail(ctx, PGA_ERR_ARG, "a target needs an ingested GDB (pga_gdb_ingest_fasta) and its index (pga_index_build)");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->st));
+  pga_target *t = new (std::nothrow) pga_target();
+  if (!t) return fail(ctx, PGA_ERR_NOMEM, "host allocation");
+  t->device = ctx->device;
+  t->ncontig = ctx->ncontig;
+  t->ctgb = ctx->ctgb;
+  t->nthr = ctx->ingest_nthr;
+  t->bps_bytes = ctx->bps_bytes;
+  t->nrec = ctx->nrec;
+  t->clen = ctx->clen;
+  t->boff = ctx->boff;
+  t->sbeg = ctx->h_sbeg;
+  t->scf4 = ctx->h_scf4;
+  t->scaf = ctx->h_scaf;
+  t->headers = ctx->h_headers;
+  for (int v = 0; v < 4; v++) t->base_count[v] = ctx->base_count[v];
+  // the buffers move: the context keeps no GDB and no index
+  std::swap(t->bps, ctx->bps);
+  std::swap(t->rec, ctx->rec);
+  std::swap(t->start, ctx->start);
+  gdb_reset(ctx);
+  *out = t;
+  return PGA_OK;
+}
+
+void pga_target_destroy(pga_target *t) {
+  if (!t) return;
+  cudaSetDevice(t->device);
+  for (DBuf *b : {&t->bps, &t->rec, &t->start})
+    if (b->p) cudaFree(b->p);
+  delete t;
+}
+
+int pga_target_info(const pga_target *t, int64_t *info4) {
+  if (!t || !info4) return PGA_ERR_ARG;
+  int64_t bases = 0;
+  for (int64_t c : t->clen) bases += c;
+  info4[0] = t->ncontig;
+  info4[1] = bases;
+  info4[2] = t->nrec;
+  info4[3] = (int64_t)(t->bps.cap + t->rec.cap + t->start.cap);
+  return PGA_OK;
+}
+
+int pga_serve_load(pga_ctx *ctx, const pga_target *t, const char *query, int64_t nbytes, int want_entries,
+                   int64_t *sizes6, int64_t *count) {
+  if (!ctx || !t) return PGA_ERR_ARG;
+  if (t->device != ctx->device) return fail(ctx, PGA_ERR_ARG, "target on device %d, context on %d", t->device, ctx->device);
+  // the query's GDB, read with the target's gap threshold
+  int r = pga_gdb_ingest_fasta(ctx, query, nbytes, t->nthr, nullptr);
+  if (r) return r;
+  ctx->have_gdb = ctx->have_scaffolds = false;
+  const int qnc = ctx->ncontig, qnh = (int)(ctx->h_scf4.size() / 4);
+  const int64_t nc64 = (int64_t)t->ncontig + qnc, nh64 = (int64_t)(t->scf4.size() / 4) + qnh;
+  if (nc64 >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%lld contigs: at most 32767 supported", (long long)nc64);
+  if (nh64 >= 32768) return fail(ctx, PGA_ERR_LIMIT, "%lld scaffolds: at most 32767 supported", (long long)nh64);
+  const int nc = (int)nc64;
+  // GDB(target, query): the target's image followed by the query's, as the
+  // ingest of the two texts one after the other lays it out
+  const int64_t tb = t->bps_bytes, qb = ctx->bps_bytes, nb = tb + qb;
+  ENSURE(ctx->io2, (size_t)((nb + 3) / 4 * 4) + 16);
+  if (tb > 0) CK(cudaMemcpyAsync(ctx->io2.p, t->bps.p, tb, cudaMemcpyDeviceToDevice, ctx->st));
+  if (qb > 0) CK(cudaMemcpyAsync(P<uint8_t>(ctx->io2) + tb, ctx->bps.p, qb, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaMemsetAsync(P<uint8_t>(ctx->io2) + nb, 0, (size_t)((nb + 3) / 4 * 4) + 16 - nb, ctx->st));
+  std::swap(ctx->bps, ctx->io2);
+  std::vector<int64_t> clen(t->clen), boff(t->boff);
+  for (int c = 0; c < qnc; c++) {
+    clen.push_back(ctx->clen[c]);
+    boff.push_back(ctx->boff[c] + tb);
+  }
+  const int64_t th = (int64_t)t->headers.size();
+  std::vector<int64_t> sbeg(t->sbeg), scf4(t->scf4);
+  std::vector<int32_t> scaf(t->scaf);
+  sbeg.insert(sbeg.end(), ctx->h_sbeg.begin(), ctx->h_sbeg.end());
+  for (int32_t s : ctx->h_scaf) scaf.push_back(s + (int32_t)(t->scf4.size() / 4));
+  for (int j = 0; j < qnh; j++) {
+    scf4.push_back(ctx->h_scf4[4 * j + 0] + t->ncontig);
+    scf4.push_back(ctx->h_scf4[4 * j + 1] + t->ncontig);
+    scf4.push_back(ctx->h_scf4[4 * j + 2]);
+    scf4.push_back(ctx->h_scf4[4 * j + 3] + th);
+  }
+  std::vector<char> headers(t->headers);
+  headers.insert(headers.end(), ctx->h_headers.begin(), ctx->h_headers.end());
+  ctx->h_sbeg.swap(sbeg);
+  ctx->h_scaf.swap(scaf);
+  ctx->h_scf4.swap(scf4);
+  ctx->h_headers.swap(headers);
+  int64_t seqtot = 0, qbases = 0;
+  for (int v = 0; v < 4; v++) {
+    ctx->base_count[v] += t->base_count[v];
+    seqtot += ctx->base_count[v];
+  }
+  // GDB.freq as Create_GDB sets it (lib/GDB.c:1083-1086)
+  for (int v = 0; v < 4; v++) ctx->base_freq[v] = (float)((1. * ctx->base_count[v]) / seqtot);
+  ctx->freq_set = true;
+  for (int c = 0; c < qnc; c++) qbases += ctx->clen[c];
+  ENSURE(ctx->dclen, sizeof(int64_t) * (nc + 1));
+  ENSURE(ctx->dboff, sizeof(int64_t) * (nc + 1));
+  CK(cudaMemcpyAsync(ctx->dclen.p, clen.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemcpyAsync(ctx->dboff.p, boff.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, ctx->st));
+  r = gdb_tables(ctx, nc, clen.data(), boff.data(), nb);
+  if (r) return r;
+  ctx->have_gdb = ctx->have_scaffolds = true;
+  ctx->ingest_nthr = t->nthr;
+  // the index: the query's records sorted alone (its tiles follow the
+  // target's), then their union with the target's
+  int q0 = 0;
+  while (q0 < ctx->ntiles && ctx->h_tile_ctg[q0] < t->ncontig) q0++;
+  r = sort_tiles(ctx, q0, ctx->ntiles - q0, qbases);
+  if (r) return r;
+  const int64_t nq = ctx->nrec, n = t->nrec + nq;
+  r = check_records_fit(ctx, n);
+  if (r) return r;
+  if (t->ctgb > ctx->ctgb) return fail(ctx, PGA_ERR_ARG, "target contig width %d above the request's %d", t->ctgb, ctx->ctgb);
+  ENSURE(ctx->rec2, sizeof(Rec) * (size_t)n + 16);
+  if (n > 0) {
+    k_union_rank<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Rec>(t->rec), P<uint32_t>(t->start), t->nrec, t->ctgb,
+                                                        P<Rec>(ctx->rec), P<uint32_t>(ctx->start), nq, ctx->ctgb,
+                                                        P<Rec>(ctx->rec2));
+    LAUNCHED(1);
+  }
+  k_add_prefix_tables<<<grid_for(NPREFIX + 1, 256), 256, 0, ctx->st>>>(P<uint32_t>(ctx->start), P<uint32_t>(t->start));
+  LAUNCHED(1);
+  CK(cudaGetLastError());
+  std::swap(ctx->rec, ctx->rec2);
+  ctx->nrec = n;
+  r = finish_index(ctx, want_entries != 0);
+  if (r) return r;
+  if (sizes6) {
+    sizes6[0] = (int64_t)(ctx->h_scf4.size() / 4);
+    sizes6[1] = nc;
+    sizes6[2] = nb;
+    sizes6[3] = (int64_t)ctx->h_headers.size();
+    sizes6[4] = ctx->maxctg;
+    sizes6[5] = seqtot;
+  }
   if (count) *count = n;
   return PGA_OK;
 }

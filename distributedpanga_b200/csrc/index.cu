@@ -567,4 +567,49 @@ __global__ void k_prefix_table(const uint32_t *__restrict__ start, int64_t *__re
   if ((threadIdx.x & 31) == 0 && best) atomicMax(maxrun, best);
 }
 
+// ---------------------------------------------------------------------------
+// Union of two sorted indices whose records all differ (a resident target's
+// and a query's: their contigs differ).  Each record goes to its rank in the
+// union: its own index plus the number of the other index's records below
+// it, which is the other index's prefix-table entry for its prefix plus a
+// lower bound inside that prefix bucket.  The a side's contig|strand field
+// is rewritten from width actgb to ctgb (the strand bit moves to the top of
+// the wider field; (strand, contig, position) order is the same in both).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ Rec rec_widen(Rec r, uint32_t from_sign, uint32_t to_sign) {
+  const uint64_t cs = (r.lo >> 32) & 0xffff;
+  const uint64_t w = (cs & (from_sign - 1)) | ((cs & from_sign) ? to_sign : 0);
+  r.lo = (r.lo & ~(0xffffull << 32)) | (w << 32);
+  return r;
+}
+
+__global__ void k_union_rank(const Rec *__restrict__ a, const uint32_t *__restrict__ sa, int64_t na, int actgb,
+                             const Rec *__restrict__ b, const uint32_t *__restrict__ sb, int64_t nb, int ctgb,
+                             Rec *__restrict__ out) {
+  const uint32_t fs = 1u << (8 * actgb - 1), ts = 1u << (8 * ctgb - 1);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const bool from_a = i < na;
+    const Rec x = from_a ? rec_widen(a[i], fs, ts) : b[i - na];
+    const uint32_t p = rec_prefix(x);
+    uint32_t lo = from_a ? sb[p] : sa[p], hi = from_a ? sb[p + 1] : sa[p + 1];
+    while (lo < hi) {
+      const uint32_t m = lo + ((hi - lo) >> 1);
+      const Rec y = from_a ? b[m] : rec_widen(a[m], fs, ts);
+      if (rec_less(y, x))
+        lo = m + 1;
+      else
+        hi = m;
+    }
+    out[(from_a ? i : i - na) + lo] = x;
+  }
+}
+
+__global__ void k_add_prefix_tables(uint32_t *__restrict__ start, const uint32_t *__restrict__ other) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p <= NPREFIX;
+       p += (int64_t)gridDim.x * blockDim.x)
+    start[p] += other[p];
+}
+
 }  // namespace pga

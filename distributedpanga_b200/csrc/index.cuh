@@ -77,5 +77,11 @@ __global__ void k_records_out(const Rec *rec, const uint8_t *lcp, int64_t n, int
                               uint8_t *out);
 __global__ void k_records_in(const uint8_t *in, int64_t n, int posb, int ctgb, Rec *rec, uint8_t *lcp);
 __global__ void k_prefix_table(const uint32_t *start, int64_t *cum, uint32_t *maxrun);
+// The union of sorted indices a (prefix table sa, contig|strand width actgb
+// <= ctgb) and b (sb, ctgb) with no record in common, written to out in order.
+__global__ void k_union_rank(const Rec *a, const uint32_t *sa, int64_t na, int actgb, const Rec *b,
+                             const uint32_t *sb, int64_t nb, int ctgb, Rec *out);
+// start[p] += other[p] for p in [0, NPREFIX].
+__global__ void k_add_prefix_tables(uint32_t *start, const uint32_t *other);
 
 }  // namespace pga

@@ -88,6 +88,10 @@ _SIGS = {
     "pga_gdb_write": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p]),
     "pga_write_1gdb": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, vp, C.c_int, vp,
                                  vp, C.c_int64, C.c_int, vp, vp, C.c_int64]),
+    "pga_target_create": (C.c_int, [vp, C.POINTER(vp)]),
+    "pga_target_destroy": (None, [vp]),
+    "pga_target_info": (C.c_int, [vp, vp]),
+    "pga_serve_load": (C.c_int, [vp, vp, C.c_char_p, C.c_int64, C.c_int, vp, vp]),
 }
 
 _LIB = None
@@ -201,6 +205,25 @@ class Device:
         sizes = np.zeros(6, dtype=np.int64)
         self._ck(self.L.pga_gdb_ingest_fasta(self.h, ptr, n, int(nthr), sizes.ctypes.data_as(vp)),
                  "gdb_ingest_fasta")
+        self.cs = None
+        if not tables:
+            return sizes
+        t = self.gdb_tables(sizes)
+        self.cs = _gdb.ContigSet(bps=t.bps, clen=t.contigs[:, 0].copy(), boff=t.contigs[:, 1].copy(),
+                                 freq=t.freq)
+        return t
+
+    def serve_load(self, target: "Target", query, want_entries: bool = False, tables: bool = False):
+        """One request against a resident target (pga_serve_load): this
+        context's GDB becomes GDB(target text + query text) and its index is
+        built by merging the query's sorted records into the target's.
+        Returns the combined GDB's sizes (or its GdbTables) and sets nrec."""
+        query = bytes(query)
+        sizes = np.zeros(6, dtype=np.int64)
+        n = C.c_int64()
+        self._ck(self.L.pga_serve_load(self.h, target.h, query, len(query), 1 if want_entries else 0,
+                                       sizes.ctypes.data_as(vp), C.byref(n)), "serve_load")
+        self.nrec = n.value
         self.cs = None
         if not tables:
             return sizes
@@ -419,6 +442,39 @@ class Device:
         return {"pairs": int(a[0]), "self_pairs": int(a[1]), "calls": int(a[2]), "alignments": int(a[4]),
                 "self_rounds": int(a[5]), "max_task_cycles": int(a[3]), "all_task_cycles": int(a[6]),
                 "max_task_calls": int(a[7])}
+
+
+class Target:
+    """A resident target (pga_target): a FASTA text ingested and indexed on
+    one device and kept there, read-only, for any number of contexts'
+    requests (Device.serve_load)."""
+
+    def __init__(self, text, nthr: int = 0, device: int = 0):
+        self.L = load_library()
+        d = Device(device)
+        try:
+            d.gdb_ingest_fasta(text, nthr=nthr, tables=False)
+            d.index_build(want_entries=False)
+            h = vp()
+            d._ck(self.L.pga_target_create(d.h, C.byref(h)), "target_create")
+        finally:
+            d.close()
+        self.h = h
+        self.device = device
+        a = np.zeros(4, dtype=np.int64)
+        self.L.pga_target_info(self.h, a.ctypes.data_as(vp))
+        self.ncontig, self.bases, self.nrec, self.device_bytes = (int(x) for x in a)
+
+    def close(self):
+        if self.h:
+            self.L.pga_target_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class GdbTables:

@@ -213,6 +213,62 @@ def make_full(seed: int = 3, scale: float = 1.0) -> list:
     return split_uniform(rng, a, lo, hi) + split_uniform(rng, b, lo, hi)
 
 
+def make_target(seed: int = 5, scale: float = 1.0) -> list:
+    """The served form's resident target: one 1 Gbp genome built as A of
+    ``chromset`` (40% GC, 10% in 300 repeat families, log-normal contigs of
+    median 2 Mbp; below scale 0.05 the contig lengths stop shrinking)."""
+    rng = np.random.default_rng(seed)
+    gc = 0.40
+    g = int(1_000_000_000 * scale)
+    a = random_bases(rng, g, gc)
+    a = plant_repeats(rng, a, 0.10, 300, max(20, int(300 * min(1.0, scale * 100))),
+                      max(40, int(6000 * min(1.0, scale * 100))), 0.10, 0.20, gc)
+    f = max(scale, 0.05)             # contig lengths shrink at most 20-fold
+    return split_lognormal(rng, a, 2_000_000 * f, 1.0, int(10_000 * f))
+
+
+def make_query(rng: np.random.Generator, target: list, size: int, divergence: float,
+               median: float = 2_000_000) -> list:
+    """A query assembly of ``size`` bases: a stretch of the target's
+    concatenated contigs (a quarter of it reverse-complemented) with
+    substitutions at ``divergence`` and indels (geometric length, mean 3) at a
+    tenth of that, cut into log-normal contigs."""
+    cat = np.concatenate(target)
+    size = min(size, len(cat))
+    p = int(rng.integers(0, len(cat) - size + 1))
+    q = cat[p:p + size]
+    if rng.random() < 0.25:
+        q = revcomp(q)
+    q = substitute(rng, q, divergence)
+    q = indels(rng, q, divergence / 10, lambda k: rng.geometric(1.0 / 3.0, size=k), 0.40)
+    return split_lognormal(rng, q, median, 1.0, max(100, min(10_000, size // 4)))
+
+
+def query_stream(target: list, n: int, rate: float, size_lo: int, size_hi: int, seed: int = 11,
+                 div_lo: float = 0.005, div_hi: float = 0.05, median: float = 2_000_000) -> list:
+    """n requests of a Poisson stream (``rate`` per second): (arrival seconds,
+    query contigs), sizes log-uniform in [size_lo, size_hi], divergence
+    uniform in [div_lo, div_hi]."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for _ in range(n):
+        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        size = int(np.exp(rng.uniform(np.log(size_lo), np.log(size_hi))))
+        out.append((t, make_query(rng, target, size, float(rng.uniform(div_lo, div_hi)), median)))
+    return out
+
+
+def fasta_bytes(contigs: list, prefix: str = "ctg", width: int = 80) -> bytes:
+    """FASTA text of numeric contigs, named <prefix><i>."""
+    letters = np.frombuffer(b"ACGT", dtype=np.uint8)
+    parts = []
+    for i, c in enumerate(contigs):
+        s = letters[c].tobytes()
+        parts.append(b">%s%d\n" % (prefix.encode(), i))
+        parts.append(b"".join(s[j:j + width] + b"\n" for j in range(0, len(s), width)))
+    return b"".join(parts)
+
+
 WORKLOADS = {"small": make_small, "chromset": make_chromset, "full": make_full}
 
 

@@ -36,6 +36,7 @@ extern "C" {
 #define PGA_ERR_LIMIT     4   /* input beyond the limits above */
 
 typedef struct pga_ctx pga_ctx;
+typedef struct pga_target pga_target;
 
 /* ---- context ------------------------------------------------------------ */
 
@@ -217,6 +218,34 @@ int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
  * takes 18 unless digits would then average more than 8192 records.  The
  * index is the same for every width. */
 int pga_index_set_digit_bits(pga_ctx *ctx, int bits);
+
+/* ---- Served form: a resident target and query requests ------------------
+ * No counterpart in the reference, which runs one GDB per job.  A request's
+ * results are, bit for bit, those of the plain path on the GDB that
+ * pga_gdb_ingest_fasta makes of the target's FASTA text followed by the
+ * query's (every pair of that GDB is aligned: the frequency cutoff and
+ * FastGA's self-pair order both depend on all of its contigs). */
+
+/* Moves ctx's GDB (ingested with pga_gdb_ingest_fasta) and its index
+ * (pga_index_build) into a new resident target; ctx is left with no GDB.  The
+ * target is read-only: any number of contexts of the same device may serve
+ * requests against it at once, each on its own stream. */
+int pga_target_create(pga_ctx *ctx, pga_target **out);
+void pga_target_destroy(pga_target *t);
+/* info4 = {contigs, bases, index records, device bytes held}. */
+int pga_target_info(const pga_target *t, int64_t *info4);
+
+/* A request: ctx's GDB becomes GDB(target's text, query text) -- the query
+ * parsed on the device with the target's gap threshold, its contigs and
+ * scaffolds numbered after the target's -- and its index is built from the
+ * query's records alone, sorted, and merged into the target's resident
+ * sorted records (k_union_rank) instead of sorting both.  Then pga_merge,
+ * pga_align and the writers run as for any GDB.  sizes6 as
+ * pga_gdb_ingest_fasta gives it for the combined GDB; count = index records.
+ * The query's errors are pga_gdb_ingest_fasta's; PGA_ERR_LIMIT when the two
+ * together pass 32767 contigs or scaffolds. */
+int pga_serve_load(pga_ctx *ctx, const pga_target *t, const char *query, int64_t nbytes, int want_entries,
+                   int64_t *sizes6, int64_t *count);
 
 /* The alignments in la_sort order: per alignment 9 ints (aread abpos aepos
  * bread bbpos bepos comp diffs tlen), trace_off (nalign+1) and the trace
