@@ -44,8 +44,16 @@ WORKLOADS = {
     "chromset": "chromset: 2 x 100 Mbp, 40% GC, log-normal contigs (median 2 Mbp, sigma 1), 10% repeats; k=40, FREQ=10",
     "full": "full: 2 x 1 Gbp, uniform ACGT, contigs U[50, 500] kbp, 40% interspersed repeats, 3% tandem arrays, "
             "B = A at 2% substitutions + 0.5% indels + 20 inversions; k=40, FREQ=10",
+    "pangenome": "pangenome: a 50 Mbp reference + 16 haplotypes (0.1-1% substitutions, a tenth as indels, "
+                 "10 inversions + 5 translocations each), log-normal contigs 10 kbp-5 Mbp, all in one GDB; "
+                 "k=40, FREQ=20 (above the 17 copies of a shared k-mer)",
 }
 WL = {"name": "chromset"}  # the workload of this run (--workload)
+FREQ = {"pangenome": 20}   # frequency cutoff per workload (10 unless listed)
+
+
+def freq_cutoff() -> int:
+    return FREQ.get(WL["name"], 10)
 
 
 def peaks():
@@ -418,10 +426,19 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     stream = torch.cuda.current_stream()
     dev.set_stream(stream.cuda_stream)
     dev.gdb_load(cs)
+    tuned = None
+    if args.autotune:
+        # untimed: pick the launch parameters on this workload, then run with them
+        from distributedpanga_b200 import autotune
+        tu = autotune.Tuner(dev, repeats=2)
+        cfg = tu.tune()
+        autotune.apply(dev, cfg)
+        tuned = {"chosen": cfg, "median_s": {k: {str(c): round(statistics.median(v), 4) for c, v in t.items()}
+                                             for k, t in tu.times.items()}}
 
     def step():
         dev.index_build(want_entries=not args.no_entries)
-        dev.merge(10)
+        dev.merge(freq_cutoff())
         dev.diag_sort(0)
         dev.diag_sort(1)
         dev.align()
@@ -472,7 +489,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         t0.record(stream)
         dev.gdb_load(cs)
         dev.index_build(want_entries=not args.no_entries)
-        dev.merge(10)
+        dev.merge(freq_cutoff())
         swide, _ = dev.diag_sort(0)
         dev.diag_sort(1)
         dev.align()
@@ -545,6 +562,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "clocks": clk,
         "gdb_ingest": ingest,
         "served_form": served,
+        "autotune": tuned,
     }
     emit(rank, line)
 
@@ -677,7 +695,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="chromset", choices=sorted(WORKLOADS),
-                    help="chromset (2 x 100 Mbp, the default) or full (2 x 1 Gbp)")
+                    help="chromset (2 x 100 Mbp, the default), full (2 x 1 Gbp) or pangenome (17 x 50 Mbp)")
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the workload's full size)")
     ap.add_argument("--ref-scale", type=float, default=None,
                     help="CPU sample scale (default 0.02 of chromset, 0.002 of full)")
@@ -693,6 +711,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=12)
     ap.add_argument("--serve-rate", type=float, default=8.0, help="request arrivals per second (Poisson)")
     ap.add_argument("--serve-slots", type=int, default=3)
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the digit width, aligner build and band-range size on the workload first "
+                         "(untimed) and run with the fastest")
     ap.add_argument("--no-serve", action="store_true",
                     help="leave the served-form measurement out of the main line")
     args = ap.parse_args()

@@ -213,6 +213,39 @@ def make_full(seed: int = 3, scale: float = 1.0) -> list:
     return split_uniform(rng, a, lo, hi) + split_uniform(rng, b, lo, hi)
 
 
+def make_pangenome(seed: int = 4, scale: float = 1.0) -> list:
+    """The batched form's pan-genome: a 50 Mbp seeded reference (uniform ACGT)
+    and 16 haplotypes of it, each with its own substitution rate in
+    [0.1%, 1%], indels at a tenth of that (geometric length, mean 3), 10
+    inversions and 5 translocations of U[1 kbp, 100 kbp]; every genome cut
+    into log-normal contigs (median 224 kbp, sigma 1) kept within
+    [10 kbp, 5 Mbp].  One contig list, the reference's first."""
+    rng = np.random.default_rng(seed)
+    g = int(50_000_000 * scale)
+    ref = random_bases(rng, g)
+    genomes = [ref]
+    svlo, svhi = max(50, int(1_000 * scale)), max(100, int(100_000 * scale))
+    for _ in range(16):
+        d = float(rng.uniform(0.001, 0.01))
+        h = substitute(rng, ref, d)
+        h = indels(rng, h, d / 10, lambda k: rng.geometric(1.0 / 3.0, size=k), 0.5)
+        h = invert(rng, h, 10, svlo, svhi)
+        h = translocate(rng, h, 5, svlo, svhi)
+        genomes.append(h)
+    f = max(scale, 0.05)
+    lo, hi, med = int(10_000 * f), int(5_000_000 * f), 224_000 * f
+    out = []
+    for s in genomes:
+        p, n = 0, len(s)
+        while p < n:
+            ln = int(min(hi, max(lo, rng.lognormal(np.log(med), 1.0))))
+            if n - p - ln < lo:
+                ln = n - p
+            out.append(s[p:p + ln])
+            p += ln
+    return out
+
+
 def make_target(seed: int = 5, scale: float = 1.0) -> list:
     """The served form's resident target: one 1 Gbp genome built as A of
     ``chromset`` (40% GC, 10% in 300 repeat families, log-normal contigs of
@@ -269,7 +302,7 @@ def fasta_bytes(contigs: list, prefix: str = "ctg", width: int = 80) -> bytes:
     return b"".join(parts)
 
 
-WORKLOADS = {"small": make_small, "chromset": make_chromset, "full": make_full}
+WORKLOADS = {"small": make_small, "chromset": make_chromset, "full": make_full, "pangenome": make_pangenome}
 
 
 def make(workload: str, seed: int | None = None, scale: float = 1.0) -> list:
