@@ -144,6 +144,7 @@ class Device:
             raise PgaError("pga_ctx_create(%d) failed: %s" % (device, _ERRNAMES.get(rc, rc)))
         self.h = h
         self.cs = None
+        self.ncontig = 0
 
     def close(self):
         if self.h:
@@ -190,6 +191,7 @@ class Device:
                                      np.ascontiguousarray(cs.clen, dtype=np.int64),
                                      np.ascontiguousarray(cs.boff, dtype=np.int64)), "gdb_load")
         self.cs = cs
+        self.ncontig = cs.ncontig
 
     def gdb_ingest_fasta(self, text, nthr: int = 0, nbytes: int | None = None, tables: bool = True):
         """Create_GDB (lib/GDB.c:442) of a FASTA text, parsed on the device;
@@ -206,6 +208,7 @@ class Device:
         self._ck(self.L.pga_gdb_ingest_fasta(self.h, ptr, n, int(nthr), sizes.ctypes.data_as(vp)),
                  "gdb_ingest_fasta")
         self.cs = None
+        self.ncontig = int(sizes[1])
         if not tables:
             return sizes
         t = self.gdb_tables(sizes)
@@ -225,6 +228,7 @@ class Device:
                                        sizes.ctypes.data_as(vp), C.byref(n)), "serve_load")
         self.nrec = n.value
         self.cs = None
+        self.ncontig = int(sizes[1])
         if not tables:
             return sizes
         t = self.gdb_tables(sizes)
@@ -348,7 +352,7 @@ class Device:
         posb, ctgb, _ = self.record_sizing()
         sb = 1 + 2 * (posb + ctgb)
         out = np.zeros((self.nseeds[comp], sb), dtype=np.uint8)
-        buck = np.zeros(self.cs.ncontig, dtype=np.int64)
+        buck = np.zeros(self.ncontig, dtype=np.int64)
         self._ck(self.L.pga_seeds_copy(self.h, comp, _ptr(out), buck.ctypes.data_as(vp)), "seeds_copy")
         return out, buck
 
@@ -359,7 +363,7 @@ class Device:
 
     def diag_records(self, comp: int, swide: int, count: int):
         out = np.zeros((count, swide), dtype=np.uint8)
-        off = np.zeros(self.cs.ncontig + 1, dtype=np.int64)
+        off = np.zeros(self.ncontig + 1, dtype=np.int64)
         self._ck(self.L.pga_diag_copy(self.h, comp, _ptr(out), off.ctypes.data_as(vp)), "diag_copy")
         return out, off
 
