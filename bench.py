@@ -322,6 +322,25 @@ def run_profile_stage(args) -> None:
     steps times on one GPU, printing each call's device times (a small
     program for ncu captures of one stage's kernels)."""
     from distributedpanga_b200 import pipeline
+    if args.profile_stage == "serve":
+        # the served load alone: a target at --serve-scale, then queries
+        # ingested and merged into its index (k_union_rank), one per call
+        from distributedpanga_b200 import synth
+        sc = args.serve_scale
+        contigs = synth.make_target(scale=sc)
+        target = pipeline.Target(synth.fasta_bytes(contigs, "t"))
+        stream = synth.query_stream(contigs, args.warmup + args.steps, 0.0, int(1_000_000 * sc * 10),
+                                    int(200_000_000 * sc), seed=31, median=2_000_000 * max(sc, 0.05))
+        dev = pipeline.Device(0)
+        for k, (_, q) in enumerate(stream):
+            t = time.perf_counter()
+            sizes = dev.serve_load(target, synth.fasta_bytes(q, "q%d_" % k))
+            print(json.dumps({"stage": "serve_load", "target_records": target.nrec, "records": dev.nrec,
+                              "query_bases": int(sizes[5]) - target.bases,
+                              "ms": round(1000 * (time.perf_counter() - t), 3)}), flush=True)
+        dev.close()
+        target.close()
+        return
     cs, _ = make_contigs(args.scale)
     dev = pipeline.Device(0)
     if args.profile_stage == "index":
@@ -702,7 +721,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-entries", action="store_true",
                     help="do not write the reference-format k-mer table entries (saves N x E bytes of HBM)")
-    ap.add_argument("--profile-stage", choices=["index", "ingest"], default=None,
+    ap.add_argument("--profile-stage", choices=["index", "ingest", "serve"], default=None,
                     help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     ap.add_argument("--serve", action="store_true",
                     help="measure the served form (resident target, concurrent requests) beside the plain one")
