@@ -1,6 +1,6 @@
 """Autotuner for the alignment path's launch parameters.
 
-Three knobs change how the device does the work but never what it computes
+Four knobs change how the device does the work but never what it computes
 (each is covered by a parity test that runs the path at several settings):
 
 * ``digit_bits`` -- width of the index sort's first-level digit
@@ -10,12 +10,15 @@ Three knobs change how the device does the work but never what it computes
   (``pga_align_set_build``: 2 CTAs per SM at 255 registers, or 3 at 168);
 * ``range_seeds`` -- how large pairs are cut into band ranges that different
   warps align (``pga_align_set_ranges``: -1 never, or a size in seeds; the
-  automatic size is max(256, seeds / (160 x 2368 warps))).
+  automatic size is max(256, seeds / (160 x 2368 warps)));
+* ``long_waves`` -- after how many wave steps a Local_Alignment call keeps
+  its SM to itself (``pga_align_set_long_waves``; 0 never, default 20000).
 
 ``Tuner.tune`` times every candidate on the GDB loaded in a context (the
 workload itself, or a sample of it): the index knob with the index build
 alone, the alignment knobs with the alignment (diagonal sorts included)
-after one adaptamer merge.  Each candidate runs ``repeats`` times and the
+after one adaptamer merge, the long-call threshold last, with the chosen
+build and range size set.  Each candidate runs ``repeats`` times and the
 one with the lowest median wins.  ``TuneCache`` keeps the choices in a JSON
 file keyed by the workload's signature (bases, contigs, seeds, each to two
 significant digits) so that a recurring workload is tuned once.
@@ -30,6 +33,8 @@ import time
 
 DIGIT_BITS = (18, 19, 20, 21, 22)
 ALIGN_BUILDS = (2, 3)
+LONG_WAVES = (0, 10000, 20000, 40000)
+LONG_WAVES_DEFAULT = 20000
 AUTO_WARPS = 148 * 16          # the alignment launch's task warps
 
 
@@ -113,10 +118,27 @@ class Tuner:
         self.seeds = ns + cs
         return choose(times)
 
+    def tune_long(self, build: int, rs: int, candidates=LONG_WAVES) -> int:
+        d = self.dev
+        times = {}
+        try:
+            d.set_build(build)
+            d.set_ranges(rs)
+            for w in candidates:
+                d.set_long_waves(w)
+                times[w] = self._time(d.align)
+        finally:
+            d.set_build(0)
+            d.set_ranges(0)
+            d.set_long_waves(LONG_WAVES_DEFAULT)
+        self.times["long_waves"] = times
+        return choose(times)
+
     def tune(self) -> dict:
         bits = self.tune_index()
         build, rs = self.tune_align()
-        return {"digit_bits": bits, "align_build": build, "range_seeds": rs}
+        lw = self.tune_long(build, rs)
+        return {"digit_bits": bits, "align_build": build, "range_seeds": rs, "long_waves": lw}
 
 
 def apply(dev, cfg: dict) -> None:
@@ -124,6 +146,7 @@ def apply(dev, cfg: dict) -> None:
     dev.set_digit_bits(int(cfg.get("digit_bits", 0)))
     dev.set_build(int(cfg.get("align_build", 0)))
     dev.set_ranges(int(cfg.get("range_seeds", 0)))
+    dev.set_long_waves(int(cfg.get("long_waves", LONG_WAVES_DEFAULT)))
 
 
 class TuneCache:

@@ -225,6 +225,9 @@ __device__ WarpWork warp_work(const AlignLaunch &P, int64_t wid) {
   W.pool.cap = P.cell_cap;
   W.chunk_next = W.chunk_end = 0;
   W.waves = W.cells = 0;
+  W.smflag = P.smflag;
+  W.long_waves = P.smflag ? P.long_waves : 0;
+  W.flagged = 0;
   return W;
 }
 
@@ -427,6 +430,15 @@ __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch
 
   while (true) {
     unsigned t = 0;
+    if (W.long_waves > 0 && !W.flagged) {
+      // another warp of this SM runs a long call: leave the SM to it (the
+      // queue is drained by the other SMs' warps, and by the flagging warps)
+      unsigned sm, f = 0;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+      if (lane == 0 && sm < SM_FLAGS) f = *(volatile unsigned *)&P.smflag[sm];
+      f = __shfl_sync(FULL, f, 0);
+      if (f) break;
+    }
     if (lane == 0) t = atomicAdd(P.next_task, 1u);
     t = __shfl_sync(FULL, t, 0);
     if (t >= (unsigned)P.ntasks + (unsigned)P.nsmall) break;

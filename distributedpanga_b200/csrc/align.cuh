@@ -48,6 +48,8 @@ struct AlignLaunch {
   const PairTask *tasks;
   int ntasks;
   unsigned *next_task;
+  unsigned *smflag;   // k_align_pairs: SM_FLAGS flags, zero at launch (null: off)
+  int long_waves;     // a wave loop past this many waves flags its SM
   const U128 *keysN, *keysC;
   SeedKeyLayout layN, layC;
   const uint8_t *fwd, *rc;

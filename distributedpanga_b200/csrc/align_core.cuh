@@ -27,6 +27,8 @@ namespace pga {
 namespace aln {
 
 // lib/align.c:164-183
+// Entries of the alignment launch's per-SM long-call flags (above any SM id).
+constexpr unsigned SM_FLAGS = 1024;
 constexpr int TRIM_LEN = 15;
 constexpr int DUB_TRIM = 45;
 constexpr int PATH_LEN = 60;

@@ -46,6 +46,9 @@ struct WarpWork {
   int64_t chunk_next, chunk_end;  // this warp's current pebble chunk (lane-uniform)
   int err;
   int64_t waves, cells;  // waves after the 0-wave, and their diagonals (lane-uniform counts)
+  unsigned *smflag;      // per SM id: a warp there runs a long call (null: not kept)
+  int long_waves;        // waves of one wave loop that make a call long (0: never)
+  int flagged;           // this warp has flagged its SM
 };
 
 constexpr int PEBBLE_CHUNK = 4096;
@@ -968,7 +971,7 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
   R.T = 0;
   bool regmode = false;
   RegCtx X{vmask, W.NA, W.pool.cells, W.pool.next, W.pool.cap, W.chunk_next, W.chunk_end, 0};
-  int nwaves = 0, ncells = 0;
+  int nwaves = 0, ncells = 0, lwaves = 0;
   // the register waves' read-only inputs, held in this loop's registers
   const AlignSpec rspec = spec;
   const Seq rA = A, rB = B;
@@ -1001,6 +1004,16 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
     if (!grow_hi) hgh -= 1;
     const bool use_reg = phgh >= plow && hgh - low + 1 <= 32;
     nwaves += 1;
+    if (W.long_waves > 0 && !W.flagged && ++lwaves >= W.long_waves) {
+      // a long call: the other warps of this SM take no new task, so that it
+      // runs with the SM to itself once their current tasks end
+      if (lane == 0) {
+        unsigned sm;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+        if (sm < SM_FLAGS) atomicExch(&W.smflag[sm], 1u);
+      }
+      W.flagged = 1;
+    }
     ncells += hgh >= low ? hgh - low + 1 : 0;
     WaveSlice WS;
     if (use_reg) {

@@ -108,6 +108,7 @@ struct pga_ctx {
   bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
   int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2 or 3 CTAs per SM
+  int long_waves = 20000;          // pga_align_set_long_waves: a call past this many waves keeps its SM
   int digit_bits = 0;              // pga_index_set_digit_bits: 0 by record count, else 18..22
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
@@ -712,7 +713,10 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     ctx->counters[1] = base[1];
     ctx->counters[2] = base[2];
     ctx->counters[3] = base[3];
-    CK(cudaMemsetAsync(ctx->task_next.p, 0, sizeof(unsigned), ctx->st));
+    // the task counter, and the per-SM long-call flags after it
+    CK(cudaMemsetAsync(ctx->task_next.p, 0, 64 + sizeof(unsigned) * aln::SM_FLAGS, ctx->st));
+    L.smflag = P<unsigned>(ctx->task_next) + 16;
+    L.long_waves = ctx->long_waves;
     CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
     CK(cudaMemcpyAsync(ctx->cand_next.p, &ctx->counters[0], 8, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->rng_next.p, &ctx->counters[1], 8, cudaMemcpyHostToDevice, ctx->st));
@@ -947,7 +951,7 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
   // overflows and reruns the launch.  Buffers keep their size across calls.
   int64_t seqtot = 0;
   for (int c = 0; c < ctx->ncontig; c++) seqtot += ctx->clen[c];
-  ENSURE(ctx->task_next, 64);
+  ENSURE(ctx->task_next, 64 + sizeof(unsigned) * aln::SM_FLAGS);
   ENSURE(ctx->wave, sizeof(int) * (size_t)L.nwarps * L.vcap * WAVE_INTS);
   ENSURE(ctx->points, sizeof(uint16_t) * (size_t)L.nwarps * L.point_cap);
   ENSURE(ctx->ovl, sizeof(aln::Ovl) * (size_t)L.nwarps * 16384);
@@ -1055,7 +1059,7 @@ int run_align(pga_ctx *ctx) {
   if (r0) return r0;
   // 3. work spaces (before the pair lists: running out of memory here is
   // cheap to recover from)
-  AlignLaunch L;
+  AlignLaunch L{};
   r0 = prepare_workspace(ctx, L, ave_path);
   if (r0) return r0;
   ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
@@ -2635,7 +2639,7 @@ int pga_local_alignment(pga_ctx *ctx, int64_t n, const int32_t *req8, int64_t *n
   int ave_path = 0;
   int r = prepare_sequences(ctx, &ave_path);
   if (r) return r;
-  AlignLaunch L;
+  AlignLaunch L{};
   r = prepare_workspace(ctx, L, ave_path);
   if (r) return r;
   ENSURE(ctx->lreq, sizeof(int32_t) * 8 * (size_t)(n + 1));
@@ -2722,6 +2726,12 @@ int pga_align_work(const pga_ctx *ctx, int64_t *work4) {
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
   if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3)) return PGA_ERR_ARG;
   ctx->align_build = ctas_per_sm;
+  return PGA_OK;
+}
+
+int pga_align_set_long_waves(pga_ctx *ctx, int waves) {
+  if (!ctx || waves < 0) return PGA_ERR_ARG;
+  ctx->long_waves = waves;
   return PGA_OK;
 }
 

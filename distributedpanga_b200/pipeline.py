@@ -69,6 +69,7 @@ _SIGS = {
     "pga_align_stats": (C.c_int, [vp, vp]),
     "pga_align_set_ranges": (C.c_int, [vp, C.c_int64]),
     "pga_align_set_build": (C.c_int, [vp, C.c_int]),
+    "pga_align_set_long_waves": (C.c_int, [vp, C.c_int]),
     "pga_index_set_digit_bits": (C.c_int, [vp, C.c_int]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
@@ -419,6 +420,10 @@ class Device:
     def set_build(self, ctas_per_sm: int):
         """Which build of the alignment kernel runs (0 automatic, 2 or 3)."""
         self._ck(self.L.pga_align_set_build(self.h, int(ctas_per_sm)), "align_set_build")
+
+    def set_long_waves(self, waves: int) -> None:
+        """Wave steps after which a call keeps its SM to itself (0: off)."""
+        self._ck(self.L.pga_align_set_long_waves(self.h, int(waves)), "align_set_long_waves")
 
     def set_digit_bits(self, bits: int) -> None:
         """Width of the index sort's first-level digit (0 automatic, 18..22)."""

@@ -213,6 +213,14 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
  * The alignments are the same either way. */
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
 
+/* Tuning, no counterpart in the reference: when one Local_Alignment call of
+ * the alignment launch passes this many wave steps (in one direction), the
+ * other warps on its SM take no new pair task, so that the long call --
+ * which bounds the launch -- soon has the SM to itself; the remaining tasks
+ * go to the other SMs.  0 turns this off; the default is 20000.  The
+ * alignments are the same for every value. */
+int pga_align_set_long_waves(pga_ctx *ctx, int waves);
+
 /* Tuning, no counterpart in the reference: the width in bits (18..22) of the
  * first-level digit of pga_index_build's two-level sort; 0 (the default)
  * takes 18 unless digits would then average more than 8192 records.  The

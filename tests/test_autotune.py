@@ -11,6 +11,7 @@ class FakeDev:
     def __init__(self, index_cost, align_cost):
         self.t = 0.0
         self.bits = self.build = self.ranges = 0
+        self.long = autotune.LONG_WAVES_DEFAULT
         self.index_cost, self.align_cost = index_cost, align_cost
         self.calls = []
 
@@ -26,6 +27,9 @@ class FakeDev:
     def set_ranges(self, r):
         self.ranges = r
 
+    def set_long_waves(self, w):
+        self.long = w
+
     def index_build(self, want_entries=True):
         self.t += self.index_cost(self.bits)
         self.calls.append(("index", self.bits))
@@ -35,7 +39,7 @@ class FakeDev:
         return 300_000_000, 100_000_000
 
     def align(self):
-        self.t += self.align_cost(self.build, self.ranges)
+        self.t += self.align_cost(self.build, self.ranges) - (0.05 if self.long == 10000 else 0.0)
         self.calls.append(("align", self.build, self.ranges))
         return 5
 
@@ -49,7 +53,8 @@ def test_picks_fastest_and_restores_defaults():
     # never-split costs 0.5, sizes above 2000 seeds 0.1: the automatic size
     # (1055 here) ties with its half and comes first
     assert cfg["range_seeds"] == autotune.auto_range_seeds(400_000_000) == 1055
-    assert (d.bits, d.build, d.ranges) == (0, 0, 0)          # automatic again after tuning
+    assert cfg["long_waves"] == 10000
+    assert (d.bits, d.build, d.ranges, d.long) == (0, 0, 0, autotune.LONG_WAVES_DEFAULT)  # defaults again
     assert sum(1 for c in d.calls if c[0] == "index") == 3 * len(autotune.DIGIT_BITS) + 1
     assert set(t.times["digit_bits"]) == set(autotune.DIGIT_BITS)
 
@@ -68,10 +73,10 @@ def test_range_candidates():
 
 def test_apply_and_cache(tmp_path):
     d = FakeDev(lambda b: 1.0, lambda b, r: 1.0)
-    autotune.apply(d, {"digit_bits": 19, "align_build": 2, "range_seeds": -1})
-    assert (d.bits, d.build, d.ranges) == (19, 2, -1)
+    autotune.apply(d, {"digit_bits": 19, "align_build": 2, "range_seeds": -1, "long_waves": 0})
+    assert (d.bits, d.build, d.ranges, d.long) == (19, 2, -1, 0)
     autotune.apply(d, {})
-    assert (d.bits, d.build, d.ranges) == (0, 0, 0)
+    assert (d.bits, d.build, d.ranges, d.long) == (0, 0, 0, autotune.LONG_WAVES_DEFAULT)
     p = str(tmp_path / "tune.json")
     c = autotune.TuneCache(p)
     sig = autotune.signature(200_123_456, 300, 1_234_567_890)

@@ -212,7 +212,9 @@ def test_alignments_independent_of_band_ranges(dev, case):
 
 @pytest.mark.parametrize("case", ["chromset_s0005", "many_contigs"])
 def test_alignments_independent_of_kernel_build(dev, case):
-    """The alignment kernel's two builds (two or three CTAs per SM) give the
+    """The alignment kernel's two builds (two or three CTAs per SM), with the
+    long-call SM flags off, at their default, and at 50 waves (nearly every
+    SM flagged, so that the flagging warps drain most of the queue), give the
     reference's alignments."""
     import gzip
     import os
@@ -226,10 +228,13 @@ def test_alignments_independent_of_kernel_build(dev, case):
     try:
         for build in (3, 2):
             dev.set_build(build)
-            dev.align()
-            assert _aln_norm(alignment_lines(*dev.alignments())) == ref, build
+            for lw in (0, 50, 20000):
+                dev.set_long_waves(lw)
+                dev.align()
+                assert _aln_norm(alignment_lines(*dev.alignments())) == ref, (build, lw)
     finally:
         dev.set_build(0)
+        dev.set_long_waves(20000)
 
 
 @pytest.mark.parametrize("case", ["small_s002", "edge_mix"])
