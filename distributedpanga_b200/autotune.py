@@ -12,7 +12,7 @@ Four knobs change how the device does the work but never what it computes
   warps align (``pga_align_set_ranges``: -1 never, or a size in seeds; the
   automatic size is max(256, seeds / (160 x 2368 warps)));
 * ``long_waves`` -- after how many wave steps a Local_Alignment call keeps
-  its SM to itself (``pga_align_set_long_waves``; 0 never, default 20000).
+  its SM to itself (``pga_align_set_long_waves``; 0 never, -1 automatic).
 
 ``Tuner.tune`` times every candidate on the GDB loaded in a context (the
 workload itself, or a sample of it): the index knob with the index build
@@ -34,7 +34,7 @@ import time
 DIGIT_BITS = (18, 19, 20, 21, 22)
 ALIGN_BUILDS = (2, 3)
 LONG_WAVES = (0, 10000, 20000, 40000)
-LONG_WAVES_DEFAULT = 20000
+LONG_WAVES_DEFAULT = -1        # automatic: 20000 for the two-CTA build, off for the three-CTA one
 AUTO_WARPS = 148 * 16          # the alignment launch's task warps
 
 

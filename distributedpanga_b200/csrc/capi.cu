@@ -108,7 +108,7 @@ struct pga_ctx {
   bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
   int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2 or 3 CTAs per SM
-  int long_waves = 20000;          // pga_align_set_long_waves: a call past this many waves keeps its SM
+  int long_waves = -1;             // pga_align_set_long_waves: -1 automatic, 0 off, else the wave count
   int digit_bits = 0;              // pga_index_set_digit_bits: 0 by record count, else 18..22
   // pool use over the launches of one pga_align: candidate trace bytes,
   // range candidates, survivors, survivor trace bytes
@@ -135,6 +135,9 @@ struct pga_target {
 };
 
 namespace {
+
+// Wave steps after which a call keeps its SM (pga_align_set_long_waves, automatic).
+constexpr int LONG_WAVES_AUTO = 20000;
 
 int fail(pga_ctx *c, int code, const char *fmt, ...) {
   va_list ap;
@@ -716,7 +719,10 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     // the task counter, and the per-SM long-call flags after it
     CK(cudaMemsetAsync(ctx->task_next.p, 0, 64 + sizeof(unsigned) * aln::SM_FLAGS, ctx->st));
     L.smflag = P<unsigned>(ctx->task_next) + 16;
-    L.long_waves = ctx->long_waves;
+    // automatic: on for launches bounded by their longest calls, off for the
+    // throughput-bound ones (the three-CTA build), whose flagged SMs would
+    // idle warps that still have queue work
+    L.long_waves = ctx->long_waves >= 0 ? ctx->long_waves : (L.min_blocks == 3 ? 0 : LONG_WAVES_AUTO);
     CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
     CK(cudaMemcpyAsync(ctx->cand_next.p, &ctx->counters[0], 8, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->rng_next.p, &ctx->counters[1], 8, cudaMemcpyHostToDevice, ctx->st));
@@ -2730,7 +2736,7 @@ int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
 }
 
 int pga_align_set_long_waves(pga_ctx *ctx, int waves) {
-  if (!ctx || waves < 0) return PGA_ERR_ARG;
+  if (!ctx || waves < -1) return PGA_ERR_ARG;
   ctx->long_waves = waves;
   return PGA_OK;
 }

@@ -422,7 +422,7 @@ class Device:
         self._ck(self.L.pga_align_set_build(self.h, int(ctas_per_sm)), "align_set_build")
 
     def set_long_waves(self, waves: int) -> None:
-        """Wave steps after which a call keeps its SM to itself (0: off)."""
+        """Wave steps after which a call keeps its SM to itself (0 off, -1 automatic)."""
         self._ck(self.L.pga_align_set_long_waves(self.h, int(waves)), "align_set_long_waves")
 
     def set_digit_bits(self, bits: int) -> None:

@@ -213,7 +213,7 @@ def test_alignments_independent_of_band_ranges(dev, case):
 @pytest.mark.parametrize("case", ["chromset_s0005", "many_contigs"])
 def test_alignments_independent_of_kernel_build(dev, case):
     """The alignment kernel's two builds (two or three CTAs per SM), with the
-    long-call SM flags off, at their default, and at 50 waves (nearly every
+    long-call SM flags off, at 20000 waves, and at 50 waves (nearly every
     SM flagged, so that the flagging warps drain most of the queue), give the
     reference's alignments."""
     import gzip
@@ -234,7 +234,7 @@ def test_alignments_independent_of_kernel_build(dev, case):
                 assert _aln_norm(alignment_lines(*dev.alignments())) == ref, (build, lw)
     finally:
         dev.set_build(0)
-        dev.set_long_waves(20000)
+        dev.set_long_waves(-1)
 
 
 @pytest.mark.parametrize("case", ["small_s002", "edge_mix"])
