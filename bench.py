@@ -591,7 +591,20 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
 
 def run_serve(args) -> None:
-    print(json.dumps(serve_measure(args)), flush=True)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        line = serve_measure(args)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
 
 
 def serve_measure(args) -> dict:
@@ -606,6 +619,9 @@ def serve_measure(args) -> dict:
     is compared with the plain one (alignment records and trace bytes)."""
     from distributedpanga_b200 import build, pipeline, serve, synth
     build.build()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     sc = args.serve_scale
     contigs = synth.make_target(scale=sc)
     ttext = synth.fasta_bytes(contigs, "t")
@@ -614,11 +630,12 @@ def serve_measure(args) -> dict:
     reqs = [serve.Request(k, synth.fasta_bytes(q, "q%d_" % k), arr, sum(len(c) for c in q))
             for k, (arr, q) in enumerate(stream)]
     t = time.monotonic()
-    target = pipeline.Target(ttext)
+    # one replica of the target per GPU; rank r serves the requests whose id
+    # is congruent to r
+    target = pipeline.Target(ttext, device=local_rank)
     target_s = time.monotonic() - t
     srv = serve.Server(target, slots=args.serve_slots)
-    dp = pipeline.Device(0)
-    phases = {}
+    dp = pipeline.Device(local_rank)
 
     def served(slot, r):
         # Server.execute with the host wall time of each call
@@ -631,9 +648,8 @@ def serve_measure(args) -> dict:
         t3 = time.monotonic()
         al = d.alignments()
         t4 = time.monotonic()
-        phases[("s", r.rid)] = [t1 - t0, t2 - t1, t3 - t2, t4 - t3]
         return {"nalign": n, "gdb_bases": int(sizes[5]), "query_bases": int(sizes[5]) - target.bases,
-                "records": d.nrec, "alignments": al}
+                "records": d.nrec, "alignments": al, "phases": [t1 - t0, t2 - t1, t3 - t2, t4 - t3]}
 
     def plain(slot, r):
         t0 = time.monotonic()
@@ -646,25 +662,25 @@ def serve_measure(args) -> dict:
         t3 = time.monotonic()
         al = dp.alignments()
         t4 = time.monotonic()
-        phases[("p", r.rid)] = [t1 - t0, t2 - t1, t3 - t2, t4 - t3]
         return {"nalign": n, "gdb_bases": target.bases + r.bases, "query_bases": r.bases, "records": dp.nrec,
-                "alignments": al}
+                "alignments": al, "phases": [t1 - t0, t2 - t1, t3 - t2, t4 - t3]}
 
     # warm-up: the largest request on every slot and on the plain context
     # (kernels loaded, every buffer at its largest size)
     big = max(reqs, key=lambda r: r.bases)
     srv.sched.run([serve.Request(k, big.text, 0.0, big.bases) for k in range(args.serve_slots)], served)
     plain(0, big)
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local_rank)
     clocks.start()
-    t = time.monotonic()
-    res = srv.sched.run(reqs, served)
-    summ = serve.summarize(res, time.monotonic() - t)
+    res, summ = serve.serve_sharded(reqs, lambda mine: srv.sched.run(mine, served), rank, world)
     plain_sched = serve.Scheduler(1, 1 << 62, lambda r: 0)
-    t = time.monotonic()
-    pres = plain_sched.run(reqs, plain)
-    psumm = serve.summarize(pres, time.monotonic() - t)
+    pres, psumm = serve.serve_sharded(reqs, lambda mine: plain_sched.run(mine, plain), rank, world)
     clk = clocks.stop()
+    if rank != 0:
+        srv.close()
+        dp.close()
+        target.close()
+        return None
     same = 0
     for a, b in zip(res, pres):
         if a.out["nalign"] == b.out["nalign"] and all(np.array_equal(x, y) for x, y in
@@ -676,12 +692,14 @@ def serve_measure(args) -> dict:
     line = {
         "metric": "served aligned Mbp/s (GDB bases of target + query per request / wall s) with p50/p99 request "
                   "latency, beside the plain form",
-        "value": round(summ["gdb_mbp_per_s"], 2), "unit": "Mbp/s", "higher_is_better": True, "n_gpus": 1,
+        "value": round(summ["gdb_mbp_per_s"], 2), "unit": "Mbp/s", "higher_is_better": True, "n_gpus": world,
+        "scaling": "strong",
         "data": "synthetic (seeded)", "dtype": "u8",
         "config": {"workload": "serve: resident target of %d Mbp (chromset generator), %d Poisson requests at "
                                "%.1f/s, query sizes log-uniform %.1f-%.1f Mbp, divergence 0.5-5%%; k=40, FREQ=10"
                                % (round(target.bases / 1e6), len(reqs), args.serve_rate, 10 * sc, 200 * sc),
                    "slots": args.serve_slots, "target_contigs": target.ncontig,
+                   "parallelism": "replicas%d: one resident target per GPU, requests sharded by id" % world,
                    "target_build_s": round(target_s, 3)},
         "served": {k: round(v, 4) if isinstance(v, float) else v for k, v in summ.items()},
         "plain": {k: round(v, 4) if isinstance(v, float) else v for k, v in psumm.items()},
@@ -690,8 +708,8 @@ def serve_measure(args) -> dict:
         "requests": [{"rid": r.rid, "query_mbp": round(q.bases / 1e6, 3), "arrival_s": round(r.arrival, 3),
                       "served_latency_s": round(r.latency, 3), "plain_latency_s": round(p.latency, 3),
                       "alignments": r.out["nalign"],
-                      "served_phases_s": [round(x, 3) for x in phases[("s", r.rid)]],
-                      "plain_phases_s": [round(x, 3) for x in phases[("p", r.rid)]]}
+                      "served_phases_s": [round(x, 3) for x in r.out["phases"]],
+                      "plain_phases_s": [round(x, 3) for x in p.out["phases"]]}
                      for r, p, q in zip(res, pres, reqs)],
         "phases": "load+index (served: query ingest + union with the resident index; plain: ingest of both texts + "
                   "index build), adaptamer merge, alignment (diagonal sorts included), alignments to the host; "

@@ -230,3 +230,36 @@ def plain_request(dev, target_text: bytes, query_text: bytes, nthr: int = 0, fre
     dev.merge(freq)
     n = dev.align()
     return {"nalign": n, "alignments": dev.alignments(), "records": dev.nrec}
+
+
+def shard(requests: list, rank: int, world: int) -> list:
+    """The requests rank `rank` of `world` serves: request ids congruent to
+    the rank (each GPU keeps its own replica of the target)."""
+    return [r for r in requests if r.rid % world == rank]
+
+
+def serve_sharded(requests: list, run_local, rank: int, world: int) -> tuple:
+    """Runs this rank's share of `requests` with `run_local(reqs) -> results`
+    between two barriers and gathers every rank's results on rank 0, which
+    gets (all results in request order, summary with wall = the slowest
+    rank's); other ranks get (None, None).  Without an initialised process
+    group (world 1) it is run_local and summarize."""
+    import torch.distributed as dist
+    mine = shard(requests, rank, world)
+    dist_on = world > 1 and dist.is_available() and dist.is_initialized()
+    if dist_on:
+        dist.barrier()
+    t = time.monotonic()
+    res = run_local(mine)
+    wall = time.monotonic() - t
+    if dist_on:
+        dist.barrier()
+        box = [None] * world
+        dist.all_gather_object(box, (wall, res))
+        if rank != 0:
+            return None, None
+        wall = max(w for w, _ in box)
+        res = [r for _, rs in box for r in rs]
+    order = {r.rid: i for i, r in enumerate(requests)}
+    res.sort(key=lambda r: order[r.rid])
+    return res, summarize(res, wall)
