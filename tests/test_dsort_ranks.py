@@ -1,0 +1,93 @@
+"""The distributed index build (distributedpanga_b200.dsort, the reference's
+stage 2) on CPU over gloo: ranks holding the records of their own contigs
+exchange them by 10-bit bucket, sort locally and fix the seam LCPs; the ranks'
+buffers in rank order equal the single-process sorted index byte for byte.
+The local sort here is the oracle's (on GPUs it is Device.sort_records)."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _contig_of(rec: np.ndarray, ctgb: int) -> np.ndarray:
+    v = np.zeros(len(rec), dtype=np.int64)
+    for b in range(ctgb):
+        v |= rec[:, rec.shape[1] - ctgb + b].astype(np.int64) << (8 * b)
+    return v & ((1 << (8 * ctgb - 1)) - 1)
+
+
+def _worker(rank, world, port, case, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import load_case
+    from distributedpanga_b200 import dsort, gdb
+    from oracle import binding as orc
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cs, _ = load_case(case)
+        posb, ctgb, _ = gdb.record_sizing(cs)
+        allrec = orc.extract(cs, posb, ctgb)
+        mine = allrec[_contig_of(allrec, ctgb) % world == rank]
+        got = dsort.run_stage2(mine, lambda r: orc.sort_records(r))
+        out[rank] = got.tobytes()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case,world", [("small_s002", 2), ("edge_mix", 3)])
+def test_stage2_equals_single_process_index(oracle, case, world):
+    from conftest import load_case
+    from distributedpanga_b200 import gdb
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_worker, args=(world, port, case, out), nprocs=world, start_method="spawn", join=True)
+        parts = [out[r] for r in range(world)]
+    cs, _ = load_case(case)
+    posb, ctgb, rsize = gdb.record_sizing(cs)
+    want = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    got = np.frombuffer(b"".join(parts), dtype=np.uint8).reshape(-1, want.shape[1])
+    assert sum(len(p) for p in parts) == want.size
+    assert all(len(p) > 0 for p in parts)                 # every rank got a share
+    assert np.array_equal(got, want)
+
+
+def test_destination_map_and_helpers():
+    from distributedpanga_b200 import dsort
+    rng = np.random.default_rng(5)
+    for world in (1, 2, 3, 8, 127):
+        counts = rng.integers(0, 50, dsort.NUM_BUCK)
+        counts[rng.integers(0, dsort.NUM_BUCK, 200)] = 0
+        ksplit, select = dsort.compute_destination_map(counts, world)
+        assert ksplit[0] == 0 and ksplit[world] == dsort.NUM_BUCK
+        assert select.min() >= 0 and select.max() <= world - 1
+        assert np.all(np.diff(select) >= 0)                # contiguous bucket ranges per rank
+        loads = np.bincount(select, weights=counts, minlength=world)
+        assert loads.sum() == counts.sum()
+        if world > 1:
+            assert loads.max() <= counts.sum() / world + counts.max() + 1
+    # no records at all: every bucket still has a rank
+    k, s = dsort.compute_destination_map(np.zeros(dsort.NUM_BUCK, np.int64), 4)
+    assert s.min() >= 0 and s.max() <= 3
+    x = np.array([0x1b] * 10, np.uint8)
+    y = x.copy()
+    assert dsort.kmer_lcp_bases(x, y) == 40
+    y[3] ^= 0x04                                           # third base of byte 3 differs
+    assert dsort.kmer_lcp_bases(x, y) == 14
+    rec = np.zeros((3, 16), np.uint8)
+    rec[:, 1] = [5, 3, 7]
+    assert dsort.verify_per_rank_sorted(rec) == (1, 1)
