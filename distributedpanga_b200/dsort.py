@@ -128,9 +128,11 @@ def _device_of(group=None):
         else torch.device("cpu")
 
 
-def verify_cross_rank_boundaries(records: np.ndarray, group=None):
-    """(violations over all ranks, the last k-mer of the nearest non-empty
-    rank before this one or None)."""
+def verify_cross_rank_boundaries(records: np.ndarray, group=None, local_bad: int = 0):
+    """(boundary violations over all ranks, the last k-mer of the nearest
+    non-empty rank before this one or None, local_bad summed over all
+    ranks).  Every rank takes the same two collectives whatever its
+    records, so a failure anywhere is seen everywhere."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
@@ -152,9 +154,9 @@ def verify_cross_rank_boundaries(records: np.ndarray, group=None):
     if prev is not None and len(records):
         first = records[0, KMER_OFFSET:KMER_OFFSET + KBYTES]
         bad = int(bytes(prev) > bytes(first))
-    t = torch.tensor([bad], dtype=torch.int64, device=dev)
+    t = torch.tensor([bad, int(local_bad)], dtype=torch.int64, device=dev)
     dist.all_reduce(t, group=group)
-    return int(t.item()), prev
+    return int(t[0].item()), prev, int(t[1].item())
 
 
 def run_stage2(records: np.ndarray, sort_fn, group=None) -> np.ndarray:
@@ -183,9 +185,10 @@ def run_stage2(records: np.ndarray, sort_fn, group=None) -> np.ndarray:
     recv = out.cpu().numpy().reshape(-1, rsize)
     recv = sort_fn(recv) if len(recv) else recv.copy()
     nbad, first_bad = verify_per_rank_sorted(recv)
-    if nbad:
-        raise Stage2Error("rank %d: local sort check failed (%d violations, first at %d)" % (rank, nbad, first_bad))
-    boundary_bad, prev = verify_cross_rank_boundaries(recv, group)
+    boundary_bad, prev, all_bad = verify_cross_rank_boundaries(recv, group, nbad)
+    if all_bad:
+        raise Stage2Error("local sort check failed: %d violations over all ranks (rank %d: %d, first at %d)"
+                          % (all_bad, rank, nbad, first_bad))
     if boundary_bad:
         raise Stage2Error("cross-rank boundary check failed (%d ranks)" % boundary_bad)
     if prev is not None and len(recv):

@@ -66,6 +66,37 @@ def test_stage2_equals_single_process_index(oracle, case, world):
     assert np.array_equal(got, want)
 
 
+def _bad_sort_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    from distributedpanga_b200 import dsort
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(rank)
+        rec = rng.integers(0, 256, (500, 16)).astype(np.uint8)
+        # rank 1's local sort is broken (returns its input unsorted); every
+        # rank must learn of it after the same collectives and raise
+        sort_fn = (lambda r: r) if rank == 1 else (lambda r: r[np.lexsort(r[:, 10:0:-1].T)])
+        try:
+            dsort.run_stage2(rec, sort_fn)
+            out[rank] = "no error"
+        except dsort.Stage2Error as e:
+            out[rank] = str(e)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_rank_fails_every_rank():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_bad_sort_worker, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
+        res = dict(out)
+    assert all("local sort check failed" in res[r] for r in range(world)), res
+
+
 def test_destination_map_and_helpers():
     from distributedpanga_b200 import dsort
     rng = np.random.default_rng(5)
