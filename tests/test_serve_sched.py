@@ -86,13 +86,14 @@ def test_oversized_request_runs_alone():
 
 
 def test_arrivals_are_waited_for():
-    rs = reqs([0.0, 0.15, 0.3], [1, 1, 1])
+    rs = reqs([0.0, 0.5, 1.0], [1, 1, 1])
     sch = Scheduler(4, 10 ** 9, lambda r: r.bases)
     rec = Recorder({i: 0.01 for i in range(3)}, sch)
     res = sch.run(rs, rec)
     for r in res:
-        assert r.admitted >= r.arrival - 1e-6
-        assert r.latency < 0.15          # nothing queued behind anything
+        assert r.admitted >= r.arrival - 1e-6   # not before it arrives
+        assert r.latency < 0.45                 # nothing queued behind anything
+    assert res[2].done >= 1.0
 
 
 def test_failure_is_raised_after_in_flight_finish():
