@@ -45,7 +45,7 @@ def reqs(arrivals, sizes):
 def test_fifo_and_slot_limit():
     rs = reqs([0.0] * 6, [10] * 6)
     sch = Scheduler(2, 10 ** 9, lambda r: r.bases)
-    rec = Recorder({i: 0.02 for i in range(6)}, sch)
+    rec = Recorder({i: 0.1 for i in range(6)}, sch)
     res = sch.run(rs, rec)
     assert rec.order == list(range(6))
     assert rec.max_running == 2
@@ -68,7 +68,7 @@ def test_budget_limits_concurrency_by_high_water():
 def test_small_requests_share_the_budget():
     rs = reqs([0.0] * 6, [30] * 6)
     sch = Scheduler(3, 100, lambda r: r.bases)
-    rec = Recorder({i: 0.05 for i in range(6)}, sch)
+    rec = Recorder({i: 0.2 for i in range(6)}, sch)
     sch.run(rs, rec)
     assert rec.max_running == 3
     assert rec.max_held <= 100
