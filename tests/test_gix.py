@@ -97,7 +97,10 @@ def gixmake(cs, work: str) -> str:
             s = letters[cs.contig(i)].tobytes()
             f.write(b">ctg%d\n" % i + b"".join(s[j:j + 80] + b"\n" for j in range(0, len(s), 80)))
     B.ref_make_gdb(fa, os.path.join(work, "g"))
-    subprocess.run([os.path.join(REF_DIR, "GIXmake_dump"), "-T8", os.path.join(work, "g.1gdb")], check=True,
+    # One thread: with -T8, on a loaded host, GIXmake now and then writes one
+    # entry's LCP against the wrong predecessor (seen once in ~30 runs under
+    # load: 6 where the first base differs); its parts are the same with -T1.
+    subprocess.run([os.path.join(REF_DIR, "GIXmake_dump"), "-T1", os.path.join(work, "g.1gdb")], check=True,
                    capture_output=True, cwd=work)
     return os.path.join(work, "g")
 
