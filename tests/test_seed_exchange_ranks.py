@@ -2,7 +2,9 @@
 the reference's stage 3 routing) on CPU over gloo: after the distributed
 index build each rank merges its own bucket range (the oracle's k-mer table
 and adaptamer merge here; the device drop-ins on GPUs) and routes its seeds;
-each rank then holds exactly the single-process seeds of the pairs it owns."""
+each rank then holds exactly the single-process seeds of the pairs it owns,
+and its diagonal sort gives the single-process panels restricted to those
+pairs, in the same order."""
 import os
 import socket
 import sys
@@ -48,7 +50,11 @@ def _worker(rank, world, port, case, out):
         rfp = sx.rank_for_pair(owner)
         rn = sx.redistribute_seeds(ns, posb, ctgb, rfp)
         rc = sx.redistribute_seeds(css, posb, ctgb, rfp)
-        out[rank] = (rn.tobytes(), rc.tobytes())
+        # each rank's diagonal sort of what it received
+        dbyte, _ = gdb.diag_sizing(cs, ctgb)
+        panels = [orc.reimport_sort(u, posb, ctgb, comp, cs.ncontig, cs.maxctg, dbyte)
+                  for comp, u in ((0, rn), (1, rc))]
+        out[rank] = (rn.tobytes(), rc.tobytes(), [(a.tobytes(), o.tolist()) for a, o in panels])
     finally:
         dist.destroy_process_group()
 
@@ -81,6 +87,26 @@ def test_each_rank_gets_the_seeds_of_its_pairs(oracle, case, world):
             assert np.array_equal(_rows(got), _rows(want)), (unit, r)
             total[unit] += len(got)
     assert total == [len(ns), len(css)] and total[0] > 0
+    # the ranks' diagonal-sorted panels are the single-process panels, each
+    # restricted to the pairs the rank owns, in the same order
+    dbyte, _ = gdb.diag_sizing(cs, ctgb)
+    for unit, allseeds in ((0, ns), (1, css)):
+        arr, off = oracle.reimport_sort(allseeds, posb, ctgb, unit, cs.ncontig, cs.maxctg, dbyte)
+        sw = arr.shape[1] if arr.ndim == 2 else 0
+        if len(arr) == 0:
+            continue
+        j = np.zeros(len(arr), dtype=np.int64)
+        for bb in range(ctgb):
+            j |= arr[:, sw - ctgb + bb].astype(np.int64) << (8 * bb)
+        j &= (1 << (8 * ctgb - 1)) - 1
+        a_of = np.repeat(np.arange(cs.ncontig), np.diff(np.asarray(off)))
+        for r in range(world):
+            got, goff = res[r][2][unit]
+            got = np.frombuffer(got, dtype=np.uint8).reshape(-1, sw)
+            keep = rfp[a_of, j] == r
+            assert np.array_equal(got, arr[keep]), (unit, r)
+            want_off = np.concatenate([[0], np.cumsum(np.bincount(a_of[keep], minlength=cs.ncontig))])
+            assert np.array_equal(np.asarray(goff), want_off), (unit, r)
 
 
 def test_assignment_and_plan():
