@@ -1,8 +1,9 @@
 // Alignment stage on the GPU: every (anchor, partner) contig pair of a unit
 // is one task; a persistent kernel gives each warp the next task (tasks come
 // largest first), and the warp runs FastGA's chain driver and Local_Alignment
-// for it (align_core.cuh, align_warp.cuh), then the pair's sort / elimination
-// / entwine step on lane 0, and appends the surviving alignments.
+// for it (align_core.cuh, align_warp.cuh), then the pair's finishing step
+// (finish.cuh: sort, elimination, joining) on the warp's lanes, and appends
+// the surviving alignments.
 //
 // Reference: search_seeds / align_contigs / Local_Alignment
 // (src/fastga_pipeline.c:576-1138, lib/align.c:1423-1576).
@@ -11,6 +12,7 @@
 #include <cuda_runtime.h>
 #include "align.cuh"
 #include "align_warp.cuh"
+#include "finish.cuh"
 #include "seeds.cuh"
 
 namespace pga {
@@ -300,15 +302,9 @@ __device__ int64_t next_band_start(const KeySeeds &S, int64_t x, int64_t hi, int
 // survivors appended to the output in the pair's order (lane 0 ranks them).
 __device__ void finish_and_emit(const AlignLaunch &P, OvlArena &O, int a, int b, int comp, PairOut &po,
                                 int lane) {
-  if (lane == 0) finish_pair(O);
-  __syncwarp();
-  // lane 0 may have taken trace bytes from the pool (entwine merges): every
-  // lane continues from its chunk
-  O.nbyte = __shfl_sync(FULL, O.nbyte, 0);
-  O.byte_cap = __shfl_sync(FULL, O.byte_cap, 0);
-  int ferr = __shfl_sync(FULL, O.err, 0);
-  if (ferr) {
-    po.err = ferr | 0x200;
+  finish_candidates(Lanes{}, O);  // every lane, with the same O
+  if (O.err) {
+    po.err = O.err | 0x200;
     return;
   }
   int ns = 0;

@@ -2206,8 +2206,9 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb,
   if (!ctx || len < 0 || (len > 0 && (!seeds || !out)) || !panel_off || posb < 1 || posb > 4 || ctgb < 1 ||
       ctgb > 2 || (comp != 0 && comp != 1) || ncontig < 1 || dbyte < 1 || dbyte > 4 || amxpos < 0)
     return PGA_ERR_ARG;
-  CK(cudaSetDevice(ctx->device));
   int sb = 1 + 2 * (posb + ctgb);
+  if (len % sb != 0) return fail(ctx, PGA_ERR_ARG, "seed bytes not a whole number of seeds");
+  CK(cudaSetDevice(ctx->device));
   int64_t n = len / sb;
   if (n >= (int64_t)0xffffffffLL) return fail(ctx, PGA_ERR_LIMIT, "too many seeds");
   ENSURE(ctx->io, (size_t)len + 16);

@@ -16,6 +16,7 @@
 // last call's contents, and this code clears what must start at zero.
 #include <cstdint>
 #include <mutex>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "merge.cuh"
@@ -47,22 +48,41 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 namespace {
 
 constexpr int MAX_DEVICES = 128;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
 std::mutex g_setup_mu;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CUcontext g_scratch_ctx[MAX_DEVICES] = {nullptr};
 unsigned char *g_scratch_dev[MAX_DEVICES] = {nullptr};
 
-// Device address of the scratch on the current device, looked up once per
-// device (with that device current).
+// Device address of the scratch on the current device.  The address is
+// looked up with that device current and kept with the context it belongs
+// to; when the device's context is a different one (cudaDeviceReset and a
+// new primary context load the module again, possibly elsewhere) it is
+// looked up again.  The context comes from the driver's cuCtxGetCurrent,
+// reached through the runtime so that the library needs no link to libcuda.
 cudaError_t scratch_address(unsigned char **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+  e = cudaFree(nullptr);  // makes the device's primary context current
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (g_scratch_dev[dev] == nullptr) {
+  if (g_ctx_get_current == nullptr) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || fn == nullptr) return cudaErrorUnknown;
+    g_ctx_get_current = (CtxGetCurrentFn)fn;
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return cudaErrorUnknown;
+  if (g_scratch_dev[dev] == nullptr || g_scratch_ctx[dev] != ctx) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_dev[dev] = (unsigned char *)p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_dev[dev];
   return cudaSuccess;
@@ -95,6 +115,7 @@ extern "C" int pga_reimport_sort_noalloc(const uint8_t *seeds_dev, int64_t len, 
       amxpos < 0)
     return PGA_ERR_ARG;
   const int sb = 1 + 2 * (posb + ctgb);
+  if (len % sb != 0) return PGA_ERR_ARG;  // not a whole number of seeds
   const int64_t n = len / sb;
   if (n > NOALLOC_MAX_SEEDS) return PGA_ERR_LIMIT;
   cudaStream_t st = (cudaStream_t)stream;

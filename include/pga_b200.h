@@ -146,7 +146,8 @@ int pga_self_adaptamer_merge(pga_ctx *ctx, const uint8_t *entries, const int64_t
  * lib/RSDsort.c:292): `len` bytes of seeds -> swide-byte records, panel by A
  * contig, each panel sorted; panel_off (ncontig+1) gets record offsets.
  * comp = 0 for N seeds, 1 for C.  out needs (len/seed_bytes) * swide bytes,
- * swide = 2*dbyte + contig_strand_bytes + 2. */
+ * swide = 2*dbyte + contig_strand_bytes + 2.  `len` must be a whole number
+ * of seeds (PGA_ERR_ARG otherwise). */
 int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int position_bytes,
                       int contig_strand_bytes, int comp, int ncontig, int64_t amxpos, int dbyte,
                       uint8_t *out, int64_t *panel_off);
@@ -340,9 +341,11 @@ int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, co
  * (ncontig+1 int64); no context is needed.  All other work space is one
  * fixed array compiled into the library (about 12 MB, held on every GPU that
  * loads it until the process exits).  At most 262,144 seeds per call
- * (PGA_ERR_LIMIT beyond).  The first call on a device looks the array's
- * address up once for that device; make that first call before any stream
- * capture.  The call synchronizes `stream` (a cudaStream_t, NULL for the
+ * (PGA_ERR_LIMIT beyond); `len` must be a whole number of seeds
+ * (PGA_ERR_ARG otherwise).  The first call on a device looks the array's
+ * address up for that device (and looks it up again after the device's
+ * context was re-created, e.g. by cudaDeviceReset); make that first call
+ * before any stream capture.  The call synchronizes `stream` (a cudaStream_t, NULL for the
  * default stream) once, midway; the last kernels are left queued on it.
  * Calls share the array: calls that overlap on the GPU (several host
  * threads or streams) race.  Returns PGA_OK, PGA_ERR_ARG, PGA_ERR_LIMIT or

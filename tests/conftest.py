@@ -15,7 +15,11 @@ sys.path.insert(0, ROOT)
 
 GOLDEN_CASES = ["small_s002", "chromset_s0005", "edge_mix", "many_contigs"]
 # golden cases whose inputs are regenerated from the seeded generator
-REGENERATED = {"small_full": ("small", 1.0)}
+REGENERATED = {"small_full": ("small", 1.0), "chromset_full": ("chromset", 1.0), "full_s001": ("full", 0.01),
+               "pangenome_s002": ("pangenome", 0.02)}
+# large golden cases (digests only, tests/helpers.py check_*_large)
+LARGE_CASES = [c for c in ("full_s001", "pangenome_s002", "chromset_full")
+               if os.path.exists(os.path.join(GOLDEN, c + ".json"))]
 
 
 def pytest_configure(config):

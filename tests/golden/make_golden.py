@@ -13,6 +13,13 @@ hooks -> alndump).  It stores
                      diagonal panels, and the .1aln record stream
   <case>.aln.txt.gz  the .1aln record stream itself (alndump text)
 
+Large cases (LARGE below: the benchmarked 2 x 100 Mbp workload and a 20 Mbp
+sample of the 2 x 1 Gbp generator) store only <case>.json, with
+order-independent multiset digests (tests/helpers.py multiset_digest) in
+place of sorted-row hashes, hashes of the per-contig arrays, and a hash per
+block of 1000 alignments; their inputs are regenerated from the seeded
+generator and pinned by input_sha.
+
 Usage (needs oracle/_ref, i.e. `make -C oracle ref` with the reference tree
 present):  python tests/golden/make_golden.py [case ...]
 """
@@ -32,7 +39,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
 from distributedpanga_b200 import gdb, synth  # noqa: E402
+from helpers import lines_digest, multiset_digest  # noqa: E402
 from oracle import binding as B  # noqa: E402
 
 
@@ -85,13 +95,22 @@ CASES = {
 # (input_sha pins them) instead of being stored.
 REGENERATED = {"small_full"}
 
+# Large cases: digests only (see the module docstring).  The reference's
+# pipeline takes about 20 s (full_s001) and 3 min (chromset_full) here.
+LARGE = {
+    "chromset_full": lambda: synth.make("chromset"),
+    "full_s001": lambda: synth.make("full", scale=0.01),
+    "pangenome_s002": lambda: synth.make("pangenome", scale=0.02),
+}
+
 
 def sha(a) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
 def run_case(name: str) -> None:
-    contigs = CASES[name]()
+    large = name in LARGE
+    contigs = LARGE[name]() if large else CASES[name]()
     cs = gdb.from_contigs(contigs)
     posb, ctgb, rsize = gdb.record_sizing(cs)
     dbyte, swide = gdb.diag_sizing(cs, ctgb)
@@ -120,14 +139,21 @@ def run_case(name: str) -> None:
                     panel = np.frombuffer(f.read(8 * npart), np.int64) // sw
                 diag[u] = {"swide": sw, "count": nel, "sha": sha(arr), "panel": panel.tolist()}
             else:
+                panel = np.zeros(cs.ncontig, np.int64)
                 diag[u] = {"swide": swide, "count": 0, "sha": sha(np.zeros((0, swide), np.uint8)),
                            "panel": [0] * cs.ncontig}
+            if large:
+                diag[u]["panel_sha"] = sha(np.asarray(panel, np.int64))
+                del diag[u]["panel"]
         aln = subprocess.run([os.path.join(B.REF_DIR, "alndump"), out["aln"]], check=True,
                              capture_output=True, text=True).stdout
         with open(stem + ".gix", "rb") as f:
             f.seek(4 * 4 + 8 * (1 << 24) + 4 * 3 + 8 + 4 * 2)
             gix_perm = np.frombuffer(f.read(4 * cs.ncontig), np.int32).tolist()
     lines = [l for l in aln.split("\n") if l and not l.startswith("#")]
+    if large:
+        write_large(name, cs, posb, ctgb, rsize, dbyte, swide, rec, ns, css, nb, cb, diag, lines, gix_perm)
+        return
     pre = (rec[:, 1].astype(np.int64) << 16) | (rec[:, 2].astype(np.int64) << 8) | rec[:, 3]
     cum = np.cumsum(np.bincount(pre, minlength=1 << 24)).astype(np.int64) if len(rec) else np.zeros(1 << 24, np.int64)
     dig = {
@@ -157,8 +183,33 @@ def run_case(name: str) -> None:
           "aln", len(lines))
 
 
+def write_large(name, cs, posb, ctgb, rsize, dbyte, swide, rec, ns, css, nb, cb, diag, lines, gix_perm):
+    from helpers import prefix_cum
+    norm = [" ".join(l.split()) for l in lines]
+    dig = {
+        "case": name, "large": True,
+        "ncontig": cs.ncontig, "maxctg": cs.maxctg, "seqtot": cs.seqtot,
+        "posb": posb, "ctgb": ctgb, "rsize": rsize, "dbyte": dbyte, "swide": swide, "freq_cutoff": 10,
+        "input_sha": sha(cs.bps) + sha(cs.clen) + sha(cs.boff),
+        "index": {"count": int(rec.shape[0]), "records_multiset": multiset_digest(rec[:, 1:]),
+                  "lcp_sha": sha(rec[:, 0]), "kmer_sha": sha(rec[:, 1:11]),
+                  "cum_sha": sha(prefix_cum(rec)) if len(rec) else sha(np.zeros(1 << 24, np.int64))},
+        "seeds": {"seed_bytes": 1 + 2 * (posb + ctgb), "n_count": int(ns.shape[0]), "c_count": int(css.shape[0]),
+                  "n_multiset": multiset_digest(ns), "c_multiset": multiset_digest(css),
+                  "nbuck_sha": sha(np.asarray(nb, np.int64)), "cbuck_sha": sha(np.asarray(cb, np.int64))},
+        "diag": diag,
+        "aln": lines_digest(norm),
+        "aligned_bases": int(sum(int(l.split()[2]) - int(l.split()[1]) for l in norm)),
+        "gix_perm_sha": sha(np.asarray(gix_perm, np.int32)),
+    }
+    with open(os.path.join(HERE, name + ".json"), "w") as f:
+        json.dump(dig, f, indent=1)
+    print(name, cs.ncontig, cs.seqtot, "records", rec.shape[0], "seeds", ns.shape[0], css.shape[0],
+          "aln", len(lines))
+
+
 if __name__ == "__main__":
     if not B.ref_available():
         sys.exit("oracle/_ref is not built: make -C oracle ref")
-    for n in (sys.argv[1:] or list(CASES)):
+    for n in (sys.argv[1:] or list(CASES) + list(LARGE)):
         run_case(n)

@@ -1,17 +1,74 @@
-// Test-only host build of the shared aligner code (align_core.cuh): runs the
+// Test-only host build of the shared chain driver (align_core.cuh) and the
+// finishing step (finish.cuh, its lanes run one after another): runs the
 // alignment stage of one unit on the CPU from diagonal-sorted seed panels so
 // the restated algorithm can be compared with the reference's .1aln on a
-// machine without a GPU.  Not part of the product library.
+// machine without a GPU.  Local_Alignment is the oracle's scalar
+// restatement (oracle/scalar_align.cuh); the oracle's finishing step can
+// stand in for the product's (aht_set_finish) and the two are compared on
+// random candidate sets (aht_finish_check).  Not part of the product library.
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
 #include "../../distributedpanga_b200/csrc/align_core.cuh"
 #include "../../distributedpanga_b200/csrc/align_spec.h"
+#include "../../distributedpanga_b200/csrc/finish.cuh"
+#include "../../oracle/scalar_align.cuh"
 
 using namespace pga::aln;
+using pga::aln::oracle::ScalarAligner;
+using pga::aln::oracle::WaveWork;
+
+static int g_oracle_finish = 0;
+
+static void finish(OvlArena &O) {
+  if (g_oracle_finish) oracle::finish_pair(O);
+  else finish_candidates(Lanes{}, O);
+}
 
 extern "C" {
+
+// Which finishing step aht_align_unit uses: 0 the product's, 1 the oracle's.
+void aht_set_finish(int use_oracle) { g_oracle_finish = use_oracle; }
+
+// The finishing step of one candidate set, by the product's code (which = 0)
+// or the oracle's (which = 1): n candidates rows6 (abpos aepos bbpos bepos
+// diffs tlen) with trace bytes at toff in trace.  Writes the survivors in
+// order (rows6 and their trace bytes, concatenated); returns 0, or 1 when
+// the arena overflowed.
+int aht_finish_check(int64_t n, const int32_t *rows6, const int64_t *toff, const uint8_t *trace, int64_t nbytes,
+                     int which, int32_t *out_rows, int64_t *out_n, uint8_t *out_trace, int64_t *out_nbytes) {
+  std::vector<Ovl> ov(n > 0 ? n : 1);
+  std::vector<int> perm(n > 0 ? n : 1), tmp(n > 0 ? n : 1);
+  const int64_t cap = 4 * nbytes + 4096;
+  std::vector<uint8_t> bytes(cap);
+  memcpy(bytes.data(), trace, nbytes);
+  for (int64_t i = 0; i < n; i++) {
+    const int32_t *r = rows6 + 6 * i;
+    ov[i].abpos = r[0]; ov[i].aepos = r[1]; ov[i].bbpos = r[2]; ov[i].bepos = r[3];
+    ov[i].diffs = r[4]; ov[i].tlen = r[5]; ov[i].toff = toff[i]; ov[i].flags = 0;
+  }
+  OvlArena O;
+  O.ovl = ov.data(); O.perm = perm.data(); O.tmp = tmp.data(); O.ovl_cap = n;
+  O.bytes = bytes.data(); O.byte_cap = cap; O.nbyte = nbytes; O.nov = n; O.err = 0;
+  O.pool_next = nullptr; O.pool_cap = 0;
+  if (which) oracle::finish_pair(O);
+  else finish_candidates(Lanes{}, O);
+  if (O.err) return 1;
+  int64_t k = 0, b = 0;
+  for (int64_t q = 0; q < n; q++) {
+    const Ovl &o = ov[perm[q]];
+    if (o.flags & ELIMINATED) continue;
+    int32_t *r = out_rows + 6 * k;
+    r[0] = o.abpos; r[1] = o.aepos; r[2] = o.bbpos; r[3] = o.bepos; r[4] = o.diffs; r[5] = o.tlen;
+    memcpy(out_trace + b, bytes.data() + o.toff, o.tlen);
+    b += o.tlen;
+    k++;
+  }
+  *out_n = k;
+  *out_nbytes = b;
+  return 0;
+}
 
 // Decodes swide records of one unit (sorted panels) and aligns every
 // (anchor, partner) pair in panel order.  Self pairs (comp == 0 and
@@ -141,7 +198,7 @@ int aht_align_unit(const uint8_t *bps, int ncontig, const int64_t *clen, const i
           if (Rg.calls > 0) R.exit_bepos = Rg.exit_bepos;
         }
       }
-      finish_pair(O);
+      finish(O);
       if (O.err) return 200 + O.err;
       if (*npairs < pair_cap) {
         int *p = pairs_out + 4 * (*npairs);

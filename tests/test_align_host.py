@@ -21,8 +21,8 @@ ALL_CASES = GOLDEN_CASES + ["small_full"]
 def aht():
     so = os.path.join(NATIVE, "libalign_host.so")
     src = os.path.join(NATIVE, "align_host.cu")
-    deps = [src] + [os.path.join(ROOT, "distributedpanga_b200", "csrc", f)
-                    for f in ("align_core.cuh", "align_spec.h")]
+    deps = [src, os.path.join(ROOT, "oracle", "scalar_align.cuh")] + [
+        os.path.join(ROOT, "distributedpanga_b200", "csrc", f) for f in ("align_core.cuh", "align_spec.h", "finish.cuh")]
     if not os.path.exists(so) or any(os.path.getmtime(d) > os.path.getmtime(so) for d in deps):
         subprocess.run(["/usr/local/cuda/bin/nvcc", "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
                         "-Wno-deprecated-gpu-targets", "-o", so, src], check=True)
@@ -31,6 +31,10 @@ def aht():
     L.aht_align_unit.argtypes = [vp, ci, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp, ci, i64, i64, vp, i64, vp, vp,
                                  i64, vp, vp, i64, vp, i64]
     L.aht_align_unit.restype = ci
+    L.aht_set_finish.argtypes = [ci]
+    L.aht_set_finish.restype = None
+    L.aht_finish_check.argtypes = [i64, vp, vp, vp, i64, ci, vp, vp, vp, vp]
+    L.aht_finish_check.restype = ci
     return L
 
 
@@ -202,3 +206,102 @@ def test_host_block_ranges_compose(oracle, aht, case):
             assert len(part) == len(whole)
             assert part == whole, (comp, split)
             assert np.array_equal(pp, pw), (comp, split)
+
+
+# ---- the finishing step against the oracle's statement-by-statement restatement
+
+def _random_candidates(rng, n, base_len=30000, T=100):
+    """n candidate alignments of one pair, drawn around one base path so that
+    they share starts and ends (duplicates, containments), meet at trace
+    points (crossings) and run beside each other at small B offsets (boxes).
+    Returns rows6 (abpos aepos bbpos bepos diffs tlen), trace offsets and the
+    trace bytes ((diffs, b-delta) per A panel)."""
+    npan = base_len // T + 1
+    bd = 100 + rng.integers(-4, 5, npan)
+    at = np.concatenate([[0], np.cumsum(bd)])
+
+    def bpos(x):
+        return int(at[x // T] + (bd[x // T] * (x % T)) // T)
+
+    rows, offs, tr = [], [], []
+    nb = 0
+    for i in range(n):
+        u = rng.random()
+        if rows and u < 0.12:                       # an exact copy of an earlier one
+            k = int(rng.integers(0, len(rows)))
+            r = list(rows[k])
+            t = tr[k].copy()
+            if rng.random() < 0.5:                  # ... with other diffs
+                t[0::2] = rng.integers(0, 12, len(t) // 2)
+                r[4] = int(t[0::2].sum())
+            rows.append(r)
+            tr.append(t)
+            offs.append(nb)
+            nb += len(t)
+            continue
+        if rows and u < 0.3:                        # same start or same end as an earlier one
+            k = int(rng.integers(0, len(rows)))
+            a0, a1 = rows[k][0], rows[k][1]
+            if rng.random() < 0.5:
+                a1 = int(min(base_len, a0 + rng.integers(150, 8000)))
+            else:
+                a0 = int(max(0, a1 - rng.integers(150, 8000)))
+            off = rows[k][2] - bpos(rows[k][0])
+        else:
+            a0 = int(rng.integers(0, base_len - 400))
+            a1 = int(min(base_len, a0 + rng.integers(150, 9000)))
+            off = int(rng.choice([0, 0, 0, 1, -2, 3, 12, -15]))
+        p0, p1 = a0 // T, (a1 - 1) // T
+        deltas = []
+        for p in range(p0, p1 + 1):
+            s, e = max(a0, p * T), min(a1, (p + 1) * T)
+            deltas.append(bpos(e) - bpos(s))
+        deltas = np.array(deltas, np.int64)
+        if len(deltas) > 2 and rng.random() < 0.4:  # wander off the path and come back
+            q = int(rng.integers(0, len(deltas) - 1))
+            w = int(rng.integers(q + 1, len(deltas)))
+            h = int(rng.integers(1, 4)) * (1 if rng.random() < 0.5 else -1)
+            deltas[q] += h
+            deltas[w] -= h
+        deltas = np.clip(deltas, 0, 255)
+        diffs = rng.integers(0, 12, len(deltas))
+        t = np.zeros(2 * len(deltas), np.uint8)
+        t[0::2] = diffs
+        t[1::2] = deltas
+        b0 = bpos(a0) + off
+        rows.append([a0, a1, b0, b0 + int(deltas.sum()), int(diffs.sum()), len(t)])
+        tr.append(t)
+        offs.append(nb)
+        nb += len(t)
+    return (np.array(rows, np.int32).reshape(-1, 6), np.array(offs, np.int64),
+            np.concatenate(tr) if tr else np.zeros(1, np.uint8))
+
+
+def _finish(L, rows, offs, tr, which):
+    n = len(rows)
+    out = np.zeros((max(1, n), 6), np.int32)
+    otr = np.zeros(max(1, 4 * tr.size), np.uint8)
+    on, ob = C.c_int64(), C.c_int64()
+    rc = L.aht_finish_check(n, np.ascontiguousarray(rows).ctypes.data, offs.ctypes.data, tr.ctypes.data, tr.size,
+                            which, out.ctypes.data, C.byref(on), otr.ctypes.data, C.byref(ob))
+    assert rc == 0
+    return out[: on.value].copy(), otr[: ob.value].copy()
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_finishing_step_matches_oracle_rules(aht, seed):
+    """The product's finishing step (finish.cuh, lanes emulated on the host)
+    against the oracle's statement-by-statement restatement of the
+    reference's sort / elimination / entwine / box rules, on random candidate
+    sets built to hit every rule (sizes 1 to 400, crossing the 32-lane
+    windows)."""
+    rng = np.random.default_rng(1000 + seed)
+    hits = 0
+    for n in (1, 2, 5, 31, 33, 64, 150, 400):
+        rows, offs, tr = _random_candidates(rng, n)
+        got = _finish(aht, rows, offs, tr, 0)
+        want = _finish(aht, rows, offs, tr, 1)
+        assert np.array_equal(got[0], want[0]), (seed, n)
+        assert np.array_equal(got[1], want[1]), (seed, n)
+        hits += n - len(want[0])
+    assert hits > 0   # some candidates were removed or joined

@@ -22,3 +22,23 @@ def test_oracle_matches_reference(oracle, case):
         arr, off = oracle.reimport_sort(seeds, posb, ctgb, 1 if u == "C" else 0, cs.ncontig,
                                         cs.maxctg, dig["dbyte"])
         check_diag(arr, off, u, dig)
+
+
+def test_oracle_matches_reference_large(oracle):
+    """The 20 Mbp sample of the 2 x 1 Gbp generator (40 % interspersed
+    repeats, tandem arrays, 7,241 contigs with 2-byte contig fields): every
+    stage of the restatement against the reference's digests."""
+    from helpers import check_diag_large, check_index_large, check_seeds_large
+    cs, dig = load_case("full_s001")
+    posb, ctgb = dig["posb"], dig["ctgb"]
+    srt = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    check_index_large(srt, dig)
+    ent, cum, _ = oracle.build_adapter(srt, posb, ctgb)
+    del srt
+    ns, css, nb, cb = oracle.merge(ent, cum, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+    del ent
+    check_seeds_large(ns, css, nb, cb, dig)
+    for u, seeds in (("N", ns), ("C", css)):
+        arr, off = oracle.reimport_sort(seeds, posb, ctgb, 1 if u == "C" else 0, cs.ncontig,
+                                        cs.maxctg, dig["dbyte"])
+        check_diag_large(arr, off, u, dig)
