@@ -77,6 +77,7 @@ struct pga_ctx {
   int64_t nseed[2] = {0, 0};
   bool have_seeds = false;
   bool seeds_released = false;  // release_for_align freed the unsorted seeds
+  bool seeds_loaded = false;    // the seeds came from pga_seeds_load, not pga_merge
   int freq = 0;
 
   // diagonal sort
@@ -491,6 +492,7 @@ int run_merge(pga_ctx *ctx, int freq) {
   CK(cudaGetLastError());
   ctx->have_seeds = true;
   ctx->seeds_released = false;
+  ctx->seeds_loaded = false;
   ctx->freq = freq;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
   return PGA_OK;
@@ -2088,6 +2090,31 @@ int pga_sort_records(pga_ctx *ctx, uint8_t *records, int64_t count, int posb, in
   return PGA_OK;
 }
 
+int pga_recalc_lcps(pga_ctx *ctx, uint8_t *records, int64_t count, int posb, int ctgb) {
+  if (!ctx || count < 0 || (count > 0 && !records) || posb < 1 || posb > 4 || ctgb < 1 || ctgb > 2)
+    return PGA_ERR_ARG;
+  if (count == 0) return PGA_OK;
+  CK(cudaSetDevice(ctx->device));
+  int r = check_records_fit(ctx, count);
+  if (r) return r;
+  const int rs = 12 + posb + ctgb;
+  ENSURE(ctx->io, (size_t)count * rs + 16);
+  ENSURE(ctx->rec, sizeof(Rec) * (size_t)count + 16);
+  ENSURE(ctx->lcp, (size_t)count + 16);
+  CK(cudaMemcpyAsync(ctx->io.p, records, (size_t)count * rs, cudaMemcpyHostToDevice, ctx->st));
+  k_records_in<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), count, posb, ctgb, P<Rec>(ctx->rec),
+                                                           P<uint8_t>(ctx->lcp));
+  k_lcp<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), count, P<uint8_t>(ctx->lcp));
+  k_records_out<<<grid_for(count, 256), 256, 0, ctx->st>>>(P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), count, posb, ctgb,
+                                                            P<uint8_t>(ctx->io));
+  LAUNCHED(3);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(records, ctx->io.p, (size_t)count * rs, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->have_index = false;
+  return PGA_OK;
+}
+
 int pga_build_kmer_adapter(pga_ctx *ctx, const uint8_t *records, int64_t count, int posb, int ctgb,
                            uint8_t *entries, int64_t *cum, int64_t *largest) {
   if (!ctx || count < 0 || (count > 0 && (!records || !entries)) || !cum || posb < 1 || posb > 4 || ctgb < 1 ||
@@ -2558,6 +2585,37 @@ int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck) {
   if (!ctx || !ctx->have_seeds || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
   if (ctx->seeds_released) return fail(ctx, PGA_ERR_ARG, "seeds were freed for the alignment; run pga_merge again");
   return copy_seeds(ctx, comp, seeds, buck);
+}
+
+int pga_seeds_load(pga_ctx *ctx, int comp, const uint8_t *seeds, int64_t len) {
+  if (!ctx || !ctx->have_gdb || (comp != 0 && comp != 1) || len < 0 || (len > 0 && !seeds)) return PGA_ERR_ARG;
+  const int sb = 1 + 2 * (ctx->posb + ctx->ctgb);
+  if (len % sb != 0) return fail(ctx, PGA_ERR_ARG, "seed bytes not a whole number of seeds");
+  const int64_t n = len / sb;
+  if (n >= (int64_t)0xffffffffLL) return fail(ctx, PGA_ERR_LIMIT, "too many seeds");
+  CK(cudaSetDevice(ctx->device));
+  // both units are present from the first load on (the other one empty
+  // until it is loaded too), as pga_merge leaves them
+  if (!ctx->have_seeds || ctx->seeds_released || !ctx->seeds_loaded) {
+    ctx->nseed[0] = ctx->nseed[1] = 0;
+    ENSURE(ctx->seed[0], 16);
+    ENSURE(ctx->seed[1], 16);
+    ctx->seeds_loaded = true;
+  }
+  ENSURE(ctx->io, (size_t)len + 16);
+  ENSURE(ctx->seed[comp], sizeof(Seed) * (size_t)n + 16);
+  if (n > 0) {
+    CK(cudaMemcpyAsync(ctx->io.p, seeds, (size_t)len, cudaMemcpyHostToDevice, ctx->st));
+    k_seeds_in<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<uint8_t>(ctx->io), n, ctx->posb, ctx->ctgb,
+                                                       P<Seed>(ctx->seed[comp]));
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+  }
+  ctx->nseed[comp] = n;
+  ctx->have_seeds = true;
+  ctx->seeds_released = false;
+  ctx->have_diag[0] = ctx->have_diag[1] = false;
+  return PGA_OK;
 }
 
 int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count) {

@@ -142,6 +142,11 @@ int pga_self_adaptamer_merge(pga_ctx *ctx, const uint8_t *entries, const int64_t
                              uint8_t **nseeds, int64_t *nlen, uint8_t **cseeds, int64_t *clen,
                              int64_t *nbuck, int64_t *cbuck);
 
+/* recalc_all_lcps (src/sort.c:38-57): byte 0 of each of `count` sorted
+ * records (reference layout) becomes the number of leading bases its k-mer
+ * shares with the previous record's (0 for the first), in place. */
+int pga_recalc_lcps(pga_ctx *ctx, uint8_t *records, int64_t count, int position_bytes, int contig_strand_bytes);
+
 /* reimport_thread + rmsd_sort (src/fastga_pipeline.c:1391-1450,
  * lib/RSDsort.c:292): `len` bytes of seeds -> swide-byte records, panel by A
  * contig, each panel sorted; panel_off (ncontig+1) gets record offsets.
@@ -178,6 +183,14 @@ int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t
 /* Adaptamer merge of the built index: seeds stay in HBM. */
 int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds);
 int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck);
+
+/* Seeds of unit comp (0 = N, 1 = C) from the host into the context, as
+ * pga_merge would leave them: `len` bytes of seeds in the reference layout
+ * (1 + 2*(posb+ctgb) bytes each, the loaded GDB's field widths), the
+ * received seed buffers pair_sort_search starts from (Recv_N_Data /
+ * Recv_C_Data, src/fastga_pipeline.c:1793-1806).  The first load after a
+ * merge (or none) empties the other unit until it is loaded too. */
+int pga_seeds_load(pga_ctx *ctx, int comp, const uint8_t *seeds, int64_t len);
 
 /* Reimport + diagonal sort of unit comp (0 = N, 1 = C) in HBM. */
 int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count);

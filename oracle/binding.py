@@ -190,8 +190,11 @@ def ref_gdbdump(stem: str):
             "clen": [r[0] for r in rows], "boff": [r[1] for r in rows]}
 
 
-def ref_run(stem: str, workdir: str, threads: int = 8, timeout: float = 3600.0) -> dict:
-    """Build the .gix and run the reference's single-process pipeline on <stem>.
+def ref_run(stem: str, workdir: str, threads: int = 8, timeout: float = 3600.0,
+            driver: str = "pga-mpi-merge") -> dict:
+    """Build the .gix and run the reference's single-process pipeline on <stem>
+    (`driver`: the stock build, or pga-mpi-merge-b200, the same driver linked
+    with the B200 drop-in stages, which writes no dumps).
 
     Returns paths of its dumps: index.bin, seeds.bin and the .1aln."""
     dump = os.path.join(workdir, "dump")
@@ -200,12 +203,14 @@ def ref_run(stem: str, workdir: str, threads: int = 8, timeout: float = 3600.0) 
     env["PATH"] = REF_DIR + os.pathsep + env.get("PATH", "")
     env["ORACLE_DUMP_DIR"] = dump
     env.setdefault("PGA_SCRATCH_DIR", "/tmp")
+    # GIXmake_dump's own text dump of every k-mer is not read here
+    env.setdefault("GIXMAKE_DUMP_PATH", os.devnull)
     with open(os.path.join(workdir, "gix.log"), "w") as log:
         subprocess.run([os.path.join(REF_DIR, "GIXmake_dump"), "-T%d" % threads, stem + ".1gdb"],
                        check=True, stdout=log, stderr=subprocess.STDOUT, cwd=workdir, env=env,
                        timeout=timeout)
     with open(os.path.join(workdir, "merge.log"), "w") as log:
-        subprocess.run([os.path.join(REF_DIR, "pga-mpi-merge"), stem], check=True, stdout=log,
+        subprocess.run([os.path.join(REF_DIR, driver), stem], check=True, stdout=log,
                        stderr=subprocess.STDOUT, cwd=workdir, env=env, timeout=timeout)
     return {"index": os.path.join(dump, "index.bin"), "seeds": os.path.join(dump, "seeds.bin"),
             "aln": os.path.join(workdir, "out.rank0.paf"), "log": os.path.join(workdir, "merge.log")}
