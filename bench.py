@@ -1,21 +1,34 @@
-"""Benchmark of the GPU alignment path on the 2 x 100 Mbp chromosome-set workload.
+"""Benchmark of the GPU alignment path.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload full|chromset|pangenome]
+
+Default workload: two 1 Gbp genomes in one GDB (the 2 x 1 Gbp configuration,
+`full`), with the 2 x 100 Mbp chromosome-set configuration (`chromset`)
+measured after it as the line's `secondary` object.
 
 One step = one pass of the whole alignment path over the contig set, inputs
 resident in HBM: closed-syncmer extraction -> 24-bit-prefix bucket sort ->
-semantic LCPs -> k-mer table entries + prefix table -> adaptamer merge ->
-seed reimport + diagonal sort of the N and C units -> chaining and
-Local_Alignment of every contig pair (FastGA-order self pairs) -> the
-alignment records in la_sort order, read back to the host.
+semantic LCPs -> adaptamer merge -> seed reimport + diagonal sort of the N
+and C units -> chaining and Local_Alignment of every contig pair
+(FastGA-order self pairs) -> the alignment records in la_sort order, left
+in HBM.  The k-mer table entries in the reference's byte layout are written
+only with --entries (nothing on the path reads them).
 
-value  = input bases (both genomes, Mbp) per second, max device time over ranks
-e2e    = the same through the C ABI with host buffers: every step also uploads
-         the .bps image and contig table
-roofline = the index build (extract + sort + LCP + entries), whose algorithmic
-         bytes are ceil(G/4) + 5*N*R + N*E + 2^27
+value  = input bases (both genomes, Mbp) per second of device time, max over
+         ranks
+e2e    = the same through the C ABI with host buffers: every e2e step uploads
+         the .bps image and contig table from pinned host memory, runs the
+         path and reads the alignment records and traces back to the host
+         (--e2e-steps steps after one warm-up)
+roofline = the index build (extract + sort + LCP [+ entries]), whose
+         algorithmic bytes are ceil(G/4) + 5*N*R [+ N*E] + 2^27
+bit_exact = the secondary (2 x 100 Mbp) workload's index, seeds, sorted
+         diagonal panels and .1aln record stream against digests of the
+         reference's own pipeline on the same seeded input
+         (tests/golden/chromset_full.json), checked outside the timed region
 cpu_baseline = the reference pipeline compiled from source (oracle/_ref), or
-         the oracle's C restatement when that is absent, on a bounded sample.
+         the oracle's C restatement when that is absent, on a bounded sample
+         of the same generator
 
 With N > 1 every rank runs an independent replica (the path has no exchange
 step on one node's workload): weak scaling, no collective in the data path.
@@ -46,10 +59,16 @@ WORKLOADS = {
             "B = A at 2% substitutions + 0.5% indels + 20 inversions; k=40, FREQ=10",
     "pangenome": "pangenome: a 50 Mbp reference + 16 haplotypes (0.1-1% substitutions, a tenth as indels, "
                  "10 inversions + 5 translocations each), log-normal contigs 10 kbp-5 Mbp, all in one GDB; "
-                 "k=40, FREQ=20 (above the 17 copies of a shared k-mer)",
+                 "k=40, FREQ=10 (the reference driver's cutoff)",
 }
-WL = {"name": "chromset"}  # the workload of this run (--workload)
-FREQ = {"pangenome": 20}   # frequency cutoff per workload (10 unless listed)
+WL = {"name": "full"}  # the workload being measured
+FREQ = {}              # frequency cutoff per workload (10, the reference driver's, unless listed)
+# golden digests of the reference's pipeline for a workload at a scale
+GOLDEN = {("chromset", 1.0): "chromset_full", ("full", 0.01): "full_s001", ("pangenome", 0.02): "pangenome_s002"}
+# CPU samples of each generator: the reference arm's per-step sample and the
+# cpu_baseline sample (about 10 s and 20 s of the reference's pipeline here)
+REF_SCALE = {"full": 0.004, "chromset": 0.05, "pangenome": 0.01}
+CPU_SCALE = {"full": 0.01, "chromset": 0.1, "pangenome": 0.02}
 
 
 def freq_cutoff() -> int:
@@ -118,13 +137,14 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_contigs(scale: float):
+def make_contigs(scale: float, name: str | None = None):
     from distributedpanga_b200 import gdb, synth
-    cache = os.path.join(tempfile.gettempdir(), "pga_%s_%g.npz" % (WL["name"], scale))
+    name = name or WL["name"]
+    cache = os.path.join(tempfile.gettempdir(), "pga_%s_%g.npz" % (name, scale))
     if os.path.exists(cache):
         z = np.load(cache)
         return gdb.ContigSet(bps=z["bps"], clen=z["clen"], boff=z["boff"], freq=z["freq"]), None
-    contigs = synth.make(WL["name"], scale=scale)
+    contigs = synth.make(name, scale=scale)
     cs = gdb.from_contigs(contigs)
     try:
         np.savez(cache, bps=cs.bps, clen=cs.clen, boff=cs.boff, freq=cs.freq)
@@ -143,25 +163,29 @@ def index_bytes(cs, nrec: int, entries: bool = True) -> float:
 # ---- reference / oracle CPU timing -------------------------------------------
 
 class ReferenceSample:
-    """The reference pipeline (oracle/_ref) on a sample of the workload: the
-    GDB and its .gix are built once; each run() times one pga-mpi-merge and
-    returns the seconds of the stages the GPU path covers (from its own
-    [o1-0] / [pr1] stage timers)."""
+    """The reference pipeline (oracle/_ref) on a sample of a workload's
+    generator: the GDB and its .gix (GIXmake from source, whose contig order
+    src/fastga_order.c reads; its own text dump off) are built once,
+    untimed; each run() times one pga-mpi-merge and returns the seconds of
+    its own stage timers."""
 
-    def __init__(self, scale: float):
+    def __init__(self, scale: float, name: str | None = None):
         from distributedpanga_b200 import gdb, synth
         from oracle import binding as orc
+        self.name = name or WL["name"]
         self.tmp = tempfile.TemporaryDirectory()
-        contigs = synth.make(WL["name"], scale=scale)
+        contigs = synth.make(self.name, scale=scale)
         self.mbp = gdb.from_contigs(contigs).seqtot / 1e6
         fa = os.path.join(self.tmp.name, "s.fa")
         self.stem = os.path.join(self.tmp.name, "s")
         synth.write_fasta(fa, contigs)
         orc.ref_make_gdb(fa, self.stem)
         env = dict(os.environ)
+        env["GIXMAKE_DUMP_PATH"] = os.devnull
         with open(os.path.join(self.tmp.name, "gix.log"), "w") as log:
-            subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T8", self.stem + ".1gdb"], check=True,
-                           stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
+            subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T%d" % max(1, min(8, os.cpu_count() or 1)),
+                            self.stem + ".1gdb"], check=True, stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name,
+                           env=env)
 
     def run(self, whole: bool = True) -> float:
         from oracle import binding as orc
@@ -185,39 +209,42 @@ class ReferenceSample:
                 float(pr["sort_n_s"]) + float(pr["sort_c_s"]))
 
 
-def port_sample(scale: float):
+def port_sample(scale: float, name: str | None = None):
     """The oracle's C restatement on a sample; returns (Mbp, seconds)."""
     from distributedpanga_b200 import gdb, synth
     from oracle import binding as orc
-    cs = gdb.from_contigs(synth.make(WL["name"], scale=scale))
+    cs = gdb.from_contigs(synth.make(name or WL["name"], scale=scale))
     posb, ctgb, _ = gdb.record_sizing(cs)
     dbyte, _ = gdb.diag_sizing(cs, ctgb)
     t0 = time.time()
     srt = orc.sort_records(orc.extract(cs, posb, ctgb))
     ent, cum, _ = orc.build_adapter(srt, posb, ctgb)
-    ns, css, _, _ = orc.merge(ent, cum, posb, ctgb, 10, cs.ncontig)
+    ns, css, _, _ = orc.merge(ent, cum, posb, ctgb, freq_cutoff(), cs.ncontig)
     orc.reimport_sort(ns, posb, ctgb, 0, cs.ncontig, cs.maxctg, dbyte)
     orc.reimport_sort(css, posb, ctgb, 1, cs.ncontig, cs.maxctg, dbyte)
     return cs.seqtot / 1e6, time.time() - t0
 
 
-def cpu_baseline(sample_scale: float) -> dict:
+def cpu_baseline(sample_scale: float, name: str | None = None) -> dict:
+    """The reference's whole pipeline (its TOTAL stage time) on a sample of
+    the workload's generator, once; host cores stated."""
     from oracle import binding as orc
+    name = name or WL["name"]
     cores_total = os.cpu_count()
     if orc.ref_available():
-        r = ReferenceSample(sample_scale)
-        sec = min(r.run() for _ in range(2))
+        r = ReferenceSample(sample_scale, name)
+        sec = r.run()
         mbp = r.mbp
         return {"value": mbp / sec, "unit": UNIT, "cores": 4, "kind": "reference",
-                "sample": WL["name"] + " generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
+                "sample": name + " generator at scale %g (%.1f Mbp), reference pga-mpi-merge world 1 "
                           "(oracle/_ref), whole path (its TOTAL stage time: extract, sort, merge, alignments); "
                           "msd_sort uses 4 threads, the rest 1; host has %d cores" % (sample_scale, mbp, cores_total),
                 "seconds": sec}
     orc.build()
-    mbp, sec = port_sample(sample_scale)
+    mbp, sec = port_sample(sample_scale, name)
     return {"value": mbp / sec, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": WL["name"] + " generator at scale %g (%.1f Mbp), oracle C restatement, 1 thread; host has %d cores"
-                      % (sample_scale, mbp, cores_total), "seconds": sec}
+            "sample": name + " generator at scale %g (%.1f Mbp), oracle C restatement (extract to diagonal sort), "
+                      "1 thread; host has %d cores" % (sample_scale, mbp, cores_total), "seconds": sec}
 
 
 # ---- GDB ingest ------------------------------------------------------------------
@@ -329,7 +356,7 @@ def run_profile_stage(args) -> None:
         sc = args.serve_scale
         contigs = synth.make_target(scale=sc)
         target = pipeline.Target(synth.fasta_bytes(contigs, "t"))
-        stream = synth.query_stream(contigs, args.warmup + args.steps, 0.0, int(1_000_000 * sc * 10),
+        stream = synth.query_stream(contigs, args.warmup + args.steps, 0.0, int(1_000_000 * sc),
                                     int(200_000_000 * sc), seed=31, median=2_000_000 * max(sc, 0.05))
         dev = pipeline.Device(0)
         for k, (_, q) in enumerate(stream):
@@ -347,7 +374,7 @@ def run_profile_stage(args) -> None:
         dev.gdb_load(cs)
         dev.enable_timing(True)
         for _ in range(args.warmup + args.steps):
-            n = dev.index_build(want_entries=not args.no_entries)
+            n = dev.index_build(want_entries=args.entries)
             st = dev.stage_times()
             print(json.dumps({"stage": "index", "records": n,
                               "ms": {k: st[k] for k in ("extract_hist", "prefix_scan", "extract_scatter",
@@ -363,6 +390,9 @@ def run_profile_stage(args) -> None:
 
 
 def run_reference(args, rank: int) -> None:
+    """The reference arm: the reference's own pipeline on the host cores, each
+    step one run on a sample of the workload's generator (REF_SCALE, or
+    --ref-scale); rank 0 alone."""
     if rank != 0:
         return
     from oracle import binding as orc
@@ -382,13 +412,13 @@ def run_reference(args, rank: int) -> None:
         detail = (mbp, kind, cores)
     v = statistics.median(vals)
     mbp, kind, cores = detail
+    sample = WL["name"] + " generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mbp / v * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOADS[WL["name"]], "sample_scale": args.ref_scale},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": WL["name"] + " generator at scale %g (%.1f Mbp) per step" % (args.ref_scale, mbp)},
+            "config": {"workload": WORKLOADS[WL["name"]], "sample_scale": args.ref_scale, "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     emit(rank, line)
 
@@ -420,26 +450,92 @@ def emit(rank: int, line: dict) -> None:
 def align_roofline(work: dict, align_ms: float) -> dict:
     """The aligner is integer-issue bound: its work in cells (one diagonal
     updated in one wave step) per second, with the SM issue utilisation of
-    k_align_pairs from the committed ncu summary when there is one."""
+    k_align_pairs from the committed ncu summary when there is one (a capture
+    on another, smaller workload: its source is stated)."""
     out = {"bound": "issue", "unit": "cells/s", "cells": work["cells"], "waves": work["waves"],
            "calls": work["calls"], "warp_tasks": work["tasks"],
            "achieved": work["cells"] / (align_ms / 1000.0) if align_ms > 0 else None,
-           "issue_util": None}
+           "issue_util": None, "issue_util_source": None}
     try:
         with open(os.path.join(ROOT, "profiles", "k_align_pairs_issue.json")) as f:
-            out["issue_util"] = json.load(f).get("sm_issue_active_pct_of_active_cycles")
+            prof = json.load(f)
+        out["issue_util"] = prof.get("sm_issue_active_pct_of_active_cycles")
+        out["issue_util_source"] = prof.get("source", "profiles/k_align_pairs_issue.json")
     except Exception:
         pass
     return out
 
 
-# ---- GPU arm ---------------------------------------------------------------------
+def index_traffic(name: str, scale: float, nrec: int):
+    """DRAM bytes per index build from a committed ncu capture of the index
+    build on this workload's generator (profiles/traffic.json), scaled by the
+    record count when the capture ran on a smaller case; with its source."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tr = json.load(f)
+    except Exception:
+        return None, None
+    cap = tr.get("index_build", {}).get(name)
+    if not cap:
+        return None, None
+    per_rec = cap["dram_bytes"] / cap["records"]
+    src = "ncu capture of the index build on %s (%d records, %s), scaled by records" % (
+        cap["case"], cap["records"], cap["file"])
+    return per_rec * nrec, src
 
-def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+
+def golden_check(dev, name: str, scale: float) -> dict:
+    """Every stage of one more pass on the loaded GDB against the golden
+    digests of the reference's pipeline for this workload and scale (index,
+    N and C seeds, sorted diagonal panels, .1aln record stream); outside the
+    timed region.  {"bit_exact": true|false|null, ...}."""
+    key = GOLDEN.get((name, scale))
+    path = os.path.join(ROOT, "tests", "golden", "%s.json" % key) if key else None
+    if not path or not os.path.exists(path):
+        return {"bit_exact": None, "reason": "no reference digests for %s at scale %g" % (name, scale)}
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers as H
+    from distributedpanga_b200.pipeline import alignment_lines
+    with open(path) as f:
+        dig = json.load(f)
+    stage = "index"
+    try:
+        dev.index_build(want_entries=False)
+        rec = dev.index_records()
+        H.check_index_large(rec, dig)
+        del rec
+        stage = "seeds"
+        dev.merge(dig["freq_cutoff"])
+        ns, nb = dev.seeds(0)
+        css, cb = dev.seeds(1)
+        H.check_seeds_large(ns, css, nb, cb, dig)
+        del ns, css
+        for comp, u in ((0, "N"), (1, "C")):
+            stage = "diag_" + u
+            sw, cnt = dev.diag_sort(comp)
+            arr, off = dev.diag_records(comp, sw, cnt)
+            H.check_diag_large(arr, off, u, dig)
+            del arr
+        stage = "aln"
+        dev.align()
+        lines = [" ".join(x.split()) for x in alignment_lines(*dev.alignments())]
+        H.check_lines(lines, dig["aln"])
+    except AssertionError as e:
+        return {"bit_exact": False, "first_difference": stage, "detail": str(e)[:200], "golden": key + ".json"}
+    return {"bit_exact": True, "golden": key + ".json", "stages": "index, N/C seeds, N/C diagonal panels, .1aln",
+            "alignments": dig["aln"]["count"]}
+
+
+def measure(args, name: str, scale: float, steps: int, warmup: int, e2e_steps: int, rank: int, world: int,
+            local_rank: int, check: bool) -> dict:
+    """One workload on this rank's GPU: `warmup` untimed steps, `steps` timed
+    steps (CUDA events on the launching stream, max over ranks), one more
+    step with per-stage times, `e2e_steps` end-to-end steps through the C ABI
+    from pinned host memory, and (check) the golden comparison."""
     import torch
     from distributedpanga_b200 import gdb, pipeline
-    torch.cuda.set_device(local_rank)
-    cs, _ = make_contigs(args.scale)
+    WL["name"] = name
+    cs, _ = make_contigs(scale, name)
     posb, ctgb, rsize = gdb.record_sizing(cs)
     dev = pipeline.Device(local_rank)
     stream = torch.cuda.current_stream()
@@ -456,13 +552,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                                              for k, t in tu.times.items()}}
 
     def step():
-        dev.index_build(want_entries=not args.no_entries)
+        dev.index_build(want_entries=args.entries)
         dev.merge(freq_cutoff())
         dev.diag_sort(0)
         dev.diag_sort(1)
         dev.align()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     barrier(world)
@@ -472,13 +568,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    launches = (dev.launches() - l0) // args.steps
+    ms = ev0.elapsed_time(ev1) / steps
+    launches = (dev.launches() - l0) // steps
     clk = clocks.stop()
     nrec = dev.nrec
     nseeds = dev.nseeds
@@ -488,7 +584,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     step()
     st = dev.stage_times()
     dev.enable_timing(False)
-
     astats = dev.align_stats()
     atimes = dev.align_times()
     awork = dev.align_work()
@@ -505,13 +600,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     pinned = torch.empty(max(1, cs.bps.size), dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[: cs.bps.size] = cs.bps
     pcs = gdb.ContigSet(bps=pinned.numpy()[: cs.bps.size], clen=cs.clen, boff=cs.boff, freq=cs.freq)
-    for it in range(args.warmup + args.steps):
+    for it in range(1 + e2e_steps):
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         dev.gdb_load(pcs)
-        dev.index_build(want_entries=not args.no_entries)
+        dev.index_build(want_entries=args.entries)
         dev.merge(freq_cutoff())
         swide, _ = dev.diag_sort(0)
         dev.diag_sort(1)
@@ -520,7 +615,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         d2h = r2.nbytes + o2.nbytes + t2.nbytes
         t1.record(stream)
         torch.cuda.synchronize()
-        if it >= args.warmup:
+        if it >= 1:
             e2e_ms.append(t0.elapsed_time(t1))
     e2e_ms_step = statistics.median(e2e_ms)
 
@@ -529,27 +624,84 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     value = world * mbp / (ms / 1000.0)
     e2e = world * mbp / (e2e_ms_step / 1000.0)
 
+    out = {"value": value, "ms_per_step": ms, "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                                                      "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+           "gpu_launches": int(launches), "clocks": clk, "autotune": tuned, "cs": cs, "dev": dev}
     if rank != 0:
-        return
+        dev.close()
+        return out
     peak, peak_kind = peaks()
-    ingest = run_ingest(dev, cs, args, stream, peak, peak_kind, not args.no_cpu_baseline)
     idx_ms = sum(st[k] for k in ("extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
                                  "entries_prefix_table"))
-    ab = index_bytes(cs, nrec, not args.no_entries)
+    ab = index_bytes(cs, nrec, args.entries)
     achieved = ab / (idx_ms / 1000.0) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tr = json.load(f)
-        traffic = tr.get("index_build_bytes_per_launch_at_scale", {}).get(str(args.scale))
-    except Exception:
-        pass
+    traffic, traffic_src = index_traffic(name, scale, nrec)
+    out.update({
+        "config": {"workload": WORKLOADS[name], "scale": scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
+                   "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
+                   "pairs": astats["pairs"], "self_pairs": astats["self_pairs"],
+                   "local_alignment_calls": astats["calls"], "alignments": astats["alignments"],
+                   "longest_warp_task_ms_at_max_clock": astats["max_task_cycles"] / 1965e3,
+                   "longest_warp_task_calls": astats["max_task_calls"],
+                   "all_tasks_warp_s_at_max_clock": astats["all_task_cycles"] / 1965e6,
+                   "aligned_bases": aligned_bases, "record_bytes": rsize, "swide": swide,
+                   "entries_written": bool(args.entries),
+                   "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "stage_ms": st,
+        "align_ms": atimes,
+        "align_roofline": align_roofline(awork, st["align"]),
+        "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
+                                               "k_lcp%s, k_prefix_table)" % (", k_entries" if args.entries else ""),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes": ab, "ms": idx_ms},
+    })
+    if check:
+        out["golden"] = golden_check(dev, name, scale)
+    return out
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    torch.cuda.set_device(local_rank)
+    name = args.workload
+    m = measure(args, name, args.scale, args.steps, args.warmup, min(args.steps, args.e2e_steps), rank, world,
+                local_rank, check=world == 1 and not args.no_check)
+    if rank != 0:
+        return
+    dev, cs = m.pop("dev"), m.pop("cs")
+    peak, peak_kind = peaks()
+    ingest = None
+    if not args.no_ingest:
+        stream = torch.cuda.current_stream()
+        ingest = run_ingest(dev, cs, args, stream, peak, peak_kind, not args.no_cpu_baseline)
+    dev.close()
+    del cs
     base = None
     if not args.no_cpu_baseline:
         try:
-            base = cpu_baseline(args.ref_scale)
+            base = cpu_baseline(args.cpu_scale, name)
         except Exception as e:  # a missing toolchain must not hide the GPU number
             base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": "failed: %s" % e}
+    golden = m.pop("golden", None) or {"bit_exact": None}
+    parity = {"full": "this workload's generator at 20 Mbp (tests/golden/full_s001.json) is bit-exact to the "
+                      "reference's pipeline in the GPU tests; the full size has no reference run (hours on the host)",
+              "pangenome": "this generator at 17 Mbp (tests/golden/pangenome_s002.json) is bit-exact in the GPU tests"}
+    secondary = None
+    if world == 1 and not args.no_secondary and name != "chromset":
+        try:
+            sm = measure(args, "chromset", 1.0, min(args.steps, 10), min(args.warmup, 3),
+                         min(args.steps, args.e2e_steps), rank, world, local_rank, check=not args.no_check)
+            sm.pop("dev").close()
+            sm.pop("cs")
+            sm.pop("autotune", None)
+            secondary = {"workload": sm["config"]["workload"], "metric": METRIC, "unit": UNIT, **sm}
+            if not args.no_cpu_baseline and args.cpu_full_c2:
+                secondary["cpu_baseline"] = cpu_baseline(1.0, "chromset")
+        except Exception as e:  # the secondary measurement must not hide the headline
+            secondary = {"error": "%s: %s" % (type(e).__name__, e)}
+        WL["name"] = name
     served = None
     if world == 1 and not args.no_serve:
         try:
@@ -557,35 +709,24 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         except Exception as e:  # the served measurement must not hide the plain number
             served = {"error": "%s: %s" % (type(e).__name__, e)}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, %s workload)" % WL["name"],
-        "config": {"workload": WORKLOADS[WL["name"]], "scale": args.scale, "input_bases": cs.seqtot, "contigs": cs.ncontig,
-                   "records": nrec, "seeds_n": nseeds[0], "seeds_c": nseeds[1],
-                   "pairs": astats["pairs"], "self_pairs": astats["self_pairs"],
-                   "local_alignment_calls": astats["calls"], "alignments": astats["alignments"],
-                   "longest_warp_task_ms_at_max_clock": astats["max_task_cycles"] / 1965e3,
-                   "longest_warp_task_calls": astats["max_task_calls"],
-                   "all_tasks_warp_s_at_max_clock": astats["all_task_cycles"] / 1965e6,
-                   "aligned_bases": aligned_bases,
-                   "record_bytes": rsize, "swide": swide,
-                   "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
-        "stage_ms": st,
-        "align_ms": atimes,
-        "align_roofline": align_roofline(awork, st["align"]),
-        "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
-                                               "k_lcp, k_entries, k_prefix_table)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes": ab,
-                     "ms": idx_ms},
+        "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, %s workload)" % name,
+        "config": m["config"],
+        "stage_ms": m["stage_ms"],
+        "align_ms": m["align_ms"],
+        "align_roofline": m["align_roofline"],
+        "roofline": m["roofline"],
         "cpu_baseline": base,
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": int(launches),
-        "clocks": clk,
+        "e2e": m["e2e"],
+        "gpu_launches": m["gpu_launches"],
+        "clocks": m["clocks"],
+        "bit_exact": golden.get("bit_exact"),
+        "parity": golden if golden.get("bit_exact") is not None else parity.get(name, golden.get("reason")),
+        "secondary": secondary,
         "gdb_ingest": ingest,
         "served_form": served,
-        "autotune": tuned,
+        "autotune": m.get("autotune"),
     }
     emit(rank, line)
 
@@ -625,7 +766,7 @@ def serve_measure(args) -> dict:
     sc = args.serve_scale
     contigs = synth.make_target(scale=sc)
     ttext = synth.fasta_bytes(contigs, "t")
-    stream = synth.query_stream(contigs, args.serve_requests, args.serve_rate, int(1_000_000 * sc * 10),
+    stream = synth.query_stream(contigs, args.serve_requests, args.serve_rate, int(1_000_000 * sc),
                                 int(200_000_000 * sc), seed=31, median=2_000_000 * max(sc, 0.05))
     reqs = [serve.Request(k, synth.fasta_bytes(q, "q%d_" % k), arr, sum(len(c) for c in q))
             for k, (arr, q) in enumerate(stream)]
@@ -697,7 +838,7 @@ def serve_measure(args) -> dict:
         "data": "synthetic (seeded)", "dtype": "u8",
         "config": {"workload": "serve: resident target of %d Mbp (chromset generator), %d Poisson requests at "
                                "%.1f/s, query sizes log-uniform %.1f-%.1f Mbp, divergence 0.5-5%%; k=40, FREQ=10"
-                               % (round(target.bases / 1e6), len(reqs), args.serve_rate, 10 * sc, 200 * sc),
+                               % (round(target.bases / 1e6), len(reqs), args.serve_rate, 1 * sc, 200 * sc),
                    "slots": args.serve_slots, "target_contigs": target.ncontig,
                    "parallelism": "replicas%d: one resident target per GPU, requests sharded by id" % world,
                    "target_build_s": round(target_s, 3)},
@@ -735,22 +876,30 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="chromset", choices=sorted(WORKLOADS),
-                    help="chromset (2 x 100 Mbp, the default), full (2 x 1 Gbp) or pangenome (17 x 50 Mbp)")
+    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS),
+                    help="full (2 x 1 Gbp, the default), chromset (2 x 100 Mbp) or pangenome (17 x 50 Mbp)")
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the workload's full size)")
     ap.add_argument("--ref-scale", type=float, default=None,
-                    help="CPU sample scale (default 0.02 of chromset, 0.002 of full)")
+                    help="the reference arm's per-step sample of the generator (default %s)" % REF_SCALE)
+    ap.add_argument("--cpu-scale", type=float, default=None,
+                    help="the cpu_baseline sample of the generator (default %s)" % CPU_SCALE)
+    ap.add_argument("--cpu-full-c2", action="store_true",
+                    help="also time the reference on the whole 2 x 100 Mbp workload (about 1.5 min, plus GIXmake)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-entries", action="store_true",
-                    help="do not write the reference-format k-mer table entries (saves N x E bytes of HBM)")
+    ap.add_argument("--entries", action="store_true",
+                    help="also write the reference-format k-mer table entries in every step (N x E bytes of HBM)")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end steps (after one warm-up), at most --steps")
+    ap.add_argument("--no-check", action="store_true", help="skip the comparison with the reference's digests")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the 2 x 100 Mbp secondary measurement")
+    ap.add_argument("--no-ingest", action="store_true", help="skip the FASTA ingest measurement")
     ap.add_argument("--profile-stage", choices=["index", "ingest", "serve"], default=None,
                     help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     ap.add_argument("--serve", action="store_true",
                     help="measure the served form (resident target, concurrent requests) beside the plain one")
-    ap.add_argument("--serve-scale", type=float, default=0.1,
-                    help="served workload scale: target 1 Gbp x S, queries 10-200 Mbp x S (default 0.1)")
+    ap.add_argument("--serve-scale", type=float, default=1.0,
+                    help="served workload scale: target 1 Gbp x S, queries 1-200 Mbp x S (default 1.0)")
     ap.add_argument("--serve-requests", type=int, default=12)
-    ap.add_argument("--serve-rate", type=float, default=8.0, help="request arrivals per second (Poisson)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="request arrivals per second (Poisson)")
     ap.add_argument("--serve-slots", type=int, default=3)
     ap.add_argument("--autotune", action="store_true",
                     help="time the digit width, aligner build and band-range size on the workload first "
@@ -763,7 +912,9 @@ def main():
         return
     WL["name"] = args.workload
     if args.ref_scale is None:
-        args.ref_scale = 0.02 if args.workload == "chromset" else 0.002
+        args.ref_scale = REF_SCALE[args.workload]
+    if args.cpu_scale is None:
+        args.cpu_scale = CPU_SCALE[args.workload]
     if args.profile_stage:
         run_profile_stage(args)
         return

@@ -30,7 +30,9 @@ struct DBuf {
   size_t cap = 0;
 };
 
-enum StageId { ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_ALIGN, ST_N };
+enum StageId {
+  ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_ALIGN, ST_DIAG_C, ST_N
+};
 
 }  // namespace
 
@@ -541,7 +543,8 @@ int run_diag(pga_ctx *ctx, int comp, int ncontig, int64_t amxpos, int dbyte, int
   ENSURE(ctx->rhist, sizeof(uint32_t) * radix_hist_elems(n) + 64);
   ENSURE(ctx->rscan, sizeof(uint32_t) * scan_tmp_elems(radix_hist_elems(n)) + 64);
   ENSURE(ctx->u64tmp, 64);
-  stage_begin(ctx, ST_DIAG);
+  const int st_diag = comp ? ST_DIAG_C : ST_DIAG;
+  stage_begin(ctx, st_diag);
   U128 *keys = P<U128>(ctx->keys[comp]);
   int passes[16], np = 0;
   if (n > 0) {
@@ -565,7 +568,7 @@ int run_diag(pga_ctx *ctx, int comp, int ncontig, int64_t amxpos, int dbyte, int
   LAUNCHED(5 * np);
   if (res != keys)  // keep the sorted keys in this unit's own buffer
     CK(cudaMemcpyAsync(keys, res, sizeof(U128) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
-  stage_end(ctx, ST_DIAG);
+  stage_end(ctx, st_diag);
   ctx->sorted[comp] = keys;
   ctx->have_diag[comp] = true;
   return PGA_OK;
@@ -1642,13 +1645,13 @@ int pga_ctx_enable_timing(pga_ctx *ctx, int on) {
   return PGA_OK;
 }
 
-int pga_stage_times(const pga_ctx *cctx, float *ms9) {
+int pga_stage_times(const pga_ctx *cctx, float *ms10) {
   pga_ctx *ctx = const_cast<pga_ctx *>(cctx);
-  if (!ctx || !ms9) return PGA_ERR_ARG;
+  if (!ctx || !ms10) return PGA_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->st));
   for (int s = 0; s < ST_N; s++) {
-    ms9[s] = 0.f;
-    if (ctx->stage_used[s]) cudaEventElapsedTime(&ms9[s], ctx->ev[s][0], ctx->ev[s][1]);
+    ms10[s] = 0.f;
+    if (ctx->stage_used[s]) cudaEventElapsedTime(&ms10[s], ctx->ev[s][0], ctx->ev[s][1]);
   }
   return PGA_OK;
 }

@@ -177,10 +177,10 @@ class Device:
         self._ck(self.L.pga_ctx_enable_timing(self.h, 1 if on else 0), "enable_timing")
 
     def stage_times(self) -> dict:
-        a = (C.c_float * 9)()
+        a = (C.c_float * 10)()
         self._ck(self.L.pga_stage_times(self.h, a), "stage_times")
         names = ["extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
-                 "entries_prefix_table", "merge", "diag_sort", "align"]
+                 "entries_prefix_table", "merge", "diag_sort_n", "align", "diag_sort_c"]
         return dict(zip(names, [float(x) for x in a]))
 
     # ---- GDB -------------------------------------------------------------

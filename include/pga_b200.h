@@ -51,10 +51,11 @@ int         pga_ctx_synchronize(pga_ctx *ctx);
 int64_t     pga_kernel_launches(const pga_ctx *ctx);
 /* Per-stage device times (ms) of the last pipeline calls when timing is on:
  * [0] extract+histogram [1] prefix scan [2] extract+scatter [3] bucket sort
- * [4] LCP [5] k-mer entries+prefix table [6] merge [7] diagonal sort (last
- * unit sorted) [8] alignment (pga_align, host steps included). */
+ * [4] LCP [5] k-mer entries+prefix table [6] merge [7] diagonal sort of the
+ * N unit [8] alignment (pga_align, host steps included) [9] diagonal sort of
+ * the C unit. */
 int         pga_ctx_enable_timing(pga_ctx *ctx, int on);
-int         pga_stage_times(const pga_ctx *ctx, float *ms9);
+int         pga_stage_times(const pga_ctx *ctx, float *ms10);
 
 /* ---- GDB ------------------------------------------------------------------ */
 

@@ -49,6 +49,6 @@ def test_serve_compact_and_cutoffs(bench):
         bench.WL["name"] = "chromset"
         assert bench.freq_cutoff() == 10
         bench.WL["name"] = "pangenome"
-        assert bench.freq_cutoff() == 20
+        assert bench.freq_cutoff() == 10    # the reference driver's cutoff (src/pga-mpi-merge.c:62)
     finally:
         bench.WL["name"] = old
