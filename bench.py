@@ -587,6 +587,7 @@ def measure(args, name: str, scale: float, steps: int, warmup: int, e2e_steps: i
     astats = dev.align_stats()
     atimes = dev.align_times()
     awork = dev.align_work()
+    aprof = dev.align_profile()
     recs, toff, tr = dev.alignments()
     aligned_bases = int((recs[:, 2] - recs[:, 1]).sum()) if len(recs) else 0
 
@@ -644,6 +645,8 @@ def measure(args, name: str, scale: float, steps: int, warmup: int, e2e_steps: i
                    "longest_warp_task_ms_at_max_clock": astats["max_task_cycles"] / 1965e3,
                    "longest_warp_task_calls": astats["max_task_calls"],
                    "all_tasks_warp_s_at_max_clock": astats["all_task_cycles"] / 1965e6,
+                   "local_alignment_warp_s_at_max_clock": aprof["local_alignment_cycles"] / 1965e6,
+                   "finish_warp_s_at_max_clock": aprof["finish_cycles"] / 1965e6,
                    "aligned_bases": aligned_bases, "record_bytes": rsize, "swide": swide,
                    "entries_written": bool(args.entries),
                    "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),

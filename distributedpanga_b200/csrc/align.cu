@@ -19,6 +19,10 @@ namespace pga {
 
 using namespace aln;
 
+// Band info bits (k_band_info): the seed starts a band; the pair's previous
+// band is the band just below.
+constexpr uint16_t BI_START = 0x8000, BI_ADJ = 0x4000;
+
 // One seed of a merged band block, staged in shared memory.
 struct BlockSeed {
   int64_t anti;
@@ -188,7 +192,10 @@ struct WarpAligner {
   const AlignSpec &spec;
   __device__ int call(const Seq &A, const Seq &B, bool acomp, Path &P, int low, int hgh, int anti, int lbord,
                       int hbord) {
-    return local_alignment_w(W, spec, A, B, acomp, P, low, hgh, anti, lbord, hbord);
+    const long long t0 = clock64();
+    const int r = local_alignment_w(W, spec, A, B, acomp, P, low, hgh, anti, lbord, hbord);
+    W.la_cycles += clock64() - t0;
+    return r;
   }
   __device__ const uint16_t *points() const { return W.points; }
   __device__ int err() const { return W.err; }
@@ -230,6 +237,7 @@ __device__ WarpWork warp_work(const AlignLaunch &P, int64_t wid) {
   W.smflag = P.smflag;
   W.long_waves = P.smflag ? P.long_waves : 0;
   W.flagged = 0;
+  W.la_cycles = 0;
   return W;
 }
 
@@ -298,11 +306,80 @@ __device__ int64_t next_band_start(const KeySeeds &S, int64_t x, int64_t hi, int
   return m ? lo + __ffs(m) - 1 : h;
 }
 
+// align_pair (align_core.cuh) for a pair's seeds on the device: the same
+// band blocks in the same order, with the same chains and calls, but the
+// blocks come from the per-seed band info, 32 seeds per step, and a block
+// whose seeds' 2*lcp sum is below CHAIN_MIN is passed over: a chain's
+// coverage is at most the sum of its seeds' spans, so no chain of it can
+// pass the hit test, and such a block makes no call and changes no state.
+// Block (c, c+1) starting at band c's first seed b is scanned when band c
+// is new (the band below it is not c-1) or band c+1 follows it, as in
+// align_pair; blocks start in [blo, bhi).
+template <class Aligner>
+__device__ int align_pair_dev(const KeySeeds &S, const uint16_t *info, bool comp, bool self, const Seq &A,
+                              const Seq &B, int64_t amxpos, int64_t maxdag, Aligner &AL, Path &path, OvlArena &O,
+                              PairResult &R, int lane, int64_t blo, int64_t bhi) {
+  const int64_t n = S.n;
+  R.calls = 0;
+  R.nhit = 0;
+  R.nlas = 0;
+  R.exit_bepos = path.bepos;
+  O.nov = 0;
+  if (bhi < 0 || bhi > n) bhi = n;
+  if (blo < 0) blo = 0;
+  if (blo >= bhi) return 0;
+  ChainSink<WarpAligner> K{comp, self, A, B, AL, path, O, R, lane, 32, amxpos, (int64_t)A.len + B.len,
+                           (int64_t)A.len - maxdag, (int64_t)A.len - amxpos, 0, 0, -1};
+  int64_t pend = -1;  // the last band start seen, its block not yet decided
+  int pend_sum = 0;
+  bool pend_new = false;
+  bool done = false;
+  for (int64_t base = blo; base < n && !done; base += 32) {
+    const int64_t i = base + lane;
+    const uint16_t v = i < n ? info[i] : 0;
+    unsigned starts = __ballot_sync(FULL, (v & BI_START) != 0);
+    while (starts) {
+      const int l = __ffs(starts) - 1;
+      starts &= starts - 1;
+      const int64_t b = base + l;
+      const uint16_t vb = __shfl_sync(FULL, v, l);
+      if (pend >= 0) {
+        const bool aux = (vb & BI_ADJ) != 0;  // band c+1 follows band c
+        if ((pend_new || aux) && pend_sum + (aux ? (vb & 0xff) : 0) >= CHAIN_MIN) {
+          const int64_t e = aux ? S.band_end(b, S.band(b)) : b;
+          K.cdiag = S.band(pend);
+          K.isnew = pend_new ? 1 : 0;
+          K.alast = -1;
+          if (S.scan_block(pend, b, e, K)) return 1;
+        }
+        pend = -1;
+      }
+      if (b >= bhi) {
+        done = true;
+        break;
+      }
+      pend = b;
+      pend_sum = vb & 0xff;
+      pend_new = (vb & BI_ADJ) == 0;
+    }
+  }
+  if (pend >= 0 && pend_new && pend_sum >= CHAIN_MIN) {  // the pair's last band: no band after it
+    K.cdiag = S.band(pend);
+    K.isnew = 1;
+    K.alast = -1;
+    if (S.scan_block(pend, n, n, K)) return 1;
+  }
+  R.exit_bepos = path.bepos;
+  return 0;
+}
+
 // The sort / elimination step of a pair whose candidates are in O, then its
 // survivors appended to the output in the pair's order (lane 0 ranks them).
 __device__ void finish_and_emit(const AlignLaunch &P, OvlArena &O, int a, int b, int comp, PairOut &po,
                                 int lane) {
+  const long long t0 = clock64();
   finish_candidates(Lanes{}, O);  // every lane, with the same O
+  if (lane == 0 && O.nov > 0) atomicAdd(&P.prof[1], (unsigned long long)(clock64() - t0));
   if (O.err) {
     po.err = O.err | 0x200;
     return;
@@ -457,7 +534,9 @@ __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch
     }
     PairResult R;
     WarpAligner AL{W, spec};
-    int rc = align_pair(S, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane, 32, blo, bhi);
+    const uint16_t *info = (tk.comp ? P.infoC : P.infoN) + tk.lo;
+    int rc = align_pair_dev(S, info, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane,
+                            blo, bhi);
     __syncwarp();
     PairOut po;
     po.waves = W.waves;
@@ -495,6 +574,7 @@ __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch
     __syncwarp();
   }
   if (lane == 0 && P.nsmall > 0) sums.flush(P);
+  if (lane == 0 && W.la_cycles > 0) atomicAdd(&P.prof[0], (unsigned long long)W.la_cycles);
 }
 
 
@@ -659,6 +739,34 @@ void launch_pack(const uint8_t *fwd, const int64_t *soff, const int64_t *clen, c
 
 // Pair boundaries of a sorted key array: flag[i] = 1 where (icont, jcont)
 // differs from key i-1.
+// Per seed of a unit's sorted keys: whether it starts a band (its (anchor,
+// partner, band) differs from the previous seed's), whether the previous
+// band of the same pair is the band just below (the block before reaches it
+// as its second stream), and at a band start the sum of 2*lcp over the
+// band's seeds capped at CHAIN_MIN.  A band start walks at most CHAIN_MIN / 2
+// seeds: every seed adds at least 2, so that many reach the cap.
+__global__ void k_band_info(const U128 *__restrict__ keys, int64_t n, SeedKeyLayout L, uint16_t *__restrict__ info) {
+  const int wb = L.off_j - L.off_band;                  // band field width
+  const int wk = L.total_bits - L.off_band;             // band + partner + anchor
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t me = key_bits(keys[i], L.off_band, wk);
+    const uint64_t prev = i > 0 ? key_bits(keys[i - 1], L.off_band, wk) : ~0ull;
+    if (i > 0 && prev == me) {
+      info[i] = 0;
+      continue;
+    }
+    const uint64_t bmask = (1ull << wb) - 1;
+    const bool adj = i > 0 && (prev >> wb) == (me >> wb) && (prev & bmask) + 1 == (me & bmask);
+    int sum = 0;
+    for (int64_t j = i; j < n && sum < CHAIN_MIN; j++) {
+      const U128 k = keys[j];
+      if (key_bits(k, L.off_band, wk) != me) break;
+      sum += (int)key_bits(k, 0, 6) << 1;
+    }
+    info[i] = BI_START | (adj ? BI_ADJ : 0) | (uint16_t)(sum < CHAIN_MIN ? sum : CHAIN_MIN);
+  }
+}
+
 __global__ void k_pair_flags(const U128 *__restrict__ keys, int64_t n, SeedKeyLayout L, uint32_t *__restrict__ flag) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     uint32_t f = 1;
@@ -792,25 +900,42 @@ __device__ __forceinline__ uint32_t small_bin(int64_t size) {
   return (uint32_t)(SMALL_BINS - 1) - (uint32_t)(size < SMALL_BINS - 1 ? size : SMALL_BINS - 1);
 }
 
-// A pair whose seeds' spans (2 lcp each) add up to less than CHAIN_MIN has
-// no chain that reaches the hit test (src/fastga_pipeline.c:656), so it makes
-// no Local_Alignment call and no alignment: it needs no task.  A pair of 8 or
-// more seeds is kept without reading them (each seed spans at least 24).
-__device__ __forceinline__ bool pair_live(const U128 *keys, int64_t lo, int64_t size) {
-  if (size >= 8) return true;
-  int sum = 0;
-  for (int64_t i = 0; i < size; i++) sum += 2 * (int)key_bits(keys[lo + i], 0, 6);
-  return sum >= CHAIN_MIN;
+// Whether a pair has a band block that can hold a chain passing the hit
+// test (src/fastga_pipeline.c:656): the blocks are a pair's runs of
+// consecutive bands taken two by two, and a band with no band just below
+// or above it alone; a block can pass only if its seeds' spans (2 lcp each)
+// add up to CHAIN_MIN.  So the pair is live iff some band start has, with
+// the band just below it (its block with that band), or alone if there is
+// none, a capped span sum of CHAIN_MIN.  The band below is found by walking
+// back at most CHAIN_MIN / 2 seeds; a band that long reaches the cap on its
+// own.  A pair that is not live makes no Local_Alignment call and no
+// alignment, and leaves the path as it found it: it needs no task.
+__global__ void k_pair_live(const uint16_t *__restrict__ info, int64_t n, const uint32_t *__restrict__ pflag,
+                            const uint32_t *__restrict__ pidx, uint8_t *__restrict__ live) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint16_t v = info[i];
+    if (!(v & BI_START)) continue;
+    int sum = v & 0xff;
+    if ((v & BI_ADJ) && sum < CHAIN_MIN) {
+      int below = CHAIN_MIN;  // a band longer than the walk
+      for (int64_t j = i - 1; j >= 0 && j >= i - CHAIN_MIN / 2; j--)
+        if (info[j] & BI_START) {
+          below = info[j] & 0xff;
+          break;
+        }
+      sum += below;
+    }
+    if (sum >= CHAIN_MIN) live[pidx[i] + pflag[i] - 1] = 1;
+  }
 }
 
 __global__ void k_small_hist(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
-                             int64_t nseeds, int comp, int64_t rs, const U128 *__restrict__ keys,
+                             int64_t nseeds, int comp, int64_t rs, const uint8_t *__restrict__ live,
                              uint32_t *__restrict__ hist) {
   for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = p0 + threadIdx.x;
     int64_t size = 0;
-    const bool small = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) &&
-                       pair_live(keys, pstart[p], size);
+    const bool small = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) && live[p];
     const uint32_t bin = small ? small_bin(size) : 0xffffffffu;
     const unsigned same = __match_any_sync(0xffffffffu, bin);
     if (small && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], (unsigned)__popc(same));
@@ -818,14 +943,13 @@ __global__ void k_small_hist(const int64_t *__restrict__ pstart, const int32_t *
 }
 
 __global__ void k_small_scatter(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
-                                int64_t nseeds, int comp, int64_t rs, const U128 *__restrict__ keys,
+                                int64_t nseeds, int comp, int64_t rs, const uint8_t *__restrict__ live,
                                 uint32_t *__restrict__ cursor, uint64_t *__restrict__ small) {
   const int lane = threadIdx.x & 31;
   for (int64_t p0 = (int64_t)blockIdx.x * blockDim.x; p0 < np; p0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = p0 + threadIdx.x;
     int64_t size = 0;
-    const bool small_p = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) &&
-                         pair_live(keys, pstart[p], size);
+    const bool small_p = p < np && !pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) && live[p];
     const uint32_t bin = small_p ? small_bin(size) : 0xffffffffu;
     const unsigned same = __match_any_sync(0xffffffffu, bin);
     const int leader = __ffs(same) - 1;
@@ -852,17 +976,30 @@ void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, i
 }
 
 void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                       const U128 *keys, uint32_t *hist, cudaStream_t st) {
+                       const uint8_t *live, uint32_t *hist, cudaStream_t st) {
   if (np <= 0) return;
   k_small_hist<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp, rs,
-                                                                                 keys, hist);
+                                                                                 live, hist);
 }
 
 void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                          const U128 *keys, uint32_t *cursor, uint64_t *small, cudaStream_t st) {
+                          const uint8_t *live, uint32_t *cursor, uint64_t *small, cudaStream_t st) {
   if (np <= 0) return;
   k_small_scatter<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp,
-                                                                                     rs, keys, cursor, small);
+                                                                                     rs, live, cursor, small);
+}
+
+void launch_pair_live(const uint16_t *info, int64_t n, const uint32_t *pflag, const uint32_t *pidx, uint8_t *live,
+                      cudaStream_t st) {
+  if (n <= 0) return;
+  k_pair_live<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, st>>>(info, n, pflag, pidx, live);
+}
+
+void launch_band_info(const U128 *keys, int64_t n, SeedKeyLayout L, uint16_t *info, cudaStream_t st) {
+  if (n <= 0) return;
+  int g = (int)((n + 255) / 256);
+  if (g > 148 * 32) g = 148 * 32;
+  k_band_info<<<g, 256, 0, st>>>(keys, n, L, info);
 }
 
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st) {

@@ -49,8 +49,14 @@ struct AlignLaunch {
   int ntasks;
   unsigned *next_task;
   unsigned *smflag;   // k_align_pairs: SM_FLAGS flags, zero at launch (null: off)
+  // SM cycles the launch's warps spent in Local_Alignment [0] and in the
+  // pairs' finishing step [1], zero at launch
+  unsigned long long *prof;
   int long_waves;     // a wave loop past this many waves flags its SM
   const U128 *keysN, *keysC;
+  // per seed of each unit: band start (bit 15), previous band of the pair
+  // adjacent (bit 14), capped 2*lcp sum of the band at its start (bits 0-7)
+  const uint16_t *infoN, *infoC;
   SeedKeyLayout layN, layC;
   const uint8_t *fwd, *rc;
   const int64_t *soff, *clen;
@@ -124,10 +130,12 @@ void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np
                            uint32_t *flag, cudaStream_t st);
 void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
                         const uint32_t *idx, int64_t *out3, cudaStream_t st);
+void launch_pair_live(const uint16_t *info, int64_t n, const uint32_t *pflag, const uint32_t *pidx, uint8_t *live,
+                      cudaStream_t st);
 void launch_small_hist(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                       const U128 *keys, uint32_t *hist, cudaStream_t st);
+                       const uint8_t *live, uint32_t *hist, cudaStream_t st);
 void launch_small_scatter(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                          const U128 *keys, uint32_t *cursor, uint64_t *small, cudaStream_t st);
+                          const uint8_t *live, uint32_t *cursor, uint64_t *small, cudaStream_t st);
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st);
 void launch_finish(const AlignLaunch &P, int grid, cudaStream_t st);
@@ -140,6 +148,7 @@ void launch_numeric(const uint8_t *bps, const int64_t *clen, const int64_t *boff
                     uint8_t *fwd, uint8_t *rc, cudaStream_t st);
 void launch_pack(const uint8_t *fwd, const int64_t *soff, const int64_t *clen, const int64_t *poff,
                  const int64_t *pwords, int ncontig, uint64_t *pk, cudaStream_t st);
+void launch_band_info(const U128 *keys, int64_t n, SeedKeyLayout L, uint16_t *info, cudaStream_t st);
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st);
 void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint32_t *flag, const uint32_t *idx,
                         int64_t *start, int32_t *ab, cudaStream_t st);

@@ -49,6 +49,7 @@ struct WarpWork {
   unsigned *smflag;      // per SM id: a warp there runs a long call (null: not kept)
   int long_waves;        // waves of one wave loop that make a call long (0: never)
   int flagged;           // this warp has flagged its SM
+  long long la_cycles;   // SM cycles spent in Local_Alignment calls (lane-uniform)
 };
 
 constexpr int PEBBLE_CHUNK = 4096;
@@ -1578,7 +1579,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
 #undef WVI
 
 // Local_Alignment, warp version (same control as local_alignment).
-__device__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
+__device__ __noinline__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
                                  Path &P, int low, int hgh, int anti, int lbord, int hbord) {
   const int lane = threadIdx.x & 31;
   int aoff, minp, maxp;

@@ -96,13 +96,14 @@ struct pga_ctx {
   DBuf pk, poff, pwords;
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
-      ridx, rout, selfb, pstart2, pab2, small, shist, fo_dev;
+      ridx, rout, selfb, pstart2, pab2, small, shist, fo_dev, binfo[2], plive[2];
   std::vector<AlnRec> h_recs;      // survivors in la_sort order
   std::vector<uint8_t> h_trace;    // their trace bytes
   std::vector<int64_t> h_toff;     // offsets into h_trace
   int64_t align_stats[8] = {0};    // pga_align_stats
   float align_ms[4] = {0};         // pga_align_times
   int64_t align_work[4] = {0};     // pga_align_work
+  int64_t align_prof[2] = {0};     // pga_align_profile: SM cycles in Local_Alignment, in finishing steps
   // pga_local_alignment: requests, paths, trace pool
   DBuf lreq, lpath, ltoff, ltrace, lnext;
   std::vector<int32_t> h_lpath;    // 7 ints per request
@@ -169,7 +170,8 @@ bool shed_align_buffers(pga_ctx *ctx) {
   DBuf *bufs[] = {&ctx->numf, &ctx->numr, &ctx->pk, &ctx->wave, &ctx->points, &ctx->cells, &ctx->ovl, &ctx->perm,
                   &ctx->cand, &ctx->recs, &ctx->outb, &ctx->rng_ovl, &ctx->tasks, &ctx->pout, &ctx->pflag,
                   &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->ftasks,
-                  &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace};
+                  &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace,
+                  &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1]};
   bool any = false;
   for (DBuf *b : bufs)
     if (b->p) {
@@ -724,6 +726,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     // the task counter, and the per-SM long-call flags after it
     CK(cudaMemsetAsync(ctx->task_next.p, 0, 64 + sizeof(unsigned) * aln::SM_FLAGS, ctx->st));
     L.smflag = P<unsigned>(ctx->task_next) + 16;
+    L.prof = (unsigned long long *)(P<uint8_t>(ctx->task_next) + 32);
     // automatic: on for launches bounded by their longest calls, off for the
     // throughput-bound ones (the three-CTA build), whose flagged SMs would
     // idle warps that still have queue work
@@ -764,7 +767,8 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     if (!rout_h.empty())
       CK(cudaMemcpyAsync(rout_h.data(), ctx->rout.p, sizeof(PairOut) * rout_h.size(), cudaMemcpyDeviceToHost,
                          ctx->st));
-    unsigned long long used[4] = {0, 0, 0, 0};
+    unsigned long long used[4] = {0, 0, 0, 0}, prof[2] = {0, 0};
+    CK(cudaMemcpyAsync(prof, L.prof, 16, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&used[0], ctx->cand_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&used[1], ctx->rng_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(&used[2], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -782,6 +786,8 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
         if (badf < 0) badf = (int)f;
       }
     if (errs == 0) {
+      ctx->align_prof[0] += (int64_t)prof[0];
+      ctx->align_prof[1] += (int64_t)prof[1];
       ctx->cand_used = used[0];
       ctx->rng_used = used[1];
       ctx->rec_used = used[2];
@@ -943,6 +949,16 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
   L.keysC = ctx->sorted[1];
   L.layN = ctx->lay[0];
   L.layC = ctx->lay[1];
+  for (int comp = 0; comp < 2; comp++) {
+    // the units' band info: which band blocks can hold a chain that passes the hit test
+    const int64_t n = ctx->nseed[comp];
+    ENSURE(ctx->binfo[comp], sizeof(uint16_t) * (size_t)n + 16);
+    launch_band_info(ctx->sorted[comp], n, ctx->lay[comp], P<uint16_t>(ctx->binfo[comp]), ctx->st);
+    LAUNCHED(n > 0 ? 1 : 0);
+  }
+  CK(cudaGetLastError());
+  L.infoN = P<uint16_t>(ctx->binfo[0]);
+  L.infoC = P<uint16_t>(ctx->binfo[1]);
   L.fwd = P<uint8_t>(ctx->numf);
   L.rc = P<uint8_t>(ctx->numr);
   L.soff = P<int64_t>(ctx->soff);
@@ -1075,6 +1091,7 @@ int run_align(pga_ctx *ctx) {
   if (r0) return r0;
   ctx->cand_used = ctx->rng_used = ctx->rec_used = ctx->out_used = 0;
   for (int i = 0; i < 4; i++) ctx->align_work[i] = 0;
+  ctx->align_prof[0] = ctx->align_prof[1] = 0;
 
   // 4. Pair lists of both units.  They stay on the device; only the pairs
   // the host plans come back: self pairs (FastGA's order) and, with band
@@ -1111,6 +1128,12 @@ int run_align(pga_ctx *ctx) {
     const int32_t *pab = P<int32_t>(*dpab[comp]);
     launch_pair_starts(ctx->sorted[comp], n, ctx->lay[comp], P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
                        (int64_t *)pst, (int32_t *)pab, ctx->st);
+    // which pairs have a band block that can pass the hit test (the others need no task)
+    ENSURE(ctx->plive[comp], (size_t)np + 16);
+    CK(cudaMemsetAsync(ctx->plive[comp].p, 0, (size_t)np + 16, ctx->st));
+    launch_pair_live(P<uint16_t>(ctx->binfo[comp]), n, P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
+                     P<uint8_t>(ctx->plive[comp]), ctx->st);
+    LAUNCHED(1);
     // the host's pairs
     launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), ctx->st);
     CK(exclusive_scan<uint32_t>(P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), np, P<uint32_t>(ctx->scan_tmp), tot,
@@ -1156,13 +1179,13 @@ int run_align(pga_ctx *ctx) {
       if (npairs[comp] - (int64_t)pairs[comp].size() <= 0) continue;
       CK(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (SMALL_BINS + 1), ctx->st));
       launch_small_hist(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
-                        ctx->sorted[comp], hist, ctx->st);
+                        P<uint8_t>(ctx->plive[comp]), hist, ctx->st);
       uint32_t *tot = P<uint32_t>(ctx->u64tmp);
       CK(exclusive_scan<uint32_t>(hist, cur, SMALL_BINS + 1, P<uint32_t>(ctx->scan_tmp), tot, ctx->st));
       uint32_t ns = 0;
       CK(cudaMemcpyAsync(&ns, tot, 4, cudaMemcpyDeviceToHost, ctx->st));
       launch_small_scatter(P<int64_t>(*dpst[comp]), P<int32_t>(*dpab[comp]), npairs[comp], ctx->nseed[comp], comp, RS,
-                           ctx->sorted[comp], cur, P<uint64_t>(ctx->small) + nsmall, ctx->st);
+                           P<uint8_t>(ctx->plive[comp]), cur, P<uint64_t>(ctx->small) + nsmall, ctx->st);
       CK(cudaStreamSynchronize(ctx->st));
       LAUNCHED(5);
       nsmall += ns;
@@ -1595,7 +1618,7 @@ void pga_ctx_destroy(pga_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->st);
-  DBuf *abufs[] = {&ctx->pk, &ctx->poff, &ctx->pwords, &ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout,
+  DBuf *abufs[] = {&ctx->pk, &ctx->poff, &ctx->pwords, &ctx->numf, &ctx->numr, &ctx->soff, &ctx->spec_tab, &ctx->tasks, &ctx->task_next, &ctx->pout, &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1],
                    &ctx->wave, &ctx->points, &ctx->cells, &ctx->cell_next, &ctx->ovl, &ctx->perm, &ctx->cand,
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
@@ -2788,6 +2811,13 @@ int pga_local_alignment_copy(pga_ctx *ctx, int32_t *path7, int64_t *trace_off, u
 int pga_align_work(const pga_ctx *ctx, int64_t *work4) {
   if (!ctx || !work4) return PGA_ERR_ARG;
   for (int i = 0; i < 4; i++) work4[i] = ctx->align_work[i];
+  return PGA_OK;
+}
+
+int pga_align_profile(const pga_ctx *ctx, int64_t *prof2) {
+  if (!ctx || !prof2) return PGA_ERR_ARG;
+  prof2[0] = ctx->align_prof[0];
+  prof2[1] = ctx->align_prof[1];
   return PGA_OK;
 }
 

@@ -73,6 +73,7 @@ _SIGS = {
     "pga_index_set_digit_bits": (C.c_int, [vp, C.c_int]),
     "pga_align_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
     "pga_align_work": (C.c_int, [vp, vp]),
+    "pga_align_profile": (C.c_int, [vp, vp]),
     "pga_local_alignment": (C.c_int, [vp, C.c_int64, vp, C.POINTER(C.c_int64)]),
     "pga_local_alignment_copy": (C.c_int, [vp, vp, vp, vp]),
     "pga_write_1aln": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
@@ -416,6 +417,13 @@ class Device:
         a = np.zeros(4, dtype=np.int64)
         self._ck(self.L.pga_align_work(self.h, a.ctypes.data_as(vp)), "align_work")
         return {"waves": int(a[0]), "cells": int(a[1]), "calls": int(a[2]), "tasks": int(a[3])}
+
+    def align_profile(self) -> dict:
+        """Warp cycles of the last align(): inside Local_Alignment and in the
+        pairs' finishing steps (summed over warps)."""
+        a = np.zeros(2, dtype=np.int64)
+        self._ck(self.L.pga_align_profile(self.h, a.ctypes.data_as(vp)), "align_profile")
+        return {"local_alignment_cycles": int(a[0]), "finish_cycles": int(a[1])}
 
     def set_build(self, ctas_per_sm: int):
         """Which build of the alignment kernel runs (0 automatic, 2 or 3)."""

@@ -221,6 +221,11 @@ int pga_align(pga_ctx *ctx, int64_t *nalign);
  * thread runs each pair there). */
 int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
 
+/* Where the last pga_align's warps spent their time: prof2[0] = SM cycles
+ * inside Local_Alignment calls, prof2[1] = SM cycles in the pairs' finishing
+ * steps, each summed over warps (the rest of a task's cycles is the chain
+ * scan and its bookkeeping). */
+int pga_align_profile(const pga_ctx *ctx, int64_t *prof2);
 /* Tuning, no counterpart in the reference: which build of the alignment
  * kernel runs -- 2 (255 registers, two CTAs per SM: best when the launch is
  * bounded by its longest alignments) or 3 (168 registers, three CTAs per SM:
