@@ -1579,7 +1579,7 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
 #undef WVI
 
 // Local_Alignment, warp version (same control as local_alignment).
-__device__ __noinline__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
+__device__ __forceinline__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
                                  Path &P, int low, int hgh, int anti, int lbord, int hbord) {
   const int lane = threadIdx.x & 31;
   int aoff, minp, maxp;

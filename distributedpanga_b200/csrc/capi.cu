@@ -730,7 +730,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     // automatic: on for launches bounded by their longest calls, off for the
     // throughput-bound ones (the three-CTA build), whose flagged SMs would
     // idle warps that still have queue work
-    L.long_waves = ctx->long_waves >= 0 ? ctx->long_waves : (L.min_blocks == 3 ? 0 : LONG_WAVES_AUTO);
+    L.long_waves = ctx->long_waves >= 0 ? ctx->long_waves : (L.min_blocks >= 3 ? 0 : LONG_WAVES_AUTO);
     CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));
     CK(cudaMemcpyAsync(ctx->cand_next.p, &ctx->counters[0], 8, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->rng_next.p, &ctx->counters[1], 8, cudaMemcpyHostToDevice, ctx->st));
@@ -1217,7 +1217,7 @@ int run_align(pga_ctx *ctx) {
   L.fo_pos = fo_pos;
   // the launch is bounded by its longest tasks up to about a million pairs,
   // by throughput beyond: then the build with more resident warps
-  L.min_blocks = ctx->align_build ? ctx->align_build : npairs[0] + npairs[1] > ALIGN_MANY_PAIRS ? 3 : 2;
+  L.min_blocks = ctx->align_build ? ctx->align_build : npairs[0] + npairs[1] > ALIGN_MANY_PAIRS ? 4 : 2;
   L.sred = sred;
   L.fo_last = sred + 8;
   L.fo_earlier = sred + 8 + nc;
@@ -2822,7 +2822,7 @@ int pga_align_profile(const pga_ctx *ctx, int64_t *prof2) {
 }
 
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
-  if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3)) return PGA_ERR_ARG;
+  if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3 && ctas_per_sm != 4)) return PGA_ERR_ARG;
   ctx->align_build = ctas_per_sm;
   return PGA_OK;
 }

@@ -228,8 +228,9 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
 int pga_align_profile(const pga_ctx *ctx, int64_t *prof2);
 /* Tuning, no counterpart in the reference: which build of the alignment
  * kernel runs -- 2 (255 registers, two CTAs per SM: best when the launch is
- * bounded by its longest alignments) or 3 (168 registers, three CTAs per SM:
- * best for launches of many pairs); 0 (the default) picks 3 above 2^20 pairs.
+ * bounded by its longest alignments), 3 (168 registers, three CTAs per SM) or
+ * 4 (128 registers, four CTAs per SM: best for launches of many pairs); 0
+ * (the default) picks 4 above 2^20 pairs, else 2.
  * The alignments are the same either way. */
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
 

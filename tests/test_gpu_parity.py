@@ -212,7 +212,7 @@ def test_alignments_independent_of_band_ranges(dev, case):
 
 @pytest.mark.parametrize("case", ["chromset_s0005", "many_contigs"])
 def test_alignments_independent_of_kernel_build(dev, case):
-    """The alignment kernel's two builds (two or three CTAs per SM), with the
+    """The alignment kernel's builds (two, three or four CTAs per SM), with the
     long-call SM flags off, at 20000 waves, and at 50 waves (nearly every
     SM flagged, so that the flagging warps drain most of the queue), give the
     reference's alignments."""
@@ -226,7 +226,7 @@ def test_alignments_independent_of_kernel_build(dev, case):
     dev.index_build(want_entries=False)
     dev.merge(dig["freq_cutoff"])
     try:
-        for build in (3, 2):
+        for build in (4, 3, 2):
             dev.set_build(build)
             for lw in (0, 50, 20000):
                 dev.set_long_waves(lw)
