@@ -778,8 +778,22 @@ def serve_measure(args) -> dict:
     # is congruent to r
     target = pipeline.Target(ttext, device=local_rank)
     target_s = time.monotonic() - t
-    srv = serve.Server(target, slots=args.serve_slots)
+    target_bases = target.bases
+    big = max(reqs, key=lambda r: r.bases)
+    # the device memory one request holds, measured on the largest one alone
+    # (a context keeps its buffers): the served scheduler's charge per base
+    import torch
     dp = pipeline.Device(local_rank)
+    free0 = torch.cuda.mem_get_info(local_rank)[0]
+    dp.gdb_ingest_fasta(ttext + big.text, tables=False)
+    dp.index_build(want_entries=False)
+    dp.merge(10)
+    dp.align()
+    held = free0 - torch.cuda.mem_get_info(local_rank)[0]
+    dp.close()
+    per_base = 1.1 * held / (target_bases + big.bases)
+    srv = serve.Server(target, slots=args.serve_slots, bytes_per_base=per_base)
+    dp = None
 
     def served(slot, r):
         # Server.execute with the host wall time of each call
@@ -806,33 +820,34 @@ def serve_measure(args) -> dict:
         t3 = time.monotonic()
         al = dp.alignments()
         t4 = time.monotonic()
-        return {"nalign": n, "gdb_bases": target.bases + r.bases, "query_bases": r.bases, "records": dp.nrec,
+        return {"nalign": n, "gdb_bases": target_bases + r.bases, "query_bases": r.bases, "records": dp.nrec,
                 "alignments": al, "phases": [t1 - t0, t2 - t1, t3 - t2, t4 - t3]}
 
-    # warm-up: the largest request on every slot and on the plain context
-    # (kernels loaded, every buffer at its largest size)
-    big = max(reqs, key=lambda r: r.bases)
+    # The two forms one after the other, each holding the device alone (the
+    # served form's slots and target are freed before the plain form runs).
+    # Warm-up: the largest request on every slot (as many at once as the
+    # memory budget admits), then on the plain context (kernels loaded, every
+    # buffer at its largest size).
     srv.sched.run([serve.Request(k, big.text, 0.0, big.bases) for k in range(args.serve_slots)], served)
-    plain(0, big)
     clocks = ClockSampler(local_rank)
     clocks.start()
     res, summ = serve.serve_sharded(reqs, lambda mine: srv.sched.run(mine, served), rank, world)
+    slots_admitted = max(1, max(len([q for q in res if q.admitted <= r.admitted < q.done]) for r in res)) if res else 0
+    srv.close()
+    target.close()
+    dp = pipeline.Device(local_rank)
+    plain(0, big)
     plain_sched = serve.Scheduler(1, 1 << 62, lambda r: 0)
     pres, psumm = serve.serve_sharded(reqs, lambda mine: plain_sched.run(mine, plain), rank, world)
     clk = clocks.stop()
+    dp.close()
     if rank != 0:
-        srv.close()
-        dp.close()
-        target.close()
         return None
     same = 0
     for a, b in zip(res, pres):
         if a.out["nalign"] == b.out["nalign"] and all(np.array_equal(x, y) for x, y in
                                                       zip(a.out["alignments"], b.out["alignments"])):
             same += 1
-    srv.close()
-    dp.close()
-    target.close()
     line = {
         "metric": "served aligned Mbp/s (GDB bases of target + query per request / wall s) with p50/p99 request "
                   "latency, beside the plain form",
@@ -842,7 +857,9 @@ def serve_measure(args) -> dict:
         "config": {"workload": "serve: resident target of %d Mbp (chromset generator), %d Poisson requests at "
                                "%.1f/s, query sizes log-uniform %.1f-%.1f Mbp, divergence 0.5-5%%; k=40, FREQ=10"
                                % (round(target.bases / 1e6), len(reqs), args.serve_rate, 1 * sc, 200 * sc),
-                   "slots": args.serve_slots, "target_contigs": target.ncontig,
+                   "slots": args.serve_slots, "max_requests_in_flight": slots_admitted,
+                   "device_bytes_per_request_base": round(per_base / 1.1, 1),
+                   "target_contigs": target.ncontig,
                    "parallelism": "replicas%d: one resident target per GPU, requests sharded by id" % world,
                    "target_build_s": round(target_s, 3)},
         "served": {k: round(v, 4) if isinstance(v, float) else v for k, v in summ.items()},

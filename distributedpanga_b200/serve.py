@@ -44,8 +44,8 @@ BYTES_PER_BASE = 64
 FIXED_BYTES = 1 << 30
 
 
-def footprint_bytes(gdb_bases: int) -> int:
-    return BYTES_PER_BASE * int(gdb_bases) + FIXED_BYTES
+def footprint_bytes(gdb_bases: int, bytes_per_base: float = BYTES_PER_BASE) -> int:
+    return int(bytes_per_base * int(gdb_bases)) + FIXED_BYTES
 
 
 @dataclass
@@ -182,10 +182,12 @@ class Server:
     """The request loop on one device: `slots` contexts serving requests
     against `target` (a pipeline.Target), FIFO under `budget_bytes` of device
     memory (default: what the device has free when the server starts, less
-    the target-independent reserve of 4 GiB)."""
+    the target-independent reserve of 4 GiB), a request charged
+    `bytes_per_base` per base of GDB(target + query) (a measured figure where
+    the caller has one: see bench.py's served measurement)."""
 
     def __init__(self, target, slots: int = 2, budget_bytes: int | None = None, freq: int = 10,
-                 keep_alignments: bool = True):
+                 keep_alignments: bool = True, bytes_per_base: float = BYTES_PER_BASE):
         from . import pipeline
         self.target = target
         self.freq = freq
@@ -196,7 +198,7 @@ class Server:
             free, _ = torch.cuda.mem_get_info(target.device)
             budget_bytes = max(0, free - (4 << 30))
         tb = target.bases
-        self.sched = Scheduler(slots, budget_bytes, lambda r: footprint_bytes(tb + r.bases))
+        self.sched = Scheduler(slots, budget_bytes, lambda r: footprint_bytes(tb + r.bases, bytes_per_base))
 
     def close(self):
         for d in self.devs:
