@@ -1578,69 +1578,73 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
 
 #undef WVI
 
-// Local_Alignment, warp version (same control as local_alignment).
-__device__ __forceinline__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, bool acomp,
-                                 Path &P, int low, int hgh, int anti, int lbord, int hbord) {
+// A path on the complemented A (and so on reversed B coordinates) in
+// forward coordinates: both intervals mirrored, and the trace-point pairs
+// (diffs, b-delta) in the opposite order, the warp's lanes swapping pair q
+// with pair npairs-1-q.
+__device__ __forceinline__ void path_to_forward(uint16_t *trace, const Seq &A, const Seq &B, Path &P) {
   const int lane = threadIdx.x & 31;
-  int aoff, minp, maxp;
-  bool fshort, rshort;
-  int maxtp = 2 * (A.len / spec.trace_space + 2);
+  const int ab = P.abpos, bb = P.bbpos;
+  P.abpos = A.len - P.aepos;
+  P.aepos = A.len - ab;
+  P.bbpos = B.len - P.bepos;
+  P.bepos = B.len - bb;
+  const int npairs = P.tlen >> 1;
+  __syncwarp();
+  for (int q = lane; q < npairs / 2; q += 32) {
+    uint32_t *x = reinterpret_cast<uint32_t *>(trace) + q, *y = reinterpret_cast<uint32_t *>(trace) + (npairs - 1 - q);
+    const uint32_t t = *x;
+    *x = *y;
+    *y = t;
+  }
+  __syncwarp();
+}
+
+// Local_Alignment (lib/align.c:1423-1576) on one warp.  The path is grown
+// forward from the seed point (antidiagonal `anti`, diagonals [low, hgh],
+// kept within `lbord` / `hbord` of them when those are set), then backward
+// from the diagonal the forward pass started on.  An end that moved fewer
+// than DUB_TRIM antidiagonals from `anti` did not get away from the seed:
+// with both ends short the path shrinks to the midpoint of the two, without
+// trace points; with one end short, that direction runs again from the end
+// the other direction reached (a forward re-run keeps the reverse pass's
+// start, a reverse re-run counts its differences afresh).  With `acomp` A is
+// the complemented contig and the path comes back in forward coordinates.
+// Returns 1 on a work-space overflow (W.err says which).
+__device__ __forceinline__ int local_alignment_w(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B,
+                                                 bool acomp, Path &P, int low, int hgh, int anti, int lbord,
+                                                 int hbord) {
+  const int maxtp = 2 * (A.len / spec.trace_space + 2);  // trace points the longest path can have
   if (2 * (int64_t)maxtp > W.point_cap) {
     W.err |= ALN_ERR_POINTS;
     return 1;
   }
   P.trace_off = maxtp;
-  while (((anti - hgh) >> 1) < 0) hgh -= 1;
-  minp = (lbord < 0) ? -I32MAX : low - lbord;
-  maxp = (hbord < 0) ? I32MAX : hgh + hbord;
-  aoff = acomp ? A.len % spec.trace_space : 0;
+  while (((anti - hgh) >> 1) < 0) hgh -= 1;  // no diagonal above the antidiagonal's start
+  const int minp = lbord < 0 ? -I32MAX : low - lbord;
+  const int maxp = hbord < 0 ? I32MAX : hgh + hbord;
+  const int aoff = acomp ? A.len % spec.trace_space : 0;
+
   if (forward_wave_w(W, spec, A, B, P, &low, hgh, anti, minp, maxp, aoff)) return 1;
-  fshort = ((P.aepos + P.bepos) - anti < DUB_TRIM);
+  const bool fwd_away = (P.aepos + P.bepos) - anti >= DUB_TRIM;
   if (reverse_wave_w(W, spec, A, B, P, low, low, anti, minp, maxp, aoff)) return 1;
-  rshort = (anti - (P.abpos + P.bbpos) < DUB_TRIM);
-  if (fshort) {
-    if (rshort) {
-      P.aepos = P.abpos = (P.abpos + P.aepos) >> 1;
-      P.bepos = P.bbpos = (P.bbpos + P.bepos) >> 1;
-      P.tlen = 0;
-    } else {
-      low = P.abpos - P.bbpos;
-      anti = P.abpos + P.bbpos;
-      P.tlen = 0;
-      if (forward_wave_w(W, spec, A, B, P, &low, low, anti, minp, maxp, aoff)) return 1;
-    }
-  } else if (rshort) {
-    low = P.aepos - P.bepos;
-    anti = P.aepos + P.bepos;
+  const bool rev_away = anti - (P.abpos + P.bbpos) >= DUB_TRIM;
+
+  if (!fwd_away && !rev_away) {
+    P.aepos = P.abpos = (P.abpos + P.aepos) >> 1;
+    P.bepos = P.bbpos = (P.bbpos + P.bepos) >> 1;
+    P.tlen = 0;
+  } else if (!fwd_away) {
+    int from = P.abpos - P.bbpos;
+    P.tlen = 0;
+    if (forward_wave_w(W, spec, A, B, P, &from, from, P.abpos + P.bbpos, minp, maxp, aoff)) return 1;
+  } else if (!rev_away) {
+    const int from = P.aepos - P.bepos, at = P.aepos + P.bepos;
     P.tlen = 0;
     P.diffs = 0;
-    if (reverse_wave_w(W, spec, A, B, P, low, low, anti, minp, maxp, aoff)) return 1;
+    if (reverse_wave_w(W, spec, A, B, P, from, from, at, minp, maxp, aoff)) return 1;
   }
-  if (acomp) {
-    uint16_t *trace = W.points + P.trace_off;
-    int i = P.abpos;
-    P.abpos = A.len - P.aepos;
-    P.aepos = A.len - i;
-    i = P.bbpos;
-    P.bbpos = B.len - P.bepos;
-    P.bepos = B.len - i;
-    __syncwarp();
-    if (lane == 0) {
-      i = P.tlen - 2;
-      int j = 0;
-      while (j < i) {
-        uint16_t p = trace[i];
-        trace[i] = trace[j];
-        trace[j] = p;
-        p = trace[i + 1];
-        trace[i + 1] = trace[j + 1];
-        trace[j + 1] = p;
-        i -= 2;
-        j += 2;
-      }
-    }
-    __syncwarp();
-  }
+  if (acomp) path_to_forward(W.points + P.trace_off, A, B, P);
   return 0;
 }
 
