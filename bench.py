@@ -370,6 +370,21 @@ def run_profile_stage(args) -> None:
         return
     cs, _ = make_contigs(args.scale)
     dev = pipeline.Device(0)
+    if args.profile_stage == "align":
+        # the alignment launch alone: the index, merge and diagonal sorts once,
+        # then warmup + steps alignments with the chosen kernel build
+        dev.gdb_load(cs)
+        dev.index_build(want_entries=False)
+        dev.merge(freq_cutoff())
+        dev.diag_sort(0)
+        dev.diag_sort(1)
+        dev.set_build(args.align_build)
+        for _ in range(args.warmup + args.steps):
+            n = dev.align()
+            print(json.dumps({"stage": "align", "alignments": n, "work": dev.align_work(),
+                              "times_ms": dev.align_times()}), flush=True)
+        dev.close()
+        return
     if args.profile_stage == "index":
         dev.gdb_load(cs)
         dev.enable_timing(True)
@@ -912,7 +927,9 @@ def main():
     ap.add_argument("--no-check", action="store_true", help="skip the comparison with the reference's digests")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 2 x 100 Mbp secondary measurement")
     ap.add_argument("--no-ingest", action="store_true", help="skip the FASTA ingest measurement")
-    ap.add_argument("--profile-stage", choices=["index", "ingest", "serve"], default=None,
+    ap.add_argument("--align-build", type=int, default=0,
+                    help="with --profile-stage align: the alignment kernel's build (0 automatic, 2, 3 or 4)")
+    ap.add_argument("--profile-stage", choices=["index", "ingest", "serve", "align"], default=None,
                     help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     ap.add_argument("--serve", action="store_true",
                     help="measure the served form (resident target, concurrent requests) beside the plain one")
