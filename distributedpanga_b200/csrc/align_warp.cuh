@@ -235,9 +235,9 @@ struct WaveSlice {
 // Lockstep snakes of a lane's diagonals: forward along A.pf / B.pf from
 // (x, x-k), reverse along A.pr / B.pr from (A.len-x, B.len-y); stops and
 // sentinel hits as snake_fwd / snake_rev.
-template <bool FWD, int J>
-__device__ __forceinline__ void lane_snakes(const Seq &A, const Seq &B, int nact, const int *k, int *x, int *run,
-                                            int *hb, int *hA) {
+template <int J>
+__device__ __forceinline__ void lane_snakes(const bool FWD, const Seq &A, const Seq &B, int nact, const int *k, int *x,
+                                            int *run, int *hb, int *hA) {
   int oa[J], ob[J], mx[J], t[J];
   bool go[J];
 #pragma unroll
@@ -320,9 +320,8 @@ __device__ __forceinline__ uint64_t join32(uint64_t w0, uint64_t w1, int sh) {
 // three words of each packed sequence loaded together.  The third word may
 // lie past this sequence's copy (its bases are beyond mx and never count);
 // the packed buffer has spare words at its end.
-template <bool FWD>
-__device__ __forceinline__ void snake1(const Seq &A, const Seq &B, bool act, int k, int &x, int &run, int &hb,
-                                       int &hA) {
+__device__ __forceinline__ void snake1(const bool FWD, const Seq &A, const Seq &B, bool act, int k, int &x, int &run,
+                                       int &hb, int &hA) {
   hb = hA = 0;
   run = 0;
   if (!act) return;
@@ -397,9 +396,9 @@ __device__ __forceinline__ int pick(const int *v, int j) {
 // One pass of a wave over visit positions [p0, p0 + 32*J): lane l takes
 // positions p0 + l*J .. p0 + l*J + J-1.  carry is the running best before
 // the pass.
-template <bool FWD, int J>
-__device__ __forceinline__ int wave_pass(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
-                                         int hgh, int w, int p0, int dif, int cur, int &carry, int &besta,
+template <int J>
+__device__ __forceinline__ int wave_pass(const bool FWD, WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B,
+                                         int low, int hgh, int w, int p0, int dif, int cur, int &carry, int &besta,
                                          int &bestx, int &lasta, int &trima, int &trimx, int &trimd, int &trimha,
                                          int &more, int &aclip, int &bclip, WaveSlice &WS) {
   const int lane = threadIdx.x & 31;
@@ -466,7 +465,7 @@ __device__ __forceinline__ int wave_pass(WarpWork &W, const AlignSpec &spec, con
       x[j] = (c[j] + k[j]) >> 1;
     }
   }
-  lane_snakes<FWD, J>(A, B, nact, k, x, run, hb, hA);
+  lane_snakes<J>(FWD, A, B, nact, k, x, run, hb, hA);
   int npl = 0;
 #pragma unroll
   for (int j = 0; j < J; j++) {
@@ -609,21 +608,20 @@ __device__ __forceinline__ int wave_pass(WarpWork &W, const AlignSpec &spec, con
 
 // The whole wave: one pass of single diagonals when it is at most 32 wide,
 // else passes of WJ diagonals per lane.
-template <bool FWD>
-__device__ __forceinline__ int wave_sweep(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
-                                          int hgh, int dif, int cur, int &besta, int &bestx, int &lasta, int &trima,
-                                          int &trimx, int &trimd, int &trimha, int &more, int &aclip, int &bclip,
-                                          WaveSlice &WS) {
+__device__ __forceinline__ int wave_sweep(const bool FWD, WarpWork &W, const AlignSpec &spec, const Seq &A,
+                                          const Seq &B, int low, int hgh, int dif, int cur, int &besta, int &bestx,
+                                          int &lasta, int &trima, int &trimx, int &trimd, int &trimha, int &more,
+                                          int &aclip, int &bclip, WaveSlice &WS) {
   const int w = hgh - low + 1;
   WS.single = w <= 32 * WJ;
   WS.nact = 0;
   WS.k0 = 0;
   int carry = besta;
   if (w <= 32)
-    return wave_pass<FWD, 1>(W, spec, A, B, low, hgh, w, 0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
+    return wave_pass<1>(FWD, W, spec, A, B, low, hgh, w, 0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
                              trimd, trimha, more, aclip, bclip, WS);
   for (int p0 = 0; p0 < w; p0 += 32 * WJ)
-    if (wave_pass<FWD, WJ>(W, spec, A, B, low, hgh, w, p0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
+    if (wave_pass<WJ>(FWD, W, spec, A, B, low, hgh, w, p0, dif, cur, carry, besta, bestx, lasta, trima, trimx,
                            trimd, trimha, more, aclip, bclip, WS))
       return 1;
   return 0;
@@ -633,9 +631,8 @@ __device__ __forceinline__ int wave_sweep(WarpWork &W, const AlignSpec &spec, co
 // hgh becomes the largest and low the smallest diagonal within WAVE_LAG of
 // the best antidiagonal, or hgh = low - 1 when none is (the reference's
 // loop from either end).  V is the new wave's buffer.
-template <bool FWD>
-__device__ __forceinline__ void wave_prune(const WarpWork &W, const int *V, int besta, int &low, int &hgh,
-                                           const WaveSlice &WS) {
+__device__ __forceinline__ void wave_prune(const bool FWD, const WarpWork &W, const int *V, int besta, int &low,
+                                           int &hgh, const WaveSlice &WS) {
   if (hgh < low) return;
   const int vmask = W.vcap - 1;
   const int n = FWD ? besta - WAVE_LAG : besta + WAVE_LAG;
@@ -725,17 +722,14 @@ __device__ __forceinline__ int64_t reg_pebbles(RegCtx &X, int cnt) {
 }
 
 // Visit position of lane l's diagonal (forward: hgh first, reverse: low first).
-template <bool FWD>
-__device__ __forceinline__ int reg_pos(int l, int low, int hgh) {
+__device__ __forceinline__ int reg_pos(const bool FWD, int l, int low, int hgh) {
   return FWD ? ((hgh - l) & 31) : ((l - low) & 31);
 }
-template <bool FWD>
-__device__ __forceinline__ int reg_lane(int p, int low, int hgh) {
+__device__ __forceinline__ int reg_lane(const bool FWD, int p, int low, int hgh) {
   return FWD ? ((hgh - p) & 31) : ((low + p) & 31);
 }
 // A lane mask reordered so that bit p is the lane at visit position p.
-template <bool FWD>
-__device__ __forceinline__ uint32_t reg_posmask(uint32_t m, int low, int hgh) {
+__device__ __forceinline__ uint32_t reg_posmask(const bool FWD, uint32_t m, int low, int hgh) {
   return FWD ? __brev(__funnelshift_l(m, m, 31 - (hgh & 31))) : __funnelshift_r(m, m, low & 31);
 }
 
@@ -772,11 +766,10 @@ __device__ __forceinline__ void reg_store(WarpWork &W, int cur, int plow, int ph
 // One wave in registers: [low, hgh] (at most 32 wide) from the previous
 // wave [plow, phgh] (not empty, inside [low-1, hgh+1]).  Same results as
 // wave_sweep; fills WS for wave_prune.
-template <bool FWD>
-__device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const Seq &A, const Seq &B, int low,
-                                        int hgh, int plow, int phgh, int dif, RegWave &R, int &besta, int &bestx,
-                                        int &lasta, int &trima, int &trimx, int &trimd, int &trimha, int &more,
-                                        int &aclip, int &bclip, WaveSlice &WS) {
+__device__ __forceinline__ int reg_wave(const bool FWD, RegCtx &X, const AlignSpec &spec, const Seq &A, const Seq &B,
+                                        int low, int hgh, int plow, int phgh, int dif, RegWave &R, int &besta,
+                                        int &bestx, int &lasta, int &trima, int &trimx, int &trimd, int &trimha,
+                                        int &more, int &aclip, int &bclip, WaveSlice &WS) {
   const int lane = threadIdx.x & 31;
   const int vmask = X.vmask;
   const int tspace = spec.trace_space;
@@ -813,7 +806,7 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
   b <<= 1;
   int x = (c + k) >> 1;
   int run[1], hb[1], hA[1];
-  snake1<FWD>(A, B, act, k, x, run[0], hb[0], hA[0]);
+  snake1(FWD, A, B, act, k, x, run[0], hb[0], hA[0]);
   int npb = 0;
   if (act) {
     history_run(b, m, run[0]);
@@ -839,10 +832,10 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
     tr = spec.table[b & TRIM_MASK] >= 0 &&
          spec.table[(b >> TRIM_LEN) & TRIM_MASK] + spec.score[b & TRIM_MASK] >= 0;
   // pebble slots in visit order
-  const int pos = reg_pos<FWD>(lane, low, hgh);
+  const int pos = reg_pos(FWD, lane, low, hgh);
   int off, tot;
   if (__ballot_sync(FULL, npb > 1) == 0) {
-    uint32_t one = reg_posmask<FWD>(__ballot_sync(FULL, npb == 1), low, hgh);
+    uint32_t one = reg_posmask(FWD, __ballot_sync(FULL, npb == 1), low, hgh);
     off = __popc(one & ((1u << pos) - 1));
     tot = __popc(one);
   } else {
@@ -850,7 +843,7 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
     int xsum = npb;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      int y = __shfl_sync(FULL, xsum, reg_lane<FWD>(pos - d, low, hgh));
+      int y = __shfl_sync(FULL, xsum, reg_lane(FWD, pos - d, low, hgh));
       if (pos >= d) xsum += y;
     }
     off = xsum - npb;
@@ -892,8 +885,8 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
   }
   // clips: bclip from the first visited diagonal that met B's end, aclip
   // from the last visited that met A's end
-  const uint32_t hbm = reg_posmask<FWD>(__ballot_sync(FULL, act && hb[0]), low, hgh);
-  const uint32_t ham = reg_posmask<FWD>(__ballot_sync(FULL, act && hA[0]), low, hgh);
+  const uint32_t hbm = reg_posmask(FWD, __ballot_sync(FULL, act && hb[0]), low, hgh);
+  const uint32_t ham = reg_posmask(FWD, __ballot_sync(FULL, act && hA[0]), low, hgh);
   if (hbm) {
     more = 0;
     const int p = __ffs(hbm) - 1;
@@ -917,9 +910,9 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
     int lp = -1, lt = -1;
     bool first = true;
     while (true) {
-      const uint32_t eq = reg_posmask<FWD>(__ballot_sync(FULL, act && c == best && pos < limit), low, hgh);
+      const uint32_t eq = reg_posmask(FWD, __ballot_sync(FULL, act && c == best && pos < limit), low, hgh);
       const int p = __ffs(eq) - 1;
-      const int L = reg_lane<FWD>(p, low, hgh);
+      const int L = reg_lane(FWD, p, low, hgh);
       if (first) {
         besta = best;
         bestx = __shfl_sync(FULL, x, L);
@@ -955,8 +948,7 @@ __device__ __forceinline__ int reg_wave(RegCtx &X, const AlignSpec &spec, const 
 // grow the band, compute the wave, clip at sequence ends, prune.  Waves of
 // at most 32 diagonals run in registers (reg_wave), wider ones through the
 // memory ring (wave_sweep).
-template <bool FWD>
-__device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B,
+__device__ __forceinline__ int wave_loop(const bool FWD, WarpWork &W, const AlignSpec &spec, const Seq &A, const Seq &B,
                                          const uint8_t *aseq, const uint8_t *bseq, int minp, int maxp, int &low,
                                          int &hgh, int &dif, int &cur, int &besta, int &bestx, int &lasta,
                                          int &trima, int &trimx, int &trimd, int &trimha, int &more, int &aclip,
@@ -1023,7 +1015,7 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
         regmode = true;
       }
       dif += 1;
-      if (reg_wave<FWD>(X, rspec, rA, rB, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
+      if (reg_wave(FWD, X, rspec, rA, rB, low, hgh, plow, phgh, dif, R, besta, bestx, lasta, trima, trimx, trimd,
                         trimha, more, aclip, bclip, WS)) {
         sync();
         return 1;
@@ -1053,7 +1045,7 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
       }
       dif += 1;
       __syncwarp();
-      if (wave_sweep<FWD>(W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
+      if (wave_sweep(FWD, W, spec, A, B, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more,
                           aclip, bclip, WS))
         return 1;
       X.chunk_next = W.chunk_next;
@@ -1122,11 +1114,49 @@ __device__ __forceinline__ int wave_loop(WarpWork &W, const AlignSpec &spec, con
           hgh = low - 1;
       }
     } else
-      wave_prune<FWD>(W, W.V[cur], besta, low, hgh, WS);
+      wave_prune(FWD, W, W.V[cur], besta, low, hgh, WS);
   }
   sync();
   __syncwarp();
   return 0;
+}
+
+// The wave loop's state across the call below.
+struct WaveState {
+  int low, hgh, dif, cur, besta, bestx, lasta, trima, trimx, trimd, trimha, more, aclip, bclip, morem, morea, morex,
+      mored, moreha;
+};
+
+// One out-of-line copy of the wave loop serves both directions (FWD is a
+// run-time flag).  The alignment kernel is bound by instruction fetch: two
+// inlined copies of this loop, one per direction, kept twice the hot code in
+// the instruction cache; one shared copy cut the pair phase of a 2 x 1 Gbp
+// genome pair by a quarter with the same alignments.
+__device__ __noinline__ int wave_loop_shared(const bool FWD, WarpWork &W, const AlignSpec &spec, const Seq &A,
+                                             const Seq &B, const uint8_t *aseq, const uint8_t *bseq, int minp,
+                                             int maxp, WaveState *io, int max_waves) {
+  WaveState s = *io;
+  const int r = wave_loop(FWD, W, spec, A, B, aseq, bseq, minp, maxp, s.low, s.hgh, s.dif, s.cur, s.besta, s.bestx,
+                          s.lasta, s.trima, s.trimx, s.trimd, s.trimha, s.more, s.aclip, s.bclip, s.morem, s.morea,
+                          s.morex, s.mored, s.moreha, max_waves);
+  *io = s;
+  return r;
+}
+
+// wave_loop through the shared copy, with the caller's variables.
+__device__ __forceinline__ int wave_loop_call(const bool FWD, WarpWork &W, const AlignSpec &spec, const Seq &A,
+                                              const Seq &B, const uint8_t *aseq, const uint8_t *bseq, int minp,
+                                              int maxp, int &low, int &hgh, int &dif, int &cur, int &besta,
+                                              int &bestx, int &lasta, int &trima, int &trimx, int &trimd,
+                                              int &trimha, int &more, int &aclip, int &bclip, int &morem, int &morea,
+                                              int &morex, int &mored, int &moreha, int max_waves) {
+  WaveState s{low,   hgh,  dif,   cur,   besta, bestx, lasta, trima, trimx, trimd,
+              trimha, more, aclip, bclip, morem, morea, morex, mored, moreha};
+  const int r = wave_loop_shared(FWD, W, spec, A, B, aseq, bseq, minp, maxp, &s, max_waves);
+  low = s.low, hgh = s.hgh, dif = s.dif, cur = s.cur, besta = s.besta, bestx = s.bestx, lasta = s.lasta;
+  trima = s.trima, trimx = s.trimx, trimd = s.trimd, trimha = s.trimha, more = s.more, aclip = s.aclip;
+  bclip = s.bclip, morem = s.morem, morea = s.morea, morex = s.morex, mored = s.mored, moreha = s.moreha;
+  return r;
 }
 
 #define WVI(k) ((k) & vmask)
@@ -1256,8 +1286,8 @@ __device__ int forward_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     }
   }
 
-  if (wave_loop<true>(W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima, trimx,
-                      trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
+  if (wave_loop_call(true, W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima,
+                     trimx, trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
     return 1;
   __syncwarp();
 
@@ -1465,8 +1495,8 @@ __device__ int reverse_wave_w(WarpWork &W, const AlignSpec &spec, const Seq &A, 
     }
   }
 
-  if (wave_loop<false>(W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima,
-                       trimx, trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
+  if (wave_loop_call(false, W, spec, A, B, aseq, bseq, minp, maxp, low, hgh, dif, cur, besta, bestx, lasta, trima,
+                     trimx, trimd, trimha, more, aclip, bclip, morem, morea, morex, mored, moreha, max_waves))
     return 1;
   __syncwarp();
 
