@@ -345,9 +345,10 @@ def run_ingest(dev, cs, args, stream, peak: float, peak_kind: str, cpu: bool) ->
 
 
 def run_profile_stage(args) -> None:
-    """--profile-stage: only the index build or only the GDB ingest, warmup +
-    steps times on one GPU, printing each call's device times (a small
-    program for ncu captures of one stage's kernels)."""
+    """--profile-stage: one stage alone (index build, GDB ingest, served load,
+    alignment launch or diagonal sorts), warmup + steps times on one GPU,
+    printing each call's device times (a small program for ncu captures of
+    one stage's kernels)."""
     from distributedpanga_b200 import pipeline
     if args.profile_stage == "serve":
         # the served load alone: a target at --serve-scale, then queries
@@ -383,6 +384,22 @@ def run_profile_stage(args) -> None:
             n = dev.align()
             print(json.dumps({"stage": "align", "alignments": n, "work": dev.align_work(),
                               "times_ms": dev.align_times()}), flush=True)
+        dev.close()
+        return
+    if args.profile_stage == "diag":
+        # the diagonal sorts alone: the index once, then warmup + steps of
+        # merge (the sort consumes the seeds) + both units' sorts
+        dev.gdb_load(cs)
+        dev.index_build(want_entries=False)
+        dev.enable_timing(True)
+        for _ in range(args.warmup + args.steps):
+            dev.merge(freq_cutoff())
+            dev.diag_sort(0)
+            dev.diag_sort(1)
+            st = dev.stage_times()
+            print(json.dumps({"stage": "diag", "seeds": dev.nseeds,
+                              "ms": {k: round(st[k], 3) for k in ("merge", "diag_sort_n", "diag_sort_c")}}),
+                  flush=True)
         dev.close()
         return
     if args.profile_stage == "index":
@@ -598,6 +615,7 @@ def measure(args, name: str, scale: float, steps: int, warmup: int, e2e_steps: i
     dev.enable_timing(True)
     step()
     st = dev.stage_times()
+    alloc = dev.alloc_times()
     dev.enable_timing(False)
     astats = dev.align_stats()
     atimes = dev.align_times()
@@ -667,6 +685,7 @@ def measure(args, name: str, scale: float, steps: int, warmup: int, e2e_steps: i
                    "l2": "inputs larger than L2 (records %.1f GB)" % (nrec * 16 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "stage_ms": st,
+        "alloc_ms": {k: round(v, 2) if isinstance(v, float) else v for k, v in alloc.items()},
         "align_ms": atimes,
         "align_roofline": align_roofline(awork, st["align"]),
         "roofline": {"bound": "hbm", "kernel": "index build (k_extract hist+scatter, prefix scan, bucket sort, "
@@ -732,6 +751,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator, %s workload)" % name,
         "config": m["config"],
         "stage_ms": m["stage_ms"],
+        "alloc_ms": m["alloc_ms"],
         "align_ms": m["align_ms"],
         "align_roofline": m["align_roofline"],
         "roofline": m["roofline"],
@@ -929,7 +949,7 @@ def main():
     ap.add_argument("--no-ingest", action="store_true", help="skip the FASTA ingest measurement")
     ap.add_argument("--align-build", type=int, default=0,
                     help="with --profile-stage align: the alignment kernel's build (0 automatic, 2, 3 or 4)")
-    ap.add_argument("--profile-stage", choices=["index", "ingest", "serve", "align"], default=None,
+    ap.add_argument("--profile-stage", choices=["index", "ingest", "serve", "align", "diag"], default=None,
                     help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     ap.add_argument("--serve", action="store_true",
                     help="measure the served form (resident target, concurrent requests) beside the plain one")

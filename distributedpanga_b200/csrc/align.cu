@@ -1019,4 +1019,66 @@ void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint
   k_pair_starts<<<g, 256, 0, st>>>(keys, n, L, flag, idx, start, ab);
 }
 
+
+// ---- la_sort order of the surviving alignments ------------------------------
+// (src/fastga_pipeline.c:1500-1515: by A contig, A begin, B contig, strand;
+// ties in the pair's own output order.)  The key holds those fields, then the
+// record's index, most significant first: aread (16 bits), abpos (32), bread
+// (16) | comp (1), rank (31), index (32).
+
+__global__ void k_aln_keys(const AlnRec *__restrict__ r, int64_t n, U128 *__restrict__ keys) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const AlnRec &a = r[i];
+    U128 k;
+    k.hi = ((uint64_t)(uint16_t)a.aread << 48) | ((uint64_t)(uint32_t)a.abpos << 16) | (uint64_t)(uint16_t)a.bread;
+    k.lo = ((uint64_t)(a.comp & 1) << 63) | ((uint64_t)((uint32_t)a.rank & 0x7fffffffu) << 32) | (uint64_t)(uint32_t)i;
+    keys[i] = k;
+  }
+}
+
+// out[i] = the record of sorted key i; len[i] its trace bytes.
+__global__ void k_aln_gather(const U128 *__restrict__ keys, int64_t n, const AlnRec *__restrict__ in,
+                             AlnRec *__restrict__ out, int64_t *__restrict__ len) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const AlnRec a = in[(uint32_t)keys[i].lo];
+    out[i] = a;
+    len[i] = a.tlen;
+  }
+}
+
+// One warp per record: its trace bytes to their place in sorted order; the
+// record's toff becomes that place.
+__global__ void k_aln_traces(AlnRec *__restrict__ recs, const int64_t *__restrict__ off, int64_t n,
+                             const uint8_t *__restrict__ src, uint8_t *__restrict__ dst) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = w0; i < n; i += nw) {
+    const int64_t from = recs[i].toff, to = off[i];
+    const int len = recs[i].tlen;
+    for (int b = lane; b < len; b += 32) dst[to + b] = src[from + b];
+    __syncwarp();
+    if (lane == 0) recs[i].toff = to;
+  }
+}
+
+void launch_aln_keys(const AlnRec *r, int64_t n, U128 *keys, cudaStream_t st) {
+  if (n <= 0) return;
+  const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_aln_keys<<<g, 256, 0, st>>>(r, n, keys);
+}
+void launch_aln_gather(const U128 *keys, int64_t n, const AlnRec *in, AlnRec *out, int64_t *len, cudaStream_t st) {
+  if (n <= 0) return;
+  const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_aln_gather<<<g, 256, 0, st>>>(keys, n, in, out, len);
+}
+void launch_aln_traces(AlnRec *recs, const int64_t *off, int64_t n, const uint8_t *src, uint8_t *dst,
+                       cudaStream_t st) {
+  if (n <= 0) return;
+  const int g = (int)std::min<int64_t>((n + 7) / 8, 148 * 16);
+  k_aln_traces<<<g, 256, 0, st>>>(recs, off, n, src, dst);
+}
+
 }  // namespace pga

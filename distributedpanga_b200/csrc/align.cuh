@@ -152,5 +152,12 @@ void launch_band_info(const U128 *keys, int64_t n, SeedKeyLayout L, uint16_t *in
 void launch_pair_flags(const U128 *keys, int64_t n, SeedKeyLayout L, uint32_t *flag, cudaStream_t st);
 void launch_pair_starts(const U128 *keys, int64_t n, SeedKeyLayout L, const uint32_t *flag, const uint32_t *idx,
                         int64_t *start, int32_t *ab, cudaStream_t st);
+// la_sort order of the surviving alignments on the device: keys, then (after
+// the keys are sorted) the records in that order with their trace lengths,
+// then the traces moved to the scanned offsets.
+void launch_aln_keys(const AlnRec *r, int64_t n, U128 *keys, cudaStream_t st);
+void launch_aln_gather(const U128 *keys, int64_t n, const AlnRec *in, AlnRec *out, int64_t *len, cudaStream_t st);
+void launch_aln_traces(AlnRec *recs, const int64_t *off, int64_t n, const uint8_t *src, uint8_t *dst,
+                       cudaStream_t st);
 
 }  // namespace pga

@@ -13,12 +13,14 @@
 #include "common.cuh"
 #include "index.cuh"
 #include "merge.cuh"
+#include "diag_sort.cuh"
 #include "radix.cuh"
 #include "scan.cuh"
 #include "seeds.cuh"
 #include "align.cuh"
 #include "align_spec.h"
 #include "ingest.cuh"
+#include "arena.h"
 #include "../../include/pga_b200.h"
 
 using namespace pga;
@@ -34,6 +36,10 @@ enum StageId {
   ST_EXTRACT_HIST, ST_SCAN, ST_EXTRACT_SCATTER, ST_BUCKET, ST_LCP, ST_ENTRIES, ST_MERGE, ST_DIAG, ST_ALIGN, ST_DIAG_C, ST_N
 };
 
+// the arena's driver calls (the context's timed cudaMalloc / cudaFree)
+int arena_malloc(void *ctx, void **p, size_t bytes);
+void arena_free(void *ctx, void *p);
+
 }  // namespace
 
 struct pga_ctx {
@@ -46,6 +52,15 @@ struct pga_ctx {
   cudaEvent_t ev[ST_N][2] = {};
   float stage_ms[ST_N] = {0};
   bool stage_used[ST_N] = {false};
+  // host time inside cudaMalloc / cudaFree, per stage (slot ST_N: outside
+  // every stage), since timing was last enabled
+  int cur_stage = ST_N;
+  int stage_prev[ST_N] = {0};
+  double alloc_ms[ST_N + 1] = {0};
+  int64_t alloc_calls = 0;
+  int64_t sheds = 0;  // shed_align_buffers calls that freed something
+  // every DBuf of the context lives in the arena
+  Arena arena{arena_malloc, arena_free, this};
 
   // GDB
   bool have_gdb = false;
@@ -83,8 +98,10 @@ struct pga_ctx {
   int freq = 0;
 
   // diagonal sort
-  DBuf keys[2], keys_alt, rhist, rscan, panel[2];
+  DBuf keys[2], dlook, dsmall, panel[2];
   U128 *sorted[2] = {nullptr, nullptr};
+  bool seeds_consumed[2] = {false, false};  // the unit's seed buffer was used by its diagonal sort
+  int diag_passes[2] = {0, 0};
   SeedKeyLayout lay[2];
   bool have_diag[2] = {false, false};
 
@@ -97,8 +114,13 @@ struct pga_ctx {
   DBuf numf, numr, soff, spec_tab, tasks, task_next, pout, wave, points, cells, cell_next, ovl, perm, cand,
       cand_next, recs, rec_next, outb, out_next, pflag, pidx, pstart, pab, rng_ovl, rng_next, ftasks, fout,
       ridx, rout, selfb, pstart2, pab2, small, shist, fo_dev, binfo[2], plive[2];
-  std::vector<AlnRec> h_recs;      // survivors in la_sort order
-  std::vector<uint8_t> h_trace;    // their trace bytes
+  // survivors in la_sort order on the device (srecs, their traces in strace,
+  // toff rewritten to offsets there), and their host copy, made when read
+  DBuf srecs, slen, strace, skeys, skeys2, lhist, lscan;
+  int64_t nalign = 0, ntrace = 0;
+  bool host_valid = false;
+  std::vector<AlnRec> h_recs;
+  std::vector<uint8_t> h_trace;
   std::vector<int64_t> h_toff;     // offsets into h_trace
   int64_t align_stats[8] = {0};    // pga_align_stats
   float align_ms[4] = {0};         // pga_align_times
@@ -161,6 +183,35 @@ int fail(pga_ctx *c, int code, const char *fmt, ...) {
 
 #define LAUNCHED(k) (ctx->launches += (k))
 
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Every device allocation and free of a context goes through these two, which
+// charge their host time to the running stage.
+cudaError_t dev_malloc(pga_ctx *ctx, void **p, size_t bytes) {
+  const double t0 = now_ms();
+  cudaError_t e = cudaMalloc(p, bytes);
+  ctx->alloc_ms[ctx->cur_stage] += now_ms() - t0;
+  ctx->alloc_calls++;
+  return e;
+}
+void dev_free(pga_ctx *ctx, void *p) {
+  if (!p) return;
+  const double t0 = now_ms();
+  cudaFree(p);
+  ctx->alloc_ms[ctx->cur_stage] += now_ms() - t0;
+  ctx->alloc_calls++;
+}
+
+int arena_malloc(void *ctx, void **p, size_t bytes) {
+  if (dev_malloc((pga_ctx *)ctx, p, bytes) == cudaSuccess) return 0;
+  cudaGetLastError();
+  *p = nullptr;
+  return 1;
+}
+void arena_free(void *ctx, void *p) { dev_free((pga_ctx *)ctx, p); }
+
 // Frees the buffers only the alignment stage uses -- sequences, pools, task
 // lists, local-alignment requests -- which the next pga_align or
 // pga_local_alignment rebuilds, so that another stage can allocate.  Not while
@@ -171,16 +222,18 @@ bool shed_align_buffers(pga_ctx *ctx) {
                   &ctx->cand, &ctx->recs, &ctx->outb, &ctx->rng_ovl, &ctx->tasks, &ctx->pout, &ctx->pflag,
                   &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->ftasks,
                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace,
-                  &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1]};
+                  &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1], &ctx->skeys, &ctx->skeys2,
+                  &ctx->lhist, &ctx->lscan};
   bool any = false;
   for (DBuf *b : bufs)
     if (b->p) {
-      cudaFree(b->p);
+      ctx->arena.release(b->p);
       b->p = nullptr;
       b->cap = 0;
       any = true;
     }
   ctx->have_numeric = false;
+  if (any) ctx->sheds++;
   return any;
 }
 
@@ -191,21 +244,24 @@ struct AlignScope {
   ~AlignScope() { c->in_align = false; }
 };
 
+// Grows b to at least `bytes` (contents not kept).  All of a context's work
+// runs on its one stream, so a range freed here and handed out again is
+// written only after the kernels that used it before.  Order of attempts: a
+// range the arena holds; the same after shedding the last alignment's
+// buffers (rebuilt by the next alignment); a new slab from the driver.
 int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.cap >= bytes) return PGA_OK;
-  if (b.p) cudaFree(b.p);
+  ctx->arena.release(b.p);
   b.p = nullptr;
   b.cap = 0;
-  cudaError_t e = cudaMalloc(&b.p, bytes);
-  if (e != cudaSuccess && shed_align_buffers(ctx)) {  // room held by the last alignment
-    cudaGetLastError();
-    e = cudaMalloc(&b.p, bytes);
-  }
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-  }
+  void *p = ctx->arena.fit(bytes);
+  if (!p && shed_align_buffers(ctx)) p = ctx->arena.fit(bytes);
+  if (!p) p = ctx->arena.alloc(bytes);
+  if (!p)
+    return fail(ctx, PGA_ERR_NOMEM, "device allocation of %zu bytes (context holds %zu, %zu of them free)", bytes,
+                ctx->arena.held_bytes(), ctx->arena.free_bytes());
+  b.p = p;
   b.cap = bytes;
   return PGA_OK;
 }
@@ -213,21 +269,18 @@ int ensure(pga_ctx *ctx, DBuf &b, size_t bytes) {
 // Grows b to `bytes`, keeping its first `keep` bytes.
 int grow_keep(pga_ctx *ctx, DBuf &b, size_t bytes, size_t keep) {
   if (b.cap >= bytes) return PGA_OK;
-  void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ctx, PGA_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-  }
+  void *p = ctx->arena.alloc(bytes);
+  if (!p)
+    return fail(ctx, PGA_ERR_NOMEM, "device allocation of %zu bytes (context holds %zu, %zu of them free)", bytes,
+                ctx->arena.held_bytes(), ctx->arena.free_bytes());
   if (keep > 0) {
-    e = cudaMemcpyAsync(p, b.p, keep, cudaMemcpyDeviceToDevice, ctx->st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    cudaError_t e = cudaMemcpyAsync(p, b.p, keep, cudaMemcpyDeviceToDevice, ctx->st);
     if (e != cudaSuccess) {
-      cudaFree(p);
+      ctx->arena.release(p);
       return fail(ctx, PGA_ERR_CUDA, "grow copy: %s", cudaGetErrorString(e));
     }
   }
-  if (b.p) cudaFree(b.p);
+  ctx->arena.release(b.p);
   b.p = p;
   b.cap = bytes;
   return PGA_OK;
@@ -252,9 +305,12 @@ int grid_for(int64_t n, int threads, int cap = 148 * 32) {
 }
 
 void stage_begin(pga_ctx *ctx, int s) {
+  ctx->stage_prev[s] = ctx->cur_stage;
+  ctx->cur_stage = s;
   if (ctx->timing) cudaEventRecord(ctx->ev[s][0], ctx->st);
 }
 void stage_end(pga_ctx *ctx, int s) {
+  ctx->cur_stage = ctx->stage_prev[s];
   if (ctx->timing) {
     cudaEventRecord(ctx->ev[s][1], ctx->st);
     ctx->stage_used[s] = true;
@@ -499,6 +555,7 @@ int run_merge(pga_ctx *ctx, int freq) {
   ctx->seeds_loaded = false;
   ctx->freq = freq;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
+  ctx->seeds_consumed[0] = ctx->seeds_consumed[1] = false;
   return PGA_OK;
 }
 
@@ -534,44 +591,30 @@ SeedKeyLayout make_layout(int comp, int ncontig, int64_t amxpos, int dbyte, int 
   return L;
 }
 
-// Seeds of unit comp in ctx->seed[comp] -> sorted keys.
+// Seeds of unit comp in ctx->seed[comp] -> sorted keys in ctx->keys[comp].
+// The seed buffer is the sort's second buffer: the seeds are consumed.
 int run_diag(pga_ctx *ctx, int comp, int ncontig, int64_t amxpos, int dbyte, int ctgb) {
   int64_t n = ctx->nseed[comp];
   SeedKeyLayout L = make_layout(comp, ncontig, amxpos, dbyte, ctgb);
   if (L.total_bits > 128) return fail(ctx, PGA_ERR_LIMIT, "diagonal sort key needs %d bits", L.total_bits);
+  if (ctx->seeds_consumed[comp]) return fail(ctx, PGA_ERR_ARG, "the seeds of this unit were already sorted");
   ctx->lay[comp] = L;
+  ENSURE(ctx->seed[comp], sizeof(Seed) * (size_t)n + 16);
   ENSURE(ctx->keys[comp], sizeof(U128) * (size_t)n + 16);
-  ENSURE(ctx->keys_alt, sizeof(U128) * (size_t)n + 16);
-  ENSURE(ctx->rhist, sizeof(uint32_t) * radix_hist_elems(n) + 64);
-  ENSURE(ctx->rscan, sizeof(uint32_t) * scan_tmp_elems(radix_hist_elems(n)) + 64);
-  ENSURE(ctx->u64tmp, 64);
+  ENSURE(ctx->dlook, diag_sort_look_bytes(n));
+  ENSURE(ctx->dsmall, DIAG_SORT_SMALL);
   const int st_diag = comp ? ST_DIAG_C : ST_DIAG;
   stage_begin(ctx, st_diag);
-  U128 *keys = P<U128>(ctx->keys[comp]);
-  int passes[16], np = 0;
-  if (n > 0) {
-    k_seed_keys<<<grid_for(n, 256), 256, 0, ctx->st>>>(P<Seed>(ctx->seed[comp]), n, L, keys);
-    LAUNCHED(1);
-    unsigned long long *acc = P<unsigned long long>(ctx->u64tmp);
-    CK(cudaMemsetAsync(acc, 0, 16, ctx->st));
-    k_u128_diffbits<<<grid_for(n, 256, 148 * 4), 256, 0, ctx->st>>>(keys, n, acc);
-    LAUNCHED(1);
-    unsigned long long diff[2];
-    CK(cudaMemcpyAsync(diff, acc, 16, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    for (int s = 0; s < 128; s += 8) {
-      uint64_t w = s < 64 ? diff[0] : diff[1];
-      if ((w >> (s & 63)) & 0xffull) passes[np++] = s;
-    }
-  }
-  U128 *res = keys;
-  CK(radix_sort_u128(keys, P<U128>(ctx->keys_alt), n, passes, np, P<uint32_t>(ctx->rhist),
-                     P<uint32_t>(ctx->rscan), &res, ctx->st));
-  LAUNCHED(5 * np);
-  if (res != keys)  // keep the sorted keys in this unit's own buffer
-    CK(cudaMemcpyAsync(keys, res, sizeof(U128) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
+  DiagSortResult R;
+  CK(diag_sort_seeds(ctx->seed[comp].p, ctx->keys[comp].p, n, L, P<unsigned long long>(ctx->dlook),
+                     ctx->dsmall.p, ctx->st, &R));
+  LAUNCHED(R.launches);
   stage_end(ctx, st_diag);
-  ctx->sorted[comp] = keys;
+  ctx->seeds_consumed[comp] = true;
+  if (R.bad) return fail(ctx, PGA_ERR_CUDA, "diagonal sort: a pass stopped waiting for a tile before it");
+  if (R.in_a) std::swap(ctx->seed[comp], ctx->keys[comp]);  // the keys ended in the seeds' buffer
+  ctx->diag_passes[comp] = R.passes;
+  ctx->sorted[comp] = P<U128>(ctx->keys[comp]);
   ctx->have_diag[comp] = true;
   return PGA_OK;
 }
@@ -1033,22 +1076,18 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
 // with <3>.
 constexpr int64_t ALIGN_MANY_PAIRS = 1 << 20;
 
-double now_ms() {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
 // Frees what the alignment no longer reads once both diagonal sorts are done
 // -- the index (records, LCPs, entries, scratch) and the unsorted seeds -- so
 // that a genome too large for all stages' buffers at once still aligns.
 // Returns whether anything was freed.
 bool release_for_align(pga_ctx *ctx) {
   if (!ctx->have_diag[0] || !ctx->have_diag[1]) return false;
-  std::vector<DBuf *> bufs = {&ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->seed[0], &ctx->seed[1]};
-  if (ctx->sorted[0] != ctx->keys_alt.p && ctx->sorted[1] != ctx->keys_alt.p) bufs.push_back(&ctx->keys_alt);
+  std::vector<DBuf *> bufs = {&ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->seed[0], &ctx->seed[1],
+                              &ctx->dlook};
   bool any = false;
   for (DBuf *b : bufs)
     if (b->p) {
-      cudaFree(b->p);
+      ctx->arena.release(b->p);
       b->p = nullptr;
       b->cap = 0;
       any = true;
@@ -1056,6 +1095,71 @@ bool release_for_align(pga_ctx *ctx) {
   ctx->have_index = ctx->have_entries = false;
   ctx->seeds_released = true;
   return any;
+}
+
+// The survivors (ctx->recs, their traces in ctx->outb) in la_sort order into
+// ctx->srecs / ctx->strace: keys (fields, then record index) radix-sorted,
+// records gathered, trace bytes moved to the scanned offsets.
+int la_sort_device(pga_ctx *ctx, int64_t n, int64_t nbytes) {
+  ctx->nalign = n;
+  ctx->ntrace = nbytes;
+  ctx->host_valid = false;
+  ENSURE(ctx->srecs, sizeof(AlnRec) * (size_t)n + 16);
+  ENSURE(ctx->slen, sizeof(int64_t) * (size_t)(n + 1) + 16);
+  ENSURE(ctx->strace, (size_t)nbytes + 16);
+  if (n == 0) return PGA_OK;
+  const int64_t he = radix_hist_elems(n);
+  ENSURE(ctx->skeys, sizeof(U128) * (size_t)n + 16);
+  ENSURE(ctx->skeys2, sizeof(U128) * (size_t)n + 16);
+  ENSURE(ctx->lhist, sizeof(uint32_t) * (size_t)he + 64);
+  ENSURE(ctx->lscan, std::max(sizeof(uint32_t) * (size_t)scan_tmp_elems(he), sizeof(int64_t) * (size_t)scan_tmp_elems(n)) +
+                         64);
+  ENSURE(ctx->u64tmp, 64);
+  U128 *keys = P<U128>(ctx->skeys);
+  launch_aln_keys(P<AlnRec>(ctx->recs), n, keys, ctx->st);
+  unsigned long long *acc = P<unsigned long long>(ctx->u64tmp);
+  CK(cudaMemsetAsync(acc, 0, 16, ctx->st));
+  k_u128_diffbits<<<grid_for(n, 256, 148 * 4), 256, 0, ctx->st>>>(keys, n, acc);
+  unsigned long long diff[2];
+  CK(cudaMemcpyAsync(diff, acc, 16, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  int passes[16], np = 0;
+  for (int sh = 0; sh < 128; sh += 8)
+    if (((sh < 64 ? diff[0] : diff[1]) >> (sh & 63)) & 0xffull) passes[np++] = sh;
+  U128 *res = keys;
+  CK(radix_sort_u128(keys, P<U128>(ctx->skeys2), n, passes, np, P<uint32_t>(ctx->lhist), P<uint32_t>(ctx->lscan),
+                     &res, ctx->st));
+  int64_t *len = P<int64_t>(ctx->slen);
+  launch_aln_gather(res, n, P<AlnRec>(ctx->recs), P<AlnRec>(ctx->srecs), len, ctx->st);
+  CK(exclusive_scan<int64_t>(len, len, n, P<int64_t>(ctx->lscan), len + n, ctx->st));
+  launch_aln_traces(P<AlnRec>(ctx->srecs), len, n, P<uint8_t>(ctx->outb), P<uint8_t>(ctx->strace), ctx->st);
+  LAUNCHED(2 + 5 * np + 3 + 3);
+  CK(cudaGetLastError());
+  return PGA_OK;
+}
+
+// The host copy of the last alignment's results (made on first read).
+int host_alignments(pga_ctx *ctx) {
+  if (ctx->host_valid) return PGA_OK;
+  const int64_t n = ctx->nalign;
+  ctx->h_recs.resize(n);
+  ctx->h_toff.assign(n + 1, 0);
+  ctx->h_trace.clear();
+  if (n > 0) {
+    CK(cudaMemcpyAsync(ctx->h_recs.data(), ctx->srecs.p, sizeof(AlnRec) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    // the survivors' traces lie back to back from offset 0
+    const int64_t total = ctx->h_recs[n - 1].toff + ctx->h_recs[n - 1].tlen;
+    if (total < 0 || total > ctx->ntrace) return fail(ctx, PGA_ERR_CUDA, "alignment traces out of range");
+    ctx->h_trace.resize(total);
+    if (total > 0)
+      CK(cudaMemcpyAsync(ctx->h_trace.data(), ctx->strace.p, total, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int64_t i = 0; i < n; i++) ctx->h_toff[i] = ctx->h_recs[i].toff;
+    ctx->h_toff[n] = total;
+  }
+  ctx->host_valid = true;
+  return PGA_OK;
 }
 
 int run_align(pga_ctx *ctx) {
@@ -1078,7 +1182,7 @@ int run_align(pga_ctx *ctx) {
     int64_t seqtot = 0;
     for (int c = 0; c < nc; c++) seqtot += ctx->clen[c];
     const double need = 16.0 * seqtot + 8.0 * (ctx->nseed[0] + ctx->nseed[1]) + (8ll << 30);
-    if ((double)free_b < need) release_for_align(ctx);
+    if ((double)free_b + (double)ctx->arena.free_bytes() < need) release_for_align(ctx);
   }
   // 2. NUMERIC and packed sequences, base frequencies, scoring tables
   int ave_path = 0;
@@ -1536,38 +1640,13 @@ int run_align(pga_ctx *ctx) {
 
   const double t_order = now_ms();
   // 7. survivors in la_sort order: (aread, abpos, bread, comp), ties in the
-  // pair's own output order (src/fastga_pipeline.c:1500-1515)
+  // pair's own output order (src/fastga_pipeline.c:1500-1515), on the device
   unsigned long long nrec = 0, nbytes = 0;
   CK(cudaMemcpyAsync(&nrec, ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaMemcpyAsync(&nbytes, ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
-  std::vector<AlnRec> recs(nrec);
-  std::vector<uint8_t> bytes(nbytes);
-  if (nrec) CK(cudaMemcpyAsync(recs.data(), ctx->recs.p, sizeof(AlnRec) * nrec, cudaMemcpyDeviceToHost, ctx->st));
-  if (nbytes) CK(cudaMemcpyAsync(bytes.data(), ctx->outb.p, nbytes, cudaMemcpyDeviceToHost, ctx->st));
-  CK(cudaStreamSynchronize(ctx->st));
-  std::vector<int64_t> order(nrec);
-  for (int64_t i = 0; i < (int64_t)nrec; i++) order[i] = i;
-  std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
-    const AlnRec &a = recs[x], &b = recs[y];
-    if (a.aread != b.aread) return a.aread < b.aread;
-    if (a.abpos != b.abpos) return a.abpos < b.abpos;
-    if (a.bread != b.bread) return a.bread < b.bread;
-    if (a.comp != b.comp) return a.comp < b.comp;
-    return a.rank < b.rank;
-  });
-  ctx->h_recs.resize(nrec);
-  ctx->h_toff.assign(nrec + 1, 0);
-  ctx->h_trace.resize(nbytes);
-  int64_t o = 0;
-  for (int64_t i = 0; i < (int64_t)nrec; i++) {
-    const AlnRec &a = recs[order[i]];
-    ctx->h_recs[i] = a;
-    ctx->h_toff[i] = o;
-    memcpy(ctx->h_trace.data() + o, bytes.data() + a.toff, a.tlen);
-    o += a.tlen;
-  }
-  ctx->h_toff[nrec] = o;
+  r0 = la_sort_device(ctx, (int64_t)nrec, (int64_t)nbytes);
+  if (r0) return r0;
   ctx->align_stats[0] = npairs[0] + npairs[1];
   ctx->align_stats[1] = (int64_t)self_idx.size();
   ctx->align_stats[2] = calls;
@@ -1623,18 +1702,18 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->cand_next, &ctx->recs, &ctx->rec_next, &ctx->outb, &ctx->out_next, &ctx->pflag,
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
                    &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb, &ctx->lreq, &ctx->lpath, &ctx->ltoff,
-                   &ctx->ltrace, &ctx->lnext, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->shist, &ctx->fo_dev};
-  for (DBuf *b : abufs)
-    if (b->p) cudaFree(b->p);
+                   &ctx->ltrace, &ctx->lnext, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->shist, &ctx->fo_dev,
+                   &ctx->srecs, &ctx->slen, &ctx->strace, &ctx->skeys, &ctx->skeys2, &ctx->lhist, &ctx->lscan};
+  for (DBuf *b : abufs) ctx->arena.release(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
                   &ctx->scan_tmp, &ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->cum, &ctx->qmed,
                   &ctx->qbig, &ctx->qcount, &ctx->maxrun, &ctx->u64tmp, &ctx->blk_n, &ctx->blk_c,
                   &ctx->blk_tmp, &ctx->seed[0], &ctx->seed[1], &ctx->keys[0], &ctx->keys[1],
-                  &ctx->keys_alt, &ctx->rhist, &ctx->rscan, &ctx->panel[0], &ctx->panel[1], &ctx->io,
+                  &ctx->dlook, &ctx->dsmall, &ctx->panel[0], &ctx->panel[1], &ctx->io,
                   &ctx->io2, &ctx->coarse, &ctx->fa_text, &ctx->fa_mask, &ctx->fa_seq, &ctx->fa_cnt, &ctx->fa_tmp,
                   &ctx->fa_tot, &ctx->fa_status, &ctx->fa_hdr, &ctx->fa_hbytes, &ctx->fa_runs, &ctx->fa_ctg};
-  for (DBuf *b : bufs)
-    if (b->p) cudaFree(b->p);
+  for (DBuf *b : bufs) ctx->arena.release(b->p);
+  ctx->arena.clear();
   for (int s = 0; s < ST_N; s++) {
     cudaEventDestroy(ctx->ev[s][0]);
     cudaEventDestroy(ctx->ev[s][1]);
@@ -1649,6 +1728,8 @@ const char *pga_last_error(const pga_ctx *ctx) { return ctx ? ctx->err : "null c
 
 int pga_ctx_set_stream(pga_ctx *ctx, void *stream) {
   if (!ctx) return PGA_ERR_ARG;
+  // the arena reuses freed ranges in stream order: drain the old stream
+  CK(cudaStreamSynchronize(ctx->st));
   ctx->st = stream ? (cudaStream_t)stream : ctx->own;
   return PGA_OK;
 }
@@ -1665,6 +1746,20 @@ int pga_ctx_enable_timing(pga_ctx *ctx, int on) {
   if (!ctx) return PGA_ERR_ARG;
   ctx->timing = on != 0;
   for (int s = 0; s < ST_N; s++) ctx->stage_used[s] = false;
+  for (int s = 0; s <= ST_N; s++) ctx->alloc_ms[s] = 0;
+  ctx->alloc_calls = 0;
+  return PGA_OK;
+}
+
+int pga_alloc_times(const pga_ctx *ctx, double *ms11, int64_t *counts4) {
+  if (!ctx || !ms11) return PGA_ERR_ARG;
+  for (int s = 0; s <= ST_N; s++) ms11[s] = ctx->alloc_ms[s];
+  if (counts4) {
+    counts4[0] = ctx->alloc_calls;
+    counts4[1] = (int64_t)ctx->arena.held_bytes();
+    counts4[2] = (int64_t)ctx->arena.free_bytes();
+    counts4[3] = ctx->sheds;
+  }
   return PGA_OK;
 }
 
@@ -2272,6 +2367,7 @@ int pga_reimport_sort(pga_ctx *ctx, const uint8_t *seeds, int64_t len, int posb,
     LAUNCHED(1);
   }
   ctx->nseed[comp] = n;
+  ctx->seeds_consumed[comp] = false;
   int r = run_diag(ctx, comp, ncontig, amxpos, dbyte, ctgb);
   if (r) return r;
   return copy_diag(ctx, comp, ncontig, out, panel_off);
@@ -2414,10 +2510,35 @@ int pga_target_create(pga_ctx *ctx, pga_target **out) {
   t->scaf = ctx->h_scaf;
   t->headers = ctx->h_headers;
   for (int v = 0; v < 4; v++) t->base_count[v] = ctx->base_count[v];
-  // the buffers move: the context keeps no GDB and no index
-  std::swap(t->bps, ctx->bps);
-  std::swap(t->rec, ctx->rec);
-  std::swap(t->start, ctx->start);
+  // the target owns its buffers (it may outlive the context): each is copied
+  // out of the context's arena, whose copy is then freed
+  struct {
+    DBuf *from, *to;
+  } mv[3] = {{&ctx->bps, &t->bps}, {&ctx->rec, &t->rec}, {&ctx->start, &t->start}};
+  for (auto &m : mv) {
+    const size_t n = m.from->cap;
+    cudaError_t e = cudaMalloc(&m.to->p, n);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      m.to->p = nullptr;
+      ctx->arena.trim();
+      e = cudaMalloc(&m.to->p, n);
+      if (e != cudaSuccess) m.to->p = nullptr;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m.to->p, m.from->p, n, cudaMemcpyDeviceToDevice, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      if (m.to->p) cudaFree(m.to->p);
+      m.to->p = nullptr;
+      pga_target_destroy(t);
+      return fail(ctx, PGA_ERR_NOMEM, "target buffer of %zu bytes: %s", n, cudaGetErrorString(e));
+    }
+    m.to->cap = n;
+    ctx->arena.release(m.from->p);
+    m.from->p = nullptr;
+    m.from->cap = 0;
+  }
   gdb_reset(ctx);
   *out = t;
   return PGA_OK;
@@ -2610,6 +2731,8 @@ int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds) {
 int pga_seeds_copy(pga_ctx *ctx, int comp, uint8_t *seeds, int64_t *buck) {
   if (!ctx || !ctx->have_seeds || (comp != 0 && comp != 1)) return PGA_ERR_ARG;
   if (ctx->seeds_released) return fail(ctx, PGA_ERR_ARG, "seeds were freed for the alignment; run pga_merge again");
+  if (ctx->seeds_consumed[comp])
+    return fail(ctx, PGA_ERR_ARG, "the unit's seeds were consumed by its diagonal sort; run pga_merge again");
   return copy_seeds(ctx, comp, seeds, buck);
 }
 
@@ -2627,6 +2750,8 @@ int pga_seeds_load(pga_ctx *ctx, int comp, const uint8_t *seeds, int64_t len) {
     ENSURE(ctx->seed[0], 16);
     ENSURE(ctx->seed[1], 16);
     ctx->seeds_loaded = true;
+    ctx->have_diag[0] = ctx->have_diag[1] = false;
+    ctx->seeds_consumed[0] = ctx->seeds_consumed[1] = false;
   }
   ENSURE(ctx->io, (size_t)len + 16);
   ENSURE(ctx->seed[comp], sizeof(Seed) * (size_t)n + 16);
@@ -2640,7 +2765,8 @@ int pga_seeds_load(pga_ctx *ctx, int comp, const uint8_t *seeds, int64_t len) {
   ctx->nseed[comp] = n;
   ctx->have_seeds = true;
   ctx->seeds_released = false;
-  ctx->have_diag[0] = ctx->have_diag[1] = false;
+  ctx->have_diag[comp] = false;
+  ctx->seeds_consumed[comp] = false;
   return PGA_OK;
 }
 
@@ -2656,8 +2782,11 @@ int pga_diag_sort(pga_ctx *ctx, int comp, int *swide, int64_t *count) {
   }
   if (dbyte > 4) return fail(ctx, PGA_ERR_LIMIT, "DBYTE %d > 4", dbyte);
   if (dbyte < 1) dbyte = 1;
-  int r = run_diag(ctx, comp, ctx->ncontig, ctx->maxctg, dbyte, ctx->ctgb);
-  if (r) return r;
+  // sorted already (its seeds were consumed): the same result again
+  if (!(ctx->seeds_consumed[comp] && ctx->have_diag[comp])) {
+    int r = run_diag(ctx, comp, ctx->ncontig, ctx->maxctg, dbyte, ctx->ctgb);
+    if (r) return r;
+  }
   if (swide) *swide = 2 * dbyte + ctx->ctgb + 2;
   if (count) *count = ctx->nseed[comp];
   return PGA_OK;
@@ -2687,12 +2816,15 @@ int pga_align(pga_ctx *ctx, int64_t *nalign) {
   }
   if (r) return r;
   stage_end(ctx, ST_ALIGN);
-  if (nalign) *nalign = (int64_t)ctx->h_recs.size();
+  if (nalign) *nalign = ctx->nalign;
   return PGA_OK;
 }
 
 int pga_align_copy(pga_ctx *ctx, int32_t *recs9, int64_t *trace_off, uint8_t *trace) {
   if (!ctx || !ctx->have_align) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int r = host_alignments(ctx);
+  if (r) return r;
   int64_t n = (int64_t)ctx->h_recs.size();
   for (int64_t i = 0; i < n; i++) {
     const AlnRec &a = ctx->h_recs[i];
@@ -2857,6 +2989,9 @@ int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, co
                          const int64_t *contig_sbeg) {
   if (!ctx || !ctx->have_align) return PGA_ERR_ARG;
   if (nscaff > 0 && scaff_fctg && scaff_fctg[nscaff] > ctx->ncontig) return PGA_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int hr = host_alignments(ctx);
+  if (hr) return hr;
   const int64_t n = (int64_t)ctx->h_recs.size();
   std::vector<int32_t> r9(9 * (size_t)n);
   for (int64_t i = 0; i < n; i++) {

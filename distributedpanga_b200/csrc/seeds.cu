@@ -15,15 +15,6 @@
 
 namespace pga {
 
-__device__ __forceinline__ void put_bits(U128 &k, int off, uint64_t v) {
-  if (off < 64) {
-    k.lo |= v << off;
-    if (off > 0) k.hi |= v >> (64 - off);
-  } else {
-    k.hi |= v << (off - 64);
-  }
-}
-
 __device__ __forceinline__ uint64_t get_bits(const U128 &k, int off, int w) {
   uint64_t v;
   if (off < 64) {
@@ -37,31 +28,8 @@ __device__ __forceinline__ uint64_t get_bits(const U128 &k, int off, int w) {
 
 __global__ void k_seed_keys(const Seed *__restrict__ sd, int64_t n, SeedKeyLayout L, U128 *__restrict__ keys) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    Seed s = sd[i];
-    int64_t ipost = (int64_t)(s.a & 0xffffffffu), jpost = (int64_t)(s.a >> 32);
-    uint64_t icont = s.b & 0xffffu;
-    uint64_t jcont = ((s.b >> 16) & 0xffffu) & L.jmask;
-    uint64_t lcp = (s.b >> 32) & 0xffu;
-    int64_t diag, anti;
-    if (L.comp) {
-      diag = L.maxdag - (ipost + jpost);
-      anti = L.amxpos - (ipost - jpost);
-    } else {
-      diag = L.bmxpos + (ipost - jpost);
-      anti = ipost + jpost;
-    }
-    int64_t band = diag >> 6;
-    uint64_t dlow = (uint64_t)(diag - (band << 6)) & 0xffu;
-    U128 k = {0, 0};
-    put_bits(k, 0, lcp);
-    put_bits(k, L.off_dlow, dlow);
-    put_bits(k, L.off_anti, (uint64_t)anti & L.dmask);
-    put_bits(k, L.off_band, (uint64_t)band & L.dmask);
-    put_bits(k, L.off_j, jcont);
-    put_bits(k, L.off_i, icont);
-    keys[i] = k;
-  }
+       i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = seed_key(sd[i], L);
 }
 
 // Sorted keys -> swide-byte records (src/fastga_pipeline.c:1434-1446).

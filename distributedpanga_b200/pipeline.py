@@ -43,6 +43,7 @@ _SIGS = {
     "pga_kernel_launches": (C.c_int64, [vp]),
     "pga_ctx_enable_timing": (C.c_int, [vp, C.c_int]),
     "pga_stage_times": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "pga_alloc_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "pga_gdb_load": (C.c_int, [vp, u8p, C.c_int64, C.c_int, i64p, i64p]),
     "pga_record_sizing": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pga_extract_to_records": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_uint8)),
@@ -61,6 +62,7 @@ _SIGS = {
     "pga_index_copy_entries": (C.c_int, [vp, vp, vp, C.POINTER(C.c_int64)]),
     "pga_merge": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "pga_seeds_copy": (C.c_int, [vp, C.c_int, vp, vp]),
+    "pga_seeds_load": (C.c_int, [vp, C.c_int, vp, C.c_int64]),
     "pga_diag_sort": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
     "pga_diag_copy": (C.c_int, [vp, C.c_int, vp, vp]),
     "pga_gdb_set_freq": (C.c_int, [vp, vp]),
@@ -135,6 +137,10 @@ def _take(L, p, nbytes: int) -> np.ndarray:
     return out
 
 
+# pga_stage_times' slots
+STAGE_NAMES = ["extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp", "entries_prefix_table",
+               "merge", "diag_sort_n", "align", "diag_sort_c"]
+
 class Device:
     """One pga_ctx on one CUDA device."""
 
@@ -180,9 +186,20 @@ class Device:
     def stage_times(self) -> dict:
         a = (C.c_float * 10)()
         self._ck(self.L.pga_stage_times(self.h, a), "stage_times")
-        names = ["extract_hist", "prefix_scan", "extract_scatter", "bucket_sort", "lcp",
-                 "entries_prefix_table", "merge", "diag_sort_n", "align", "diag_sort_c"]
-        return dict(zip(names, [float(x) for x in a]))
+        return dict(zip(STAGE_NAMES, [float(x) for x in a]))
+
+    def alloc_times(self) -> dict:
+        """Host ms inside cudaMalloc / cudaFree per stage (key "other":
+        outside every stage) since timing was enabled, the number of those
+        driver calls ("calls"), the bytes the context's arena holds
+        ("held_bytes", "free_bytes") and how often the alignment buffers were
+        freed to make room ("sheds")."""
+        a = (C.c_double * 11)()
+        n = (C.c_int64 * 4)()
+        self._ck(self.L.pga_alloc_times(self.h, a, n), "alloc_times")
+        d = dict(zip(STAGE_NAMES + ["other"], [float(x) for x in a]))
+        d.update(calls=int(n[0]), held_bytes=int(n[1]), free_bytes=int(n[2]), sheds=int(n[3]))
+        return d
 
     # ---- GDB -------------------------------------------------------------
     def gdb_load(self, cs: _gdb.ContigSet):
@@ -347,7 +364,8 @@ class Device:
     def merge(self, freq: int = 10):
         a, b = C.c_int64(), C.c_int64()
         self._ck(self.L.pga_merge(self.h, freq, C.byref(a), C.byref(b)), "merge")
-        self.nseeds = (a.value, b.value)
+        self.nseeds = [a.value, b.value]
+        self._seeds_loaded = False
         return a.value, b.value
 
     def seeds(self, comp: int):
@@ -357,6 +375,19 @@ class Device:
         buck = np.zeros(self.ncontig, dtype=np.int64)
         self._ck(self.L.pga_seeds_copy(self.h, comp, _ptr(out), buck.ctypes.data_as(vp)), "seeds_copy")
         return out, buck
+
+    def seeds_load(self, comp: int, seeds: np.ndarray):
+        """Unit comp's seeds in the reference's byte format (pga_seeds_load),
+        in place of the merge's; the first load after a merge leaves the
+        other unit empty until it is loaded too."""
+        a = np.ascontiguousarray(seeds, dtype=np.uint8)
+        buf = a if a.size else np.zeros(1, np.uint8)
+        self._ck(self.L.pga_seeds_load(self.h, comp, _ptr(buf), int(a.size)), "seeds_load")
+        posb, ctgb, _ = self.record_sizing()
+        if not getattr(self, "_seeds_loaded", False):
+            self.nseeds = [0, 0]
+            self._seeds_loaded = True
+        self.nseeds[comp] = a.size // (1 + 2 * (posb + ctgb))
 
     def diag_sort(self, comp: int):
         sw, n = C.c_int(), C.c_int64()

@@ -56,6 +56,16 @@ int64_t     pga_kernel_launches(const pga_ctx *ctx);
  * the C unit. */
 int         pga_ctx_enable_timing(pga_ctx *ctx, int on);
 int         pga_stage_times(const pga_ctx *ctx, float *ms10);
+/* Device memory.  A context keeps the memory it frees (an arena of slabs
+ * from cudaMalloc) and hands it out again, so a repeated pipeline pass makes
+ * no driver allocation calls; the memory goes back to the driver when the
+ * context is destroyed, or when a request does not fit and slabs with
+ * nothing live in them are returned to make room.  ms11: host time (ms)
+ * inside cudaMalloc / cudaFree since timing was last enabled, charged to the
+ * stage that asked ([0..9] as above, [10] outside every stage); counts4
+ * (may be NULL): driver calls, bytes held, bytes held but free, times the
+ * alignment buffers were freed to make room. */
+int         pga_alloc_times(const pga_ctx *ctx, double *ms11, int64_t *counts4);
 
 /* ---- GDB ------------------------------------------------------------------ */
 

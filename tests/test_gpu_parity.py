@@ -262,3 +262,30 @@ def test_1aln_file_matches_reference(dev, case):
     ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n")
            if l.strip()]
     assert mine == ref
+
+
+def test_diag_sort_consumes_seeds(dev, oracle):
+    """The diagonal sort uses a unit's seed buffer as its second key buffer:
+    after it the unit's seeds cannot be copied, sorting the unit again gives
+    the same panels without re-sorting, and loading seeds makes it sortable
+    again with the same result."""
+    from distributedpanga_b200.pipeline import PgaError
+    cs, dig = load_case("small_s002")
+    dev.gdb_load(cs)
+    dev.index_build(want_entries=False)
+    dev.merge(dig["freq_cutoff"])
+    ns, _ = dev.seeds(0)
+    sw, cnt = dev.diag_sort(0)
+    a0, o0 = dev.diag_records(0, sw, cnt)
+    with pytest.raises(PgaError):
+        dev.seeds(0)
+    css, _ = dev.seeds(1)                  # the other unit is untouched
+    assert (sw, cnt) == dev.diag_sort(0)
+    a1, o1 = dev.diag_records(0, sw, cnt)
+    assert np.array_equal(a0, a1) and np.array_equal(o0, o1)
+    dev.seeds_load(0, ns)
+    dev.seeds_load(1, css)
+    assert (sw, cnt) == dev.diag_sort(0)
+    a2, o2 = dev.diag_records(0, sw, cnt)
+    assert np.array_equal(a0, a2) and np.array_equal(o0, o2)
+    check_diag(a2, o2, "N", dig)
