@@ -1133,7 +1133,7 @@ int la_sort_device(pga_ctx *ctx, int64_t n, int64_t nbytes) {
   launch_aln_gather(res, n, P<AlnRec>(ctx->recs), P<AlnRec>(ctx->srecs), len, ctx->st);
   CK(exclusive_scan<int64_t>(len, len, n, P<int64_t>(ctx->lscan), len + n, ctx->st));
   launch_aln_traces(P<AlnRec>(ctx->srecs), len, n, P<uint8_t>(ctx->outb), P<uint8_t>(ctx->strace), ctx->st);
-  LAUNCHED(2 + 5 * np + 3 + 3);
+  LAUNCHED(2 + 5 * np + 5);  // keys, bits; np x (hist, 3 scan, scatter); gather, 3 scan, traces
   CK(cudaGetLastError());
   return PGA_OK;
 }
