@@ -52,6 +52,10 @@ struct AlignLaunch {
   // SM cycles the launch's warps spent in Local_Alignment [0] and in the
   // pairs' finishing step [1], zero at launch
   unsigned long long *prof;
+  // per pair of unit u (null: off): (1 << 32 | exit_bepos) when the
+  // device-planned pair made a call, else 0 -- recorded for a resident
+  // target's pair cache
+  unsigned long long *cap_fo[2];
   int long_waves;     // a wave loop past this many waves flags its SM
   const U128 *keysN, *keysC;
   // per seed of each unit: band start (bit 15), previous band of the pair
@@ -127,7 +131,7 @@ struct AlignLaunch {
 // CHAIN_MIN) as `small` codes, largest first (sizes clamped to 65535).
 constexpr int SMALL_BINS = 65536;
 void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                           uint32_t *flag, cudaStream_t st);
+                           uint32_t *flag, const uint32_t *reuse, cudaStream_t st);
 void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
                         const uint32_t *idx, int64_t *out3, cudaStream_t st);
 void launch_pair_live(const uint16_t *info, int64_t n, const uint32_t *pflag, const uint32_t *pidx, uint8_t *live,
@@ -159,5 +163,34 @@ void launch_aln_keys(const AlnRec *r, int64_t n, U128 *keys, cudaStream_t st);
 void launch_aln_gather(const U128 *keys, int64_t n, const AlnRec *in, AlnRec *out, int64_t *len, cudaStream_t st);
 void launch_aln_traces(AlnRec *recs, const int64_t *off, int64_t n, const uint8_t *src, uint8_t *dst,
                        cudaStream_t st);
+
+// One unit of a resident target's pair cache: the target's own run's
+// non-self pairs that had work, by (a << 32 | b) ascending; each with its
+// seeds' low key bits (the bits below the contig fields) at low[seg_off ..
+// seg_off + seg_len), its surviving alignments at recs[rec_off .. rec_off +
+// rec_cnt) in rank order, whose traces lie at tr[tr_off .. tr_off + tr_len).
+struct ReuseUnit {
+  const uint64_t *key;
+  const int64_t *seg_off, *seg_len, *rec_off, *tr_off, *tr_len;
+  const int32_t *rec_cnt;
+  const uint64_t *low;
+  int64_t n;
+};
+
+// reuse[p] = entry + 1 when pair p of the unit (both contigs below nT, not a
+// self pair) has exactly the cached entry's seeds (low key bits under
+// lowmask, in order), else 0; a reused pair's live flag is cleared and
+// (unit << 63 | entry) is appended to list (count at *count).
+void launch_pair_reuse(const U128 *keys, const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds,
+                       int comp, int nT, uint64_t lowmask, ReuseUnit U, uint32_t *reuse, uint8_t *live,
+                       unsigned long long *list, unsigned long long *count, cudaStream_t st);
+// The cached alignments of the listed entries appended to the launch's
+// record and trace pools (rec_next / out_next), toff rewritten; err set when
+// a pool is too small.
+void launch_reuse_emit(const unsigned long long *list, int64_t n, ReuseUnit U0, ReuseUnit U1, const AlnRec *crecs,
+                       const uint8_t *ctrace, AlnRec *recs, uint8_t *out, unsigned long long *rec_next,
+                       unsigned long long *out_next, int64_t rec_cap, int64_t out_cap, int *err, cudaStream_t st);
+// out[i] = keys[i].lo & lowmask
+void launch_key_low(const U128 *keys, int64_t n, uint64_t lowmask, uint64_t *out, cudaStream_t st);
 
 }  // namespace pga

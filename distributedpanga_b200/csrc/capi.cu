@@ -1,6 +1,8 @@
 // C-ABI layer: context, device buffers, stage drivers and the drop-in entry
 // points declared in include/pga_b200.h.
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cstdarg>
 #include <chrono>
 #include <cstdint>
@@ -101,6 +103,22 @@ struct pga_ctx {
   DBuf keys[2], dlook, dsmall, panel[2];
   U128 *sorted[2] = {nullptr, nullptr};
   bool seeds_consumed[2] = {false, false};  // the unit's seed buffer was used by its diagonal sort
+  // served requests: the resident target whose pair cache pga_align may use
+  // (set by pga_serve_load), buffers of that check, and its outcome for the
+  // last alignment: {used, pairs reused, alignments reused, reason it was
+  // not used: 0 none, 1 no cache, 2 key layout, 3 scoring tables}
+  const pga_target *reuse_t = nullptr;
+  DBuf reuse_map[2], reuse_list, reuse_cnt;
+  int64_t reuse_stats[4] = {0, 0, 0, 0};
+  // recording a target's own run (pga_target_create_reuse): per device pair
+  // its call flag and exit bepos; per host-planned pair {comp, a, b, value}
+  bool capture = false;
+  DBuf cap_fo[2];
+  std::vector<std::array<int64_t, 4>> cap_host;
+  int64_t cap_np[2] = {0, 0}, cap_rs = 0;
+  // the scoring tables of the last alignment
+  std::vector<int16_t> spec_host;
+  int ave_path_host = 0;
   int diag_passes[2] = {0, 0};
   SeedKeyLayout lay[2];
   bool have_diag[2] = {false, false};
@@ -158,6 +176,22 @@ struct pga_target {
   std::vector<char> headers;
   int64_t base_count[4] = {0, 0, 0, 0};
   DBuf bps, rec, start;  // sequence image, sorted records, prefix table (NPREFIX + 1)
+  // The target's own run's pairs, for requests whose pairs of two target
+  // contigs have the same seeds (pga_target_create_reuse): per unit the
+  // entries of a ReuseUnit, their low key bits, alignments and traces; the
+  // key layout and scoring tables they were made with; per entry, whether
+  // the pair called and its exit bepos (FastGA's order keys, N unit).
+  struct Reuse {
+    bool valid = false;
+    SeedKeyLayout lay[2];
+    std::vector<int16_t> spec;
+    int ave_path = 0;
+    int64_t n[2] = {0, 0};
+    std::vector<uint64_t> hkey[2], hfo[2];
+    std::vector<int32_t> hcnt[2];
+    std::vector<int64_t> htrl[2];
+    DBuf key[2], seg_off[2], seg_len[2], rec_off[2], rec_cnt[2], tr_off[2], tr_len[2], low[2], recs, trace;
+  } reuse;
 };
 
 namespace {
@@ -223,7 +257,8 @@ bool shed_align_buffers(pga_ctx *ctx) {
                   &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->ftasks,
                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace,
                   &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1], &ctx->skeys, &ctx->skeys2,
-                  &ctx->lhist, &ctx->lscan};
+                  &ctx->lhist, &ctx->lscan, &ctx->reuse_map[0], &ctx->reuse_map[1], &ctx->reuse_list,
+                  &ctx->reuse_cnt, &ctx->cap_fo[0], &ctx->cap_fo[1]};
   bool any = false;
   for (DBuf *b : bufs)
     if (b->p) {
@@ -980,6 +1015,8 @@ int prepare_sequences(pga_ctx *ctx, int *ave_path) {
   *ave_path = aln::build_align_spec(ctx->base_freq, tab.data(), tab.data() + 32768);
   ENSURE(ctx->spec_tab, sizeof(int16_t) * tab.size());
   CK(cudaMemcpyAsync(ctx->spec_tab.p, tab.data(), sizeof(int16_t) * tab.size(), cudaMemcpyHostToDevice, ctx->st));
+  ctx->spec_host.swap(tab);  // (a pageable source is staged before the copy call returns)
+  ctx->ave_path_host = *ave_path;
 
   return PGA_OK;
 }
@@ -1210,6 +1247,51 @@ int run_align(pga_ctx *ctx) {
   std::vector<PairTask> pairs[2];
   int64_t npairs[2] = {0, 0};
   DBuf *dpst[2] = {&ctx->pstart, &ctx->pstart2}, *dpab[2] = {&ctx->pab, &ctx->pab2};
+  // A resident target's pair cache (requests of the served form): used when
+  // this GDB's low key bits are laid out as in the target's run and the
+  // scoring tables are the same; pairs of two target contigs with the same
+  // seeds then take the cached alignments instead of tasks.
+  const pga_target *rt = ctx->reuse_t;
+  bool reuse_on = false;
+  ReuseUnit RU[2] = {};
+  uint64_t lowmask[2] = {0, 0};
+  for (int i = 0; i < 4; i++) ctx->reuse_stats[i] = 0;
+  if (rt) {
+    const pga_target::Reuse &R = rt->reuse;
+    int why = R.valid ? 0 : 1;
+    for (int u = 0; u < 2 && !why; u++) {
+      const SeedKeyLayout &a = R.lay[u], &b = ctx->lay[u];
+      if (a.comp != b.comp || a.amxpos != b.amxpos || a.bmxpos != b.bmxpos || a.maxdag != b.maxdag ||
+          a.dmask != b.dmask || a.dbyte != b.dbyte || a.off_dlow != b.off_dlow || a.off_anti != b.off_anti ||
+          a.off_band != b.off_band || a.off_j != b.off_j || b.off_j > 64)
+        why = 2;
+    }
+    if (!why && (R.spec != ctx->spec_host || R.ave_path != ctx->ave_path_host)) why = 3;
+    ctx->reuse_stats[3] = why;
+    if (!why) {
+      reuse_on = true;
+      for (int u = 0; u < 2; u++) {
+        RU[u].key = P<uint64_t>(R.key[u]);
+        RU[u].seg_off = P<int64_t>(R.seg_off[u]);
+        RU[u].seg_len = P<int64_t>(R.seg_len[u]);
+        RU[u].rec_off = P<int64_t>(R.rec_off[u]);
+        RU[u].tr_off = P<int64_t>(R.tr_off[u]);
+        RU[u].tr_len = P<int64_t>(R.tr_len[u]);
+        RU[u].rec_cnt = P<int32_t>(R.rec_cnt[u]);
+        RU[u].low = P<uint64_t>(R.low[u]);
+        RU[u].n = R.n[u];
+        lowmask[u] = ctx->lay[u].off_j >= 64 ? ~0ull : ((1ull << ctx->lay[u].off_j) - 1);
+      }
+      ENSURE(ctx->reuse_list, sizeof(unsigned long long) * (size_t)(R.n[0] + R.n[1] + 1));
+      ENSURE(ctx->reuse_cnt, 16);
+      CK(cudaMemsetAsync(ctx->reuse_cnt.p, 0, 16, ctx->st));
+    }
+  }
+  if (ctx->capture) {
+    ctx->cap_host.clear();
+    ctx->cap_rs = RS;
+    ctx->cap_np[0] = ctx->cap_np[1] = 0;
+  }
   for (int comp = 0; comp < 2; comp++) {
     int64_t n = ctx->nseed[comp];
     if (n == 0) continue;
@@ -1238,8 +1320,24 @@ int run_align(pga_ctx *ctx) {
     launch_pair_live(P<uint16_t>(ctx->binfo[comp]), n, P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
                      P<uint8_t>(ctx->plive[comp]), ctx->st);
     LAUNCHED(1);
+    // pairs with the cached seeds of the target's run: no task
+    uint32_t *rmap = nullptr;
+    if (reuse_on) {
+      ENSURE(ctx->reuse_map[comp], sizeof(uint32_t) * (size_t)(np + 1));
+      rmap = P<uint32_t>(ctx->reuse_map[comp]);
+      launch_pair_reuse(ctx->sorted[comp], pst, pab, np, n, comp, rt->ncontig, lowmask[comp], RU[comp], rmap,
+                        P<uint8_t>(ctx->plive[comp]), P<unsigned long long>(ctx->reuse_list),
+                        P<unsigned long long>(ctx->reuse_cnt), ctx->st);
+      LAUNCHED(np > 0 ? 1 : 0);
+    }
+    if (ctx->capture) {
+      ENSURE(ctx->cap_fo[comp], sizeof(unsigned long long) * (size_t)(np + 1));
+      CK(cudaMemsetAsync(ctx->cap_fo[comp].p, 0, sizeof(unsigned long long) * (size_t)(np + 1), ctx->st));
+      L.cap_fo[comp] = P<unsigned long long>(ctx->cap_fo[comp]);
+      ctx->cap_np[comp] = np;
+    }
     // the host's pairs
-    launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), ctx->st);
+    launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), rmap, ctx->st);
     CK(exclusive_scan<uint32_t>(P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), np, P<uint32_t>(ctx->scan_tmp), tot,
                                 ctx->st));
     LAUNCHED(5);
@@ -1469,8 +1567,40 @@ int run_align(pga_ctx *ctx) {
     }
   }
   L.nsmall = 0;  // the later launches run host-planned tasks only
+  // the reused pairs: N pairs that called enter FastGA's order keys (their
+  // alignments join the others before the final order)
+  std::vector<unsigned long long> rlist;
+  if (reuse_on) {
+    unsigned long long nr = 0;
+    CK(cudaMemcpyAsync(&nr, ctx->reuse_cnt.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    rlist.resize(nr);
+    if (nr > 0) {
+      CK(cudaMemcpyAsync(rlist.data(), ctx->reuse_list.p, 8 * nr, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+    }
+    ctx->reuse_stats[0] = 1;
+    ctx->reuse_stats[1] = (int64_t)nr;
+    for (unsigned long long code : rlist) {
+      const int u = (int)(code >> 63);
+      const int64_t e = (int64_t)(code & 0x7fffffffffffffffull);
+      ctx->reuse_stats[2] += rt->reuse.hcnt[u][e];
+      const uint64_t fo = rt->reuse.hfo[u][e];
+      if (u != 0 || !(fo >> 32)) continue;
+      const int a = (int)(rt->reuse.hkey[u][e] >> 32), b = (int)(uint32_t)rt->reuse.hkey[u][e];
+      const int xa = F.pos[a], xb = F.pos[b];
+      const int64_t key = fo_key(xb, (int)(uint32_t)fo);
+      if (key > Lk[xa]) Lk[xa] = key;
+      if (xb < xa && key > ebest[xa]) ebest[xa] = key;
+    }
+  }
   std::vector<PairOut> out1(first.size());
   for (size_t i = 0; i < first.size(); i++) {
+    if (ctx->capture) {
+      const PairOut &po = first_task[i] >= 0 ? tout[first_task[i]] : fout[first_fin[i]];
+      ctx->cap_host.push_back(
+          {first[i].comp, first[i].a, first[i].b, po.calls > 0 ? ((int64_t)1 << 32) | (uint32_t)po.exit_bepos : 0});
+    }
     if (first_task[i] >= 0) {
       out1[i] = tout[first_task[i]];
     } else {
@@ -1640,7 +1770,39 @@ int run_align(pga_ctx *ctx) {
 
   const double t_order = now_ms();
   // 7. survivors in la_sort order: (aread, abpos, bread, comp), ties in the
-  // pair's own output order (src/fastga_pipeline.c:1500-1515), on the device
+  // pair's own output order (src/fastga_pipeline.c:1500-1515), on the device;
+  // first the reused pairs' cached alignments join the pools
+  if (!rlist.empty()) {
+    int64_t add_r = 0, add_b = 0;
+    for (unsigned long long code : rlist) {
+      const int u = (int)(code >> 63);
+      const int64_t e = (int64_t)(code & 0x7fffffffffffffffull);
+      add_r += rt->reuse.hcnt[u][e];
+      add_b += rt->reuse.htrl[u][e];
+    }
+    if (add_r > 0) {
+      unsigned long long cur[2];
+      CK(cudaMemcpyAsync(&cur[0], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(&cur[1], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+      int r = grow_keep(ctx, ctx->recs, sizeof(AlnRec) * (size_t)(cur[0] + add_r) + 16, sizeof(AlnRec) * cur[0]);
+      if (!r) r = grow_keep(ctx, ctx->outb, (size_t)(cur[1] + add_b) + 16, cur[1]);
+      if (r) return r;
+      ENSURE(ctx->u64tmp, 64);
+      int *err = P<int>(ctx->u64tmp);
+      CK(cudaMemsetAsync(err, 0, 4, ctx->st));
+      launch_reuse_emit(P<unsigned long long>(ctx->reuse_list), (int64_t)rlist.size(), RU[0], RU[1],
+                        P<AlnRec>(rt->reuse.recs), P<uint8_t>(rt->reuse.trace), P<AlnRec>(ctx->recs),
+                        P<uint8_t>(ctx->outb), P<unsigned long long>(ctx->rec_next),
+                        P<unsigned long long>(ctx->out_next), (int64_t)(ctx->recs.cap / sizeof(AlnRec)),
+                        (int64_t)ctx->outb.cap, err, ctx->st);
+      LAUNCHED(1);
+      int bad = 0;
+      CK(cudaMemcpyAsync(&bad, err, 4, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+      if (bad) return fail(ctx, PGA_ERR_CUDA, "reused alignments overflowed the record pools");
+    }
+  }
   unsigned long long nrec = 0, nbytes = 0;
   CK(cudaMemcpyAsync(&nrec, ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaMemcpyAsync(&nbytes, ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -1703,7 +1865,9 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->rng_ovl, &ctx->rng_next, &ctx->ftasks,
                    &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb, &ctx->lreq, &ctx->lpath, &ctx->ltoff,
                    &ctx->ltrace, &ctx->lnext, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->shist, &ctx->fo_dev,
-                   &ctx->srecs, &ctx->slen, &ctx->strace, &ctx->skeys, &ctx->skeys2, &ctx->lhist, &ctx->lscan};
+                   &ctx->srecs, &ctx->slen, &ctx->strace, &ctx->skeys, &ctx->skeys2, &ctx->lhist, &ctx->lscan,
+                   &ctx->reuse_map[0], &ctx->reuse_map[1], &ctx->reuse_list, &ctx->reuse_cnt, &ctx->cap_fo[0],
+                   &ctx->cap_fo[1]};
   for (DBuf *b : abufs) ctx->arena.release(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
                   &ctx->scan_tmp, &ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->cum, &ctx->qmed,
@@ -1827,6 +1991,7 @@ void gdb_reset(pga_ctx *ctx) {
   ctx->have_numeric = false;
   ctx->have_diag[0] = ctx->have_diag[1] = false;
   ctx->have_align = false;
+  ctx->reuse_t = nullptr;
 }
 
 }  // namespace
@@ -2488,7 +2653,10 @@ int pga_index_build(pga_ctx *ctx, int want_entries, int64_t *count) {
   return PGA_OK;
 }
 
-int pga_target_create(pga_ctx *ctx, pga_target **out) {
+namespace {
+
+// pga_target_create; with keep, the context keeps its GDB and index.
+int target_create(pga_ctx *ctx, pga_target **out, bool keep) {
   if (!ctx || !out) return PGA_ERR_ARG;
   *out = nullptr;
   if (!ctx->have_scaffolds || !ctx->have_index)
@@ -2535,11 +2703,164 @@ int pga_target_create(pga_ctx *ctx, pga_target **out) {
       return fail(ctx, PGA_ERR_NOMEM, "target buffer of %zu bytes: %s", n, cudaGetErrorString(e));
     }
     m.to->cap = n;
-    ctx->arena.release(m.from->p);
-    m.from->p = nullptr;
-    m.from->cap = 0;
+    if (!keep) {
+      ctx->arena.release(m.from->p);
+      m.from->p = nullptr;
+      m.from->cap = 0;
+    }
   }
+  if (!keep) gdb_reset(ctx);
+  *out = t;
+  return PGA_OK;
+}
+
+int target_upload(pga_ctx *ctx, DBuf &b, const void *src, size_t bytes) {
+  b.cap = bytes + 16;
+  cudaError_t e = cudaMalloc(&b.p, b.cap);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    b.cap = 0;
+    return fail(ctx, PGA_ERR_NOMEM, "target cache buffer of %zu bytes: %s", bytes, cudaGetErrorString(e));
+  }
+  if (bytes > 0 && src) CK(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return PGA_OK;
+}
+
+// The target's pair cache from the context's recorded run of the target's
+// own GDB: per unit, every non-self pair that had work (live, or run in
+// ranges) with its seeds, its call flag / exit bepos and its alignments.
+int build_reuse(pga_ctx *ctx, pga_target *t) {
+  int r = host_alignments(ctx);
+  if (r) return r;
+  pga_target::Reuse &R = t->reuse;
+  auto K = [](int u, int a, int b) {
+    return ((uint64_t)u << 63) | ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+  };
+  std::map<uint64_t, std::vector<int64_t>> byp;  // a pair's alignments, in rank order
+  int64_t nonself = 0;
+  for (int64_t i = 0; i < (int64_t)ctx->h_recs.size(); i++) {
+    const AlnRec &x = ctx->h_recs[i];
+    if (x.comp == 0 && x.aread == x.bread) continue;
+    byp[K(x.comp, x.aread, x.bread)].push_back(i);
+    nonself++;
+  }
+  for (auto &kv : byp)
+    std::sort(kv.second.begin(), kv.second.end(),
+              [&](int64_t x, int64_t y) { return ctx->h_recs[x].rank < ctx->h_recs[y].rank; });
+  std::map<uint64_t, int64_t> hostfo;
+  for (const auto &h : ctx->cap_host) hostfo[K((int)h[0], (int)h[1], (int)h[2])] = h[3];
+  std::vector<AlnRec> crecs;
+  std::vector<uint8_t> ctr;
+  int64_t matched = 0;
+  bool ok = true;
+  DBuf *dpst[2] = {&ctx->pstart, &ctx->pstart2}, *dpab[2] = {&ctx->pab, &ctx->pab2};
+  for (int u = 0; u < 2; u++) {
+    const int64_t np = ctx->cap_np[u], n = ctx->nseed[u];
+    std::vector<int64_t> pst(np + 1), key, soff, slen, roff, toff, tlen;
+    std::vector<int32_t> pab(2 * np + 2), rcnt;
+    std::vector<uint8_t> live(np + 1);
+    std::vector<uint64_t> cfo(np + 1), fo;
+    if (np > 0) {
+      CK(cudaMemcpyAsync(pst.data(), dpst[u]->p, sizeof(int64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(pab.data(), dpab[u]->p, sizeof(int32_t) * 2 * np, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(live.data(), ctx->plive[u].p, np, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaMemcpyAsync(cfo.data(), ctx->cap_fo[u].p, sizeof(uint64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+    }
+    for (int64_t p = 0; p < np; p++) {
+      const int a = pab[2 * p], b = pab[2 * p + 1];
+      if (u == 0 && a == b) continue;
+      const int64_t lo = pst[p], hi = p + 1 < np ? pst[p + 1] : n;
+      const bool ranges = ctx->cap_rs > 0 && hi - lo > ctx->cap_rs;
+      if (!live[p] && !ranges) continue;
+      uint64_t f = cfo[p];
+      if (ranges) {
+        auto it = hostfo.find(K(u, a, b));
+        if (it == hostfo.end()) {
+          ok = false;
+          continue;
+        }
+        f = (uint64_t)it->second;
+      }
+      key.push_back((int64_t)(((uint64_t)(uint32_t)a << 32) | (uint32_t)b));
+      soff.push_back(lo);
+      slen.push_back(hi - lo);
+      fo.push_back(f);
+      roff.push_back((int64_t)crecs.size());
+      toff.push_back((int64_t)ctr.size());
+      auto it = byp.find(K(u, a, b));
+      int c = 0;
+      if (it != byp.end()) {
+        for (int64_t i : it->second) {
+          AlnRec x = ctx->h_recs[i];
+          const int64_t t0 = ctx->h_toff[i], t1 = ctx->h_toff[i + 1];
+          x.toff = (int64_t)ctr.size();
+          ctr.insert(ctr.end(), ctx->h_trace.begin() + t0, ctx->h_trace.begin() + t1);
+          crecs.push_back(x);
+          c++;
+        }
+        byp.erase(it);
+      }
+      matched += c;
+      rcnt.push_back(c);
+      tlen.push_back((int64_t)ctr.size() - toff.back());
+    }
+    const size_t m = key.size();
+    for (size_t i = 1; i < m; i++)
+      if ((uint64_t)key[i] <= (uint64_t)key[i - 1]) ok = false;  // pairs come in (a, b) order
+    R.n[u] = (int64_t)m;
+    R.hkey[u].assign(key.begin(), key.end());
+    R.hfo[u] = fo;
+    R.hcnt[u] = rcnt;
+    R.htrl[u] = tlen;
+    if ((r = target_upload(ctx, R.key[u], key.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.seg_off[u], soff.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.seg_len[u], slen.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.rec_off[u], roff.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.tr_off[u], toff.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.tr_len[u], tlen.data(), 8 * m))) return r;
+    if ((r = target_upload(ctx, R.rec_cnt[u], rcnt.data(), 4 * m))) return r;
+    if ((r = target_upload(ctx, R.low[u], nullptr, 8 * (size_t)n))) return r;
+    const SeedKeyLayout &L = ctx->lay[u];
+    if (L.off_j > 64) ok = false;
+    launch_key_low(ctx->sorted[u], n, L.off_j >= 64 ? ~0ull : ((1ull << L.off_j) - 1), P<uint64_t>(R.low[u]),
+                   ctx->st);
+    LAUNCHED(n > 0 ? 1 : 0);
+    CK(cudaGetLastError());
+    R.lay[u] = L;
+  }
+  if ((r = target_upload(ctx, R.recs, crecs.data(), sizeof(AlnRec) * crecs.size()))) return r;
+  if ((r = target_upload(ctx, R.trace, ctr.data(), ctr.size()))) return r;
+  R.spec = ctx->spec_host;
+  R.ave_path = ctx->ave_path_host;
+  // every alignment of a non-self pair belongs to a cached pair
+  R.valid = ok && matched == nonself;
+  return PGA_OK;
+}
+
+}  // namespace
+
+int pga_target_create(pga_ctx *ctx, pga_target **out) { return target_create(ctx, out, false); }
+
+int pga_target_create_reuse(pga_ctx *ctx, int freq, pga_target **out) {
+  if (!ctx || !out || freq < 1) return PGA_ERR_ARG;
+  pga_target *t = nullptr;
+  int r = target_create(ctx, &t, true);
+  if (r) return r;
+  // the target's own run, every pair's outcome recorded
+  ctx->capture = true;
+  r = run_merge(ctx, freq);
+  int64_t nal = 0;
+  if (!r) r = pga_align(ctx, &nal);
+  ctx->capture = false;
+  if (!r) r = build_reuse(ctx, t);
   gdb_reset(ctx);
+  if (r) {
+    pga_target_destroy(t);
+    return r;
+  }
   *out = t;
   return PGA_OK;
 }
@@ -2548,6 +2869,13 @@ void pga_target_destroy(pga_target *t) {
   if (!t) return;
   cudaSetDevice(t->device);
   for (DBuf *b : {&t->bps, &t->rec, &t->start})
+    if (b->p) cudaFree(b->p);
+  pga_target::Reuse &R = t->reuse;
+  for (int u = 0; u < 2; u++)
+    for (DBuf *b : {&R.key[u], &R.seg_off[u], &R.seg_len[u], &R.rec_off[u], &R.rec_cnt[u], &R.tr_off[u],
+                    &R.tr_len[u], &R.low[u]})
+      if (b->p) cudaFree(b->p);
+  for (DBuf *b : {&R.recs, &R.trace})
     if (b->p) cudaFree(b->p);
   delete t;
 }
@@ -2559,7 +2887,18 @@ int pga_target_info(const pga_target *t, int64_t *info4) {
   info4[0] = t->ncontig;
   info4[1] = bases;
   info4[2] = t->nrec;
-  info4[3] = (int64_t)(t->bps.cap + t->rec.cap + t->start.cap);
+  size_t cache = t->reuse.recs.cap + t->reuse.trace.cap;
+  for (int u = 0; u < 2; u++)
+    for (const DBuf *b : {&t->reuse.key[u], &t->reuse.seg_off[u], &t->reuse.seg_len[u], &t->reuse.rec_off[u],
+                          &t->reuse.rec_cnt[u], &t->reuse.tr_off[u], &t->reuse.tr_len[u], &t->reuse.low[u]})
+      cache += b->cap;
+  info4[3] = (int64_t)(t->bps.cap + t->rec.cap + t->start.cap + cache);
+  return PGA_OK;
+}
+
+int pga_align_reuse_stats(const pga_ctx *ctx, int64_t *stats4) {
+  if (!ctx || !stats4) return PGA_ERR_ARG;
+  for (int i = 0; i < 4; i++) stats4[i] = ctx->reuse_stats[i];
   return PGA_OK;
 }
 
@@ -2656,6 +2995,7 @@ int pga_serve_load(pga_ctx *ctx, const pga_target *t, const char *query, int64_t
     sizes6[5] = seqtot;
   }
   if (count) *count = n;
+  ctx->reuse_t = t;  // its pair cache, if it has one, serves this GDB's alignment
   return PGA_OK;
 }
 

@@ -93,6 +93,8 @@ _SIGS = {
     "pga_write_1gdb": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, vp, C.c_int, vp,
                                  vp, C.c_int64, C.c_int, vp, vp, C.c_int64]),
     "pga_target_create": (C.c_int, [vp, C.POINTER(vp)]),
+    "pga_target_create_reuse": (C.c_int, [vp, C.c_int, C.POINTER(vp)]),
+    "pga_align_reuse_stats": (C.c_int, [vp, vp]),
     "pga_target_destroy": (None, [vp]),
     "pga_target_info": (C.c_int, [vp, vp]),
     "pga_serve_load": (C.c_int, [vp, vp, C.c_char_p, C.c_int64, C.c_int, vp, vp]),
@@ -484,6 +486,14 @@ class Device:
         self._ck(self.L.pga_align_copy(self.h, None, None, tr.ctypes.data_as(vp)), "align_copy")
         return recs, toff, tr[: int(toff[-1])]
 
+    def reuse_stats(self) -> dict:
+        """The last alignment's use of a resident target's pair cache
+        (pga_align_reuse_stats)."""
+        a = np.zeros(4, dtype=np.int64)
+        self._ck(self.L.pga_align_reuse_stats(self.h, a.ctypes.data_as(vp)), "align_reuse_stats")
+        why = {0: None, 1: "no cache", 2: "key layout differs", 3: "scoring tables differ"}
+        return {"used": bool(a[0]), "pairs": int(a[1]), "alignments": int(a[2]), "not_used": why.get(int(a[3]))}
+
     def align_stats(self) -> dict:
         a = np.zeros(8, dtype=np.int64)
         self._ck(self.L.pga_align_stats(self.h, a.ctypes.data_as(vp)), "align_stats")
@@ -495,18 +505,25 @@ class Device:
 class Target:
     """A resident target (pga_target): a FASTA text ingested and indexed on
     one device and kept there, read-only, for any number of contexts'
-    requests (Device.serve_load)."""
+    requests (Device.serve_load).  With reuse, the target's own GDB is also
+    aligned once (FREQ = freq) and its pairs' results kept: a request's pairs
+    of two target contigs with the same seeds take them instead of being
+    aligned (pga_target_create_reuse; same results)."""
 
-    def __init__(self, text, nthr: int = 0, device: int = 0):
+    def __init__(self, text, nthr: int = 0, device: int = 0, reuse: bool = False, freq: int = 10):
         self.L = load_library()
         d = Device(device)
         try:
             d.gdb_ingest_fasta(text, nthr=nthr, tables=False)
             d.index_build(want_entries=False)
             h = vp()
-            d._ck(self.L.pga_target_create(d.h, C.byref(h)), "target_create")
+            if reuse:
+                d._ck(self.L.pga_target_create_reuse(d.h, freq, C.byref(h)), "target_create_reuse")
+            else:
+                d._ck(self.L.pga_target_create(d.h, C.byref(h)), "target_create")
         finally:
             d.close()
+        self.reuse = reuse
         self.h = h
         self.device = device
         a = np.zeros(4, dtype=np.int64)

@@ -211,7 +211,7 @@ class Server:
         d.merge(self.freq)
         n = d.align()
         out = {"nalign": n, "gdb_bases": int(sizes[5]), "query_bases": int(sizes[5]) - self.target.bases,
-               "records": d.nrec}
+               "records": d.nrec, "reuse": d.reuse_stats()}
         if self.keep:
             out["alignments"] = d.alignments()
         return out

@@ -55,3 +55,21 @@ def test_dropin_driver_defines_reference_signatures():
     assert all(re.search(r"\b%s\s*\(" % n, src) for n in names)
     ldd = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
     assert "libpga_b200.so" in ldd
+
+
+def test_wrappers_marshal_their_arguments():
+    """Wrappers whose entry points return before touching a device when the
+    context is null: their arguments marshal through the declared ctypes
+    signatures (no ArgumentError) and the library answers PGA_ERR_ARG."""
+    import numpy as np
+    import pytest
+    from distributedpanga_b200 import pipeline
+    d = object.__new__(pipeline.Device)
+    d.L = pipeline.load_library()
+    d.h = None
+    d.nseeds = [0, 0]
+    calls = [d.reuse_stats, d.alloc_times, d.stage_times, d.align_stats, d.align_times,
+             lambda: d.seeds_load(0, np.zeros(7, np.uint8))]
+    for call in calls:
+        with pytest.raises(pipeline.PgaError):
+            call()

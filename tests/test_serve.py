@@ -105,3 +105,42 @@ def test_served_mix_equals_plain_alone(small_target):
                 assert np.array_equal(a, b)
     finally:
         dp.close()
+
+
+def test_served_pair_reuse_equals_plain(dev):
+    """A target with a pair cache: a request's pairs of two target contigs
+    with the target run's seeds take the cached alignments, and every
+    request's alignments are still, bit for bit, the plain path's.  A query
+    contig longer than the target's longest changes the key layout: the
+    cache is not used and the result is the plain one all the same."""
+    from distributedpanga_b200 import pipeline, serve, synth
+    contigs = synth.make_target(scale=0.005)
+    ttext = synth.fasta_bytes(contigs, "t")
+    target = pipeline.Target(ttext, reuse=True)
+    dp = pipeline.Device(0)
+    try:
+        queries = [q for _, q in synth.query_stream(contigs, 3, 0.0, 20_000, 600_000, seed=23, median=100_000)]
+        longest = max(range(len(contigs)), key=lambda i: len(contigs[i]))
+        other = (longest + 1) % len(contigs)
+        queries.append([np.concatenate([contigs[longest], contigs[other]])])
+        used = 0
+        for k, q in enumerate(queries):
+            qtext = synth.fasta_bytes(q, "q%d_" % k)
+            dev.serve_load(target, qtext)
+            dev.merge(10)
+            n = dev.align()
+            st = dev.reuse_stats()
+            got = dev.alignments()
+            p = serve.plain_request(dp, ttext, qtext)
+            assert n == p["nalign"] > 0
+            for a, b in zip(got, p["alignments"]):
+                assert np.array_equal(a, b)
+            if k < 3:
+                assert st["used"] and st["not_used"] is None
+                used += st["pairs"]
+            else:
+                assert not st["used"] and st["not_used"] == "key layout differs"
+        assert used > 0
+    finally:
+        dp.close()
+        target.close()
