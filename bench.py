@@ -811,8 +811,9 @@ def serve_measure(args) -> dict:
     t = time.monotonic()
     # one replica of the target per GPU; rank r serves the requests whose id
     # is congruent to r
-    # with its pair cache: the target's own GDB aligned once, its pairs'
-    # results kept for requests whose target pairs have the same seeds
+    # with the record of its own Local_Alignment calls (the target's GDB
+    # aligned once more, every call kept) for the requests' calls on target
+    # contigs
     target = pipeline.Target(ttext, device=local_rank, reuse=True)
     target_s = time.monotonic() - t
     target_bases = target.bases
@@ -904,14 +905,15 @@ def serve_measure(args) -> dict:
         "plain": {k: round(v, 4) if isinstance(v, float) else v for k, v in psumm.items()},
         "served_over_plain": round(summ["gdb_mbp_per_s"] / psumm["gdb_mbp_per_s"], 3),
         "bit_exact_requests": "%d/%d" % (same, len(reqs)),
-        "pair_cache": {"requests_using_it": sum(1 for r in res if r.out["reuse"]["used"]),
-                       "alignments_from_cache": sum(r.out["reuse"]["alignments"] for r in res),
-                       "alignments": sum(r.out["nalign"] for r in res),
-                       "not_used": sorted({r.out["reuse"]["not_used"] for r in res if not r.out["reuse"]["used"]}),
-                       "target_build_s": round(target_s, 3)},
+        "call_record": {"requests_using_it": sum(1 for r in res if r.out["reuse"]["used"]),
+                        "calls_from_record": sum(r.out["reuse"]["calls_from_record"] for r in res),
+                        "calls": sum(r.out["reuse"]["calls"] for r in res),
+                        "not_used": sorted({r.out["reuse"]["not_used"] for r in res if not r.out["reuse"]["used"]}),
+                        "target_build_s": round(target_s, 3)},
         "requests": [{"rid": r.rid, "query_mbp": round(q.bases / 1e6, 3), "arrival_s": round(r.arrival, 3),
                       "served_latency_s": round(r.latency, 3), "plain_latency_s": round(p.latency, 3),
-                      "alignments": r.out["nalign"], "alignments_from_cache": r.out["reuse"]["alignments"],
+                      "alignments": r.out["nalign"], "calls_from_record": r.out["reuse"]["calls_from_record"],
+                      "calls": r.out["reuse"]["calls"],
                       "served_phases_s": [round(x, 3) for x in r.out["phases"]],
                       "plain_phases_s": [round(x, 3) for x in p.out["phases"]]}
                      for r, p, q in zip(res, pres, reqs)],
@@ -930,7 +932,7 @@ def serve_compact(m: dict) -> dict:
             "value": m["value"], "unit": "Mbp/s", "workload": m["config"]["workload"],
             "slots": m["config"]["slots"], "served": {k: m["served"][k] for k in keep},
             "plain": {k: m["plain"][k] for k in keep}, "served_over_plain": m["served_over_plain"],
-            "bit_exact_requests": m["bit_exact_requests"], "pair_cache": m["pair_cache"], "clocks": m["clocks"]}
+            "bit_exact_requests": m["bit_exact_requests"], "call_record": m["call_record"], "clocks": m["clocks"]}
 
 
 def main():

@@ -190,10 +190,74 @@ struct KeySeeds {
 struct WarpAligner {
   WarpWork &W;
   const AlignSpec &spec;
+  const CallMemo &M;
+  int a, b;  // the pair's contigs (A's and B's)
   __device__ int call(const Seq &A, const Seq &B, bool acomp, Path &P, int low, int hgh, int anti, int lbord,
                       int hbord) {
     const long long t0 = clock64();
+    const int lane = threadIdx.x & 31;
+    // a call on two target contigs: its recorded result, if the target's run made it
+    const bool keyed = (M.cap > 0 || M.lkey) && a < M.nt && b < M.nt;
+    uint32_t k[MEMO_KEY];
+    k[0] = (uint32_t)a | ((uint32_t)b << 15) | ((uint32_t)acomp << 30);
+    k[1] = (uint32_t)low;
+    k[2] = (uint32_t)hgh;
+    k[3] = (uint32_t)anti;
+    k[4] = (uint32_t)lbord;
+    k[5] = (uint32_t)hbord;
+    if (keyed && M.cap > 0) {
+      const uint64_t mask = (uint64_t)M.cap - 1;
+      for (uint64_t s = memo_hash(k) & mask, probe = 0; probe <= mask; probe++, s = (s + 1) & mask) {
+        const uint32_t *q = M.key + MEMO_KEY * s;
+        if (q[0] == 0xffffffffu) break;
+        bool same = true;
+        for (int i = 0; i < MEMO_KEY; i++) same &= q[i] == k[i];
+        if (!same) continue;
+        const int32_t *v = M.val + MEMO_VAL * s;
+        if (v[5] > W.point_cap) break;  // computed below, which reports the overflow
+        const uint8_t *tr = M.trace + M.toff[s];
+        for (int i = lane; i < v[5]; i += 32) W.points[i] = tr[i];
+        __syncwarp();
+        P.abpos = v[0];
+        P.aepos = v[1];
+        P.bbpos = v[2];
+        P.bepos = v[3];
+        P.diffs = v[4];
+        P.tlen = v[5];
+        P.trace_off = 0;
+        if (lane == 0) atomicAdd(M.hits, 1ull);
+        W.la_cycles += clock64() - t0;
+        return 0;
+      }
+    }
     const int r = local_alignment_w(W, spec, A, B, acomp, P, low, hgh, anti, lbord, hbord);
+    if (keyed && M.lkey && r == 0) {
+      // the target's own run: append the call to the log
+      unsigned long long e = 0, tb = 0;
+      if (lane == 0) {
+        e = atomicAdd(M.lnext, 1ull);
+        tb = atomicAdd(M.lbytes, (unsigned long long)P.tlen);
+      }
+      e = __shfl_sync(FULL, e, 0);
+      tb = __shfl_sync(FULL, tb, 0);
+      if ((int64_t)e < M.lcap) {
+        const bool fits = (int64_t)(tb + P.tlen) <= M.lbytes_cap;
+        if (fits)
+          for (int i = lane; i < P.tlen; i += 32) M.ltrace[tb + i] = (uint8_t)W.points[P.trace_off + i];
+        if (lane == 0) {
+          for (int i = 0; i < MEMO_KEY; i++) M.lkey[MEMO_KEY * e + i] = k[i];
+          int32_t *v = M.lval + MEMO_VAL * e;
+          v[0] = P.abpos;
+          v[1] = P.aepos;
+          v[2] = P.bbpos;
+          v[3] = P.bepos;
+          v[4] = P.diffs;
+          v[5] = P.tlen;
+          M.ltoff[e] = fits ? (int64_t)tb : -1;
+        }
+      }
+      __syncwarp();
+    }
     W.la_cycles += clock64() - t0;
     return r;
   }
@@ -455,10 +519,7 @@ __device__ __forceinline__ PairTask small_task(const AlignLaunch &P, uint64_t co
 // A warp's running reduction of its device-planned pairs' outcomes (lane 0).
 struct SmallSums {
   unsigned long long calls = 0, cycles = 0, maxkey = 0, err = 0, waves = 0, cells = 0, bad = ~0ull;
-  __device__ void add(const AlignLaunch &P, const PairTask &tk, const PairOut &po, unsigned t, uint64_t code) {
-    if (P.cap_fo[tk.comp])
-      P.cap_fo[tk.comp][code & 0x7fffffffffffffffull] =
-          po.calls > 0 ? (1ull << 32) | (uint32_t)po.exit_bepos : 0ull;
+  __device__ void add(const AlignLaunch &P, const PairTask &tk, const PairOut &po, unsigned t) {
     calls += (unsigned long long)po.calls;
     cycles += (unsigned long long)po.cycles;
     const unsigned long long k = ((unsigned long long)po.cycles << 16) | (unsigned)min(po.calls, 65535);
@@ -537,7 +598,7 @@ __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch
       bhi = next_band_start(S, tk.shi - tk.lo, S.n, lane);
     }
     PairResult R;
-    WarpAligner AL{W, spec};
+    WarpAligner AL{W, spec, P.memo, tk.a, tk.b};
     const uint16_t *info = (tk.comp ? P.infoC : P.infoN) + tk.lo;
     int rc = align_pair_dev(S, info, tk.comp != 0, tk.self != 0, A, B, P.amxpos, P.maxdag, AL, path, O, R, lane,
                             blo, bhi);
@@ -573,7 +634,7 @@ __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch
     }
     if (lane == 0) {
       if (t < (unsigned)P.ntasks) P.pout[t] = po;
-      else sums.add(P, tk, po, t, P.small[t - P.ntasks]);
+      else sums.add(P, tk, po, t);
     }
     __syncwarp();
   }
@@ -880,11 +941,10 @@ __device__ __forceinline__ bool pair_hostbound(const int64_t *pstart, const int3
 }
 
 __global__ void k_pair_hostbound(const int64_t *__restrict__ pstart, const int32_t *__restrict__ pab, int64_t np,
-                                 int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ flag,
-                                 const uint32_t *__restrict__ reuse) {
+                                 int64_t nseeds, int comp, int64_t rs, uint32_t *__restrict__ flag) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
     int64_t size;
-    flag[p] = pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) && !(reuse && reuse[p]) ? 1u : 0u;
+    flag[p] = pair_hostbound(pstart, pab, np, nseeds, comp, rs, p, &size) ? 1u : 0u;
   }
 }
 
@@ -968,10 +1028,10 @@ __global__ void k_small_scatter(const int64_t *__restrict__ pstart, const int32_
 }
 
 void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                           uint32_t *flag, const uint32_t *reuse, cudaStream_t st) {
+                           uint32_t *flag, cudaStream_t st) {
   if (np <= 0) return;
   k_pair_hostbound<<<(int)std::min<int64_t>((np + 255) / 256, 148 * 32), 256, 0, st>>>(pstart, pab, np, nseeds, comp,
-                                                                                     rs, flag, reuse);
+                                                                                     rs, flag);
 }
 
 void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
@@ -1083,115 +1143,6 @@ void launch_aln_traces(AlnRec *recs, const int64_t *off, int64_t n, const uint8_
   if (n <= 0) return;
   const int g = (int)std::min<int64_t>((n + 7) / 8, 148 * 16);
   k_aln_traces<<<g, 256, 0, st>>>(recs, off, n, src, dst);
-}
-
-
-// ---- a resident target's pair cache ------------------------------------------
-// A pair of two target contigs (not a self pair) whose seeds are exactly those
-// of the target's own run makes exactly that run's alignments: a non-self
-// pair's alignments depend only on its seeds, the two contigs' bases and the
-// scoring tables (the caller checks that the layout of the low key bits and
-// the tables are the target run's).
-
-__global__ void k_pair_reuse(const U128 *__restrict__ keys, const int64_t *__restrict__ pstart,
-                             const int32_t *__restrict__ pab, int64_t np, int64_t nseeds, int comp, int nT,
-                             uint64_t lowmask, ReuseUnit U, uint32_t *__restrict__ reuse, uint8_t *__restrict__ live,
-                             unsigned long long *__restrict__ list, unsigned long long *__restrict__ count) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t p = w0; p < np; p += nw) {
-    const int a = pab[2 * p], b = pab[2 * p + 1];
-    const int64_t lo = pstart[p], hi = p + 1 < np ? pstart[p + 1] : nseeds;
-    int64_t e = -1;
-    if (a < nT && b < nT && !(comp == 0 && a == b) && U.n > 0) {
-      const uint64_t want = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
-      int64_t l = 0, h = U.n;  // first entry >= want
-      while (l < h) {
-        const int64_t m = (l + h) >> 1;
-        if (U.key[m] < want) l = m + 1;
-        else h = m;
-      }
-      if (l < U.n && U.key[l] == want && U.seg_len[l] == hi - lo) e = l;
-    }
-    bool same = e >= 0;
-    if (same) {
-      const uint64_t *c = U.low + U.seg_off[e];
-      bool diff = false;
-      for (int64_t k = lane; k < hi - lo; k += 32) diff |= (keys[lo + k].lo & lowmask) != c[k];
-      same = !__any_sync(0xffffffffu, diff);
-    }
-    if (lane == 0) {
-      reuse[p] = same ? (uint32_t)(e + 1) : 0u;
-      if (same) {
-        live[p] = 0;
-        list[atomicAdd(count, 1ull)] = ((unsigned long long)comp << 63) | (unsigned long long)e;
-      }
-    }
-  }
-}
-
-__global__ void k_reuse_emit(const unsigned long long *__restrict__ list, int64_t n, ReuseUnit U0, ReuseUnit U1,
-                             const AlnRec *__restrict__ crecs, const uint8_t *__restrict__ ctrace,
-                             AlnRec *__restrict__ recs, uint8_t *__restrict__ out,
-                             unsigned long long *__restrict__ rec_next, unsigned long long *__restrict__ out_next,
-                             int64_t rec_cap, int64_t out_cap, int *__restrict__ err) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t q = w0; q < n; q += nw) {
-    const unsigned long long code = list[q];
-    const ReuseUnit &U = (code >> 63) ? U1 : U0;
-    const int64_t e = (int64_t)(code & 0x7fffffffffffffffull);
-    const int cnt = U.rec_cnt[e];
-    if (cnt == 0) continue;
-    const int64_t r0 = U.rec_off[e], t0 = U.tr_off[e], tl = U.tr_len[e];
-    unsigned long long rb = 0, bb = 0;
-    if (lane == 0) {
-      rb = atomicAdd(rec_next, (unsigned long long)cnt);
-      bb = atomicAdd(out_next, (unsigned long long)tl);
-    }
-    rb = __shfl_sync(0xffffffffu, rb, 0);
-    bb = __shfl_sync(0xffffffffu, bb, 0);
-    if ((int64_t)(rb + cnt) > rec_cap || (int64_t)(bb + tl) > out_cap) {
-      if (lane == 0) atomicExch(err, 1);
-      continue;
-    }
-    for (int k = lane; k < cnt; k += 32) {
-      AlnRec r = crecs[r0 + k];
-      r.toff = (int64_t)bb + (r.toff - t0);
-      recs[rb + k] = r;
-    }
-    for (int64_t k = lane; k < tl; k += 32) out[bb + k] = ctrace[t0 + k];
-  }
-}
-
-__global__ void k_key_low(const U128 *__restrict__ keys, int64_t n, uint64_t lowmask, uint64_t *__restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = keys[i].lo & lowmask;
-}
-
-void launch_pair_reuse(const U128 *keys, const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds,
-                       int comp, int nT, uint64_t lowmask, ReuseUnit U, uint32_t *reuse, uint8_t *live,
-                       unsigned long long *list, unsigned long long *count, cudaStream_t st) {
-  if (np <= 0) return;
-  const int g = (int)std::min<int64_t>((np + 7) / 8, 148 * 32);
-  k_pair_reuse<<<g, 256, 0, st>>>(keys, pstart, pab, np, nseeds, comp, nT, lowmask, U, reuse, live, list, count);
-}
-
-void launch_reuse_emit(const unsigned long long *list, int64_t n, ReuseUnit U0, ReuseUnit U1, const AlnRec *crecs,
-                       const uint8_t *ctrace, AlnRec *recs, uint8_t *out, unsigned long long *rec_next,
-                       unsigned long long *out_next, int64_t rec_cap, int64_t out_cap, int *err, cudaStream_t st) {
-  if (n <= 0) return;
-  const int g = (int)std::min<int64_t>((n + 7) / 8, 148 * 16);
-  k_reuse_emit<<<g, 256, 0, st>>>(list, n, U0, U1, crecs, ctrace, recs, out, rec_next, out_next, rec_cap, out_cap,
-                                  err);
-}
-
-void launch_key_low(const U128 *keys, int64_t n, uint64_t lowmask, uint64_t *out, cudaStream_t st) {
-  if (n <= 0) return;
-  const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
-  k_key_low<<<g, 256, 0, st>>>(keys, n, lowmask, out);
 }
 
 }  // namespace pga

@@ -44,6 +44,44 @@ struct AlnRec {
   int64_t toff;
 };
 
+// A resident target's Local_Alignment results (pga_target_create_reuse).
+// A call's result -- the path and its trace points -- is a function of its
+// inputs: the two contigs (their bases), the orientation, low, hgh, anti,
+// lbord, hbord, and the scoring tables.  The target's own run appends every
+// call to a log (capture); a request's calls on two target contigs look
+// their inputs up in a table built from it and take the recorded result
+// instead of running the wave loop.
+struct CallMemo {
+  // table of cap slots (a power of two; 0: none), MEMO_KEY words of key per
+  // slot (word 0 all ones: empty), MEMO_VAL of value (abpos, aepos, bbpos,
+  // bepos, diffs, tlen), and the offset of its trace bytes in trace
+  const uint32_t *key;
+  const int32_t *val;
+  const int64_t *toff;
+  const uint8_t *trace;
+  int64_t cap;
+  int nt;                      // the target's contigs: 0 .. nt-1
+  unsigned long long *hits;    // calls answered from the table
+  // capture log (lkey null: off): up to lcap calls, lbytes_cap trace bytes
+  uint32_t *lkey;
+  int32_t *lval;
+  int64_t *ltoff;
+  uint8_t *ltrace;
+  unsigned long long *lnext, *lbytes;
+  int64_t lcap, lbytes_cap;
+};
+constexpr int MEMO_KEY = 6, MEMO_VAL = 6;
+
+__host__ __device__ inline uint64_t memo_hash(const uint32_t *k) {
+  uint64_t h = 0x243f6a8885a308d3ull;
+  for (int i = 0; i < MEMO_KEY; i++) {
+    h ^= k[i];
+    h *= 0x9e3779b97f4a7c15ull;
+    h ^= h >> 29;
+  }
+  return h;
+}
+
 struct AlignLaunch {
   const PairTask *tasks;
   int ntasks;
@@ -52,10 +90,7 @@ struct AlignLaunch {
   // SM cycles the launch's warps spent in Local_Alignment [0] and in the
   // pairs' finishing step [1], zero at launch
   unsigned long long *prof;
-  // per pair of unit u (null: off): (1 << 32 | exit_bepos) when the
-  // device-planned pair made a call, else 0 -- recorded for a resident
-  // target's pair cache
-  unsigned long long *cap_fo[2];
+  CallMemo memo;
   int long_waves;     // a wave loop past this many waves flags its SM
   const U128 *keysN, *keysC;
   // per seed of each unit: band start (bit 15), previous band of the pair
@@ -131,7 +166,7 @@ struct AlignLaunch {
 // CHAIN_MIN) as `small` codes, largest first (sizes clamped to 65535).
 constexpr int SMALL_BINS = 65536;
 void launch_pair_hostbound(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, int comp, int64_t rs,
-                           uint32_t *flag, const uint32_t *reuse, cudaStream_t st);
+                           uint32_t *flag, cudaStream_t st);
 void launch_pair_gather(const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds, const uint32_t *flag,
                         const uint32_t *idx, int64_t *out3, cudaStream_t st);
 void launch_pair_live(const uint16_t *info, int64_t n, const uint32_t *pflag, const uint32_t *pidx, uint8_t *live,
@@ -164,33 +199,5 @@ void launch_aln_gather(const U128 *keys, int64_t n, const AlnRec *in, AlnRec *ou
 void launch_aln_traces(AlnRec *recs, const int64_t *off, int64_t n, const uint8_t *src, uint8_t *dst,
                        cudaStream_t st);
 
-// One unit of a resident target's pair cache: the target's own run's
-// non-self pairs that had work, by (a << 32 | b) ascending; each with its
-// seeds' low key bits (the bits below the contig fields) at low[seg_off ..
-// seg_off + seg_len), its surviving alignments at recs[rec_off .. rec_off +
-// rec_cnt) in rank order, whose traces lie at tr[tr_off .. tr_off + tr_len).
-struct ReuseUnit {
-  const uint64_t *key;
-  const int64_t *seg_off, *seg_len, *rec_off, *tr_off, *tr_len;
-  const int32_t *rec_cnt;
-  const uint64_t *low;
-  int64_t n;
-};
-
-// reuse[p] = entry + 1 when pair p of the unit (both contigs below nT, not a
-// self pair) has exactly the cached entry's seeds (low key bits under
-// lowmask, in order), else 0; a reused pair's live flag is cleared and
-// (unit << 63 | entry) is appended to list (count at *count).
-void launch_pair_reuse(const U128 *keys, const int64_t *pstart, const int32_t *pab, int64_t np, int64_t nseeds,
-                       int comp, int nT, uint64_t lowmask, ReuseUnit U, uint32_t *reuse, uint8_t *live,
-                       unsigned long long *list, unsigned long long *count, cudaStream_t st);
-// The cached alignments of the listed entries appended to the launch's
-// record and trace pools (rec_next / out_next), toff rewritten; err set when
-// a pool is too small.
-void launch_reuse_emit(const unsigned long long *list, int64_t n, ReuseUnit U0, ReuseUnit U1, const AlnRec *crecs,
-                       const uint8_t *ctrace, AlnRec *recs, uint8_t *out, unsigned long long *rec_next,
-                       unsigned long long *out_next, int64_t rec_cap, int64_t out_cap, int *err, cudaStream_t st);
-// out[i] = keys[i].lo & lowmask
-void launch_key_low(const U128 *keys, int64_t n, uint64_t lowmask, uint64_t *out, cudaStream_t st);
 
 }  // namespace pga

@@ -1,8 +1,6 @@
 // C-ABI layer: context, device buffers, stage drivers and the drop-in entry
 // points declared in include/pga_b200.h.
 #include <algorithm>
-#include <array>
-#include <map>
 #include <cstdarg>
 #include <chrono>
 #include <cstdint>
@@ -103,19 +101,19 @@ struct pga_ctx {
   DBuf keys[2], dlook, dsmall, panel[2];
   U128 *sorted[2] = {nullptr, nullptr};
   bool seeds_consumed[2] = {false, false};  // the unit's seed buffer was used by its diagonal sort
-  // served requests: the resident target whose pair cache pga_align may use
-  // (set by pga_serve_load), buffers of that check, and its outcome for the
-  // last alignment: {used, pairs reused, alignments reused, reason it was
-  // not used: 0 none, 1 no cache, 2 key layout, 3 scoring tables}
+  // served requests: the resident target whose recorded Local_Alignment
+  // calls pga_align may use (set by pga_serve_load), the hit counter, and
+  // the outcome for the last alignment: {used, calls answered from the
+  // record, calls made, reason it was not used: 0 none, 1 no record,
+  // 3 scoring tables differ}
   const pga_target *reuse_t = nullptr;
-  DBuf reuse_map[2], reuse_list, reuse_cnt;
+  DBuf memo_hits;
   int64_t reuse_stats[4] = {0, 0, 0, 0};
-  // recording a target's own run (pga_target_create_reuse): per device pair
-  // its call flag and exit bepos; per host-planned pair {comp, a, b, value}
+  // recording a target's own run (pga_target_create_reuse): the log of its
+  // calls, sized for cap_calls calls and cap_bytes trace bytes
   bool capture = false;
-  DBuf cap_fo[2];
-  std::vector<std::array<int64_t, 4>> cap_host;
-  int64_t cap_np[2] = {0, 0}, cap_rs = 0;
+  DBuf mlog_key, mlog_val, mlog_toff, mlog_trace, mlog_ctr;
+  int64_t cap_calls = 0, cap_bytes = 0;
   // the scoring tables of the last alignment
   std::vector<int16_t> spec_host;
   int ave_path_host = 0;
@@ -176,22 +174,16 @@ struct pga_target {
   std::vector<char> headers;
   int64_t base_count[4] = {0, 0, 0, 0};
   DBuf bps, rec, start;  // sequence image, sorted records, prefix table (NPREFIX + 1)
-  // The target's own run's pairs, for requests whose pairs of two target
-  // contigs have the same seeds (pga_target_create_reuse): per unit the
-  // entries of a ReuseUnit, their low key bits, alignments and traces; the
-  // key layout and scoring tables they were made with; per entry, whether
-  // the pair called and its exit bepos (FastGA's order keys, N unit).
-  struct Reuse {
+  // The target's own run's Local_Alignment calls (pga_target_create_reuse):
+  // a table of their inputs and results (CallMemo), and the scoring tables
+  // they were made with.
+  struct Memo {
     bool valid = false;
-    SeedKeyLayout lay[2];
     std::vector<int16_t> spec;
     int ave_path = 0;
-    int64_t n[2] = {0, 0};
-    std::vector<uint64_t> hkey[2], hfo[2];
-    std::vector<int32_t> hcnt[2];
-    std::vector<int64_t> htrl[2];
-    DBuf key[2], seg_off[2], seg_len[2], rec_off[2], rec_cnt[2], tr_off[2], tr_len[2], low[2], recs, trace;
-  } reuse;
+    int64_t entries = 0, cap = 0;
+    DBuf key, val, toff, trace;
+  } memo;
 };
 
 namespace {
@@ -257,8 +249,8 @@ bool shed_align_buffers(pga_ctx *ctx) {
                   &ctx->pidx, &ctx->pstart, &ctx->pab, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->ftasks,
                   &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->lreq, &ctx->lpath, &ctx->ltoff, &ctx->ltrace,
                   &ctx->binfo[0], &ctx->binfo[1], &ctx->plive[0], &ctx->plive[1], &ctx->skeys, &ctx->skeys2,
-                  &ctx->lhist, &ctx->lscan, &ctx->reuse_map[0], &ctx->reuse_map[1], &ctx->reuse_list,
-                  &ctx->reuse_cnt, &ctx->cap_fo[0], &ctx->cap_fo[1]};
+                  &ctx->lhist, &ctx->lscan, &ctx->memo_hits, &ctx->mlog_key, &ctx->mlog_val, &ctx->mlog_toff,
+                  &ctx->mlog_trace, &ctx->mlog_ctr};
   bool any = false;
   for (DBuf *b : bufs)
     if (b->p) {
@@ -1247,50 +1239,47 @@ int run_align(pga_ctx *ctx) {
   std::vector<PairTask> pairs[2];
   int64_t npairs[2] = {0, 0};
   DBuf *dpst[2] = {&ctx->pstart, &ctx->pstart2}, *dpab[2] = {&ctx->pab, &ctx->pab2};
-  // A resident target's pair cache (requests of the served form): used when
-  // this GDB's low key bits are laid out as in the target's run and the
-  // scoring tables are the same; pairs of two target contigs with the same
-  // seeds then take the cached alignments instead of tasks.
+  // A resident target's Local_Alignment results (requests of the served
+  // form): used when the scoring tables are those of the target's run; the
+  // target's own run records them (capture)
   const pga_target *rt = ctx->reuse_t;
-  bool reuse_on = false;
-  ReuseUnit RU[2] = {};
-  uint64_t lowmask[2] = {0, 0};
   for (int i = 0; i < 4; i++) ctx->reuse_stats[i] = 0;
+  bool memo_on = false;
   if (rt) {
-    const pga_target::Reuse &R = rt->reuse;
-    int why = R.valid ? 0 : 1;
-    for (int u = 0; u < 2 && !why; u++) {
-      const SeedKeyLayout &a = R.lay[u], &b = ctx->lay[u];
-      if (a.comp != b.comp || a.amxpos != b.amxpos || a.bmxpos != b.bmxpos || a.maxdag != b.maxdag ||
-          a.dmask != b.dmask || a.dbyte != b.dbyte || a.off_dlow != b.off_dlow || a.off_anti != b.off_anti ||
-          a.off_band != b.off_band || a.off_j != b.off_j || b.off_j > 64)
-        why = 2;
-    }
-    if (!why && (R.spec != ctx->spec_host || R.ave_path != ctx->ave_path_host)) why = 3;
+    const pga_target::Memo &M = rt->memo;
+    int why = M.valid ? 0 : 1;
+    if (!why && (M.spec != ctx->spec_host || M.ave_path != ctx->ave_path_host)) why = 3;
     ctx->reuse_stats[3] = why;
     if (!why) {
-      reuse_on = true;
-      for (int u = 0; u < 2; u++) {
-        RU[u].key = P<uint64_t>(R.key[u]);
-        RU[u].seg_off = P<int64_t>(R.seg_off[u]);
-        RU[u].seg_len = P<int64_t>(R.seg_len[u]);
-        RU[u].rec_off = P<int64_t>(R.rec_off[u]);
-        RU[u].tr_off = P<int64_t>(R.tr_off[u]);
-        RU[u].tr_len = P<int64_t>(R.tr_len[u]);
-        RU[u].rec_cnt = P<int32_t>(R.rec_cnt[u]);
-        RU[u].low = P<uint64_t>(R.low[u]);
-        RU[u].n = R.n[u];
-        lowmask[u] = ctx->lay[u].off_j >= 64 ? ~0ull : ((1ull << ctx->lay[u].off_j) - 1);
-      }
-      ENSURE(ctx->reuse_list, sizeof(unsigned long long) * (size_t)(R.n[0] + R.n[1] + 1));
-      ENSURE(ctx->reuse_cnt, 16);
-      CK(cudaMemsetAsync(ctx->reuse_cnt.p, 0, 16, ctx->st));
+      memo_on = true;
+      L.memo.key = P<uint32_t>(M.key);
+      L.memo.val = P<int32_t>(M.val);
+      L.memo.toff = P<int64_t>(M.toff);
+      L.memo.trace = P<uint8_t>(M.trace);
+      L.memo.cap = M.cap;
+      L.memo.nt = rt->ncontig;
+      ENSURE(ctx->memo_hits, 16);
+      CK(cudaMemsetAsync(ctx->memo_hits.p, 0, 16, ctx->st));
+      L.memo.hits = P<unsigned long long>(ctx->memo_hits);
     }
   }
   if (ctx->capture) {
-    ctx->cap_host.clear();
-    ctx->cap_rs = RS;
-    ctx->cap_np[0] = ctx->cap_np[1] = 0;
+    const int64_t lc = ctx->cap_calls > 0 ? ctx->cap_calls : 1, lb = ctx->cap_bytes > 0 ? ctx->cap_bytes : 16;
+    ENSURE(ctx->mlog_key, sizeof(uint32_t) * MEMO_KEY * (size_t)lc);
+    ENSURE(ctx->mlog_val, sizeof(int32_t) * MEMO_VAL * (size_t)lc);
+    ENSURE(ctx->mlog_toff, sizeof(int64_t) * (size_t)lc);
+    ENSURE(ctx->mlog_trace, (size_t)lb);
+    ENSURE(ctx->mlog_ctr, 16);
+    CK(cudaMemsetAsync(ctx->mlog_ctr.p, 0, 16, ctx->st));
+    L.memo.nt = nc;  // every contig is the target's
+    L.memo.lkey = P<uint32_t>(ctx->mlog_key);
+    L.memo.lval = P<int32_t>(ctx->mlog_val);
+    L.memo.ltoff = P<int64_t>(ctx->mlog_toff);
+    L.memo.ltrace = P<uint8_t>(ctx->mlog_trace);
+    L.memo.lnext = P<unsigned long long>(ctx->mlog_ctr);
+    L.memo.lbytes = L.memo.lnext + 1;
+    L.memo.lcap = lc;
+    L.memo.lbytes_cap = lb;
   }
   for (int comp = 0; comp < 2; comp++) {
     int64_t n = ctx->nseed[comp];
@@ -1320,24 +1309,8 @@ int run_align(pga_ctx *ctx) {
     launch_pair_live(P<uint16_t>(ctx->binfo[comp]), n, P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx),
                      P<uint8_t>(ctx->plive[comp]), ctx->st);
     LAUNCHED(1);
-    // pairs with the cached seeds of the target's run: no task
-    uint32_t *rmap = nullptr;
-    if (reuse_on) {
-      ENSURE(ctx->reuse_map[comp], sizeof(uint32_t) * (size_t)(np + 1));
-      rmap = P<uint32_t>(ctx->reuse_map[comp]);
-      launch_pair_reuse(ctx->sorted[comp], pst, pab, np, n, comp, rt->ncontig, lowmask[comp], RU[comp], rmap,
-                        P<uint8_t>(ctx->plive[comp]), P<unsigned long long>(ctx->reuse_list),
-                        P<unsigned long long>(ctx->reuse_cnt), ctx->st);
-      LAUNCHED(np > 0 ? 1 : 0);
-    }
-    if (ctx->capture) {
-      ENSURE(ctx->cap_fo[comp], sizeof(unsigned long long) * (size_t)(np + 1));
-      CK(cudaMemsetAsync(ctx->cap_fo[comp].p, 0, sizeof(unsigned long long) * (size_t)(np + 1), ctx->st));
-      L.cap_fo[comp] = P<unsigned long long>(ctx->cap_fo[comp]);
-      ctx->cap_np[comp] = np;
-    }
     // the host's pairs
-    launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), rmap, ctx->st);
+    launch_pair_hostbound(pst, pab, np, n, comp, RS, P<uint32_t>(ctx->pflag), ctx->st);
     CK(exclusive_scan<uint32_t>(P<uint32_t>(ctx->pflag), P<uint32_t>(ctx->pidx), np, P<uint32_t>(ctx->scan_tmp), tot,
                                 ctx->st));
     LAUNCHED(5);
@@ -1567,40 +1540,8 @@ int run_align(pga_ctx *ctx) {
     }
   }
   L.nsmall = 0;  // the later launches run host-planned tasks only
-  // the reused pairs: N pairs that called enter FastGA's order keys (their
-  // alignments join the others before the final order)
-  std::vector<unsigned long long> rlist;
-  if (reuse_on) {
-    unsigned long long nr = 0;
-    CK(cudaMemcpyAsync(&nr, ctx->reuse_cnt.p, 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    rlist.resize(nr);
-    if (nr > 0) {
-      CK(cudaMemcpyAsync(rlist.data(), ctx->reuse_list.p, 8 * nr, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaStreamSynchronize(ctx->st));
-    }
-    ctx->reuse_stats[0] = 1;
-    ctx->reuse_stats[1] = (int64_t)nr;
-    for (unsigned long long code : rlist) {
-      const int u = (int)(code >> 63);
-      const int64_t e = (int64_t)(code & 0x7fffffffffffffffull);
-      ctx->reuse_stats[2] += rt->reuse.hcnt[u][e];
-      const uint64_t fo = rt->reuse.hfo[u][e];
-      if (u != 0 || !(fo >> 32)) continue;
-      const int a = (int)(rt->reuse.hkey[u][e] >> 32), b = (int)(uint32_t)rt->reuse.hkey[u][e];
-      const int xa = F.pos[a], xb = F.pos[b];
-      const int64_t key = fo_key(xb, (int)(uint32_t)fo);
-      if (key > Lk[xa]) Lk[xa] = key;
-      if (xb < xa && key > ebest[xa]) ebest[xa] = key;
-    }
-  }
   std::vector<PairOut> out1(first.size());
   for (size_t i = 0; i < first.size(); i++) {
-    if (ctx->capture) {
-      const PairOut &po = first_task[i] >= 0 ? tout[first_task[i]] : fout[first_fin[i]];
-      ctx->cap_host.push_back(
-          {first[i].comp, first[i].a, first[i].b, po.calls > 0 ? ((int64_t)1 << 32) | (uint32_t)po.exit_bepos : 0});
-    }
     if (first_task[i] >= 0) {
       out1[i] = tout[first_task[i]];
     } else {
@@ -1770,38 +1711,14 @@ int run_align(pga_ctx *ctx) {
 
   const double t_order = now_ms();
   // 7. survivors in la_sort order: (aread, abpos, bread, comp), ties in the
-  // pair's own output order (src/fastga_pipeline.c:1500-1515), on the device;
-  // first the reused pairs' cached alignments join the pools
-  if (!rlist.empty()) {
-    int64_t add_r = 0, add_b = 0;
-    for (unsigned long long code : rlist) {
-      const int u = (int)(code >> 63);
-      const int64_t e = (int64_t)(code & 0x7fffffffffffffffull);
-      add_r += rt->reuse.hcnt[u][e];
-      add_b += rt->reuse.htrl[u][e];
-    }
-    if (add_r > 0) {
-      unsigned long long cur[2];
-      CK(cudaMemcpyAsync(&cur[0], ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaMemcpyAsync(&cur[1], ctx->out_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaStreamSynchronize(ctx->st));
-      int r = grow_keep(ctx, ctx->recs, sizeof(AlnRec) * (size_t)(cur[0] + add_r) + 16, sizeof(AlnRec) * cur[0]);
-      if (!r) r = grow_keep(ctx, ctx->outb, (size_t)(cur[1] + add_b) + 16, cur[1]);
-      if (r) return r;
-      ENSURE(ctx->u64tmp, 64);
-      int *err = P<int>(ctx->u64tmp);
-      CK(cudaMemsetAsync(err, 0, 4, ctx->st));
-      launch_reuse_emit(P<unsigned long long>(ctx->reuse_list), (int64_t)rlist.size(), RU[0], RU[1],
-                        P<AlnRec>(rt->reuse.recs), P<uint8_t>(rt->reuse.trace), P<AlnRec>(ctx->recs),
-                        P<uint8_t>(ctx->outb), P<unsigned long long>(ctx->rec_next),
-                        P<unsigned long long>(ctx->out_next), (int64_t)(ctx->recs.cap / sizeof(AlnRec)),
-                        (int64_t)ctx->outb.cap, err, ctx->st);
-      LAUNCHED(1);
-      int bad = 0;
-      CK(cudaMemcpyAsync(&bad, err, 4, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaStreamSynchronize(ctx->st));
-      if (bad) return fail(ctx, PGA_ERR_CUDA, "reused alignments overflowed the record pools");
-    }
+  // pair's own output order (src/fastga_pipeline.c:1500-1515), on the device
+  if (memo_on) {
+    unsigned long long hits = 0;
+    CK(cudaMemcpyAsync(&hits, ctx->memo_hits.p, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->reuse_stats[0] = 1;
+    ctx->reuse_stats[1] = (int64_t)hits;
+    ctx->reuse_stats[2] = calls;
   }
   unsigned long long nrec = 0, nbytes = 0;
   CK(cudaMemcpyAsync(&nrec, ctx->rec_next.p, 8, cudaMemcpyDeviceToHost, ctx->st));
@@ -1866,8 +1783,8 @@ void pga_ctx_destroy(pga_ctx *ctx) {
                    &ctx->fout, &ctx->ridx, &ctx->rout, &ctx->selfb, &ctx->lreq, &ctx->lpath, &ctx->ltoff,
                    &ctx->ltrace, &ctx->lnext, &ctx->pstart2, &ctx->pab2, &ctx->small, &ctx->shist, &ctx->fo_dev,
                    &ctx->srecs, &ctx->slen, &ctx->strace, &ctx->skeys, &ctx->skeys2, &ctx->lhist, &ctx->lscan,
-                   &ctx->reuse_map[0], &ctx->reuse_map[1], &ctx->reuse_list, &ctx->reuse_cnt, &ctx->cap_fo[0],
-                   &ctx->cap_fo[1]};
+                   &ctx->memo_hits, &ctx->mlog_key, &ctx->mlog_val, &ctx->mlog_toff, &ctx->mlog_trace,
+                   &ctx->mlog_ctr};
   for (DBuf *b : abufs) ctx->arena.release(b->p);
   DBuf *bufs[] = {&ctx->bps, &ctx->dclen, &ctx->dboff, &ctx->tile_ctg, &ctx->tile_j0, &ctx->hist, &ctx->start,
                   &ctx->scan_tmp, &ctx->rec, &ctx->rec2, &ctx->lcp, &ctx->ent, &ctx->cum, &ctx->qmed,
@@ -2728,115 +2645,60 @@ int target_upload(pga_ctx *ctx, DBuf &b, const void *src, size_t bytes) {
   return PGA_OK;
 }
 
-// The target's pair cache from the context's recorded run of the target's
-// own GDB: per unit, every non-self pair that had work (live, or run in
-// ranges) with its seeds, its call flag / exit bepos and its alignments.
-int build_reuse(pga_ctx *ctx, pga_target *t) {
-  int r = host_alignments(ctx);
-  if (r) return r;
-  pga_target::Reuse &R = t->reuse;
-  auto K = [](int u, int a, int b) {
-    return ((uint64_t)u << 63) | ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
-  };
-  std::map<uint64_t, std::vector<int64_t>> byp;  // a pair's alignments, in rank order
-  int64_t nonself = 0;
-  for (int64_t i = 0; i < (int64_t)ctx->h_recs.size(); i++) {
-    const AlnRec &x = ctx->h_recs[i];
-    if (x.comp == 0 && x.aread == x.bread) continue;
-    byp[K(x.comp, x.aread, x.bread)].push_back(i);
-    nonself++;
+// The target's table of Local_Alignment calls from the context's log of its
+// own run: every logged call whose trace was kept, once per distinct input,
+// in an open-addressing table of twice as many slots (a power of two).
+int build_memo(pga_ctx *ctx, pga_target *t) {
+  unsigned long long ctr[2];
+  CK(cudaMemcpyAsync(ctr, ctx->mlog_ctr.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  const int64_t e = std::min<int64_t>((int64_t)ctr[0], ctx->cap_calls);
+  const int64_t tb = std::min<int64_t>((int64_t)ctr[1], ctx->cap_bytes);
+  std::vector<uint32_t> lk(MEMO_KEY * (size_t)e);
+  std::vector<int32_t> lv(MEMO_VAL * (size_t)e);
+  std::vector<int64_t> lt(e);
+  if (e > 0) {
+    CK(cudaMemcpyAsync(lk.data(), ctx->mlog_key.p, 4 * lk.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(lv.data(), ctx->mlog_val.p, 4 * lv.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(lt.data(), ctx->mlog_toff.p, 8 * lt.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
   }
-  for (auto &kv : byp)
-    std::sort(kv.second.begin(), kv.second.end(),
-              [&](int64_t x, int64_t y) { return ctx->h_recs[x].rank < ctx->h_recs[y].rank; });
-  std::map<uint64_t, int64_t> hostfo;
-  for (const auto &h : ctx->cap_host) hostfo[K((int)h[0], (int)h[1], (int)h[2])] = h[3];
-  std::vector<AlnRec> crecs;
-  std::vector<uint8_t> ctr;
-  int64_t matched = 0;
-  bool ok = true;
-  DBuf *dpst[2] = {&ctx->pstart, &ctx->pstart2}, *dpab[2] = {&ctx->pab, &ctx->pab2};
-  for (int u = 0; u < 2; u++) {
-    const int64_t np = ctx->cap_np[u], n = ctx->nseed[u];
-    std::vector<int64_t> pst(np + 1), key, soff, slen, roff, toff, tlen;
-    std::vector<int32_t> pab(2 * np + 2), rcnt;
-    std::vector<uint8_t> live(np + 1);
-    std::vector<uint64_t> cfo(np + 1), fo;
-    if (np > 0) {
-      CK(cudaMemcpyAsync(pst.data(), dpst[u]->p, sizeof(int64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaMemcpyAsync(pab.data(), dpab[u]->p, sizeof(int32_t) * 2 * np, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaMemcpyAsync(live.data(), ctx->plive[u].p, np, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaMemcpyAsync(cfo.data(), ctx->cap_fo[u].p, sizeof(uint64_t) * np, cudaMemcpyDeviceToHost, ctx->st));
-      CK(cudaStreamSynchronize(ctx->st));
-    }
-    for (int64_t p = 0; p < np; p++) {
-      const int a = pab[2 * p], b = pab[2 * p + 1];
-      if (u == 0 && a == b) continue;
-      const int64_t lo = pst[p], hi = p + 1 < np ? pst[p + 1] : n;
-      const bool ranges = ctx->cap_rs > 0 && hi - lo > ctx->cap_rs;
-      if (!live[p] && !ranges) continue;
-      uint64_t f = cfo[p];
-      if (ranges) {
-        auto it = hostfo.find(K(u, a, b));
-        if (it == hostfo.end()) {
-          ok = false;
-          continue;
-        }
-        f = (uint64_t)it->second;
+  int64_t cap = 16;
+  while (cap < 2 * e) cap <<= 1;
+  std::vector<uint32_t> key(MEMO_KEY * (size_t)cap, 0xffffffffu);
+  std::vector<int32_t> val(MEMO_VAL * (size_t)cap, 0);
+  std::vector<int64_t> toff(cap, 0);
+  int64_t entries = 0;
+  for (int64_t q = 0; q < e; q++) {
+    if (lt[q] < 0) continue;  // its trace did not fit the log
+    const uint32_t *k = &lk[MEMO_KEY * q];
+    uint64_t s = memo_hash(k) & (uint64_t)(cap - 1);
+    while (true) {
+      uint32_t *slot = &key[MEMO_KEY * s];
+      if (slot[0] == 0xffffffffu) {
+        std::copy(k, k + MEMO_KEY, slot);
+        std::copy(&lv[MEMO_VAL * q], &lv[MEMO_VAL * q] + MEMO_VAL, &val[MEMO_VAL * s]);
+        toff[s] = lt[q];
+        entries++;
+        break;
       }
-      key.push_back((int64_t)(((uint64_t)(uint32_t)a << 32) | (uint32_t)b));
-      soff.push_back(lo);
-      slen.push_back(hi - lo);
-      fo.push_back(f);
-      roff.push_back((int64_t)crecs.size());
-      toff.push_back((int64_t)ctr.size());
-      auto it = byp.find(K(u, a, b));
-      int c = 0;
-      if (it != byp.end()) {
-        for (int64_t i : it->second) {
-          AlnRec x = ctx->h_recs[i];
-          const int64_t t0 = ctx->h_toff[i], t1 = ctx->h_toff[i + 1];
-          x.toff = (int64_t)ctr.size();
-          ctr.insert(ctr.end(), ctx->h_trace.begin() + t0, ctx->h_trace.begin() + t1);
-          crecs.push_back(x);
-          c++;
-        }
-        byp.erase(it);
-      }
-      matched += c;
-      rcnt.push_back(c);
-      tlen.push_back((int64_t)ctr.size() - toff.back());
+      if (std::equal(k, k + MEMO_KEY, slot)) break;  // the same call again: the same result
+      s = (s + 1) & (uint64_t)(cap - 1);
     }
-    const size_t m = key.size();
-    for (size_t i = 1; i < m; i++)
-      if ((uint64_t)key[i] <= (uint64_t)key[i - 1]) ok = false;  // pairs come in (a, b) order
-    R.n[u] = (int64_t)m;
-    R.hkey[u].assign(key.begin(), key.end());
-    R.hfo[u] = fo;
-    R.hcnt[u] = rcnt;
-    R.htrl[u] = tlen;
-    if ((r = target_upload(ctx, R.key[u], key.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.seg_off[u], soff.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.seg_len[u], slen.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.rec_off[u], roff.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.tr_off[u], toff.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.tr_len[u], tlen.data(), 8 * m))) return r;
-    if ((r = target_upload(ctx, R.rec_cnt[u], rcnt.data(), 4 * m))) return r;
-    if ((r = target_upload(ctx, R.low[u], nullptr, 8 * (size_t)n))) return r;
-    const SeedKeyLayout &L = ctx->lay[u];
-    if (L.off_j > 64) ok = false;
-    launch_key_low(ctx->sorted[u], n, L.off_j >= 64 ? ~0ull : ((1ull << L.off_j) - 1), P<uint64_t>(R.low[u]),
-                   ctx->st);
-    LAUNCHED(n > 0 ? 1 : 0);
-    CK(cudaGetLastError());
-    R.lay[u] = L;
   }
-  if ((r = target_upload(ctx, R.recs, crecs.data(), sizeof(AlnRec) * crecs.size()))) return r;
-  if ((r = target_upload(ctx, R.trace, ctr.data(), ctr.size()))) return r;
-  R.spec = ctx->spec_host;
-  R.ave_path = ctx->ave_path_host;
-  // every alignment of a non-self pair belongs to a cached pair
-  R.valid = ok && matched == nonself;
+  pga_target::Memo &M = t->memo;
+  int r;
+  if ((r = target_upload(ctx, M.key, key.data(), 4 * key.size()))) return r;
+  if ((r = target_upload(ctx, M.val, val.data(), 4 * val.size()))) return r;
+  if ((r = target_upload(ctx, M.toff, toff.data(), 8 * toff.size()))) return r;
+  if ((r = target_upload(ctx, M.trace, nullptr, (size_t)tb))) return r;
+  if (tb > 0) CK(cudaMemcpyAsync(M.trace.p, ctx->mlog_trace.p, (size_t)tb, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  M.cap = cap;
+  M.entries = entries;
+  M.spec = ctx->spec_host;
+  M.ave_path = ctx->ave_path_host;
+  M.valid = true;
   return PGA_OK;
 }
 
@@ -2849,13 +2711,27 @@ int pga_target_create_reuse(pga_ctx *ctx, int freq, pga_target **out) {
   pga_target *t = nullptr;
   int r = target_create(ctx, &t, true);
   if (r) return r;
-  // the target's own run, every pair's outcome recorded
-  ctx->capture = true;
+  // the target's own run: once to count its calls, then again with every
+  // call logged (and once more if the log was too small for the traces)
   r = run_merge(ctx, freq);
   int64_t nal = 0;
   if (!r) r = pga_align(ctx, &nal);
+  ctx->cap_calls = ctx->align_work[2] + 1024;
+  ctx->cap_bytes = 64 * ctx->cap_calls + (16 << 20);
+  for (int attempt = 0; !r && attempt < 2; attempt++) {
+    ctx->capture = true;
+    r = pga_align(ctx, &nal);
+    ctx->capture = false;
+    if (r) break;
+    unsigned long long ctr[2];
+    CK(cudaMemcpyAsync(ctr, ctx->mlog_ctr.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if ((int64_t)ctr[0] <= ctx->cap_calls && (int64_t)ctr[1] <= ctx->cap_bytes) break;
+    ctx->cap_calls = (int64_t)ctr[0] + 1024;
+    ctx->cap_bytes = (int64_t)ctr[1] + (16 << 20);
+  }
+  if (!r) r = build_memo(ctx, t);
   ctx->capture = false;
-  if (!r) r = build_reuse(ctx, t);
   gdb_reset(ctx);
   if (r) {
     pga_target_destroy(t);
@@ -2870,12 +2746,7 @@ void pga_target_destroy(pga_target *t) {
   cudaSetDevice(t->device);
   for (DBuf *b : {&t->bps, &t->rec, &t->start})
     if (b->p) cudaFree(b->p);
-  pga_target::Reuse &R = t->reuse;
-  for (int u = 0; u < 2; u++)
-    for (DBuf *b : {&R.key[u], &R.seg_off[u], &R.seg_len[u], &R.rec_off[u], &R.rec_cnt[u], &R.tr_off[u],
-                    &R.tr_len[u], &R.low[u]})
-      if (b->p) cudaFree(b->p);
-  for (DBuf *b : {&R.recs, &R.trace})
+  for (DBuf *b : {&t->memo.key, &t->memo.val, &t->memo.toff, &t->memo.trace})
     if (b->p) cudaFree(b->p);
   delete t;
 }
@@ -2887,11 +2758,7 @@ int pga_target_info(const pga_target *t, int64_t *info4) {
   info4[0] = t->ncontig;
   info4[1] = bases;
   info4[2] = t->nrec;
-  size_t cache = t->reuse.recs.cap + t->reuse.trace.cap;
-  for (int u = 0; u < 2; u++)
-    for (const DBuf *b : {&t->reuse.key[u], &t->reuse.seg_off[u], &t->reuse.seg_len[u], &t->reuse.rec_off[u],
-                          &t->reuse.rec_cnt[u], &t->reuse.tr_off[u], &t->reuse.tr_len[u], &t->reuse.low[u]})
-      cache += b->cap;
+  const size_t cache = t->memo.key.cap + t->memo.val.cap + t->memo.toff.cap + t->memo.trace.cap;
   info4[3] = (int64_t)(t->bps.cap + t->rec.cap + t->start.cap + cache);
   return PGA_OK;
 }

@@ -487,12 +487,14 @@ class Device:
         return recs, toff, tr[: int(toff[-1])]
 
     def reuse_stats(self) -> dict:
-        """The last alignment's use of a resident target's pair cache
-        (pga_align_reuse_stats)."""
+        """The last alignment's use of a resident target's record of its own
+        Local_Alignment calls (pga_align_reuse_stats): calls answered from
+        it, of all calls made."""
         a = np.zeros(4, dtype=np.int64)
         self._ck(self.L.pga_align_reuse_stats(self.h, a.ctypes.data_as(vp)), "align_reuse_stats")
-        why = {0: None, 1: "no cache", 2: "key layout differs", 3: "scoring tables differ"}
-        return {"used": bool(a[0]), "pairs": int(a[1]), "alignments": int(a[2]), "not_used": why.get(int(a[3]))}
+        why = {0: None, 1: "no record", 3: "scoring tables differ"}
+        return {"used": bool(a[0]), "calls_from_record": int(a[1]), "calls": int(a[2]),
+                "not_used": why.get(int(a[3]))}
 
     def align_stats(self) -> dict:
         a = np.zeros(8, dtype=np.int64)
@@ -506,9 +508,9 @@ class Target:
     """A resident target (pga_target): a FASTA text ingested and indexed on
     one device and kept there, read-only, for any number of contexts'
     requests (Device.serve_load).  With reuse, the target's own GDB is also
-    aligned once (FREQ = freq) and its pairs' results kept: a request's pairs
-    of two target contigs with the same seeds take them instead of being
-    aligned (pga_target_create_reuse; same results)."""
+    aligned (FREQ = freq) and every Local_Alignment call it makes is kept: a
+    request's call on two target contigs with the same inputs takes the kept
+    result instead of being run (pga_target_create_reuse; same results)."""
 
     def __init__(self, text, nthr: int = 0, device: int = 0, reuse: bool = False, freq: int = 10):
         self.L = load_library()

@@ -272,27 +272,24 @@ int pga_index_set_digit_bits(pga_ctx *ctx, int bits);
  * target is read-only: any number of contexts of the same device may serve
  * requests against it at once, each on its own stream. */
 int pga_target_create(pga_ctx *ctx, pga_target **out);
-/* The same, with a pair cache: ctx first runs the target's own GDB through
- * the adaptamer merge (FREQ = freq) and the alignment, and the target keeps,
- * for every pair of two target contigs that is not a self pair and had
- * work, its seeds (the key bits below the contig fields), its alignments and
- * what FastGA's order reads of it (whether it called; its last call's
- * bepos).  pga_align on a request's GDB (pga_serve_load) then gives such a
- * pair whose seeds are exactly the cached ones its cached alignments instead
- * of aligning it -- the same alignments, since a non-self pair's alignments
- * depend only on its seeds, the two contigs' bases and the scoring tables --
- * when the request's key layout and scoring tables are the target's run's
- * (otherwise every pair is aligned).  Self pairs and pairs with a query
- * contig are always aligned. */
+/* The same, with a record of the target's own Local_Alignment calls: ctx
+ * first runs the target's GDB through the adaptamer merge (FREQ = freq) and
+ * the alignment, logging every call -- its inputs (the two contigs, the
+ * orientation, low, hgh, anti, lbord, hbord) and its result (the path and
+ * its trace points) -- and the target keeps them in a table.  pga_align on a
+ * request's GDB (pga_serve_load) then answers a call on two target contigs
+ * whose inputs are in the table with the recorded result instead of running
+ * the wave loop: the same result, since a call's result is a function of its
+ * inputs, the two contigs' bases and the scoring tables, and the table is
+ * used only when the request's scoring tables are the target run's. */
 int pga_target_create_reuse(pga_ctx *ctx, int freq, pga_target **out);
 void pga_target_destroy(pga_target *t);
 /* info4 = {contigs, bases, index records, device bytes held}. */
 int pga_target_info(const pga_target *t, int64_t *info4);
-/* The last pga_align's use of a target's pair cache: stats4 = {cache used
- * (0/1), pairs given their cached alignments, alignments taken from the
- * cache, why it was not used: 0 it was, or no target / 1 the target has no
- * cache / 2 the key layout differs (a query contig longer than the target's
- * longest) / 3 the scoring tables differ (base composition)}. */
+/* The last pga_align's use of a target's record of calls: stats4 = {used
+ * (0/1), calls answered from the record, calls made in all, why it was not
+ * used: 0 it was, or no target / 1 the target has no record / 3 the scoring
+ * tables differ (base composition)}. */
 int pga_align_reuse_stats(const pga_ctx *ctx, int64_t *stats4);
 
 /* A request: ctx's GDB becomes GDB(target's text, query text) -- the query

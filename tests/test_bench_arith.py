@@ -40,10 +40,10 @@ def test_serve_compact_and_cutoffs(bench):
     summ = {k: float(i) for i, k in enumerate(keep)}
     m = {"value": 1.5, "config": {"workload": "w", "slots": 3}, "served": dict(summ, extra=1),
          "plain": dict(summ, extra=2), "served_over_plain": 1.1, "bit_exact_requests": "12/12",
-         "pair_cache": {"requests_using_it": 11}, "clocks": {"sm_mhz": 1965.0}}
+         "call_record": {"requests_using_it": 11}, "clocks": {"sm_mhz": 1965.0}}
     c = bench.serve_compact(m)
     assert c["served"] == summ and c["plain"] == summ and c["bit_exact_requests"] == "12/12"
-    assert c["pair_cache"] == {"requests_using_it": 11}
+    assert c["call_record"] == {"requests_using_it": 11}
     assert c["slots"] == 3 and c["value"] == 1.5
     old = bench.WL["name"]
     try:
