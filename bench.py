@@ -183,9 +183,10 @@ class ReferenceSample:
         env = dict(os.environ)
         env["GIXMAKE_DUMP_PATH"] = os.devnull
         with open(os.path.join(self.tmp.name, "gix.log"), "w") as log:
-            subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T%d" % max(1, min(8, os.cpu_count() or 1)),
-                            self.stem + ".1gdb"], check=True, stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name,
-                           env=env)
+            # one thread: untimed set-up, and GIXmake's multi-threaded build now
+            # and then writes an LCP against the wrong predecessor on a loaded host
+            subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T1", self.stem + ".1gdb"], check=True,
+                           stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
 
     def run(self, whole: bool = True) -> float:
         from oracle import binding as orc
@@ -958,7 +959,7 @@ def main():
     ap.add_argument("--no-secondary", action="store_true", help="skip the 2 x 100 Mbp secondary measurement")
     ap.add_argument("--no-ingest", action="store_true", help="skip the FASTA ingest measurement")
     ap.add_argument("--align-build", type=int, default=0,
-                    help="with --profile-stage align: the alignment kernel's build (0 automatic, 2, 3 or 4)")
+                    help="with --profile-stage align: the alignment kernel's build (0 automatic, 2 to 5)")
     ap.add_argument("--profile-stage", choices=["index", "ingest", "serve", "align", "diag"], default=None,
                     help="run only this stage (warmup + steps calls) and print its device times; for profiling")
     ap.add_argument("--serve", action="store_true",

@@ -33,7 +33,7 @@ import statistics
 import time
 
 DIGIT_BITS = (18, 19, 20, 21, 22)
-ALIGN_BUILDS = (2, 3, 4)
+ALIGN_BUILDS = (2, 3, 4, 5)
 LONG_WAVES = (0, 10000, 20000, 40000)
 LONG_WAVES_DEFAULT = -1        # automatic: 20000 for the two-CTA build, off for the three-CTA one
 AUTO_WARPS = 148 * 16          # the alignment launch's task warps

@@ -548,12 +548,13 @@ struct SmallSums {
   }
 };
 
-// The persistent alignment loop, in three builds: MINB = 1 keeps every
+// The persistent alignment loop, in four builds: MINB = 1 keeps every
 // register a warp's wave loop wants (255, two CTAs per SM), for launches
-// bounded by their longest task; MINB = 3 and 4 trade spills for more
-// resident warps (three or four CTAs per SM: 168 or 128 registers), for
+// bounded by their longest task; MINB = 3, 4 and 5 trade spills for more
+// resident warps (three to five CTAs per SM: 168, 128 or 96 registers), for
 // launches bounded by throughput (many pairs), where a wave step's latency
-// is hidden by the other warps of its SM.
+// is hidden by the other warps of its SM (five: the 2 x 1 Gbp pair launch
+// 3.50 s against 3.70 with four).
 template <int MINB>
 __global__ void __launch_bounds__(ALIGN_THREADS, MINB) k_align_pairs(AlignLaunch P) {
   __shared__ BlockSeed s_block[ALIGN_THREADS / 32][32];
@@ -889,7 +890,8 @@ void launch_base_counts(const uint8_t *bps, const int64_t *clen, const int64_t *
 }
 
 void launch_align(const AlignLaunch &P, int grid, cudaStream_t st) {
-  if (P.min_blocks == 4) k_align_pairs<4><<<grid, ALIGN_THREADS, 0, st>>>(P);
+  if (P.min_blocks == 5) k_align_pairs<5><<<grid, ALIGN_THREADS, 0, st>>>(P);
+  else if (P.min_blocks == 4) k_align_pairs<4><<<grid, ALIGN_THREADS, 0, st>>>(P);
   else if (P.min_blocks == 3) k_align_pairs<3><<<grid, ALIGN_THREADS, 0, st>>>(P);
   else k_align_pairs<1><<<grid, ALIGN_THREADS, 0, st>>>(P);
 }

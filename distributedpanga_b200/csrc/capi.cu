@@ -149,7 +149,7 @@ struct pga_ctx {
   std::vector<uint16_t> h_ltrace;
   bool have_local = false;
   int64_t range_seeds = 0;         // pga_align_set_ranges
-  int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2 or 3 CTAs per SM
+  int align_build = 0;             // pga_align_set_build: 0 by pair count, else 2..5 CTAs per SM
   int long_waves = -1;             // pga_align_set_long_waves: -1 automatic, 0 off, else the wave count
   int digit_bits = 0;              // pga_index_set_digit_bits: 0 by record count, else 18..22
   // pool use over the launches of one pga_align: candidate trace bytes,
@@ -544,7 +544,8 @@ __global__ void k_entries_in(const uint8_t *__restrict__ ent, const int64_t *__r
 
 int run_merge(pga_ctx *ctx, int freq) {
   int64_t n = ctx->nrec;
-  int nb = (int)((n + MERGE_THREADS - 1) / MERGE_THREADS);
+  if (freq > MERGE_MAX_FREQ) return fail(ctx, PGA_ERR_LIMIT, "FREQ %d above %d", freq, MERGE_MAX_FREQ);
+  int nb = (int)((n + MERGE_TILE - 1) / MERGE_TILE);
   if (nb < 1) nb = 1;
   ENSURE(ctx->blk_n, sizeof(uint32_t) * (nb + 1));
   ENSURE(ctx->blk_c, sizeof(uint32_t) * (nb + 1));
@@ -555,8 +556,8 @@ int run_merge(pga_ctx *ctx, int freq) {
   CK(cudaMemsetAsync(bn, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
   CK(cudaMemsetAsync(bc, 0, sizeof(uint32_t) * (nb + 1), ctx->st));
   if (n > 0) {
-    launch_merge(false, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc, nullptr, nullptr,
-                 ctx->ctgb);
+    CK(launch_merge(false, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc, nullptr, nullptr,
+                    ctx->ctgb));
     LAUNCHED(1);
   }
   uint32_t *tot = P<uint32_t>(ctx->u64tmp);
@@ -571,8 +572,8 @@ int run_merge(pga_ctx *ctx, int freq) {
   ENSURE(ctx->seed[0], sizeof(Seed) * (size_t)t[0] + 16);
   ENSURE(ctx->seed[1], sizeof(Seed) * (size_t)t[1] + 16);
   if (n > 0) {
-    launch_merge(true, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
-                 P<Seed>(ctx->seed[0]), P<Seed>(ctx->seed[1]), ctx->ctgb);
+    CK(launch_merge(true, nb, ctx->st, P<Rec>(ctx->rec), P<uint8_t>(ctx->lcp), n, freq, bn, bc,
+                    P<Seed>(ctx->seed[0]), P<Seed>(ctx->seed[1]), ctx->ctgb));
     LAUNCHED(1);
   }
   stage_end(ctx, ST_MERGE);
@@ -1043,7 +1044,7 @@ int prepare_workspace(pga_ctx *ctx, AlignLaunch &L, int ave_path) {
   L.ave_path = ave_path;
   L.amxpos = ctx->maxctg;
   L.maxdag = 2 * ctx->maxctg;
-  L.nwarps = 148 * 16;
+  L.nwarps = 148 * 20;  // work spaces for the five-CTA build's resident warps
   L.vcap = 8192;
   L.point_cap = 4 * (ctx->maxctg / 100 + 4) + 64;
   // Pools sized from the sequence total; align_run_tasks grows one that
@@ -1392,7 +1393,7 @@ int run_align(pga_ctx *ctx) {
   L.fo_pos = fo_pos;
   // the launch is bounded by its longest tasks up to about a million pairs,
   // by throughput beyond: then the build with more resident warps
-  L.min_blocks = ctx->align_build ? ctx->align_build : npairs[0] + npairs[1] > ALIGN_MANY_PAIRS ? 4 : 2;
+  L.min_blocks = ctx->align_build ? ctx->align_build : npairs[0] + npairs[1] > ALIGN_MANY_PAIRS ? 5 : 2;
   L.sred = sred;
   L.fo_last = sred + 8;
   L.fo_earlier = sred + 8 + nc;
@@ -3161,7 +3162,7 @@ int pga_align_profile(const pga_ctx *ctx, int64_t *prof2) {
 }
 
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm) {
-  if (!ctx || (ctas_per_sm != 0 && ctas_per_sm != 2 && ctas_per_sm != 3 && ctas_per_sm != 4)) return PGA_ERR_ARG;
+  if (!ctx || (ctas_per_sm != 0 && (ctas_per_sm < 2 || ctas_per_sm > 5))) return PGA_ERR_ARG;
   ctx->align_build = ctas_per_sm;
   return PGA_OK;
 }

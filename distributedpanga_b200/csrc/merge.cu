@@ -1,5 +1,5 @@
-// FastGA's self adaptamer seed merge on the GPU, one thread per k-mer table
-// entry.
+// FastGA's self adaptamer seed merge on the GPU: each k-mer table entry's
+// seeds found by one thread from a tile of entries staged in shared memory.
 //
 // Reference: new_self_merge_thread / self_adaptamer_merge,
 // src/fastga_pipeline.c:245-499.  The reference walks each 24-bit prefix
@@ -25,65 +25,79 @@
 
 namespace pga {
 
-struct Run {
-  int64_t s, t;
-  int plen;
-  bool emit;
-};
-
-__device__ __forceinline__ Run adaptamer_run(const uint8_t *__restrict__ lcp, int64_t n, int64_t i, int freq) {
-  Run r;
-  int li = lcp[i];
-  int ln = (i + 1 < n) ? lcp[i + 1] : 0;
-  r.plen = li > ln ? li : ln;
-  r.emit = false;
-  r.s = r.t = i;
-  if (r.plen < 12) return r;
-  // run start: the last r <= i with lcp[r] < plen, or the table's first entry
-  int64_t s = i;
-  while (s > 0 && lcp[s] >= r.plen) {
-    s--;
-    if (i + 1 - s >= freq) return r;
-  }
-  // run end: the first t > i with lcp[t] < plen
-  int64_t t = i + 1;
-  while (t < n && lcp[t] >= r.plen) {
-    t++;
-    if (t - s >= freq) return r;
-  }
-  r.s = s;
-  r.t = t;
-  r.emit = (t - s) < freq;
-  return r;
-}
-
+// A tile of MERGE_TILE entries per CTA, MERGE_ITEMS consecutive entries per
+// thread (so a thread's seeds are consecutive in the output), with the LCP
+// bytes, contig|strand fields and positions of the tile and of `halo`
+// (FREQ + 1) entries on either side staged in shared memory: an entry's run
+// lies within FREQ - 1 entries of it, so every read of the scan is there.
 template <bool WRITE>
 __global__ void __launch_bounds__(MERGE_THREADS)
-k_merge(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n, int freq,
-        uint32_t *__restrict__ blk_n, uint32_t *__restrict__ blk_c,
-        Seed *__restrict__ nseed, Seed *__restrict__ cseed, int ctgb) {
+k_merge(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n, int freq, int halo,
+        uint32_t *__restrict__ blk_n, uint32_t *__restrict__ blk_c, Seed *__restrict__ nseed,
+        Seed *__restrict__ cseed, int ctgb) {
+  extern __shared__ __align__(16) unsigned char msm[];
   __shared__ uint32_t sm[33];
-  const int64_t i = (int64_t)blockIdx.x * MERGE_THREADS + threadIdx.x;
+  const int span = MERGE_TILE + 2 * halo;
+  uint32_t *spos = reinterpret_cast<uint32_t *>(msm);
+  uint16_t *scs = reinterpret_cast<uint16_t *>(spos + span);
+  uint8_t *slcp = reinterpret_cast<uint8_t *>(scs + span);
+  const int64_t t0 = (int64_t)blockIdx.x * MERGE_TILE, g0 = t0 - halo;  // entry of slot 0
+  for (int q = threadIdx.x; q < span; q += MERGE_THREADS) {
+    const int64_t g = g0 + q;
+    const bool in = g >= 0 && g < n;
+    const uint64_t lo = in ? rec[g].lo : 0ull;
+    if (WRITE) spos[q] = (uint32_t)lo;
+    scs[q] = (uint16_t)(lo >> 32);
+    slcp[q] = in ? lcp[g] : 0;
+  }
+  __syncthreads();
   const uint32_t sbit = 1u << (8 * ctgb - 1);
   uint32_t cn = 0, cc = 0;
-  Run r;
-  r.emit = false;
-  uint32_t cs_i = 0;
-  if (i < n) {
-    r = adaptamer_run(lcp, n, i, freq);
-    if (r.emit) {
-      cs_i = rec_cs(rec[i]);
-      for (int64_t j = r.s; j < r.t; j++) {
-        if (j == i) continue;
-        uint32_t cs_j = rec_cs(rec[j]);
-        if ((cs_i & sbit) == (cs_j & sbit)) cn++;
-        else cc++;
+  int rs[MERGE_ITEMS], rt[MERGE_ITEMS], rp[MERGE_ITEMS];
+#pragma unroll
+  for (int e = 0; e < MERGE_ITEMS; e++) {
+    rs[e] = rt[e] = 0;
+    rp[e] = -1;
+    const int64_t i = t0 + (int64_t)threadIdx.x * MERGE_ITEMS + e;
+    if (i >= n) continue;
+    const int x = (int)(i - g0);  // slot of i
+    const int li = slcp[x], ln = i + 1 < n ? slcp[x + 1] : 0;
+    const int plen = li > ln ? li : ln;
+    if (plen < 12) continue;
+    // run start: the last r <= i with lcp[r] < plen, or the table's first entry
+    int64_t s = i;
+    bool cut = false;
+    while (s > 0 && slcp[s - g0] >= plen) {
+      s--;
+      if (i + 1 - s >= freq) {
+        cut = true;
+        break;
       }
+    }
+    if (cut) continue;
+    // run end: the first t > i with lcp[t] < plen
+    int64_t t = i + 1;
+    while (t < n && slcp[t - g0] >= plen) {
+      t++;
+      if (t - s >= freq) {
+        cut = true;
+        break;
+      }
+    }
+    if (cut || t - s >= freq) continue;
+    rs[e] = (int)(s - g0);
+    rt[e] = (int)(t - g0);
+    rp[e] = plen;
+    const uint32_t si = scs[x] & sbit;
+    for (int y = rs[e]; y < rt[e]; y++) {
+      if (y == x) continue;
+      if ((scs[y] & sbit) == si) cn++;
+      else cc++;
     }
   }
   uint32_t tn, tc;
-  uint32_t on = block_exclusive_scan<uint32_t>(cn, sm, &tn);
-  uint32_t oc = block_exclusive_scan<uint32_t>(cc, sm, &tc);
+  const uint32_t on = block_exclusive_scan<uint32_t>(cn, sm, &tn);
+  const uint32_t oc = block_exclusive_scan<uint32_t>(cc, sm, &tc);
   if (!WRITE) {
     if (threadIdx.x == 0) {
       blk_n[blockIdx.x] = tn;
@@ -91,31 +105,42 @@ k_merge(const Rec *__restrict__ rec, const uint8_t *__restrict__ lcp, int64_t n,
     }
     return;
   }
-  if (!r.emit) return;
-  uint64_t wn = (uint64_t)blk_n[blockIdx.x] + on;
-  uint64_t wc = (uint64_t)blk_c[blockIdx.x] + oc;
-  Rec ri = rec[i];
-  uint64_t ipos = rec_pos(ri);
-  uint64_t icont = cs_i & (sbit - 1u);
-  for (int64_t j = r.s; j < r.t; j++) {
-    if (j == i) continue;
-    Rec rj = rec[j];
-    uint32_t cs_j = rec_cs(rj);
-    Seed sd;
-    sd.a = ipos | ((uint64_t)rec_pos(rj) << 32);
-    sd.b = icont | ((uint64_t)cs_j << 16) | ((uint64_t)r.plen << 32);
-    if ((cs_i & sbit) == (cs_j & sbit)) nseed[wn++] = sd;
-    else cseed[wc++] = sd;
+  uint64_t wn = (uint64_t)blk_n[blockIdx.x] + on, wc = (uint64_t)blk_c[blockIdx.x] + oc;
+#pragma unroll
+  for (int e = 0; e < MERGE_ITEMS; e++) {
+    if (rp[e] < 0) continue;
+    const int x = threadIdx.x * MERGE_ITEMS + e + halo;
+    const uint32_t csi = scs[x];
+    const uint64_t ipos = spos[x], icont = csi & (sbit - 1u);
+    for (int y = rs[e]; y < rt[e]; y++) {
+      if (y == x) continue;
+      const uint32_t csj = scs[y];
+      Seed sd;
+      sd.a = ipos | ((uint64_t)spos[y] << 32);
+      sd.b = icont | ((uint64_t)csj << 16) | ((uint64_t)rp[e] << 32);
+      if ((csi & sbit) == (csj & sbit)) nseed[wn++] = sd;
+      else cseed[wc++] = sd;
+    }
   }
 }
 
-void launch_merge(bool write, int nb, cudaStream_t st, const Rec *rec, const uint8_t *lcp, int64_t n, int freq,
-                  uint32_t *blk_n, uint32_t *blk_c, Seed *nseed, Seed *cseed, int ctgb) {
-  if (nb <= 0) return;
-  if (write)
-    k_merge<true><<<nb, MERGE_THREADS, 0, st>>>(rec, lcp, n, freq, blk_n, blk_c, nseed, cseed, ctgb);
-  else
-    k_merge<false><<<nb, MERGE_THREADS, 0, st>>>(rec, lcp, n, freq, blk_n, blk_c, nseed, cseed, ctgb);
+size_t merge_smem(int freq) { return (size_t)(MERGE_TILE + 2 * (freq + 1)) * 7; }
+
+cudaError_t launch_merge(bool write, int nb, cudaStream_t st, const Rec *rec, const uint8_t *lcp, int64_t n, int freq,
+                         uint32_t *blk_n, uint32_t *blk_c, Seed *nseed, Seed *cseed, int ctgb) {
+  if (nb <= 0) return cudaSuccess;
+  const size_t smem = merge_smem(freq);
+  const int halo = freq + 1;
+  if (write) {
+    cudaError_t e = cudaFuncSetAttribute(k_merge<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_merge<true><<<nb, MERGE_THREADS, smem, st>>>(rec, lcp, n, freq, halo, blk_n, blk_c, nseed, cseed, ctgb);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_merge<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_merge<false><<<nb, MERGE_THREADS, smem, st>>>(rec, lcp, n, freq, halo, blk_n, blk_c, nseed, cseed, ctgb);
+  }
+  return cudaGetLastError();
 }
 
 // Seeds in the reference's byte format (src/fastga_pipeline.c:391-397):

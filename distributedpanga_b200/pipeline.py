@@ -459,7 +459,7 @@ class Device:
         return {"local_alignment_cycles": int(a[0]), "finish_cycles": int(a[1])}
 
     def set_build(self, ctas_per_sm: int):
-        """Which build of the alignment kernel runs (0 automatic, 2, 3 or 4 CTAs per SM)."""
+        """Which build of the alignment kernel runs (0 automatic, or 2 to 5 CTAs per SM)."""
         self._ck(self.L.pga_align_set_build(self.h, int(ctas_per_sm)), "align_set_build")
 
     def set_long_waves(self, waves: int) -> None:

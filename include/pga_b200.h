@@ -238,9 +238,9 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds);
 int pga_align_profile(const pga_ctx *ctx, int64_t *prof2);
 /* Tuning, no counterpart in the reference: which build of the alignment
  * kernel runs -- 2 (255 registers, two CTAs per SM: best when the launch is
- * bounded by its longest alignments), 3 (168 registers, three CTAs per SM) or
- * 4 (128 registers, four CTAs per SM: best for launches of many pairs); 0
- * (the default) picks 4 above 2^20 pairs, else 2.
+ * bounded by its longest alignments), 3 (168 registers, three CTAs per SM),
+ * 4 (128 registers, four) or 5 (96 registers, five CTAs per SM: best for
+ * launches of many pairs); 0 (the default) picks 5 above 2^20 pairs, else 2.
  * The alignments are the same either way. */
 int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
 
@@ -390,9 +390,10 @@ int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, co
  * (PGA_ERR_LIMIT beyond); `len` must be a whole number of seeds
  * (PGA_ERR_ARG otherwise).  The first call on a device looks the array's
  * address up for that device (and looks it up again after the device's
- * context was re-created, e.g. by cudaDeviceReset); make that first call
- * before any stream capture.  The call synchronizes `stream` (a cudaStream_t, NULL for the
- * default stream) once, midway; the last kernels are left queued on it.
+ * context was re-created, e.g. by cudaDeviceReset).  The call cannot be
+ * captured into a CUDA graph: it synchronizes `stream` (a cudaStream_t, NULL
+ * for the default stream) once, midway; the last kernels are left queued on
+ * it.
  * Calls share the array: calls that overlap on the GPU (several host
  * threads or streams) race.  Returns PGA_OK, PGA_ERR_ARG, PGA_ERR_LIMIT or
  * PGA_ERR_CUDA. */

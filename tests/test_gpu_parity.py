@@ -226,7 +226,7 @@ def test_alignments_independent_of_kernel_build(dev, case):
     dev.index_build(want_entries=False)
     dev.merge(dig["freq_cutoff"])
     try:
-        for build in (4, 3, 2):
+        for build in (5, 4, 3, 2):
             dev.set_build(build)
             for lw in (0, 50, 20000):
                 dev.set_long_waves(lw)
