@@ -405,6 +405,8 @@ def run_profile_stage(args) -> None:
         return
     if args.profile_stage == "index":
         dev.gdb_load(cs)
+        if args.digit_bits:
+            dev.set_digit_bits(args.digit_bits)
         dev.enable_timing(True)
         for _ in range(args.warmup + args.steps):
             n = dev.index_build(want_entries=args.entries)
@@ -958,6 +960,8 @@ def main():
     ap.add_argument("--no-check", action="store_true", help="skip the comparison with the reference's digests")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 2 x 100 Mbp secondary measurement")
     ap.add_argument("--no-ingest", action="store_true", help="skip the FASTA ingest measurement")
+    ap.add_argument("--digit-bits", type=int, default=0,
+                    help="with --profile-stage index: the index sort's first digit width (0 automatic, 18..22)")
     ap.add_argument("--align-build", type=int, default=0,
                     help="with --profile-stage align: the alignment kernel's build (0 automatic, 2 to 5)")
     ap.add_argument("--profile-stage", choices=["index", "ingest", "serve", "align", "diag"], default=None,

@@ -209,7 +209,7 @@ struct WarpAligner {
       const uint64_t mask = (uint64_t)M.cap - 1;
       for (uint64_t s = memo_hash(k) & mask, probe = 0; probe <= mask; probe++, s = (s + 1) & mask) {
         const uint32_t *q = M.key + MEMO_KEY * s;
-        if (q[0] == 0xffffffffu) break;
+        if (q[0] == MEMO_EMPTY) break;
         bool same = true;
         for (int i = 0; i < MEMO_KEY; i++) same &= q[i] == k[i];
         if (!same) continue;

@@ -5,6 +5,7 @@
 #include "align_core.cuh"
 #include "common.cuh"
 #include "seeds.cuh"
+#include "memo.h"
 
 namespace pga {
 
@@ -70,17 +71,6 @@ struct CallMemo {
   unsigned long long *lnext, *lbytes;
   int64_t lcap, lbytes_cap;
 };
-constexpr int MEMO_KEY = 6, MEMO_VAL = 6;
-
-__host__ __device__ inline uint64_t memo_hash(const uint32_t *k) {
-  uint64_t h = 0x243f6a8885a308d3ull;
-  for (int i = 0; i < MEMO_KEY; i++) {
-    h ^= k[i];
-    h *= 0x9e3779b97f4a7c15ull;
-    h ^= h >> 29;
-  }
-  return h;
-}
 
 struct AlignLaunch {
   const PairTask *tasks;

@@ -2664,39 +2664,17 @@ int build_memo(pga_ctx *ctx, pga_target *t) {
     CK(cudaMemcpyAsync(lt.data(), ctx->mlog_toff.p, 8 * lt.size(), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
   }
-  int64_t cap = 16;
-  while (cap < 2 * e) cap <<= 1;
-  std::vector<uint32_t> key(MEMO_KEY * (size_t)cap, 0xffffffffu);
-  std::vector<int32_t> val(MEMO_VAL * (size_t)cap, 0);
-  std::vector<int64_t> toff(cap, 0);
-  int64_t entries = 0;
-  for (int64_t q = 0; q < e; q++) {
-    if (lt[q] < 0) continue;  // its trace did not fit the log
-    const uint32_t *k = &lk[MEMO_KEY * q];
-    uint64_t s = memo_hash(k) & (uint64_t)(cap - 1);
-    while (true) {
-      uint32_t *slot = &key[MEMO_KEY * s];
-      if (slot[0] == 0xffffffffu) {
-        std::copy(k, k + MEMO_KEY, slot);
-        std::copy(&lv[MEMO_VAL * q], &lv[MEMO_VAL * q] + MEMO_VAL, &val[MEMO_VAL * s]);
-        toff[s] = lt[q];
-        entries++;
-        break;
-      }
-      if (std::equal(k, k + MEMO_KEY, slot)) break;  // the same call again: the same result
-      s = (s + 1) & (uint64_t)(cap - 1);
-    }
-  }
+  const MemoTable T = memo_table(lk.data(), lv.data(), lt.data(), e);
   pga_target::Memo &M = t->memo;
   int r;
-  if ((r = target_upload(ctx, M.key, key.data(), 4 * key.size()))) return r;
-  if ((r = target_upload(ctx, M.val, val.data(), 4 * val.size()))) return r;
-  if ((r = target_upload(ctx, M.toff, toff.data(), 8 * toff.size()))) return r;
+  if ((r = target_upload(ctx, M.key, T.key.data(), 4 * T.key.size()))) return r;
+  if ((r = target_upload(ctx, M.val, T.val.data(), 4 * T.val.size()))) return r;
+  if ((r = target_upload(ctx, M.toff, T.toff.data(), 8 * T.toff.size()))) return r;
   if ((r = target_upload(ctx, M.trace, nullptr, (size_t)tb))) return r;
   if (tb > 0) CK(cudaMemcpyAsync(M.trace.p, ctx->mlog_trace.p, (size_t)tb, cudaMemcpyDeviceToDevice, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
-  M.cap = cap;
-  M.entries = entries;
+  M.cap = T.cap;
+  M.entries = T.entries;
   M.spec = ctx->spec_host;
   M.ave_path = ctx->ave_path_host;
   M.valid = true;
