@@ -146,8 +146,10 @@ def make_contigs(scale: float, name: str | None = None):
         return gdb.ContigSet(bps=z["bps"], clen=z["clen"], boff=z["boff"], freq=z["freq"]), None
     contigs = synth.make(name, scale=scale)
     cs = gdb.from_contigs(contigs)
-    try:
-        np.savez(cache, bps=cs.bps, clen=cs.clen, boff=cs.boff, freq=cs.freq)
+    try:  # written whole, then renamed: ranks of one run may build it at once
+        tmp = "%s.%d.tmp.npz" % (cache[:-4], os.getpid())
+        np.savez(tmp, bps=cs.bps, clen=cs.clen, boff=cs.boff, freq=cs.freq)
+        os.replace(tmp, cache)
     except OSError:
         pass
     return cs, contigs
@@ -183,8 +185,10 @@ class ReferenceSample:
         env = dict(os.environ)
         env["GIXMAKE_DUMP_PATH"] = os.devnull
         with open(os.path.join(self.tmp.name, "gix.log"), "w") as log:
-            # one thread: untimed set-up, and GIXmake's multi-threaded build now
-            # and then writes an LCP against the wrong predecessor on a loaded host
+            # untimed set-up, one thread: on a loaded host GIXmake's threaded
+            # build is slower here and now and then writes an entry's LCP against
+            # the wrong predecessor (the driver reads only the .gix header and its
+            # contig order, src/fastga_order_core.c:11-48)
             subprocess.run([os.path.join(orc.REF_DIR, "GIXmake_dump"), "-T1", self.stem + ".1gdb"], check=True,
                            stdout=log, stderr=subprocess.STDOUT, cwd=self.tmp.name, env=env)
 
@@ -737,7 +741,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             sm.pop("cs")
             sm.pop("autotune", None)
             secondary = {"workload": sm["config"]["workload"], "metric": METRIC, "unit": UNIT, **sm}
-            if not args.no_cpu_baseline and args.cpu_full_c2:
+            if not args.no_cpu_baseline and not args.no_cpu_full_c2:
+                # the reference's own pipeline on the same 2 x 100 Mbp input
                 secondary["cpu_baseline"] = cpu_baseline(1.0, "chromset")
         except Exception as e:  # the secondary measurement must not hide the headline
             secondary = {"error": "%s: %s" % (type(e).__name__, e)}
@@ -951,8 +956,9 @@ def main():
                     help="the reference arm's per-step sample of the generator (default %s)" % REF_SCALE)
     ap.add_argument("--cpu-scale", type=float, default=None,
                     help="the cpu_baseline sample of the generator (default %s)" % CPU_SCALE)
-    ap.add_argument("--cpu-full-c2", action="store_true",
-                    help="also time the reference on the whole 2 x 100 Mbp workload (about 1.5 min, plus GIXmake)")
+    ap.add_argument("--no-cpu-full-c2", action="store_true",
+                    help="skip timing the reference on the whole 2 x 100 Mbp workload (the secondary's cpu_baseline; "
+                         "about 1.5 min plus GIXmake)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--entries", action="store_true",
                     help="also write the reference-format k-mer table entries in every step (N x E bytes of HBM)")
