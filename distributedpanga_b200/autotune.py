@@ -7,11 +7,11 @@ Four knobs change how the device does the work but never what it computes
   (``pga_index_set_digit_bits``, 18..22).  Wider digits mean more, smaller
   shared-memory sorts and more scatter fronts;
 * ``align_build`` -- which build of the alignment kernel runs
-  (``pga_align_set_build``: 2 CTAs per SM at 255 registers, 3 at 168 or 4
-  at 128);
+  (``pga_align_set_build``: 2 CTAs per SM at 255 registers, 3 at 168, 4 at
+  128 or 5 at 96);
 * ``range_seeds`` -- how large pairs are cut into band ranges that different
   warps align (``pga_align_set_ranges``: -1 never, or a size in seeds; the
-  automatic size is max(256, seeds / (160 x 2368 warps)));
+  automatic size is max(256, seeds / (160 x 2960 warps)));
 * ``long_waves`` -- after how many wave steps a Local_Alignment call keeps
   its SM to itself (``pga_align_set_long_waves``; 0 never, -1 automatic).
 
@@ -36,7 +36,7 @@ DIGIT_BITS = (18, 19, 20, 21, 22)
 ALIGN_BUILDS = (2, 3, 4, 5)
 LONG_WAVES = (0, 10000, 20000, 40000)
 LONG_WAVES_DEFAULT = -1        # automatic: 20000 for the two-CTA build, off for the three-CTA one
-AUTO_WARPS = 148 * 16          # the alignment launch's task warps
+AUTO_WARPS = 148 * 20          # the alignment launch's task warps (pga_align's work spaces)
 
 
 def auto_range_seeds(all_seeds: int) -> int:

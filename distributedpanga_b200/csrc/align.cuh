@@ -146,7 +146,7 @@ struct AlignLaunch {
   int64_t npairs[2], nseeds[2];
   const int *fo_pos;
   unsigned long long *sred, *fo_last, *fo_earlier;
-  // build of k_align_pairs: 2 (all registers) or 3 resident CTAs per SM
+  // build of k_align_pairs: 2 (all registers), 3, 4 or 5 resident CTAs per SM
   int min_blocks;
 };
 

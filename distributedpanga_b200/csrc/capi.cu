@@ -799,7 +799,7 @@ int align_launch(pga_ctx *ctx, AlignLaunch &L, const LaunchPlan &plan, std::vect
     L.smflag = P<unsigned>(ctx->task_next) + 16;
     L.prof = (unsigned long long *)(P<uint8_t>(ctx->task_next) + 32);
     // automatic: on for launches bounded by their longest calls, off for the
-    // throughput-bound ones (the three-CTA build), whose flagged SMs would
+    // throughput-bound ones (the builds of three or more CTAs per SM), whose flagged SMs would
     // idle warps that still have queue work
     L.long_waves = ctx->long_waves >= 0 ? ctx->long_waves : (L.min_blocks >= 3 ? 0 : LONG_WAVES_AUTO);
     CK(cudaMemsetAsync(ctx->cell_next.p, 0, 8, ctx->st));

@@ -250,8 +250,9 @@ int pga_align_set_build(pga_ctx *ctx, int ctas_per_sm);
  * which bounds the launch -- soon has the SM to itself; the remaining tasks
  * go to the other SMs.  0 turns this off;
  * -1 (the default) is 20000 for launches of the two-CTA build and off for
- * the three-CTA build (launches of more than 2^20 pairs, bounded by
- * throughput).  The alignments are the same for every value. */
+ * the builds of three to five CTAs per SM (launches of more than 2^20
+ * pairs, bounded by throughput).  The alignments are the same for every
+ * value. */
 int pga_align_set_long_waves(pga_ctx *ctx, int waves);
 
 /* Tuning, no counterpart in the reference: the width in bits (18..22) of the

@@ -51,8 +51,8 @@ def test_picks_fastest_and_restores_defaults():
     assert cfg["digit_bits"] == 20
     assert cfg["align_build"] == 3
     # never-split costs 0.5, sizes above 2000 seeds 0.1: the automatic size
-    # (1055 here) ties with its half and comes first
-    assert cfg["range_seeds"] == autotune.auto_range_seeds(400_000_000) == 1055
+    # (844 here) ties with its half and comes first
+    assert cfg["range_seeds"] == autotune.auto_range_seeds(400_000_000) == 844
     assert cfg["long_waves"] == 10000
     assert (d.bits, d.build, d.ranges, d.long) == (0, 0, 0, autotune.LONG_WAVES_DEFAULT)  # defaults again
     assert sum(1 for c in d.calls if c[0] == "index") == 3 * len(autotune.DIGIT_BITS) + 1
