@@ -28,7 +28,12 @@ bit_exact = the secondary (2 x 100 Mbp) workload's index, seeds, sorted
          (tests/golden/chromset_full.json), checked outside the timed region
 cpu_baseline = the reference pipeline compiled from source (oracle/_ref), or
          the oracle's C restatement when that is absent, on a bounded sample
-         of the same generator
+         of the same generator; the secondary object's cpu_baseline is the
+         reference on the whole 2 x 100 Mbp input (the same bytes)
+served_form = a resident 1 Gbp target (with the record of its own
+         Local_Alignment calls) against a Poisson stream of 12 query
+         assemblies, beside the plain form on the same requests; every served
+         result is compared with the plain one
 
 With N > 1 every rank runs an independent replica (the path has no exchange
 step on one node's workload): weak scaling, no collective in the data path.
