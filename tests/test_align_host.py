@@ -17,8 +17,9 @@ NATIVE = os.path.join(ROOT, "tests", "native")
 ALL_CASES = GOLDEN_CASES + ["small_full"]
 
 
-@pytest.fixture(scope="module")
-def aht():
+def load_aht():
+    """The host aligner harness (tests/native/align_host.cu), rebuilt when a
+    source is newer than the library."""
     so = os.path.join(NATIVE, "libalign_host.so")
     src = os.path.join(NATIVE, "align_host.cu")
     deps = [src, os.path.join(ROOT, "oracle", "scalar_align.cuh")] + [
@@ -36,6 +37,11 @@ def aht():
     L.aht_finish_check.argtypes = [i64, vp, vp, vp, i64, ci, vp, vp, vp, vp]
     L.aht_finish_check.restype = ci
     return L
+
+
+@pytest.fixture(scope="module")
+def aht():
+    return load_aht()
 
 
 def run_unit(L, cs, arr, off, dig, comp, self_entry=None, split=0):

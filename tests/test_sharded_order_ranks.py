@@ -1,0 +1,185 @@
+"""FastGA's self-pair order across ranks (distributedpanga_b200.sharded_order).
+
+On CPU over gloo: the sharded index build, the seed routing by pair owner,
+each rank aligning the pairs it owns with the host aligner (align_core.cuh,
+the code the GPU kernel's chain driver shares), and the order values combined
+with all-reduce(MAX).  The union of the ranks' alignments must be the
+reference's .1aln record stream of the single-process run, and every rank
+must decide the same entry value for every self pair."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from conftest import GOLDEN, ROOT
+from test_align_host import aht  # noqa: F401  (the host aligner fixture)
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _contig_of(rec, ctgb):
+    v = np.zeros(len(rec), dtype=np.int64)
+    for b in range(ctgb):
+        v |= rec[:, rec.shape[1] - ctgb + b].astype(np.int64) << (8 * b)
+    return v & ((1 << (8 * ctgb - 1)) - 1)
+
+
+def _worker(rank, world, port, case, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import load_case
+    from test_align_host import aln_lines, load_aht, run_unit
+    from distributedpanga_b200 import dsort, seed_exchange as sx, sharded_order as so
+    from oracle import binding as orc
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def allreduce(a, op):
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64))
+        dist.all_reduce(t, op=op)
+        return t.numpy()
+
+    try:
+        aht = load_aht()
+        cs, dig = load_case(case)
+        n, posb, ctgb = cs.ncontig, dig["posb"], dig["ctgb"]
+        allrec = orc.extract(cs, posb, ctgb)
+        mine = dsort.run_stage2(allrec[_contig_of(allrec, ctgb) % world == rank], orc.sort_records)
+        ent, cum, _ = orc.build_adapter(mine, posb, ctgb)
+        ns, css, nb, _ = orc.merge(ent, cum, posb, ctgb, dig["freq_cutoff"], n)
+        rfp = sx.rank_for_pair(sx.contig_assignment_build(cs.clen, world)[0])
+        rn = sx.redistribute_seeds(ns, posb, ctgb, rfp)
+        rc = sx.redistribute_seeds(css, posb, ctgb, rfp)
+        arrN, offN = orc.reimport_sort(rn, posb, ctgb, 0, n, cs.maxctg, dig["dbyte"])
+        arrC, offC = orc.reimport_sort(rc, posb, ctgb, 1, n, cs.maxctg, dig["dbyte"])
+        nb = allreduce(nb, dist.ReduceOp.SUM)
+
+        perm, pos = so.order_positions(cs.clen)
+        rs = so.range_starts(cs.clen, nb, dig["swide"], perm)
+        # first pass: every pair this rank owns; those of two contigs are final
+        _, pairsN = run_unit(aht, cs, arrN, offN, dig, 0)
+        lk, eb = so.local_keys(pairsN, pos, n)
+        st = np.zeros(n, dtype=np.int64)
+        for a, b, _, _ in pairsN:
+            if a == b:
+                st[pos[a]] = 1
+        lk, eb, st = (allreduce(v, dist.ReduceOp.MAX) for v in (lk, eb, st))
+
+        entry = np.zeros(n, dtype=np.int32)
+        aligned = []
+
+        def align_round(new):
+            for c, v in new.items():
+                entry[c] = v
+            own = [c for c in new if rfp[c, c] == rank]
+            if not own:
+                return {}
+            _, pr = run_unit(aht, cs, arrN, offN, dig, 0, entry)
+            res = {(int(a), int(b)): (int(k), int(e)) for a, b, k, e in pr}
+            aligned.extend(own)
+            return {c: res[(c, c)] for c in own}
+
+        values, rounds = so.resolve(n, pos, rs, lk, eb, st, align_round,
+                                    lambda a: allreduce(a, dist.ReduceOp.MAX))
+        outN, _ = run_unit(aht, cs, arrN, offN, dig, 0, entry)
+        outC, _ = run_unit(aht, cs, arrC, offC, dig, 1)
+        out[rank] = (aln_lines(outN + outC), sorted(values.items()), rounds, sorted(aligned),
+                     int((st == 1).sum()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case,world,nself", [("small_s002", 2, 6), ("small_s002", 3, 6), ("chromset_s0005", 3, 2),
+                                              ("many_contigs", 3, 0)])
+def test_ranks_alignments_are_the_single_process_stream(oracle, aht, case, world, nself):
+    import gzip
+    from conftest import load_case
+    from distributedpanga_b200 import seed_exchange as sx
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_worker, args=(world, port, case, out), nprocs=world, start_method="spawn", join=True)
+        res = {r: out[r] for r in range(world)}
+    cs, dig = load_case(case)
+    ref = sorted(" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read()
+                 .split("\n") if l.strip())
+    mine = sorted(" ".join(l.split()) for r in range(world) for l in res[r][0])
+    assert len(mine) == dig["aln"]["count"]
+    assert mine == ref
+    # every rank decided the same values in the same number of rounds, each
+    # self pair was aligned by its owner alone, and every one of them got a value
+    assert all(res[r][1] == res[0][1] and res[r][2] == res[0][2] for r in range(world))
+    assert res[0][4] == len(res[0][1]) == nself
+    rfp = sx.rank_for_pair(sx.contig_assignment_build(cs.clen, world)[0])
+    got = sorted(c for r in range(world) for c in res[r][3])
+    assert got == sorted(c for c, _ in res[0][1])
+    assert all(rfp[c, c] == r for r in range(world) for c in res[r][3])
+    if nself > 2:
+        assert sum(1 for r in range(world) if res[r][3]) >= 2
+
+
+def _fake_round(outcomes, log):
+    """align_round of one rank that owns every self pair: outcomes[c] =
+    (calls, exit bepos) whatever the entry value."""
+    def run(new):
+        log.append(dict(new))
+        return {c: outcomes[c] for c in new if c in outcomes}
+    return run
+
+
+def test_resolve_rows_and_waits():
+    from distributedpanga_b200 import sharded_order as so
+    # contigs 0..4 in order 0..4 (lengths decreasing), one range [0, 5)
+    pos, rs, n = np.arange(5), [0] * 5, 5
+    lk = np.zeros(n, dtype=np.int64)
+    eb = np.zeros(n, dtype=np.int64)
+    st = np.array([0, 1, 0, 1, 1], dtype=np.int64)
+    # row 2 has a later partner (position 4) that called: its exit bepos 77
+    lk[2] = (5 << 32) | 77
+    log = []
+    vals, rounds = so.resolve(n, pos, rs, lk, eb, st, _fake_round({1: (3, 41), 3: (0, 0), 4: (2, 9)}, log),
+                              lambda a: a)
+    # 1: nothing earlier in the first range (the unset value); 3: row 2's
+    # later partner; 4: waits for 3, which made no call, then row 2 again
+    assert vals == {1: so.UNSET_MAIN, 3: 77, 4: 77}
+    assert rounds == 2 and log == [{1: so.UNSET_MAIN, 3: 77}, {4: 77}]
+    # the same self pairs in a range that starts at 1: position 1 opens it (0)
+    vals, _ = so.resolve(n, pos, [0, 1, 1, 1, 1], lk, eb, st, _fake_round({1: (3, 41), 3: (0, 0), 4: (2, 9)}, []),
+                         lambda a: a)
+    assert vals == {1: 0, 3: 77, 4: 77}
+    # without row 2's call, 3 takes 1's exit bepos, and 4 then takes 3's
+    lk[2] = 0
+    vals, rounds = so.resolve(n, pos, rs, lk, eb, st, _fake_round({1: (3, 41), 3: (1, 12), 4: (2, 9)}, []),
+                              lambda a: a)
+    assert vals == {1: so.UNSET_MAIN, 3: 41, 4: 12} and rounds == 3
+    # an earlier partner that called decides at once
+    eb[4] = (2 << 32) | 5
+    vals, rounds = so.resolve(n, pos, rs, lk, eb, st, _fake_round({1: (3, 41), 3: (1, 12), 4: (2, 9)}, []),
+                              lambda a: a)
+    assert vals == {1: so.UNSET_MAIN, 3: 41, 4: 5} and rounds == 2
+    # a self pair that no rank reports stays pending: an error on every rank
+    with pytest.raises(RuntimeError):
+        so.resolve(n, pos, rs, lk, eb, st, _fake_round({1: (3, 41), 4: (2, 9)}, []), lambda a: a)
+
+
+def test_range_starts_and_keys():
+    from distributedpanga_b200 import sharded_order as so
+    perm, pos = so.order_positions([5, 9, 9, 1])
+    assert perm.tolist() == [1, 2, 0, 3] and pos.tolist() == [2, 0, 1, 3]
+    # four contigs of one part; seeds split into ranges of about 1/32 of the part
+    rs = so.range_starts([5, 9, 9, 1], [0, 10, 0, 0], 1, perm)
+    assert rs == [0, 1, 2, 3]
+    lk, eb = so.local_keys([(0, 1, 2, 30), (0, 3, 1, 40), (0, 0, 5, 1), (2, 0, 0, 7)], pos, 4)
+    # anchor 0 at position 2: partner 1 (position 0, earlier) and 3 (position 3, later)
+    assert lk.tolist() == [0, 0, (4 << 32) | 40, 0]
+    assert eb.tolist() == [0, 0, (1 << 32) | 30, 0]
