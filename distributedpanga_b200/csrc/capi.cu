@@ -3169,10 +3169,10 @@ int pga_align_set_ranges(pga_ctx *ctx, int64_t range_seeds) {
   return PGA_OK;
 }
 
-int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, const char *version,
-                         const char *command, const char *db_name, const char *cwd, int nscaff,
-                         const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
-                         const int64_t *contig_sbeg) {
+static int align_write_1aln(pga_ctx *ctx, bool binary, const char *path, const char *program, const char *version,
+                            const char *command, const char *db_name, const char *cwd, int nscaff,
+                            const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
+                            const int64_t *contig_sbeg) {
   if (!ctx || !ctx->have_align) return PGA_ERR_ARG;
   if (nscaff > 0 && scaff_fctg && scaff_fctg[nscaff] > ctx->ncontig) return PGA_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
@@ -3193,9 +3193,26 @@ int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, co
     r[7] = a.diffs;
     r[8] = a.tlen;
   }
-  return pga_write_1aln(path, program, version, command, db_name, cwd, aln::TSPACE, nscaff, scaff_name, scaff_len,
-                        scaff_fctg, contig_sbeg, ctx->clen.data(), n, r9.data(), ctx->h_toff.data(),
-                        ctx->h_trace.data());
+  return (binary ? pga_write_1aln_binary : pga_write_1aln)(path, program, version, command, db_name, cwd,
+                                                           aln::TSPACE, nscaff, scaff_name, scaff_len, scaff_fctg,
+                                                           contig_sbeg, ctx->clen.data(), n, r9.data(),
+                                                           ctx->h_toff.data(), ctx->h_trace.data());
+}
+
+int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, const char *version,
+                         const char *command, const char *db_name, const char *cwd, int nscaff,
+                         const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
+                         const int64_t *contig_sbeg) {
+  return align_write_1aln(ctx, false, path, program, version, command, db_name, cwd, nscaff, scaff_name, scaff_len,
+                          scaff_fctg, contig_sbeg);
+}
+
+int pga_align_write_1aln_binary(pga_ctx *ctx, const char *path, const char *program, const char *version,
+                                const char *command, const char *db_name, const char *cwd, int nscaff,
+                                const char *const *scaff_name, const int64_t *scaff_len,
+                                const int32_t *scaff_fctg, const int64_t *contig_sbeg) {
+  return align_write_1aln(ctx, true, path, program, version, command, db_name, cwd, nscaff, scaff_name, scaff_len,
+                          scaff_fctg, contig_sbeg);
 }
 
 int pga_align_stats(const pga_ctx *ctx, int64_t *stats8) {

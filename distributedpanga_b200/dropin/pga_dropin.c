@@ -433,9 +433,9 @@ void pair_sort_search(GDB *gdb1, GDB *gdb2) {
   int64_t nalign = 0;
   check(pga_align(ctx, &nalign), "pga_align");
   Pair_Search_Stats.search_s[0] = now_s() - t0;
-  /* la_merge's file: ONE "aln", its provenance and references, the skeleton
-   * of gdb1 (Write_Skeleton, lib/GDB.c:2059), then the alignments in la_sort
-   * order */
+  /* la_merge's file: ONE "aln" in the binary encoding open_Aln_Write asks
+   * for, its provenance and references, the skeleton of gdb1
+   * (Write_Skeleton, lib/GDB.c:2059), then the alignments in la_sort order */
   t0 = now_s();
   const int ns = gdb1->nscaff;
   const char **names = malloc(sizeof(char *) * (ns > 0 ? ns : 1));
@@ -455,8 +455,9 @@ void pair_sort_search(GDB *gdb1, GDB *gdb2) {
   char *cwd = getcwd(NULL, 0);
   if (!path) die("malloc", PGA_ERR_NOMEM);
   snprintf(path, plen, "%s/%s.1aln", SORT_PATH, ALGN_UNIQ);
-  check(pga_align_write_1aln(ctx, path, "pga-merge", "0.1", "pga-merge", path, cwd, ns, names, slen, fctg, sbeg),
-        "pga_align_write_1aln");
+  check(pga_align_write_1aln_binary(ctx, path, "pga-merge", "0.1", "pga-merge", path, cwd, ns, names, slen, fctg,
+                                    sbeg),
+        "pga_align_write_1aln_binary");
   Pair_Search_Stats.la_merge_s = now_s() - t0;
   free(cwd);
   free(path);

@@ -82,6 +82,10 @@ _SIGS = {
                                  C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
     "pga_align_write_1aln": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                        C.c_char_p, C.c_int, vp, vp, vp, vp]),
+    "pga_write_1aln_binary": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                        C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
+    "pga_align_write_1aln_binary": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+                                              C.c_char_p, C.c_int, vp, vp, vp, vp]),
     "pga_reimport_sort_noalloc": (C.c_int, [vp, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64,
                                             C.c_int, vp, vp, vp]),
     "pga_gdb_ingest_fasta": (C.c_int, [vp, C.c_char_p, C.c_int64, C.c_int, vp]),
@@ -419,14 +423,15 @@ class Device:
         self._ck(self.L.pga_align_times(self.h, a), "align_times")
         return {"setup": a[0], "pairs": a[1], "self_pairs": a[2], "order": a[3]}
 
-    def write_1aln(self, path, skeleton=None, db_name="", cwd=None, command="distributedpanga_b200"):
-        """The last align()'s alignments as a .1aln file."""
+    def write_1aln(self, path, skeleton=None, db_name="", cwd=None, command="distributedpanga_b200", binary=False):
+        """The last align()'s alignments as a .1aln file, in ONE's ASCII or
+        (binary=True, as the reference writes it) binary encoding."""
         sk = skeleton or Skeleton.per_contig(self.cs.clen)
         names = sk.c_names()
-        self._ck(self.L.pga_align_write_1aln(self.h, path.encode(), _PROG, _VERSION, command.encode(),
-                                             db_name.encode(), cwd.encode() if cwd else None, len(sk.names), names,
-                                             sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp),
-                                             sk.sbeg.ctypes.data_as(vp)), "align_write_1aln")
+        fn = self.L.pga_align_write_1aln_binary if binary else self.L.pga_align_write_1aln
+        self._ck(fn(self.h, path.encode(), _PROG, _VERSION, command.encode(), db_name.encode(),
+                    cwd.encode() if cwd else None, len(sk.names), names, sk.scaff_len.ctypes.data_as(vp),
+                    sk.fctg.ctypes.data_as(vp), sk.sbeg.ctypes.data_as(vp)), "align_write_1aln")
 
     def local_alignment(self, requests):
         """Local_Alignment for each request row (a, b, comp, low, hgh, anti,
@@ -604,9 +609,10 @@ _VERSION = b"0.1"
 
 
 def write_1aln(path, recs, toff, trace, contig_len, skeleton=None, db_name="", cwd=None,
-               command="distributedpanga_b200", tspace=100):
+               command="distributedpanga_b200", tspace=100, binary=False):
     """Writes alignments (as Device.alignments() returns them) as a .1aln file
-    (la_merge's output, src/fastga_pipeline.c:1616-1656)."""
+    (la_merge's output, src/fastga_pipeline.c:1616-1656), in ONE's ASCII or
+    (binary=True, as the reference writes it) binary encoding."""
     L = load_library()
     contig_len = np.ascontiguousarray(contig_len, dtype=np.int64)
     sk = skeleton or Skeleton.per_contig(contig_len)
@@ -616,11 +622,11 @@ def write_1aln(path, recs, toff, trace, contig_len, skeleton=None, db_name="", c
     if trace.size == 0:
         trace = np.zeros(1, dtype=np.uint8)
     names = sk.c_names()
-    rc = L.pga_write_1aln(path.encode(), _PROG, _VERSION, command.encode(), db_name.encode(),
-                          cwd.encode() if cwd else None, int(tspace), len(sk.names), names,
-                          sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp), sk.sbeg.ctypes.data_as(vp),
-                          contig_len.ctypes.data_as(vp), int(len(recs)), recs.ctypes.data_as(vp),
-                          toff.ctypes.data_as(vp), trace.ctypes.data_as(vp))
+    fn = L.pga_write_1aln_binary if binary else L.pga_write_1aln
+    rc = fn(path.encode(), _PROG, _VERSION, command.encode(), db_name.encode(), cwd.encode() if cwd else None,
+            int(tspace), len(sk.names), names, sk.scaff_len.ctypes.data_as(vp), sk.fctg.ctypes.data_as(vp),
+            sk.sbeg.ctypes.data_as(vp), contig_len.ctypes.data_as(vp), int(len(recs)), recs.ctypes.data_as(vp),
+            toff.ctypes.data_as(vp), trace.ctypes.data_as(vp))
     if rc != 0:
         raise PgaError("write_1aln(%s): status %d" % (path, rc))
 

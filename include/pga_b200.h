@@ -369,12 +369,31 @@ int pga_write_1aln(const char *path, const char *program, const char *version, c
                    const int64_t *contig_len, int64_t nalign, const int32_t *recs9, const int64_t *trace_off,
                    const uint8_t *trace);
 
+/* The same file in ONE's binary encoding, the one the reference's
+ * open_Aln_Write asks ONElib for (lib/alncode.c:251, isBinary true): the
+ * same header up to the line definitions, then "$ 0" (little-endian), the
+ * lines as one code byte and their fields (variable-length integers,
+ * difference-coded integer lists), and a footer with the counts, list
+ * maxima and totals, per-object statistics and the objects' byte index that
+ * ONE readers use.  Lists are written uncompressed (ONElib Huffman-codes
+ * them after 100,000 bytes; its readers decode either per line).  Host
+ * only. */
+int pga_write_1aln_binary(const char *path, const char *program, const char *version, const char *command,
+                          const char *db_name, const char *cwd, int tspace, int nscaff,
+                          const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
+                          const int64_t *contig_sbeg, const int64_t *contig_len, int64_t nalign,
+                          const int32_t *recs9, const int64_t *trace_off, const uint8_t *trace);
+
 /* The same for the alignments of the last pga_align, with the loaded
- * contigs' lengths. */
+ * contigs' lengths: ASCII, or binary (pga_align_write_1aln_binary). */
 int pga_align_write_1aln(pga_ctx *ctx, const char *path, const char *program, const char *version,
                          const char *command, const char *db_name, const char *cwd, int nscaff,
                          const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,
                          const int64_t *contig_sbeg);
+int pga_align_write_1aln_binary(pga_ctx *ctx, const char *path, const char *program, const char *version,
+                                const char *command, const char *db_name, const char *cwd, int nscaff,
+                                const char *const *scaff_name, const int64_t *scaff_len,
+                                const int32_t *scaff_fctg, const int64_t *contig_sbeg);
 
 /* ---- seed diagonal sort without device allocation ---------------------------- */
 

@@ -1,6 +1,9 @@
-"""The .1aln writer (pga_write_1aln): files it writes read back, through the
-reference's own ONE reader (oracle/_ref/alndump, open_Aln_Read), as the
-reference's alignment record stream and GDB skeleton."""
+"""The .1aln writers (pga_write_1aln, ONE's ASCII encoding, and
+pga_write_1aln_binary, its binary one): files they write read back, through
+the reference's own ONE reader (oracle/_ref/alndump, open_Aln_Read), as the
+reference's alignment record stream and GDB skeleton; a binary file's footer
+(counts, list sizes, per-object statistics, the objects' byte index) reads
+back as the reference's own binary file's does (oracle/_ref/onestat)."""
 import gzip
 import os
 import subprocess
@@ -12,7 +15,9 @@ import pytest
 from conftest import GOLDEN, GOLDEN_CASES, ROOT, load_case
 
 ALNDUMP = os.path.join(ROOT, "oracle", "_ref", "alndump")
-needs_ref = pytest.mark.skipif(not os.path.exists(ALNDUMP), reason="oracle/_ref not built")
+ONESTAT = os.path.join(ROOT, "oracle", "_ref", "onestat")
+needs_ref = pytest.mark.skipif(not os.path.exists(ALNDUMP) or not os.path.exists(ONESTAT),
+                               reason="oracle/_ref not built")
 
 
 def parse_lines(lines):
@@ -39,9 +44,14 @@ def dump(path, skel=False):
     return [" ".join(l.split()) for l in out.split("\n") if l.strip() and not l.startswith("#")]
 
 
+def stat(path):
+    return subprocess.run([ONESTAT, path], check=True, capture_output=True, text=True).stdout.split("\n")
+
+
 @needs_ref
+@pytest.mark.parametrize("binary", [False, True])
 @pytest.mark.parametrize("case", GOLDEN_CASES + ["small_full"])
-def test_written_file_reads_back_as_reference_stream(case):
+def test_written_file_reads_back_as_reference_stream(case, binary):
     from distributedpanga_b200 import pipeline
     cs, dig = load_case(case)
     ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n")
@@ -49,38 +59,94 @@ def test_written_file_reads_back_as_reference_stream(case):
     recs, toff, tr = parse_lines(ref)
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "out.1aln")
-        pipeline.write_1aln(p, recs, toff, tr, cs.clen, db_name="g.1gdb", cwd=d)
+        pipeline.write_1aln(p, recs, toff, tr, cs.clen, db_name="g.1gdb", cwd=d, binary=binary)
         got = dump(p)
+        st = stat(p)
     assert len(got) == dig["aln"]["count"]
     assert got == ref
+    assert st[0] == "binary %d" % binary
+    if binary:  # every alignment reached through the index, last first
+        assert [l.split()[3:] for l in st if l.startswith("@ A ")] == [l.split()[:6] for l in reversed(ref)]
 
 
 @needs_ref
-def test_skeleton_and_records_equal_reference_file():
-    """The reference's own .1aln for a small contig set and the file written
-    here from its records and the FASTA's contigs read back identically,
-    skeleton included."""
+@pytest.mark.parametrize("kind,scale", [("small", 0.02), ("pangenome", 0.01)])
+def test_skeleton_and_records_equal_reference_file(kind, scale):
+    """The reference's own .1aln for a contig set and the files written here
+    from its records and the FASTA's contigs read back identically, skeleton
+    included; the binary one's footer reads back as the reference's does
+    (the pan-genome's lists pass the 100,000 bytes after which the
+    reference's ONElib Huffman-codes them; the lists here stay uncoded)."""
     from distributedpanga_b200 import pipeline, synth
     from oracle import binding as B
-    contigs = synth.make("small", scale=0.02)
+    contigs = synth.make(kind, scale=scale)
     with tempfile.TemporaryDirectory() as d:
         fa = os.path.join(d, "g.fa")
         synth.write_fasta(fa, contigs)
         B.ref_make_gdb(fa, os.path.join(d, "g"))
         out = B.ref_run(os.path.join(d, "g"), d)
         ref_full = dump(out["aln"], skel=True)
+        ref_stat = stat(out["aln"])
         ref_recs = [l for l in ref_full if ";" in l]
         recs, toff, tr = parse_lines(ref_recs)
-        p = os.path.join(d, "mine.1aln")
-        pipeline.write_1aln(p, recs, toff, tr, [len(c) for c in contigs], db_name="g.1gdb", cwd=d)
-        mine_full = dump(p, skel=True)
+        mine = {}
+        for binary in (False, True):
+            p = os.path.join(d, "mine%d.1aln" % binary)
+            pipeline.write_1aln(p, recs, toff, tr, [len(c) for c in contigs], db_name="g.1gdb", cwd=d,
+                                binary=binary)
+            mine[binary] = (dump(p, skel=True), stat(p))
     assert len(ref_recs) > 0
     assert any(l.startswith("S ") for l in ref_full)
-    assert mine_full == ref_full
+    assert ref_stat[0] == "binary 1"
+    assert mine[False][0] == ref_full
+    assert mine[True][0] == ref_full
+    assert mine[True][1] == ref_stat
+
+
+@needs_ref
+def test_binary_encoding_edges():
+    """Values at every width of ONE's variable-length integers, trace lists of
+    0, 1 and many values whose differences need one or two bytes, scaffolds
+    with leading, inner and trailing gaps, and files with no skeleton or no
+    alignments: the binary file reads back as the ASCII one does, and its
+    index reaches every object."""
+    from distributedpanga_b200 import pipeline
+    rng = np.random.default_rng(7)
+    widths = [0, 1, 63, 64, 8191, 8192, 65535, 65536, 2 ** 24 - 1, 2 ** 24, 2 ** 31 - 1]
+    recs, toff, tr = [], [0], []
+    for i, v in enumerate(widths * 3):
+        n = [0, 1, 2, 37, 200][i % 5]
+        t = rng.integers(0, 256, 2 * n) if i % 2 else rng.integers(0, 40, 2 * n)
+        recs.append([i % 4, v, v, (i + 1) % 4, widths[(i + 3) % len(widths)], v, i % 2, v, 2 * n])
+        tr += t.tolist()
+        toff.append(len(tr))
+    recs = np.array(recs, dtype=np.int64).clip(0, 2 ** 31 - 1).astype(np.int32)
+    toff = np.array(toff, dtype=np.int64)
+    tr = np.array(tr, dtype=np.uint8)
+    clen = np.array([2 ** 33, 70, 9000, 5], dtype=np.int64)
+    sk = pipeline.Skeleton(["chr with space", "b" * 300, "c"], [2 ** 33 + 100, 10000, 5], [0, 1, 3, 4],
+                           [100, 0, 500, 0])
+    with tempfile.TemporaryDirectory() as d:
+        for skel, n in ((sk, len(recs)), (sk, 0), (None, len(recs))):
+            got = {}
+            for binary in (False, True):
+                p = os.path.join(d, "e%d.1aln" % binary)
+                pipeline.write_1aln(p, recs[:n], toff[:n + 1], tr, clen, skeleton=skel, db_name="g.1gdb",
+                                    binary=binary)
+                got[binary] = (dump(p, skel=True), stat(p))
+            assert got[True][0] == got[False][0]
+            st = got[True][1]
+            assert [int(l.split()[2]) for l in st if l.startswith("@ A ")] == list(range(n, 0, -1))
+            assert all("unreachable" not in l for l in st)
+            if n:
+                assert ("# A %d 0 0" % n) in st
 
 
 def test_writer_rejects_bad_arguments():
     from distributedpanga_b200 import pipeline
     L = pipeline.load_library()
-    assert L.pga_write_1aln(b"/tmp/x.1aln", None, b"v", b"c", b"db", None, 100, 0, None, None, None, None, None,
-                            0, None, None, None) == 2
+    for fn in (L.pga_write_1aln, L.pga_write_1aln_binary):
+        assert fn(b"/tmp/x.1aln", None, b"v", b"c", b"db", None, 100, 0, None, None, None, None, None,
+                  0, None, None, None) == 2
+        assert fn(b"/tmp/x.1aln", b"p", b"v", b"c", b"db", None, 0, 0, None, None, None, None, None,
+                  0, None, None, None) == 2

@@ -237,10 +237,11 @@ def test_alignments_independent_of_kernel_build(dev, case):
         dev.set_long_waves(-1)
 
 
+@pytest.mark.parametrize("binary", [False, True])
 @pytest.mark.parametrize("case", ["small_s002", "edge_mix"])
-def test_1aln_file_matches_reference(dev, case):
-    """The GPU path's .1aln file, read by the reference's own reader, is the
-    reference's record stream."""
+def test_1aln_file_matches_reference(dev, case, binary):
+    """The GPU path's .1aln file, in either ONE encoding, read by the
+    reference's own reader, is the reference's record stream."""
     import gzip
     import os
     import subprocess
@@ -256,7 +257,7 @@ def test_1aln_file_matches_reference(dev, case):
     dev.align()
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "out.1aln")
-        dev.write_1aln(p, db_name="g.1gdb", cwd=d)
+        dev.write_1aln(p, db_name="g.1gdb", cwd=d, binary=binary)
         out = subprocess.run([alndump, p], check=True, capture_output=True, text=True).stdout
     mine = [" ".join(l.split()) for l in out.split("\n") if l.strip() and not l.startswith("#")]
     ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, case + ".aln.txt.gz"), "rt").read().split("\n")
