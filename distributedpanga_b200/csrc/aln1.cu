@@ -15,10 +15,12 @@
 //   X n differences per trace interval
 //
 // Host code only; it needs no GPU.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <memory>
 #include <string>
 #include <vector>
 #include "../../include/pga_b200.h"
@@ -118,13 +120,16 @@ void write_head(FILE *f, const char *program, const char *version, const char *c
 // the type, then offset 0 = the data's start and offset i = object i's
 // line).  "^\n" ends it, and the file's last 8 bytes are the footer's offset.
 //
-// The line code is 0x80 | c << 1, c = 0-25 for 'A'-'Z', 26-51 for 'a'-'z'
-// and 53 for '&'.  Bit 0 set says the line's list is Huffman-coded with a
-// codec trained on the file's earlier lists (ONElib switches to one after
-// 100,000 list bytes); it stays clear here, every list is written as it is,
-// and readers decode either per line.
+// The line code is 0x80 | c << 1, c = 0-25 for 'A'-'Z', 26-51 for 'a'-'z',
+// 52 for a list codec line ';' and 53 for '&'.  Bit 0 set says the line's
+// list is coded with its type's list codec: the number of bits, then the
+// coded bytes.  The codec is a ';' line of the footer (the type, then the
+// serialized codec as a string).  ONElib builds one from a type's first
+// 100,000 list bytes and codes every later list; here the trace lists' codec
+// is built from all of them, and a list is coded where that is shorter.
+// Readers decode per line, either way.
 uint8_t line_code(char t) {
-  int c = (t >= 'A' && t <= 'Z') ? t - 'A' : (t >= 'a' && t <= 'z') ? 26 + t - 'a' : 53;
+  int c = (t >= 'A' && t <= 'Z') ? t - 'A' : (t >= 'a' && t <= 'z') ? 26 + t - 'a' : t == ';' ? 52 : 53;
   return (uint8_t)(0x80 | (c << 1));
 }
 
@@ -151,6 +156,154 @@ int ltf(uint8_t *u, int64_t v) {
   return 1 + k;
 }
 
+// An integer list's bytes after its first value: the width w (1..8) of its
+// successive differences, and each difference's w low bytes, little-endian
+// (sign-extended on reading).  w is the fewest bytes that hold every
+// difference with its sign bit.
+int compact_diffs(const int64_t *v, int64_t n, std::vector<uint8_t> &out) {
+  uint64_t m = 0;
+  for (int64_t i = 1; i < n; i++) {
+    const int64_t d = v[i] - v[i - 1];
+    m |= d >= 0 ? (uint64_t)d : ~(uint64_t)d;
+  }
+  int w = 1;
+  for (m >>= 7; w < 8 && m != 0; m >>= 8) w++;
+  out.clear();
+  for (int64_t i = 1; i < n; i++) {
+    const uint64_t d = (uint64_t)(v[i] - v[i - 1]);
+    for (int b = 0; b < w; b++) out.push_back((uint8_t)(d >> (8 * b)));
+  }
+  return w;
+}
+
+// A line type's list codec: a prefix code over bytes with codes of at most
+// CODE_MAX bits, in the form ONE readers take (vcDeserialize / vcDecode,
+// lib/ONElib.c:3338-3735).  The code lengths are the optimal ones under
+// that limit, by package-merge (Larmore & Hirschberg, J. ACM 37(3), 1990)
+// over the byte histogram of all the type's lists; codes are canonical
+// (by length, then byte).  Every byte that occurs has a code, so there is
+// no escape code.
+struct ListCodec {
+  static constexpr int CODE_MAX = 12;
+  uint8_t len[256] = {};
+  uint16_t bits[256] = {};
+
+  explicit ListCodec(const uint64_t *hist) {
+    std::vector<int> sym;
+    for (int s = 0; s < 256; s++)
+      if (hist[s]) sym.push_back(s);
+    const int n = (int)sym.size();
+    if (n == 0) return;
+    if (n == 1) {
+      len[sym[0]] = 1;
+    } else {
+      std::stable_sort(sym.begin(), sym.end(), [&](int a, int b) { return hist[a] < hist[b]; });
+      // items: a weight and how often each symbol (by rank) is in it
+      struct Item {
+        uint64_t w;
+        std::vector<uint16_t> c;
+      };
+      std::vector<Item> leaves((size_t)n), cur;
+      for (int i = 0; i < n; i++) {
+        leaves[(size_t)i].w = hist[sym[(size_t)i]];
+        leaves[(size_t)i].c.assign((size_t)n, 0);
+        leaves[(size_t)i].c[(size_t)i] = 1;
+      }
+      cur = leaves;
+      for (int level = 1; level < CODE_MAX; level++) {
+        std::vector<Item> pk;
+        for (size_t k = 0; k + 1 < cur.size(); k += 2) {
+          Item p{cur[k].w + cur[k + 1].w, cur[k].c};
+          for (int i = 0; i < n; i++) p.c[(size_t)i] += cur[k + 1].c[(size_t)i];
+          pk.push_back(std::move(p));
+        }
+        std::vector<Item> next;
+        size_t a = 0, b = 0;
+        while (a < leaves.size() || b < pk.size())
+          if (b >= pk.size() || (a < leaves.size() && leaves[a].w <= pk[b].w))
+            next.push_back(leaves[a++]);
+          else
+            next.push_back(std::move(pk[b++]));
+        cur = std::move(next);
+      }
+      for (size_t k = 0; k < (size_t)(2 * n - 2); k++)
+        for (int i = 0; i < n; i++) len[sym[(size_t)i]] = (uint8_t)(len[sym[(size_t)i]] + cur[k].c[(size_t)i]);
+    }
+    std::vector<int> order;
+    for (int s = 0; s < 256; s++)
+      if (len[s]) order.push_back(s);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return len[a] < len[b]; });
+    uint32_t code = 0;
+    int prev = len[order[0]];
+    for (int s : order) {
+      code <<= (len[s] - prev);
+      prev = len[s];
+      bits[s] = (uint16_t)code++;
+    }
+  }
+
+  // vcSerialize's layout: big-endian flag, escape code and its length (two
+  // ints), then per byte its code length and, where nonzero, its code.
+  std::vector<uint8_t> serial() const {
+    std::vector<uint8_t> o;
+    o.push_back(0);
+    const int32_t esc = -1, elen = 0;
+    for (int32_t v : {esc, elen})
+      for (int b = 0; b < 4; b++) o.push_back((uint8_t)((uint32_t)v >> (8 * b)));
+    for (int s = 0; s < 256; s++) {
+      o.push_back(len[s]);
+      if (len[s]) {
+        o.push_back((uint8_t)(bits[s] & 0xff));
+        o.push_back((uint8_t)(bits[s] >> 8));
+      }
+    }
+    return o;
+  }
+
+  // The coded form of in (vcEncode's): a bit stream of two flag bits (0 0:
+  // written little-endian) and the bytes' codes, cut into 64-bit words
+  // whose first bit is the most significant; each whole word stored as a
+  // little-endian integer, the last part word's bytes most significant
+  // first, and, when there is a whole word, the file's bytes 0 and 7
+  // exchanged so that the flag bits come first.  Returns the bit count.
+  int64_t encode(const std::vector<uint8_t> &in, std::vector<uint8_t> &out) const {
+    std::vector<uint64_t> words;
+    uint64_t cur = 0;
+    int used = 0;
+    int64_t nbits = 0;
+    auto put = [&](uint32_t c, int l) {
+      nbits += l;
+      if (used + l <= 64) {
+        cur |= (uint64_t)c << (64 - used - l);
+        used += l;
+      } else {
+        const int r = used + l - 64;
+        cur |= (uint64_t)c >> r;
+        words.push_back(cur);
+        cur = (uint64_t)c << (64 - r);
+        used = r;
+      }
+      if (used == 64) {
+        words.push_back(cur);
+        cur = 0;
+        used = 0;
+      }
+    };
+    put(0, 2);
+    for (uint8_t x : in) put(bits[x], len[x]);
+    out.clear();
+    for (uint64_t w : words)
+      for (int b = 0; b < 8; b++) out.push_back((uint8_t)(w >> (8 * b)));
+    for (int k = 0; k < (used + 7) / 8; k++) out.push_back((uint8_t)(cur >> (56 - 8 * k)));
+    if (!words.empty()) std::swap(out[0], out[7]);
+    return nbits;
+  }
+};
+
+// Trace lists are coded only when their compacted bytes reach this many
+// (below it the codec's own ~300 bytes would not pay).
+constexpr uint64_t CODEC_MIN_BYTES = 4096;
+
 class BinOut {
  public:
   BinOut(FILE *f, int64_t pos) : f_(f), pos_(pos) { buf_.reserve(CHUNK + 4096); }
@@ -168,23 +321,13 @@ class BinOut {
     uint8_t u[9];
     bytes(u, (size_t)ltf(u, v));
   }
-  // an integer list of n >= 1 values, after its length
+  // an uncoded integer list of n >= 1 values, after its length
   void int_list(const int64_t *v, int64_t n) {
     integer(v[0]);
     if (n == 1) return;
-    uint64_t m = 0;
-    for (int64_t i = 1; i < n; i++) {
-      const int64_t d = v[i] - v[i - 1];
-      m |= d >= 0 ? (uint64_t)d : ~(uint64_t)d;
-    }
-    int w = 1;
-    for (m >>= 7; w < 8 && m != 0; m >>= 8) w++;
+    const int w = compact_diffs(v, n, tmp_);
     byte((uint8_t)w);
-    for (int64_t i = 1; i < n; i++) {
-      const uint64_t d = (uint64_t)(v[i] - v[i - 1]);
-      for (int b = 0; b < w; b++) buf_.push_back((uint8_t)(d >> (8 * b)));
-      spill();
-    }
+    bytes(tmp_.data(), tmp_.size());
   }
   void text(const char *fmt, long long a, long long b = 0) {
     char line[96];
@@ -206,7 +349,7 @@ class BinOut {
   }
   FILE *f_;
   int64_t pos_;
-  std::vector<uint8_t> buf_;
+  std::vector<uint8_t> buf_, tmp_;
   bool ok_ = true;
 };
 
@@ -343,7 +486,32 @@ extern "C" int pga_write_1aln_binary(const char *path, const char *program, cons
   }
 
   // alignments
+  // the trace lists' codecs (T: b-deltas, the odd trace bytes; X: diffs, the
+  // even ones), from the byte histogram of all their compacted lists
   std::vector<int64_t> list;
+  std::vector<uint8_t> raw, enc;
+  auto trace_list = [&](const uint8_t *tr, int64_t n, int pass) {
+    list.resize((size_t)n);
+    for (int64_t x = 0; x < n; x++) list[(size_t)x] = tr[2 * x + (pass ? 0 : 1)];
+  };
+  std::unique_ptr<ListCodec> codec[2];
+  {
+    uint64_t hist[2][256] = {};
+    uint64_t total[2] = {0, 0};
+    for (int64_t i = 0; i < nalign; i++) {
+      const int64_t n = recs9[9 * i + 8] / 2;
+      if (n < 2) continue;
+      for (int pass = 0; pass < 2; pass++) {
+        trace_list(trace + trace_off[i], n, pass);
+        compact_diffs(list.data(), n, raw);
+        for (uint8_t x : raw) hist[pass][x]++;
+        total[pass] += raw.size();
+      }
+    }
+    for (int pass = 0; pass < 2; pass++)
+      if (total[pass] >= CODEC_MIN_BYTES) codec[pass].reset(new ListCodec(hist[pass]));
+  }
+
   ix_A.reserve((size_t)nalign + 1);
   for (int64_t i = 0; i < nalign; i++) {
     const int32_t *r = recs9 + 9 * i;
@@ -358,13 +526,31 @@ extern "C" int pga_write_1aln_binary(const char *path, const char *program, cons
     }
     o.byte(line_code('D'));
     o.integer(r[7]);
-    list.resize((size_t)n);
-    for (int pass = 0; pass < 2; pass++) {  // T: b-deltas (odd bytes), X: diffs (even bytes)
-      o.byte(line_code(pass ? 'X' : 'T'));
+    for (int pass = 0; pass < 2; pass++) {
+      trace_list(tr, n, pass);
+      int w = 0;
+      int64_t nbits = 0;
+      bool coded = false;
+      if (n >= 2) {
+        w = compact_diffs(list.data(), n, raw);
+        if (codec[pass]) {
+          uint8_t u[9];
+          nbits = codec[pass]->encode(raw, enc);
+          coded = ltf(u, nbits) + enc.size() < raw.size();
+        }
+      }
+      o.byte((uint8_t)(line_code(pass ? 'X' : 'T') | (coded ? 1 : 0)));
       o.integer(n);
       if (n == 0) continue;
-      for (int64_t x = 0; x < n; x++) list[(size_t)x] = tr[2 * x + (pass ? 0 : 1)];
-      o.int_list(list.data(), n);
+      o.integer(list[0]);
+      if (n == 1) continue;
+      o.byte((uint8_t)w);
+      if (coded) {
+        o.integer(nbits);
+        o.bytes(enc.data(), enc.size());
+      } else {
+        o.bytes(raw.data(), raw.size());
+      }
     }
     tmax = n > tmax ? n : tmax;
     ttot += n;
@@ -407,10 +593,17 @@ extern "C" int pga_write_1aln_binary(const char *path, const char *program, cons
     index('A', ix_A);
     if (nR) o.text("# R %lld\n", nR);
     o.text("# D %lld\n", nalign);
-    for (char t : {'T', 'X'}) {
-      o.text(t == 'T' ? "# T %lld\n" : "# X %lld\n", nalign);
-      if (tmax) o.text(t == 'T' ? "@ T %lld\n" : "@ X %lld\n", tmax);
-      if (ttot) o.text(t == 'T' ? "+ T %lld\n" : "+ X %lld\n", ttot);
+    for (int pass = 0; pass < 2; pass++) {
+      o.text(pass ? "# X %lld\n" : "# T %lld\n", nalign);
+      if (tmax) o.text(pass ? "@ X %lld\n" : "@ T %lld\n", tmax);
+      if (ttot) o.text(pass ? "+ X %lld\n" : "+ T %lld\n", ttot);
+      if (codec[pass]) {
+        const std::vector<uint8_t> ser = codec[pass]->serial();
+        o.byte(line_code(';'));
+        o.byte((uint8_t)(pass ? 'X' : 'T'));
+        o.integer((int64_t)ser.size());
+        o.bytes(ser.data(), ser.size());
+      }
     }
   }
   o.text("^\n", 0);

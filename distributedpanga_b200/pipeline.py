@@ -423,9 +423,9 @@ class Device:
         self._ck(self.L.pga_align_times(self.h, a), "align_times")
         return {"setup": a[0], "pairs": a[1], "self_pairs": a[2], "order": a[3]}
 
-    def write_1aln(self, path, skeleton=None, db_name="", cwd=None, command="distributedpanga_b200", binary=False):
-        """The last align()'s alignments as a .1aln file, in ONE's ASCII or
-        (binary=True, as the reference writes it) binary encoding."""
+    def write_1aln(self, path, skeleton=None, db_name="", cwd=None, command="distributedpanga_b200", binary=True):
+        """The last align()'s alignments as a .1aln file, in ONE's binary
+        encoding as the reference writes it, or (binary=False) its ASCII one."""
         sk = skeleton or Skeleton.per_contig(self.cs.clen)
         names = sk.c_names()
         fn = self.L.pga_align_write_1aln_binary if binary else self.L.pga_align_write_1aln
@@ -609,10 +609,10 @@ _VERSION = b"0.1"
 
 
 def write_1aln(path, recs, toff, trace, contig_len, skeleton=None, db_name="", cwd=None,
-               command="distributedpanga_b200", tspace=100, binary=False):
+               command="distributedpanga_b200", tspace=100, binary=True):
     """Writes alignments (as Device.alignments() returns them) as a .1aln file
-    (la_merge's output, src/fastga_pipeline.c:1616-1656), in ONE's ASCII or
-    (binary=True, as the reference writes it) binary encoding."""
+    (la_merge's output, src/fastga_pipeline.c:1616-1656), in ONE's binary
+    encoding as the reference writes it, or (binary=False) its ASCII one."""
     L = load_library()
     contig_len = np.ascontiguousarray(contig_len, dtype=np.int64)
     sk = skeleton or Skeleton.per_contig(contig_len)

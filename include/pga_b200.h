@@ -375,9 +375,10 @@ int pga_write_1aln(const char *path, const char *program, const char *version, c
  * lines as one code byte and their fields (variable-length integers,
  * difference-coded integer lists), and a footer with the counts, list
  * maxima and totals, per-object statistics and the objects' byte index that
- * ONE readers use.  Lists are written uncompressed (ONElib Huffman-codes
- * them after 100,000 bytes; its readers decode either per line).  Host
- * only. */
+ * ONE readers use.  Trace lists are coded with a length-limited Huffman
+ * code built from all of them (stored in the footer as ONElib stores its
+ * codecs) wherever that is shorter; ONElib builds its code from a type's
+ * first 100,000 list bytes.  Host only. */
 int pga_write_1aln_binary(const char *path, const char *program, const char *version, const char *command,
                           const char *db_name, const char *cwd, int tspace, int nscaff,
                           const char *const *scaff_name, const int64_t *scaff_len, const int32_t *scaff_fctg,

@@ -74,9 +74,11 @@ def test_written_file_reads_back_as_reference_stream(case, binary):
 def test_skeleton_and_records_equal_reference_file(kind, scale):
     """The reference's own .1aln for a contig set and the files written here
     from its records and the FASTA's contigs read back identically, skeleton
-    included; the binary one's footer reads back as the reference's does
-    (the pan-genome's lists pass the 100,000 bytes after which the
-    reference's ONElib Huffman-codes them; the lists here stay uncoded)."""
+    included; the binary one's footer reads back as the reference's does.
+    The pan-genome's trace lists pass the 100,000 bytes after which the
+    reference's ONElib codes them, and the binary file here codes them too
+    (its codec built from all of them): it is no larger than the
+    reference's."""
     from distributedpanga_b200 import pipeline, synth
     from oracle import binding as B
     contigs = synth.make(kind, scale=scale)
@@ -95,28 +97,38 @@ def test_skeleton_and_records_equal_reference_file(kind, scale):
             pipeline.write_1aln(p, recs, toff, tr, [len(c) for c in contigs], db_name="g.1gdb", cwd=d,
                                 binary=binary)
             mine[binary] = (dump(p, skel=True), stat(p))
+        sizes = (os.path.getsize(out["aln"]), os.path.getsize(os.path.join(d, "mine1.1aln")))
     assert len(ref_recs) > 0
     assert any(l.startswith("S ") for l in ref_full)
     assert ref_stat[0] == "binary 1"
     assert mine[False][0] == ref_full
     assert mine[True][0] == ref_full
     assert mine[True][1] == ref_stat
+    if kind == "pangenome":
+        assert sizes[1] <= sizes[0], sizes
 
 
 @needs_ref
-def test_binary_encoding_edges():
+@pytest.mark.parametrize("regime", ["few", "many", "constant"])
+def test_binary_encoding_edges(regime):
     """Values at every width of ONE's variable-length integers, trace lists of
     0, 1 and many values whose differences need one or two bytes, scaffolds
     with leading, inner and trailing gaps, and files with no skeleton or no
     alignments: the binary file reads back as the ASCII one does, and its
-    index reaches every object."""
+    index reaches every object.  "few" stays below the size at which trace
+    lists are coded; "many" codes them (differences of one and two bytes,
+    lists left uncoded where coding does not pay); "constant" codes lists
+    whose bytes are all one value (a one-symbol code)."""
     from distributedpanga_b200 import pipeline
     rng = np.random.default_rng(7)
     widths = [0, 1, 63, 64, 8191, 8192, 65535, 65536, 2 ** 24 - 1, 2 ** 24, 2 ** 31 - 1]
     recs, toff, tr = [], [0], []
-    for i, v in enumerate(widths * 3):
+    for i, v in enumerate(widths * (3 if regime == "few" else 40)):
         n = [0, 1, 2, 37, 200][i % 5]
-        t = rng.integers(0, 256, 2 * n) if i % 2 else rng.integers(0, 40, 2 * n)
+        if regime == "constant":
+            t = np.full(2 * n, 100)
+        else:
+            t = rng.integers(0, 256, 2 * n) if i % 2 else rng.integers(0, 40, 2 * n)
         recs.append([i % 4, v, v, (i + 1) % 4, widths[(i + 3) % len(widths)], v, i % 2, v, 2 * n])
         tr += t.tolist()
         toff.append(len(tr))
@@ -134,6 +146,10 @@ def test_binary_encoding_edges():
                 pipeline.write_1aln(p, recs[:n], toff[:n + 1], tr, clen, skeleton=skel, db_name="g.1gdb",
                                     binary=binary)
                 got[binary] = (dump(p, skel=True), stat(p))
+                if binary:  # the footer (at the offset in the last 8 bytes) has the trace codecs or not
+                    b = open(p, "rb").read()
+                    foot = b[int.from_bytes(b[-8:], "little"):]
+                    assert (b"\xe8T" in foot) == (regime != "few" and n > 0)
             assert got[True][0] == got[False][0]
             st = got[True][1]
             assert [int(l.split()[2]) for l in st if l.startswith("@ A ")] == list(range(n, 0, -1))
