@@ -329,9 +329,17 @@ class BinOut {
     byte((uint8_t)w);
     bytes(tmp_.data(), tmp_.size());
   }
-  void text(const char *fmt, long long a, long long b = 0) {
-    char line[96];
-    const int n = snprintf(line, sizeof(line), fmt, a, b);
+  // footer text lines: "k t v" for k = '#' count, '@' largest list, '+'
+  // list total; "% t k u v" for object type t's largest count (k '#') or
+  // list total (k '+') of line type u within one object
+  void count(char k, char t, int64_t v) {
+    char line[64];
+    const int n = snprintf(line, sizeof(line), "%c %c %lld\n", k, t, (long long)v);
+    bytes(line, (size_t)n);
+  }
+  void stat(char t, char k, char u, int64_t v) {
+    char line[64];
+    const int n = snprintf(line, sizeof(line), "%% %c %c %c %lld\n", t, k, u, (long long)v);
     bytes(line, (size_t)n);
   }
   bool flush() {
@@ -565,48 +573,49 @@ extern "C" int pga_write_1aln_binary(const char *path, const char *program, cons
     o.integer((int64_t)ix.size());
     o.int_list(ix.data(), (int64_t)ix.size());
   };
-  o.text("# t %lld\n", 1);
+  o.count('#', 't', 1);
   if (nscaff > 0) {
-    o.text("# g %lld\n", 1);
-    if (nC) o.text("%% g # C %lld\n", nC);
-    if (nG) o.text("%% g # G %lld\n", nG);
-    o.text("%% g # S %lld\n", nscaff);
-    if (stot) o.text("%% g + S %lld\n", stot);
+    o.count('#', 'g', 1);
+    if (nC) o.stat('g', '#', 'C', nC);
+    if (nG) o.stat('g', '#', 'G', nG);
+    o.stat('g', '#', 'S', nscaff);
+    if (stot) o.stat('g', '+', 'S', stot);
     index('g', ix_g);
-    o.text("# S %lld\n", nscaff);
-    if (smax) o.text("@ S %lld\n", smax);
-    if (stot) o.text("+ S %lld\n", stot);
-    if (sC) o.text("%% S # C %lld\n", sC);
-    if (sG) o.text("%% S # G %lld\n", sG);
+    o.count('#', 'S', nscaff);
+    if (smax) o.count('@', 'S', smax);
+    if (stot) o.count('+', 'S', stot);
+    if (sC) o.stat('S', '#', 'C', sC);
+    if (sG) o.stat('S', '#', 'G', sG);
     index('S', ix_S);
-    if (nG) o.text("# G %lld\n", nG);
-    if (nC) o.text("# C %lld\n", nC);
+    if (nG) o.count('#', 'G', nG);
+    if (nC) o.count('#', 'C', nC);
   }
   if (nalign > 0) {
-    o.text("# A %lld\n", nalign);
-    o.text("%% A # D %lld\n", 1);
-    if (nR) o.text("%% A # R %lld\n", 1);
-    o.text("%% A # T %lld\n", 1);
-    if (tmax) o.text("%% A + T %lld\n", tmax);
-    o.text("%% A # X %lld\n", 1);
-    if (tmax) o.text("%% A + X %lld\n", tmax);
+    o.count('#', 'A', nalign);
+    o.stat('A', '#', 'D', 1);
+    if (nR) o.stat('A', '#', 'R', 1);
+    o.stat('A', '#', 'T', 1);
+    if (tmax) o.stat('A', '+', 'T', tmax);
+    o.stat('A', '#', 'X', 1);
+    if (tmax) o.stat('A', '+', 'X', tmax);
     index('A', ix_A);
-    if (nR) o.text("# R %lld\n", nR);
-    o.text("# D %lld\n", nalign);
+    if (nR) o.count('#', 'R', nR);
+    o.count('#', 'D', nalign);
     for (int pass = 0; pass < 2; pass++) {
-      o.text(pass ? "# X %lld\n" : "# T %lld\n", nalign);
-      if (tmax) o.text(pass ? "@ X %lld\n" : "@ T %lld\n", tmax);
-      if (ttot) o.text(pass ? "+ X %lld\n" : "+ T %lld\n", ttot);
+      const char t = pass ? 'X' : 'T';
+      o.count('#', t, nalign);
+      if (tmax) o.count('@', t, tmax);
+      if (ttot) o.count('+', t, ttot);
       if (codec[pass]) {
         const std::vector<uint8_t> ser = codec[pass]->serial();
         o.byte(line_code(';'));
-        o.byte((uint8_t)(pass ? 'X' : 'T'));
+        o.byte((uint8_t)t);
         o.integer((int64_t)ser.size());
         o.bytes(ser.data(), ser.size());
       }
     }
   }
-  o.text("^\n", 0);
+  o.bytes("^\n", 2);
   uint8_t off8[8];
   for (int b = 0; b < 8; b++) off8[b] = (uint8_t)((uint64_t)foot >> (8 * b));
   o.bytes(off8, 8);
