@@ -158,6 +158,50 @@ def test_binary_encoding_edges(regime):
                 assert ("# A %d 0 0" % n) in st
 
 
+ALNWRITE = os.path.join(ROOT, "oracle", "_ref", "alnwrite")
+
+
+@needs_ref
+@pytest.mark.skipif(not os.path.exists(ALNWRITE), reason="oracle/_ref/alnwrite not built")
+@pytest.mark.parametrize("source", ["small_full", "synthetic"])
+def test_c_caller_with_reference_types(source):
+    """oracle/_ref/alnwrite, a C program holding the alignments in the
+    reference's Overlap records and GDB skeleton, writes them through the
+    reference's own writer (as la_merge does) and through
+    pga_write_1aln_binary: the reference's reader gets the same records,
+    skeleton, counts, per-object statistics and index from both files.  The
+    synthetic set's lists pass the size at which both writers code them."""
+    from distributedpanga_b200 import pipeline
+    if source == "small_full":
+        cs, _ = load_case(source)
+        ref = [" ".join(l.split()) for l in gzip.open(os.path.join(GOLDEN, source + ".aln.txt.gz"), "rt").read()
+               .split("\n") if l.strip()]
+        recs, toff, tr = parse_lines(ref)
+        clen = cs.clen
+        sk = None
+    else:
+        rng = np.random.default_rng(3)
+        recs, toff, tr = [], [0], []
+        for i in range(3000):
+            n = [0, 1, 2, 37, 200][i % 5]
+            t = rng.integers(0, 256, 2 * n) if i % 2 else rng.integers(0, 40, 2 * n)
+            recs.append([i % 4, i, i + 5, (i + 1) % 4, 7 * i, 9 * i, i % 2, i % 50, 2 * n])
+            tr += t.tolist()
+            toff.append(len(tr))
+        recs, toff, tr = np.array(recs, np.int32), np.array(toff), np.array(tr, np.uint8)
+        clen = [2 ** 33, 70, 9000, 5]
+        sk = pipeline.Skeleton(["chr with space", "b" * 300, "c"], [2 ** 33 + 100, 10000, 5], [0, 1, 3, 4],
+                               [100, 0, 500, 0])
+    with tempfile.TemporaryDirectory() as d:
+        src, a, b = (os.path.join(d, f) for f in ("in.1aln", "ref.1aln", "pga.1aln"))
+        pipeline.write_1aln(src, recs, toff, tr, clen, skeleton=sk, db_name="g.1gdb", cwd=d)
+        subprocess.run([ALNWRITE, src, a, b], check=True, capture_output=True)
+        assert dump(a, skel=True) == dump(b, skel=True) == dump(src, skel=True)
+        assert stat(a) == stat(b)
+        if source == "synthetic":
+            assert os.path.getsize(b) <= os.path.getsize(a)
+
+
 def test_writer_rejects_bad_arguments():
     from distributedpanga_b200 import pipeline
     L = pipeline.load_library()
