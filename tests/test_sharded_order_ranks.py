@@ -183,3 +183,78 @@ def test_range_starts_and_keys():
     # anchor 0 at position 2: partner 1 (position 0, earlier) and 3 (position 3, later)
     assert lk.tolist() == [0, 0, (4 << 32) | 40, 0]
     assert eb.tolist() == [0, 0, (1 << 32) | 30, 0]
+
+
+def _fastga_loop(n, rs, partners, self_pairs, pair_out, self_out):
+    """Entry values by FastGA's own loop: in each range, rows in order, each
+    row's partners in order with the self pair at its own position, the last
+    Local_Alignment call's exit bepos carried along (the unset value at a
+    range start).  Contig c sits at order position c."""
+    entry = {}
+    last = None
+    for x in range(n):
+        if rs[x] == x:
+            last = 32767 if x == 0 else 0
+        for b in sorted(partners[x] | ({x} if x in self_pairs else set())):
+            if b == x:
+                entry[x] = last
+                calls, bep = self_out(x, last)
+            else:
+                calls, bep = pair_out[(x, b)]
+            if calls > 0:
+                last = bep
+    return entry
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_resolve_equals_fastga_loop(seed):
+    """Random orders, ranges, pair outcomes and self pairs whose outcome
+    depends on their entry value: the values resolve() decides are those of
+    FastGA's sequential loop, alone and with the self pairs owned by three
+    ranks that combine their states with all-reduce(MAX) (threads here)."""
+    import threading
+    from distributedpanga_b200 import sharded_order as so
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 40))
+    cuts = sorted(set([0] + rng.integers(1, max(2, n), int(rng.integers(0, 5))).tolist()))
+    rs = [max(c for c in cuts if c <= x) for x in range(n)]
+    partners = [set(int(b) for b in rng.choice(n, int(rng.integers(0, min(n, 6))), replace=False)) - {x}
+                for x in range(n)]
+    pair_out = {(x, b): (int(rng.random() < 0.5), int(rng.integers(0, 5000))) for x in range(n) for b in partners[x]}
+    self_pairs = set(int(x) for x in np.nonzero(rng.random(n) < 0.6)[0])
+    salt = int(rng.integers(1, 1000))
+
+    def self_out(x, entry):
+        return int((entry + salt + x) % 3 != 0), (entry * 7 + salt + x) % 4000
+
+    want = _fastga_loop(n, rs, partners, self_pairs, pair_out, self_out)
+    pos = np.arange(n)
+    lk, eb = so.local_keys([(x, b, c, e) for (x, b), (c, e) in pair_out.items()], pos, n)
+    st = np.zeros(n, dtype=np.int64)
+    st[list(self_pairs)] = 1
+
+    got, _ = so.resolve(n, pos, rs, lk, eb, st, lambda new: {c: self_out(c, v) for c, v in new.items()},
+                        lambda a: a)
+    assert got == want
+
+    world = 3
+    vals, cells = [None] * world, [None] * world
+    bar = threading.Barrier(world)
+
+    def allreduce_max(r, a):
+        cells[r] = np.array(a)
+        bar.wait()
+        out = np.max(np.stack(cells), axis=0)
+        bar.wait()
+        return out
+
+    def rank(r):
+        own = lambda new: {c: self_out(c, v) for c, v in new.items() if c % world == r}
+        vals[r] = so.resolve(n, pos, rs, lk, eb, st, own, lambda a: allreduce_max(r, a))[0]
+
+    ts = [threading.Thread(target=rank, args=(r,)) for r in range(world)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert all(v == want for v in vals)
