@@ -258,3 +258,107 @@ def test_resolve_equals_fastga_loop(seed):
     for t in ts:
         t.join()
     assert all(v == want for v in vals)
+
+
+FO_CORE = os.path.join(ROOT, "oracle", "_ref", "libfo_core.so")
+needs_fo = pytest.mark.skipif(not os.path.exists(FO_CORE), reason="oracle/_ref/libfo_core.so not built")
+
+
+def _fo_core():
+    """The reference's own rules (src/fastga_order_core.c, compiled into
+    oracle/_ref by oracle/Makefile)."""
+    import ctypes as C
+    L = C.CDLL(FO_CORE)
+    vp, ci, i64 = C.c_void_p, C.c_int, C.c_int64
+    L.fo_compute_ranges.argtypes = [ci, vp, i64, vp, i64, ci, vp, vp, vp, vp]
+    L.fo_compute_ranges.restype = ci
+    L.fo_from_rows.argtypes = [vp, vp, ci, ci, ci, vp, vp, vp]
+    L.fo_from_rows.restype = ci
+    L.fo_from_answers.argtypes = [vp, ci, ci, ci, ci, vp, vp]
+    L.fo_from_answers.restype = ci
+    return L
+
+
+@needs_fo
+def test_range_starts_equal_reference():
+    """range_starts equals the reference's fo_compute_ranges on random
+    contig sets (lengths over five decades, contigs without seeds, 1 to 32
+    threads)."""
+    import ctypes as C
+    from distributedpanga_b200 import sharded_order as so
+    L = _fo_core()
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        n = int(rng.integers(1, 300))
+        clen = (10 ** rng.uniform(2, 7, n)).astype(np.int64)
+        seeds = np.where(rng.random(n) < 0.3, 0, rng.integers(1, 10 ** 5, n)).astype(np.int64)
+        swide, T = int(rng.integers(9, 15)), int(rng.choice([1, 2, 7, 32]))
+        perm, _ = so.order_positions(clen)
+        cp = np.ascontiguousarray(clen[perm])
+        sp = np.ascontiguousarray(seeds[perm])
+        rs = np.zeros(n, dtype=np.int32)
+        nparts = C.c_int()
+        L.fo_compute_ranges(n, cp.ctypes.data, int(clen.sum()), sp.ctypes.data, swide, T, rs.ctypes.data, None,
+                            None, C.byref(nparts))
+        assert so.range_starts(clen, seeds, swide, perm, T) == rs.tolist()
+
+
+@needs_fo
+def test_row_and_partner_rules_equal_reference():
+    """from_rows equals fo_from_rows, and the values first_values decides
+    before any self pair runs equal fo_from_answers with every answer in
+    (bepos 0 a real value), on random rows, states and partners."""
+    import ctypes as C
+    from distributedpanga_b200 import sharded_order as so
+    L = _fo_core()
+    rng = np.random.default_rng(12)
+    bep, row, frm, k = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    for _ in range(3000):
+        n = int(rng.integers(1, 30))
+        x = int(rng.integers(0, n))
+        rs = [0] * n
+        rs[x] = int(rng.integers(0, x + 1))
+        lk = np.zeros(n, dtype=np.int64)
+        st = np.zeros(n, dtype=np.int64)
+        for y in range(n):
+            if rng.random() < 0.5:
+                b = int(rng.integers(0, n))
+                if b != y:
+                    lk[y] = ((b + 1) << 32) | int(rng.choice([0, int(rng.integers(0, 5000))]))
+            st[y] = int(rng.choice([0, 1, 2, 3, 3 + int(rng.integers(0, 5000))]))
+        rc = L.fo_from_rows(lk.ctypes.data, st.ctypes.data, x, rs[x], so.UNSET_MAIN, C.byref(bep), C.byref(row),
+                            C.byref(frm))
+        val, wait = so.from_rows(x, lk, st, rs)
+        assert wait == (rc == 0)
+        if rc == 1:
+            assert (val is None) == (row.value == -1)
+            assert (val if val is not None else (so.UNSET_MAIN if rs[x] == 0 else 0)) == bep.value
+        # the earlier partners of x, nearest first, each with its outcome
+        near = sorted(set(int(b) for b in rng.integers(0, x + 1, int(rng.integers(0, 6)))) - {x}, reverse=True)
+        out = [(int(rng.random() < 0.5), int(rng.choice([0, int(rng.integers(0, 5000))]))) for _ in near]
+        answers = np.array([e if c else -2 for c, e in out] or [0], dtype=np.int32)
+        eb = np.zeros(n, dtype=np.int64)
+        for b, (c, e) in zip(near, out):
+            if c:
+                eb[x] = max(eb[x], ((b + 1) << 32) | e)
+        s1 = np.zeros(n, dtype=np.int64)
+        s1[x] = 1
+        rc = L.fo_from_answers(answers.ctypes.data, len(near), x, rs[x], so.UNSET_MAIN, C.byref(bep), C.byref(k))
+        known = so.first_values(s1, eb, rs)
+        assert (x in known) == (rc == 1)
+        if rc == 1:
+            assert known[x] == bep.value
+
+
+@pytest.mark.parametrize("k", range(1, 13))
+def test_dependent_chain_takes_k_rounds(k):
+    """A chain of k self pairs, each taking its value from the one before it
+    (one range, no partners), resolves in exactly k rounds."""
+    from distributedpanga_b200 import sharded_order as so
+    pos = np.arange(k)
+    st = np.ones(k, dtype=np.int64)
+    zero = np.zeros(k, dtype=np.int64)
+    vals, rounds = so.resolve(k, pos, [0] * k, zero, zero, st, lambda new: {c: (1, v + 1 if c else 5)
+                                                                             for c, v in new.items()}, lambda a: a)
+    assert rounds == k
+    assert vals == {c: (so.UNSET_MAIN if c == 0 else 5 + c - 1) for c in range(k)}
