@@ -3221,4 +3221,17 @@ int pga_align_stats(const pga_ctx *ctx, int64_t *stats8) {
   return PGA_OK;
 }
 
+int pga_fastga_ranges(int n, const int64_t *clen_pos, int64_t npost, const int64_t *seeds_pos, int64_t swide,
+                      int nthreads, int *range_start) {
+  if (n < 0 || nthreads <= 0 || swide <= 0 || npost < 0 ||
+      (n > 0 && (!clen_pos || !seeds_pos || !range_start)))
+    return PGA_ERR_ARG;
+  if (n == 0) return PGA_OK;
+  std::vector<int64_t> c(clen_pos, clen_pos + n), sd(seeds_pos, seeds_pos + n);
+  std::vector<int> rs;
+  fo_ranges(n, c, npost, sd, swide, nthreads, rs);
+  std::copy(rs.begin(), rs.end(), range_start);
+  return PGA_OK;
+}
+
 }  // extern "C"

@@ -82,6 +82,7 @@ _SIGS = {
                                  C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
     "pga_align_write_1aln": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                        C.c_char_p, C.c_int, vp, vp, vp, vp]),
+    "pga_fastga_ranges": (C.c_int, [C.c_int, vp, C.c_int64, vp, C.c_int64, C.c_int, vp]),
     "pga_write_1aln_binary": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                         C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
     "pga_align_write_1aln_binary": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,

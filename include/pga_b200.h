@@ -222,6 +222,15 @@ int pga_gdb_set_freq(pga_ctx *ctx, const float *freq4);
  * needed.  *nalign = surviving alignments. */
 int pga_align(pga_ctx *ctx, int64_t *nalign);
 
+/* FastGA's thread ranges over its contig order, the split pga_align's
+ * self-pair rules use (fo_compute_ranges, src/fastga_order_core.c:50-140):
+ * clen_pos and seeds_pos by order position (lengths, N-unit seed counts),
+ * npost the GDB's total bases, swide the sorted-seed record width, nthreads
+ * FastGA's thread count (32 in the reference's driver).  Fills
+ * range_start[x] = the first position of x's range.  Host only. */
+int pga_fastga_ranges(int n, const int64_t *clen_pos, int64_t npost, const int64_t *seeds_pos, int64_t swide,
+                      int nthreads, int *range_start);
+
 /* How pga_align spreads large pairs of two different contigs over warps: it
  * cuts such a pair into ranges of about range_seeds seeds at band
  * boundaries, aligns the ranges on different warps (a pair's band blocks are
