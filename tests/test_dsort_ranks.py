@@ -122,3 +122,37 @@ def test_destination_map_and_helpers():
     rec = np.zeros((3, 16), np.uint8)
     rec[:, 1] = [5, 3, 7]
     assert dsort.verify_per_rank_sorted(rec) == (1, 1)
+
+
+SPLIT_DUMP = os.path.join(ROOT, "oracle", "_ref", "split_dump")
+
+
+@pytest.mark.skipif(not os.path.exists(SPLIT_DUMP), reason="oracle/_ref/split_dump not built")
+def test_splitter_equals_reference():
+    """compute_destination_map equals the reference's (src/dsort.c, compiled
+    here) on random global bucket counts -- sparse, skewed, all in one
+    bucket, all zero -- at world sizes 1 to 16."""
+    import subprocess
+    from distributedpanga_b200 import dsort
+    rng = np.random.default_rng(9)
+    cases = []
+    for _ in range(150):
+        kind = int(rng.integers(0, 4))
+        if kind == 0:
+            c = rng.integers(0, 10 ** 6, 1024)
+        elif kind == 1:
+            c = np.where(rng.random(1024) < 0.9, 0, rng.integers(1, 10 ** 9, 1024))
+        elif kind == 2:
+            c = (10 ** rng.uniform(0, 9, 1024)).astype(np.int64)
+        else:
+            c = np.zeros(1024, np.int64)
+            c[int(rng.integers(0, 1024))] = int(rng.integers(1, 10 ** 6))
+        cases.append(c)
+    cases.append(np.zeros(1024, np.int64))
+    for c in cases:
+        world = int(rng.integers(1, 17))
+        out = subprocess.run([SPLIT_DUMP], input="%d\n%s\n" % (world, " ".join(str(int(v)) for v in c)),
+                             capture_output=True, text=True, check=True).stdout.split("\n")
+        ksplit, select = dsort.compute_destination_map(np.asarray(c, np.int64), world)
+        assert list(ksplit) == [int(v) for v in out[0].split()]
+        assert list(select) == [int(v) for v in out[1].split()]

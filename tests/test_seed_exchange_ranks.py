@@ -125,3 +125,27 @@ def test_assignment_and_plan():
     assert sx.plan_byte_exchange([2 ** 30, 2 ** 30]) == -3
     with pytest.raises(ValueError):
         sx.contig_assignment_build(clen, 128)
+
+
+ASSIGN_DUMP = os.path.join(ROOT, "oracle", "_ref", "assign_dump")
+
+
+@pytest.mark.skipif(not os.path.exists(ASSIGN_DUMP), reason="oracle/_ref/assign_dump not built")
+def test_assignment_equals_reference():
+    """contig_assignment_build equals the reference's own (src/contig_assignment.c,
+    compiled here) on random contig sets with many equal lengths (ties in
+    weight and in load decide by pair and by rank) at world sizes 1 to 9."""
+    import subprocess
+    from distributedpanga_b200 import seed_exchange as sx
+    rng = np.random.default_rng(5)
+    for _ in range(120):
+        n = int(rng.integers(1, 45))
+        world = int(rng.integers(1, 10))
+        clen = rng.choice(rng.integers(1, 3000, int(rng.integers(1, 6))), n)
+        txt = "%d %d\n%s\n" % (n, world, " ".join(str(int(c)) for c in clen))
+        out = subprocess.run([ASSIGN_DUMP], input=txt, capture_output=True, text=True, check=True).stdout.split("\n")
+        ref_owner = np.array([[int(v) for v in l.split()] for l in out[:n]], dtype=np.int8)
+        ref_load = np.array([int(v) for v in out[n].split()], dtype=np.int64)
+        owner, load = sx.contig_assignment_build(clen, world)
+        assert np.array_equal(owner, ref_owner)
+        assert np.array_equal(load, ref_load)
