@@ -156,3 +156,73 @@ def test_splitter_equals_reference():
         ksplit, select = dsort.compute_destination_map(np.asarray(c, np.int64), world)
         assert list(ksplit) == [int(v) for v in out[0].split()]
         assert list(select) == [int(v) for v in out[1].split()]
+        # the reference's S-08 invariants: select non-decreasing and in range,
+        # ksplit non-decreasing and ending at the bucket count
+        sel = np.asarray(select)
+        assert np.all(np.diff(sel) >= 0) and sel.min() >= 0 and sel.max() < world
+        assert np.all(np.diff(np.asarray(ksplit)) >= 0) and ksplit[world] == 1024
+    ksplit, select = dsort.compute_destination_map(np.full(1024, 7, np.int64), 4)
+    assert list(select) == [b // 256 for b in range(1024)]
+
+
+def _seam_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    from distributedpanga_b200 import dsort
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rec = _seam_records()
+        counts = dsort.bucket_local_counts(rec)
+        _, select = dsort.compute_destination_map(counts, world)
+
+        def sort_fn(r):
+            r = r[np.lexsort(r[:, 10:0:-1].T)].copy()
+            r[0, 0] = 0
+            for i in range(1, len(r)):
+                r[i, 0] = dsort.kmer_lcp_bases(r[i - 1, 1:11], r[i, 1:11])
+            return r
+
+        got = dsort.run_stage2(rec[rank::world], sort_fn)
+        out[rank] = (got.tobytes(), [int(select[768]), int(select[769]), int(select[770])])
+    finally:
+        dist.destroy_process_group()
+
+
+def _seam_records():
+    """The reference's R-01 fixture: every k-mer's first byte 0xC0, four
+    records in bucket 768 (second byte's top bits 00) and four in bucket 770
+    (10), distinct in bytes 2..9; bucket 769 empty."""
+    rng = np.random.default_rng(21)
+    rec = np.zeros((8, 16), np.uint8)
+    rec[:, 1] = 0xC0
+    rec[:4, 2] = 0x00
+    rec[4:, 2] = 0x80
+    rec[:, 3:11] = rng.integers(0, 256, (8, 8))
+    rec[:, 11:] = np.arange(8)[:, None]
+    return rec
+
+
+def test_r01_seam_lcp_past_an_empty_rank():
+    """World 4: the splitter sends bucket 768 to rank 0, the empty 769 to
+    rank 1 and 770 to rank 2, so rank 1 holds nothing and rank 2's first
+    record takes its LCP from rank 0's last k-mer: 4 bases (the first byte
+    and nothing of the second).  The ranks' slices in order are the sorted
+    index with its LCPs."""
+    from distributedpanga_b200 import dsort
+    world = 4
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_seam_worker, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
+        res = {r: out[r] for r in range(world)}
+    assert res[0][1] == [0, 1, 2]
+    parts = [np.frombuffer(res[r][0], np.uint8).reshape(-1, 16) for r in range(world)]
+    assert [len(p) for p in parts] == [4, 0, 4, 0]
+    assert parts[2][0, 0] == 4
+    rec = _seam_records()
+    want = rec[np.lexsort(rec[:, 10:0:-1].T)].copy()
+    want[0, 0] = 0
+    for i in range(1, 8):
+        want[i, 0] = dsort.kmer_lcp_bases(want[i - 1, 1:11], want[i, 1:11])
+    assert np.array_equal(np.concatenate(parts), want)

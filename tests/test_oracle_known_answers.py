@@ -1,7 +1,7 @@
 """The oracle against the reference's own known answers for this path.
 
 Cases restate the fixtures of the reference's unit tests (test IDs from its
-tests/CATALOG.md): E-01/E-02 packing, E-06 the syncmer contract against an
+tests/CATALOG.md): E-01/E-02 packing, E-04/E-05 window edges, E-06 the syncmer contract against an
 independent pure-Python extractor, E-08/E-09 emission ranges, S-01/S-02 LCP
 values, R-03 the position-256 sizing, K-03 the k-mer table entry layout."""
 import numpy as np
@@ -31,6 +31,20 @@ def test_e01_forward_packing(oracle):
     want = {0: 0x1B, 1: 0x6C, 2: 0xB1, 3: 0xC6}
     for r, p in zip(fwd, pos[strand == 0]):
         assert np.all(r[1:11] == want[p % 4])
+
+
+def test_e04_e05_window_edges(oracle):
+    # a 52-base contig: a forward 40-mer at offset j needs [j, j+40) inside
+    # (j <= 12); an RC one reads [j-28, j+12) (28 <= j <= 40) and is stored at
+    # j + 12; over 400 random contigs every edge offset is selected somewhere
+    rng = np.random.default_rng(4)
+    rec, posb, ctgb = records(oracle, [rng.integers(0, 4, 52).astype(np.uint8) for _ in range(400)])
+    assert posb == 1
+    pos = rec[:, 12].astype(int)
+    strand = rec[:, 12 + posb + ctgb - 1] >> 7
+    fwd, rc = pos[strand == 0], pos[strand == 1] - 12
+    assert fwd.min() >= 0 and fwd.max() == 12
+    assert rc.min() == 28 and rc.max() == 40
 
 
 def test_e02_rc_packing(oracle):
