@@ -120,3 +120,112 @@ extern "C" int pga_write_gix(const char *stem, int nparts, int post_bytes, int c
   if (fclose(f) != 0) ok = false;
   return ok ? PGA_OK : PGA_ERR_ARG;
 }
+
+namespace {
+
+bool get(FILE *f, void *p, size_t n) { return fread(p, 1, n, f) == n; }
+
+// Bases two k-mers share from the start; a k-mer is its 3 prefix bytes (the
+// entry's place in the 2^24 table) and the entry's 7 suffix bytes.
+int kmer_lcp(uint32_t pa, const uint8_t *sa, uint32_t pb, const uint8_t *sb) {
+  uint8_t a[10], b[10];
+  a[0] = (uint8_t)(pa >> 16), a[1] = (uint8_t)(pa >> 8), a[2] = (uint8_t)pa;
+  b[0] = (uint8_t)(pb >> 16), b[1] = (uint8_t)(pb >> 8), b[2] = (uint8_t)pb;
+  memcpy(a + 3, sa, 7);
+  memcpy(b + 3, sb, 7);
+  for (int i = 0; i < 10; i++)
+    if (a[i] != b[i]) {
+      int z = 0;
+      while (z < 3 && !((a[i] ^ b[i]) & (0xc0 >> (2 * z)))) z++;
+      return 4 * i + z;
+    }
+  return GIX_KMER;
+}
+
+}  // namespace
+
+extern "C" int pga_read_gix(const char *stem, int *hdr6, int32_t *order, int64_t order_cap, int64_t *cum,
+                            int64_t *largest, int64_t *nentries, uint8_t *entries, int64_t entries_cap) {
+  if (!stem || !hdr6 || !largest || !nentries) return PGA_ERR_ARG;
+  std::string s(stem);
+  const size_t slash = s.rfind('/');
+  const std::string dir = slash == std::string::npos ? "." : s.substr(0, slash);
+  const std::string root = slash == std::string::npos ? s : s.substr(slash + 1);
+
+  FILE *f = fopen((dir + "/" + root + ".gix").c_str(), "rb");
+  if (!f) return PGA_ERR_ARG;
+  int head[4], pc[3], freq = 0, nctg = 0;
+  std::vector<int64_t> table((size_t)1 << 24);
+  int64_t big = 0, end = 0;
+  bool ok = get(f, head, sizeof(head)) && get(f, table.data(), sizeof(int64_t) << 24) && get(f, pc, sizeof(pc)) &&
+            get(f, &big, sizeof(big)) && get(f, &freq, sizeof(int)) && get(f, &nctg, sizeof(int));
+  std::vector<int32_t> ord;
+  if (ok && nctg >= 0 && nctg <= (1 << 30)) {
+    ord.resize((size_t)nctg);
+    ok = (nctg == 0 || get(f, ord.data(), sizeof(int32_t) * (size_t)nctg)) && get(f, &end, sizeof(end));
+  } else {
+    ok = false;
+  }
+  fclose(f);
+  const int nparts = head[1], post_bytes = pc[0], cont_bytes = pc[1];
+  if (!ok || head[0] != GIX_KMER || nparts < 1 || nparts > NPANEL || pc[2] != nparts || post_bytes < 1 ||
+      post_bytes > 8 || cont_bytes < 1 || cont_bytes > 8 || end != -1)
+    return PGA_ERR_ARG;
+  std::vector<char> seen((size_t)nctg, 0);
+  for (int i = 0; i < nctg; i++) {
+    if (ord[(size_t)i] < 0 || ord[(size_t)i] >= nctg || seen[(size_t)ord[(size_t)i]]) return PGA_ERR_ARG;
+    seen[(size_t)ord[(size_t)i]] = 1;
+  }
+  const int64_t n = table[((size_t)1 << 24) - 1];
+  hdr6[0] = GIX_KMER, hdr6[1] = nparts, hdr6[2] = post_bytes, hdr6[3] = cont_bytes, hdr6[4] = freq,
+  hdr6[5] = nctg;
+  *largest = big;
+  *nentries = n;
+  if (!entries) return PGA_OK;  // sizes only
+  if (entries_cap < n || !cum || (nctg > 0 && (!order || order_cap < nctg))) return PGA_ERR_ARG;
+  std::copy(table.begin(), table.end(), cum);
+  std::copy(ord.begin(), ord.end(), order);
+
+  // the parts, back to back; contigs renumbered from places in the order
+  const int eb = 9 + post_bytes + cont_bytes;
+  const uint64_t sign = (uint64_t)1 << (8 * cont_bytes - 1);
+  int64_t at = 0;
+  std::vector<int64_t> part_start;
+  for (int p = 1; p <= nparts; p++) {
+    FILE *g = fopen((dir + "/." + root + ".ktab." + std::to_string(p)).c_str(), "rb");
+    if (!g) return PGA_ERR_ARG;
+    int k = 0;
+    int64_t m = -1;
+    bool pok = get(g, &k, sizeof(int)) && get(g, &m, sizeof(int64_t)) && k == GIX_KMER && m >= 0 && at + m <= n &&
+               (m == 0 || get(g, entries + at * eb, (size_t)(m * eb)));
+    fclose(g);
+    if (!pok) return PGA_ERR_ARG;
+    part_start.push_back(at);
+    at += m;
+  }
+  if (at != n) return PGA_ERR_ARG;
+  for (int64_t i = 0; i < n; i++) {
+    uint8_t *e = entries + i * eb;
+    uint64_t cs = 0;
+    for (int q = 0; q < cont_bytes; q++) cs |= (uint64_t)e[9 + post_bytes + q] << (8 * q);
+    const uint64_t place = cs & (sign - 1);
+    if ((int64_t)place >= nctg) return PGA_ERR_ARG;
+    cs = (uint64_t)ord[(size_t)place] | (cs & sign);
+    for (int q = 0; q < cont_bytes; q++) e[9 + post_bytes + q] = (uint8_t)(cs >> (8 * q));
+  }
+  // a part's first entry: its LCP to the entry before it (the index's first: 0)
+  uint32_t pfx = 0;
+  for (int64_t ps : part_start) {
+    if (ps >= n) continue;
+    if (ps == 0) {
+      entries[8] = 0;
+      continue;
+    }
+    while (pfx < ((uint32_t)1 << 24) && table[pfx] <= ps - 1) pfx++;
+    const uint32_t pa = pfx;  // prefix of entry ps - 1
+    uint32_t pb = pa;
+    while (pb < ((uint32_t)1 << 24) && table[pb] <= ps) pb++;
+    entries[ps * eb + 8] = (uint8_t)kmer_lcp(pa, entries + (ps - 1) * eb, pb, entries + ps * eb);
+  }
+  return PGA_OK;
+}

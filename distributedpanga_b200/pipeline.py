@@ -82,6 +82,7 @@ _SIGS = {
                                  C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
     "pga_align_write_1aln": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                        C.c_char_p, C.c_int, vp, vp, vp, vp]),
+    "pga_read_gix": (C.c_int, [C.c_char_p, vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]),
     "pga_fastga_ranges": (C.c_int, [C.c_int, vp, C.c_int64, vp, C.c_int64, C.c_int, vp]),
     "pga_write_1aln_binary": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
                                         C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int64, vp, vp, vp]),
@@ -630,6 +631,30 @@ def write_1aln(path, recs, toff, trace, contig_len, skeleton=None, db_name="", c
             toff.ctypes.data_as(vp), trace.ctypes.data_as(vp))
     if rc != 0:
         raise PgaError("write_1aln(%s): status %d" % (path, rc))
+
+
+def read_gix(stem):
+    """A GIX on disk (<stem>.gix and the .ktab parts beside it, from GIXmake
+    or Device.index_write_gix) as the k-mer table view: {"kmer", "parts",
+    "post_bytes", "cont_bytes", "freq", "order", "cum", "largest",
+    "entries"}, contigs numbered as in the GDB (pga_read_gix)."""
+    L = load_library()
+    hdr = np.zeros(6, dtype=np.int32)
+    largest, n = C.c_int64(), C.c_int64()
+    rc = L.pga_read_gix(stem.encode(), hdr.ctypes.data_as(vp), None, 0, None, C.byref(largest), C.byref(n), None, 0)
+    if rc != 0:
+        raise PgaError("read_gix(%s): status %d" % (stem, rc))
+    eb = 9 + int(hdr[2]) + int(hdr[3])
+    order = np.zeros(max(1, int(hdr[5])), dtype=np.int32)
+    cum = np.zeros(1 << 24, dtype=np.int64)
+    ent = np.zeros((max(1, n.value), eb), dtype=np.uint8)
+    rc = L.pga_read_gix(stem.encode(), hdr.ctypes.data_as(vp), order.ctypes.data_as(vp), len(order),
+                        cum.ctypes.data_as(vp), C.byref(largest), C.byref(n), ent.ctypes.data_as(vp), n.value)
+    if rc != 0:
+        raise PgaError("read_gix(%s): status %d" % (stem, rc))
+    return {"kmer": int(hdr[0]), "parts": int(hdr[1]), "post_bytes": int(hdr[2]), "cont_bytes": int(hdr[3]),
+            "freq": int(hdr[4]), "order": order[:int(hdr[5])], "cum": cum, "largest": largest.value,
+            "entries": ent[:n.value]}
 
 
 def alignment_lines(recs, toff, tr):

@@ -190,6 +190,18 @@ int pga_index_write_gix(pga_ctx *ctx, const char *stem, int nparts);
 int pga_write_gix(const char *stem, int nparts, int post_bytes, int cont_bytes, int ncontig, const int32_t *order,
                   const int64_t *cum, int64_t largest, int64_t nentries, const uint8_t *entries);
 int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t *largest_group);
+/* The reader: a GIX on disk (written by GIXmake or pga_write_gix) as the
+ * k-mer table view pga_self_adaptamer_merge takes.  hdr6 = {K, parts,
+ * post_bytes, cont_bytes, frequency cutoff, ncontig}; *largest the largest
+ * prefix group; *nentries.  With entries NULL only these are filled (the
+ * sizes); otherwise also order[ncontig] (contigs longest first), cum[2^24]
+ * and the entries (9 + post_bytes + cont_bytes bytes each), the parts back
+ * to back, contigs numbered as in the GDB again (GIXmake numbers them by
+ * their place in the order) and each part's first LCP byte taken to the
+ * entry before it (GIXmake's part-by-part sort leaves another value there).
+ * Runs of equal k-mers keep the file's order.  Needs no device. */
+int pga_read_gix(const char *stem, int *hdr6, int32_t *order, int64_t order_cap, int64_t *cum, int64_t *largest,
+                 int64_t *nentries, uint8_t *entries, int64_t entries_cap);
 
 /* Adaptamer merge of the built index: seeds stay in HBM. */
 int pga_merge(pga_ctx *ctx, int freq, int64_t *nseeds, int64_t *cseeds);

@@ -186,3 +186,78 @@ def test_index_gix_equals_oracle_gix(dev, oracle, case):
             ref = read_gix(gixmake(cs, work))
             if ref["head"][1] == 8:
                 check_against_gixmake(read_gix(os.path.join(work, "gpu", "g")), ref)
+
+
+# ---- the reader (pga_read_gix): a GIX on disk as the k-mer table view
+
+def _oracle_table(oracle, cs):
+    from distributedpanga_b200 import gdb
+    posb, ctgb, _ = gdb.record_sizing(cs)
+    rec = oracle.sort_records(oracle.extract(cs, posb, ctgb))
+    return oracle.build_adapter(rec, posb, ctgb), posb, ctgb
+
+
+@pytest.mark.parametrize("case,nparts", [("small_s002", 1), ("edge_mix", 16), ("many_contigs", 8),
+                                         ("chromset_s0005", 1024)])
+def test_reader_inverts_writer(oracle, case, nparts):
+    """Written by pga_write_gix and read back by pga_read_gix, the k-mer
+    table is the index's, entry for entry: contigs numbered as in the GDB
+    again, and every part's first LCP byte the LCP to the entry before it."""
+    from distributedpanga_b200 import pipeline
+    cs, _ = load_case(case)
+    (ent, cum, big), posb, ctgb = _oracle_table(oracle, cs)
+    with tempfile.TemporaryDirectory() as work:
+        write_from_oracle(oracle, cs, os.path.join(work, "g"), nparts=nparts)
+        g = pipeline.read_gix(os.path.join(work, "g"))
+    assert (g["kmer"], g["parts"], g["post_bytes"], g["cont_bytes"], g["freq"]) == (40, nparts, posb, ctgb, 0)
+    assert np.array_equal(g["order"], np.argsort(-cs.clen, kind="stable"))
+    assert np.array_equal(g["cum"], cum) and g["largest"] == big
+    assert np.array_equal(g["entries"], ent)
+
+
+@pytest.mark.skipif(not HAVE_GIXMAKE, reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_reader_on_gixmake_output(oracle, case):
+    """GIXmake's own index, read by pga_read_gix, is the oracle's k-mer table
+    once runs of equal k-mers are put in one order (GIXmake leaves them in an
+    unspecified one), part starts included."""
+    from distributedpanga_b200 import pipeline
+    cs, _ = load_case(case)
+    (ent, cum, big), _, _ = _oracle_table(oracle, cs)
+    with tempfile.TemporaryDirectory() as work:
+        g = pipeline.read_gix(gixmake(cs, work))
+    assert np.array_equal(g["cum"], cum)
+    assert np.array_equal(g["order"], np.argsort(-cs.clen, kind="stable"))
+    assert np.array_equal(canonical(g["entries"].copy()), canonical(ent.copy()))
+
+
+def test_reader_rejects_bad_files():
+    from distributedpanga_b200 import pipeline
+    with tempfile.TemporaryDirectory() as work:
+        with pytest.raises(pipeline.PgaError):
+            pipeline.read_gix(os.path.join(work, "missing"))
+        with open(os.path.join(work, "short.gix"), "wb") as f:
+            f.write(np.array([40, 1, 1, 3], np.int32).tobytes())
+        with pytest.raises(pipeline.PgaError):
+            pipeline.read_gix(os.path.join(work, "short"))
+
+
+@pytest.mark.skipif(not HAVE_GIXMAKE, reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", ["small_s002", "chromset_s0005"])
+def test_gixmake_index_feeds_the_merge(oracle, case):
+    """The k-mer table read from GIXmake's files is a merge input like the
+    built index's: merged (the oracle's adaptamer merge stands in for
+    pga_self_adaptamer_merge, which takes the same table) and diagonal
+    sorted, its N and C panels are the built index's."""
+    from distributedpanga_b200 import pipeline
+    cs, dig = load_case(case)
+    (ent, cum, _), posb, ctgb = _oracle_table(oracle, cs)
+    with tempfile.TemporaryDirectory() as work:
+        g = pipeline.read_gix(gixmake(cs, work))
+    panels = []
+    for e, c in ((ent, cum), (g["entries"], g["cum"])):
+        ns, css, _, _ = oracle.merge(e, c, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+        panels.append([oracle.reimport_sort(u, posb, ctgb, comp, cs.ncontig, cs.maxctg, dig["dbyte"])
+                       for comp, u in ((0, ns), (1, css))])
+    for (a, ao), (b, bo) in zip(panels[0], panels[1]):
+        assert np.array_equal(ao, bo) and np.array_equal(a, b)
