@@ -191,7 +191,9 @@ int pga_write_gix(const char *stem, int nparts, int post_bytes, int cont_bytes, 
                   const int64_t *cum, int64_t largest, int64_t nentries, const uint8_t *entries);
 int pga_index_copy_entries(pga_ctx *ctx, uint8_t *entries, int64_t *cum, int64_t *largest_group);
 /* The reader: a GIX on disk (written by GIXmake or pga_write_gix) as the
- * k-mer table view pga_self_adaptamer_merge takes.  hdr6 = {K, parts,
+ * k-mer table view pga_self_adaptamer_merge takes (the reference reads the
+ * header and contig order of the same file in fo_read_gix_perm,
+ * src/fastga_order_core.c:11-52, and FastGA the parts).  hdr6 = {K, parts,
  * post_bytes, cont_bytes, frequency cutoff, ncontig}; *largest the largest
  * prefix group; *nentries.  With entries NULL only these are filled (the
  * sizes); otherwise also order[ncontig] (contigs longest first), cum[2^24]
