@@ -50,43 +50,23 @@ def range_starts(clen, seeds_by_contig, swide: int, perm, nthreads: int = 32) ->
     """rs[x]: the first position of the order range that position x falls in
     (fo_compute_ranges, src/fastga_order_core.c:50-140): the order is cut
     into parts of about equal sequence, each part into ranges of about equal
-    seed bytes."""
+    seed bytes.  The library's own rule, the one pga_align uses
+    (pga_fastga_ranges)."""
+    import ctypes as C
+    from . import pipeline
     n = len(clen)
-    clen_pos = np.asarray(clen, dtype=np.int64)[perm]
-    seeds_pos = np.asarray(seeds_by_contig, dtype=np.int64)[perm]
-    T, npost = nthreads, int(np.sum(clen))
-    split, p, r, t = [0] * (T + 1), 0, T, npost // T
-    cum = int(clen_pos[0]) if n else 0
-    for x in range(1, n):
-        if cum >= t and x >= r:
-            p += 1
-            split[p] = x
-            t = (npost * (p + 1)) // T
-            r += T
-        cum += int(clen_pos[x])
-    nparts = p + 1
-    split[nparts] = n
-    rs = list(range(n))
-    for i in range(nparts):
-        asize = sum(int(seeds_pos[x]) * swide for x in range(split[i], split[i + 1]))
-        if asize == 0:
-            continue
-        k, thr, s = 0, asize // T, 0
-        x = split[i]
-        while x < split[i + 1] and seeds_pos[x] == 0:
-            x += 1
-        beg = x
-        while x < split[i + 1]:
-            if seeds_pos[x] > 0:
-                s += int(seeds_pos[x]) * swide
-                if s >= thr:
-                    for y in range(beg, x + 1):
-                        rs[y] = beg
-                    k += 1
-                    thr = (asize * (k + 1)) // T
-                    beg = x + 1
-            x += 1
-    return rs
+    if n == 0:
+        return []
+    clen = np.asarray(clen, dtype=np.int64)
+    cp = np.ascontiguousarray(clen[perm])
+    sp = np.ascontiguousarray(np.asarray(seeds_by_contig, dtype=np.int64)[perm])
+    rs = np.zeros(n, dtype=np.int32)
+    rc = pipeline.load_library().pga_fastga_ranges(n, cp.ctypes.data_as(C.c_void_p), int(clen.sum()),
+                                                   sp.ctypes.data_as(C.c_void_p), int(swide), int(nthreads),
+                                                   rs.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise pipeline.PgaError("pga_fastga_ranges: status %d" % rc)
+    return rs.tolist()
 
 
 def local_keys(pairs_n, pos, n: int):
