@@ -113,7 +113,8 @@ def test_skeleton_and_records_equal_reference_file(kind, scale):
 def test_binary_encoding_edges(regime):
     """Values at every width of ONE's variable-length integers, trace lists of
     0, 1 and many values whose differences need one or two bytes, scaffolds
-    with leading, inner and trailing gaps, and files with no skeleton or no
+    with leading, inner and trailing gaps and one of gap alone, and files
+    with no skeleton or no
     alignments: the binary file reads back as the ASCII one does, and its
     index reaches every object.  "few" stays below the size at which trace
     lists are coded; "many" codes them (differences of one and two bytes,
@@ -136,8 +137,8 @@ def test_binary_encoding_edges(regime):
     toff = np.array(toff, dtype=np.int64)
     tr = np.array(tr, dtype=np.uint8)
     clen = np.array([2 ** 33, 70, 9000, 5], dtype=np.int64)
-    sk = pipeline.Skeleton(["chr with space", "b" * 300, "c"], [2 ** 33 + 100, 10000, 5], [0, 1, 3, 4],
-                           [100, 0, 500, 0])
+    sk = pipeline.Skeleton(["chr with space", "b" * 300, "c", "all gap"], [2 ** 33 + 100, 10000, 5, 77],
+                           [0, 1, 3, 4, 4], [100, 0, 500, 0])
     with tempfile.TemporaryDirectory() as d:
         for skel, n in ((sk, len(recs)), (sk, 0), (None, len(recs))):
             got = {}
