@@ -243,21 +243,22 @@ def test_reader_rejects_bad_files():
 
 
 @pytest.mark.skipif(not HAVE_GIXMAKE, reason="oracle/_ref not built")
-@pytest.mark.parametrize("case", ["small_s002", "chromset_s0005"])
+@pytest.mark.parametrize("case", GOLDEN_CASES)
 def test_gixmake_index_feeds_the_merge(oracle, case):
     """The k-mer table read from GIXmake's files is a merge input like the
     built index's: merged (the oracle's adaptamer merge stands in for
-    pga_self_adaptamer_merge, which takes the same table) and diagonal
-    sorted, its N and C panels are the built index's."""
+    pga_self_adaptamer_merge, which takes the same table; its GPU run is in
+    test_zzz_gix_merge.py) and diagonal sorted, its seeds and N and C
+    panels are the reference's (golden digests)."""
+    from helpers import check_diag, check_seeds
     from distributedpanga_b200 import pipeline
     cs, dig = load_case(case)
-    (ent, cum, _), posb, ctgb = _oracle_table(oracle, cs)
+    posb, ctgb = dig["posb"], dig["ctgb"]
     with tempfile.TemporaryDirectory() as work:
         g = pipeline.read_gix(gixmake(cs, work))
-    panels = []
-    for e, c in ((ent, cum), (g["entries"], g["cum"])):
-        ns, css, _, _ = oracle.merge(e, c, posb, ctgb, dig["freq_cutoff"], cs.ncontig)
-        panels.append([oracle.reimport_sort(u, posb, ctgb, comp, cs.ncontig, cs.maxctg, dig["dbyte"])
-                       for comp, u in ((0, ns), (1, css))])
-    for (a, ao), (b, bo) in zip(panels[0], panels[1]):
-        assert np.array_equal(ao, bo) and np.array_equal(a, b)
+    ns, css, nb, cb = oracle.merge(g["entries"], g["cum"], posb, ctgb, dig["freq_cutoff"], cs.ncontig)
+    check_seeds(ns, css, nb, cb, dig)
+    for u, seeds in (("N", ns), ("C", css)):
+        arr, off = oracle.reimport_sort(seeds, posb, ctgb, 1 if u == "C" else 0, cs.ncontig, cs.maxctg,
+                                        dig["dbyte"])
+        check_diag(arr, off, u, dig)
