@@ -28,7 +28,7 @@ int main(int argc, char *argv[])
   GDB      gdb;
   Overlap *ovl;
   uint8   *tbuf, *trace;
-  int64   *toff, *t64;
+  int64   *toff, *t64, tlmax;
   int32_t *recs9;
 
   Prog_Name    = "alnwrite";
@@ -53,10 +53,15 @@ int main(int argc, char *argv[])
       have_skel = 1;
     }
 
-  /* the records in the reference's Overlap, their traces back to back */
+  /* the records in the reference's Overlap, their traces back to back
+     (a trace holds 2 bytes per T value; the file's largest T list sizes it) */
+  { I64 tmax = 0;
+    oneStats(in, 'T', NULL, &tmax, NULL);
+    tlmax = 2 * (tmax > 0 ? tmax : 1);
+  }
   ovl   = malloc(sizeof(Overlap) * (novl > 0 ? novl : 1));
   toff  = malloc(sizeof(int64) * (novl + 1));
-  tbuf  = malloc(1 << 20);
+  tbuf  = malloc(tlmax);
   tcap  = 1 << 20;
   trace = malloc(tcap);
   tbytes = 0;
@@ -88,7 +93,7 @@ int main(int argc, char *argv[])
     return 1;
   if (have_skel)
     Write_Skeleton(out, &gdb);
-  t64 = malloc(sizeof(int64) * (1 << 20));
+  t64 = malloc(sizeof(int64) * tlmax);
   for (k = 0; k < novl; k++)
     { Write_Aln_Overlap(out, &ovl[k]);
       Write_Aln_Trace(out, trace + toff[k], ovl[k].path.tlen, t64, 0);
