@@ -262,3 +262,43 @@ def test_gixmake_index_feeds_the_merge(oracle, case):
         arr, off = oracle.reimport_sort(seeds, posb, ctgb, 1 if u == "C" else 0, cs.ncontig, cs.maxctg,
                                         dig["dbyte"])
         check_diag(arr, off, u, dig)
+
+
+def test_reader_rejects_corrupt_indexes(oracle):
+    """A GIX damaged in each field the reader trusts -- the .gix cut short,
+    a contig order that is not a permutation, a part that claims more
+    entries than the prefix table holds, a contig place past the last
+    contig, a part missing -- is refused with an error, never read past
+    its buffers."""
+    import shutil
+    from distributedpanga_b200 import pipeline
+    cs, _ = load_case("edge_mix")
+    with tempfile.TemporaryDirectory() as work:
+        good = os.path.join(work, "good")
+        os.makedirs(good)
+        write_from_oracle(oracle, cs, os.path.join(good, "g"), nparts=4)
+        g = pipeline.read_gix(os.path.join(good, "g"))
+        eb = 9 + g["post_bytes"] + g["cont_bytes"]
+        order_at = 16 + 8 * (1 << 24) + 12 + 8 + 8
+
+        def damaged(name, edit):
+            d = os.path.join(work, name)
+            shutil.copytree(good, d)
+            edit(d)
+            with pytest.raises(pipeline.PgaError):
+                pipeline.read_gix(os.path.join(d, "g"))
+
+        def patch(path, at, data):
+            with open(path, "r+b") as f:
+                f.seek(at)
+                f.write(data)
+
+        damaged("short", lambda d: os.truncate(os.path.join(d, "g.gix"), order_at))
+        damaged("perm", lambda d: patch(os.path.join(d, "g.gix"), order_at + 4,
+                                        np.int32(g["order"][0]).tobytes()))
+        damaged("count", lambda d: patch(os.path.join(d, ".g.ktab.1"), 4, np.int64(1 << 40).tobytes()))
+        place = np.zeros(g["cont_bytes"], np.uint8)
+        place[:] = 0xff
+        place[-1] = 0x7f
+        damaged("place", lambda d: patch(os.path.join(d, ".g.ktab.2"), 12 + 9 + g["post_bytes"], place.tobytes()))
+        damaged("missing", lambda d: os.remove(os.path.join(d, ".g.ktab.3")))
